@@ -1,0 +1,223 @@
+/*
+ * rq.h — C ABI of the B200 ray-query engine (librq.so).
+ *
+ * This is the drop-in boundary for the reference's BVH build and software
+ * traversal path.  Every entry point names the reference interface it stands
+ * in for (file:line inside the reference project).  Conventions:
+ *   - plain C types only; device buffers are passed as raw device pointers,
+ *     CUDA streams as opaque `rq_stream` (a cudaStream_t, NULL = legacy stream);
+ *   - every call returns an rq_status; no C++ exception crosses the ABI;
+ *   - calls are stream-ordered and asynchronous unless documented otherwise;
+ *   - one rq_ctx owns its scratch memory, so calls that share a ctx must be
+ *     ordered on one stream (use one ctx per concurrently used stream).
+ */
+#ifndef RQ_H
+#define RQ_H
+
+#include "rq_layouts.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* rq_stream;
+typedef struct rq_ctx rq_ctx;
+typedef struct rq_bvh rq_bvh;
+
+typedef enum rq_status {
+    RQ_OK = 0,
+    RQ_ERR_INVALID_ARG = 1,     /* null pointer, zero size where one is needed, bad flag */
+    RQ_ERR_SIZE = 2,            /* an output buffer is smaller than required */
+    RQ_ERR_CUDA = 3,            /* a CUDA runtime call failed (rq_ctx_last_error has text) */
+    RQ_ERR_OOM = 4,             /* device allocation failed */
+    RQ_ERR_DEVICE_TIMEOUT = 5,  /* a bounded device-side wait gave up */
+    RQ_ERR_UNSUPPORTED = 6,     /* input outside what the kernels handle (e.g. > 2^27 triangles) */
+    RQ_ERR_BUDGET = 7,          /* serving: request does not fit the memory budget */
+    RQ_ERR_NO_DEVICE = 8,       /* no CUDA device, or the device is not sm_100 */
+    RQ_ERR_STATE = 9            /* handle used before it was built */
+} rq_status;
+
+/* ------------------------------------------------------------------ */
+/* Context                                                             */
+/* ------------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device`.  Fails with RQ_ERR_NO_DEVICE on
+ * anything other than a compute-capability 10.x device. */
+int rq_ctx_create(int device, rq_ctx** out);
+int rq_ctx_destroy(rq_ctx* ctx);
+const char* rq_status_string(int status);
+/* Text of the last error recorded on this context ("" if none). */
+const char* rq_ctx_last_error(const rq_ctx* ctx);
+/* Synchronise `stream`, then read and clear the context's device error word
+ * (set by kernels whose bounded waits gave up).  RQ_OK when clean. */
+int rq_ctx_check(rq_ctx* ctx, rq_stream stream);
+/* Bytes of device scratch the context currently holds. */
+uint64_t rq_ctx_scratch_bytes(const rq_ctx* ctx);
+
+/* ------------------------------------------------------------------ */
+/* Mesh generation and deformation (inputs of the BVH path)            */
+/* ------------------------------------------------------------------ */
+
+/* Height-field grid on the host: (qx+1)*(qy+1) vertices on [x0,x1]x[y0,y1],
+ * z = amp*sin(freq*x)*cos(freq*y) + N(0, sigma) per vertex (seeded), two
+ * triangles per quad wound like generate_dynamic_grid_mesh
+ * (include/radv_bvh.hpp:257-274).  `pos` gets 3 floats per vertex, `idx`
+ * 6 uint32 per quad.  Host pointers.  Replaces the input side of
+ * MeshGenerator::createTessellatedTerrain (common/mesh_gen.hpp:29-83). */
+int rq_scene_grid(uint32_t qx, uint32_t qy, float x0, float x1, float y0, float y1,
+                  float amp, float freq, float sigma, uint64_t seed,
+                  float* pos, uint32_t* idx);
+
+/* Rays on the host for the plain workload: origins uniform in
+ * [x0,x1]x[y0,y1] at height z, directions normalize(U(-s,s), U(-s,s), -1),
+ * the given tmin/tmax; SplitMix64 (seeded), double precision rounded once.
+ * Host pointer `rays` (n entries). */
+int rq_scene_rays_down(uint32_t n, float x0, float x1, float y0, float y1, float z, float spread, float tmin,
+                       float tmax, uint64_t seed, rq_ray* rays);
+
+/* Device kernel: out[v].z = base[v].z + amp*sin(t + freq*base[v].x), x and y
+ * copied.  3 floats per vertex, device pointers (in-place allowed).  The
+ * per-frame deformation step (benchmarks/expA_async/shaders/mesh_deform.comp:25-34). */
+int rq_deform_wave(rq_ctx* ctx, const float* base, float* out, uint32_t num_vertices,
+                   float t, float amp, float freq, rq_stream stream);
+
+/* ------------------------------------------------------------------ */
+/* BVH build (LBVH: Morton codes, onesweep radix sort, Karras emission, */
+/* atomic bottom-up refit, BVH4 collapse)                              */
+/* ------------------------------------------------------------------ */
+
+#define RQ_BUILD_BVH4 1u /* also collapse to the 4-wide layout (needed by rq_trace) */
+
+/* Build a binary BVH over `num_triangles` triangles.  Device pointers.
+ * `positions`: float xyz per vertex with `stride_bytes` between vertices
+ * (>= 12, multiple of 4).  `indices`: 3 uint32 per triangle, or NULL for a
+ * non-indexed mesh (triangle i uses vertices 3i, 3i+1, 3i+2).
+ * Leaves hold at most `max_leaf` (1..16) primitives.  The result, in the
+ * byte layouts of common/software_bvh.hpp, lives in a library-owned handle.
+ * If *out is non-NULL and has capacity for num_triangles, it is rebuilt in
+ * place (the per-frame path; no allocation).
+ * Replaces SoftwareBVH::build (common/software_bvh.hpp:35-87); with
+ * RQ_BUILD_BVH4 also SoftwareBVH4::fromBVH2 (:193-199). */
+int rq_build(rq_ctx* ctx, const float* positions, uint32_t stride_bytes, uint32_t num_vertices,
+             const uint32_t* indices, uint32_t num_triangles, uint32_t max_leaf, uint32_t flags,
+             rq_bvh** out, rq_stream stream);
+
+/* Collapse the handle's binary BVH to the 4-wide layout with the greedy
+ * largest-surface-area rule of SoftwareBVH4::collapse
+ * (common/software_bvh.hpp:202-291), nodes in the same depth-first order. */
+int rq_collapse4(rq_ctx* ctx, rq_bvh* bvh, rq_stream stream);
+
+/* Refit after the vertices moved: same topology, new triangle copies and
+ * boxes for both layouts.  `positions` as in rq_build; the index buffer must
+ * be the one the handle was built with (it is not stored).  Replaces the
+ * driver refit (common/vk_bvh.cpp:558-611) for this BVH. */
+int rq_refit(rq_ctx* ctx, rq_bvh* bvh, const float* positions, uint32_t stride_bytes,
+             const uint32_t* indices, rq_stream stream);
+
+/* Wrap foreign device arrays (for example a SoftwareBVH uploaded from the
+ * host) in a handle: the arrays are copied.  `perm` maps leaf order to
+ * original primitive IDs and may be NULL (then IDs are leaf-order indices,
+ * as the reference shaders report them). */
+int rq_bvh_import2(rq_ctx* ctx, const rq_bvh2_node* nodes, uint32_t num_nodes,
+                   const rq_triangle* tris, const uint32_t* perm, uint32_t num_triangles,
+                   rq_bvh** out, rq_stream stream);
+int rq_bvh_import4(rq_ctx* ctx, const rq_bvh4_node* nodes, uint32_t num_nodes,
+                   const rq_triangle* tris, const uint32_t* perm, uint32_t num_triangles,
+                   rq_bvh** out, rq_stream stream);
+
+typedef struct rq_bvh_info {
+    uint32_t num_triangles;
+    uint32_t num_nodes2;   /* binary nodes (0 if the handle only has a 4-wide BVH) */
+    uint32_t num_nodes4;   /* 4-wide nodes (0 until collapsed) */
+    uint32_t depth4;       /* levels of the 4-wide tree (root = 1) */
+    uint32_t max_leaf;
+    uint32_t stack_bound;  /* traversal stack entries the tree can need */
+    uint64_t device_bytes; /* bytes the handle holds on the device */
+} rq_bvh_info;
+
+/* Synchronises the handle's last build stream, then fills `info`. */
+int rq_bvh_info_get(rq_bvh* bvh, rq_bvh_info* info);
+
+/* Copy the layouts out (device-to-device or device-to-host; `host` selects
+ * which the destination pointers are).  Any destination may be NULL.
+ * Capacities are in elements; RQ_ERR_SIZE when one is too small.
+ * morton/sorted_ids expose the sort stage (keys and permutation). */
+int rq_bvh_download(rq_bvh* bvh, int host,
+                    rq_bvh2_node* nodes2, uint32_t cap_nodes2,
+                    rq_triangle* tris, uint32_t cap_tris,
+                    rq_bvh4_node* nodes4, uint32_t cap_nodes4,
+                    uint32_t* perm, uint32_t cap_perm);
+int rq_bvh_download_sort(rq_bvh* bvh, int host, uint32_t* morton, uint32_t* sorted_ids, uint32_t cap);
+int rq_bvh_destroy(rq_bvh* bvh);
+
+/* ------------------------------------------------------------------ */
+/* Traversal                                                           */
+/* ------------------------------------------------------------------ */
+
+/* flags */
+#define RQ_TRACE_CLOSEST 0u     /* full traversal, nearest hit (gl_RayFlagsNoneEXT/Opaque) */
+#define RQ_TRACE_ANY 1u         /* stop at the first accepted hit (TerminateOnFirstHit) */
+#define RQ_TRI_WATERTIGHT 0u    /* Woop-Benthin-Wald 2013 watertight test */
+#define RQ_TRI_MT 2u            /* Moller-Trumbore with the reference's arithmetic */
+
+/* Trace `n` rays against the handle's 4-wide BVH.  Accept tmin <= t < best,
+ * best starting at the ray's tmax.  Hits carry the ORIGINAL primitive ID.
+ * `bary` (2 floats per ray, barycentrics of v1 and v2) and `stats`
+ * (per-ray node/triangle test counts) may be NULL.
+ * Stands in for rayQueryEXT over a BLAS (benchmarks/exp0_probe/shaders/
+ * probe_triangle.comp:28-64) and the software traversals of
+ * software_bvh_bvh4.comp:60-196. */
+int rq_trace(rq_ctx* ctx, const rq_bvh* bvh, const rq_ray* rays, uint32_t n, uint32_t flags,
+             rq_hit* hits, float* bary, rq_ray_stats* stats, rq_stream stream);
+
+/* The reference's own software traversal semantics, kept for parity and for
+ * callers that depend on its quirks:
+ *  - rq_trace_ref_bvh4: software_bvh_bvh4.comp:96-195 (24-entry stack that
+ *    drops overflow, leaves tested inline far-to-near, MT with |a|<1e-7,
+ *    1/d replaced by 1e6 when |d|<=1e-6).  Writes RayStats and hits; hit IDs
+ *    are leaf-order indices as the shader reports them.
+ *  - rq_trace_ref_bvh2: software_bvh_lds.comp:86-175 (32-entry stack, MT with
+ *    |a|<1e-8, accept t>t_eps) — t_eps 0.001 for the LDS shader, 0.01 for
+ *    software_bvh_procedural.comp.  Writes the hitFound flag per ray. */
+int rq_trace_ref_bvh4(rq_ctx* ctx, const rq_bvh4_node* nodes, const rq_triangle* tris,
+                      const rq_ray* rays, uint32_t n, rq_ray_stats* stats, rq_hit* hits,
+                      rq_stream stream);
+int rq_trace_ref_bvh2(rq_ctx* ctx, const rq_bvh2_node* nodes, const rq_triangle* tris,
+                      const rq_ray* rays, uint32_t n, float t_eps, uint32_t* hit_flags,
+                      rq_stream stream);
+
+/* Procedural rays of software_bvh_bvh4.comp:60-94: coherent = 1024-wide
+ * camera grid from cam_pos toward look_at (x0.55 field), otherwise PCG-hashed
+ * origins in [-40,40]x[15,30]x[-40,40] heading down.  tmin 0.01, tmax 1000. */
+int rq_gen_rays_procedural(rq_ctx* ctx, const float cam_pos[3], const float look_at[3],
+                           uint32_t count, uint32_t coherent, rq_ray* rays, rq_stream stream);
+
+/* ------------------------------------------------------------------ */
+/* RADV image (fast_bvh_builder.comp)                                  */
+/* ------------------------------------------------------------------ */
+
+/* compute_tree_layout (include/radv_bvh.hpp:193-215).  Host only. */
+int rq_radv_layout_get(uint32_t num_triangles, rq_radv_layout* out);
+/* Bytes of the image: 192 + 128*boxes + 64*triangles. */
+uint64_t rq_radv_size(uint32_t num_triangles);
+
+/* Write the RADV image of shaders/fast_bvh_builder.comp:91-257 for any
+ * triangle count: 64-B triangle nodes in input order, Box32 leaves over 4
+ * consecutive triangles, bottom-up Box32 levels, the 136-B header and the
+ * two pre-root dwords.  `tri9`: 9 floats per triangle (device).  Byte-identical
+ * to the shader's output wherever the shader is defined (N <= 4096).
+ * RQ_ERR_SIZE if as_bytes < rq_radv_size(num_triangles). */
+int rq_build_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* as_image,
+                  uint64_t as_bytes, rq_stream stream);
+
+/* Trace rays through a RADV image (the rayQueryEXT role of
+ * shaders/verify_rayquery.comp:41-59): primitive IDs are the nodes'
+ * triangle_id; `bary` as in rq_trace. */
+int rq_trace_radv(rq_ctx* ctx, const void* as_image, uint64_t as_bytes, const rq_ray* rays,
+                  uint32_t n, uint32_t flags, rq_hit* hits, float* bary, rq_stream stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* RQ_H */

@@ -1,0 +1,1052 @@
+// oracle.cpp — TEST INFRASTRUCTURE, not product code.
+//
+// CPU restatement of the reference's BVH build and software traversal path,
+// used only as the checker by tests/, __graft_entry__.smoke() and the CPU
+// legs of bench.py.  Built to oracle/_build/liboracle.so with
+// -ffp-contract=off so every float operation is a single IEEE rounding
+// (explicit fmaf where the specification says fused).
+//
+// Contents (each function cites what it restates):
+//   Oracle B — LBVH: prim setup, 30-bit Morton codes, (code, id) sort, Karras
+//              2012 hierarchy, <= max_leaf leaves, depth-first emission in the
+//              layouts of common/software_bvh.hpp, and the greedy 4-wide
+//              collapse of software_bvh.hpp:202-291.
+//   Oracle C — fast_bvh_builder.comp:91-257: the RADV image of an implicit
+//              4-ary tree over the triangles in input order.
+//   Traversals — software_bvh_bvh4.comp:96-195 and software_bvh_lds.comp:86-175
+//              as published (reference semantics), plus the engine's own
+//              4-wide traversal and RADV-image traversal specification.
+//   Ray generators — software_bvh_bvh4.comp:50-94 (PCG procedural rays),
+//              visbuf_raycast.comp:15-51 (primary rays, with jitter),
+//              tiled_lighting_ra.comp:118-158 (shadow rays), rq_ao.comp:18-94
+//              (cosine-hemisphere AO rays).
+//
+// Parity status: Oracle B and the engine's traversal specification are
+// restatements written for this engine (the reference has no LBVH and no CPU
+// traversal); they are pinned by the tests against the reference's own
+// compiled SoftwareBVH (oracle/_ref) and the golden statistics in the
+// reference's results/exp0_ray_stats.csv.
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../include/rq_layouts.h"
+
+namespace {
+
+// ---------------------------------------------------------------- helpers --
+
+inline float fmin_(float a, float b) { return std::fmin(a, b); }
+inline float fmax_(float a, float b) { return std::fmax(a, b); }
+
+struct V3 {
+    float x, y, z;
+};
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 mul(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline float dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline V3 normalize(V3 v) {
+    float len = std::sqrt(dot(v, v));
+    return {v.x / len, v.y / len, v.z / len};
+}
+inline float comp(V3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+template <class F>
+void parallel_for(uint32_t n, int threads, F&& f) {
+    if (threads <= 1 || n < 4096) {
+        for (uint32_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<uint32_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            uint32_t b = next.fetch_add(1024);
+            if (b >= n) break;
+            uint32_t e = std::min(n, b + 1024);
+            for (uint32_t i = b; i < e; ++i) f(i);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto& th : pool) th.join();
+}
+
+inline V3 load_vertex(const float* pos, uint32_t stride_floats, uint32_t v) {
+    const float* p = pos + size_t(v) * stride_floats;
+    return {p[0], p[1], p[2]};
+}
+
+inline void tri_vertices(const float* pos, uint32_t stride_floats, const uint32_t* idx, uint32_t t,
+                         V3& p0, V3& p1, V3& p2) {
+    uint32_t i0 = idx ? idx[3 * size_t(t)] : 3 * t;
+    uint32_t i1 = idx ? idx[3 * size_t(t) + 1] : 3 * t + 1;
+    uint32_t i2 = idx ? idx[3 * size_t(t) + 2] : 3 * t + 2;
+    p0 = load_vertex(pos, stride_floats, i0);
+    p1 = load_vertex(pos, stride_floats, i1);
+    p2 = load_vertex(pos, stride_floats, i2);
+}
+
+// ------------------------------------------------------------- Oracle B --
+
+struct Prim {
+    float mn[3], mx[3], c[3];
+};
+
+// Per-triangle box and centroid exactly as SoftwareBVH::build
+// (common/software_bvh.hpp:40-55): centroid = ((p0 + p1) + p2) / 3.0f.
+Prim make_prim(V3 p0, V3 p1, V3 p2) {
+    Prim p;
+    for (int k = 0; k < 3; ++k) {
+        float a = comp(p0, k), b = comp(p1, k), c = comp(p2, k);
+        p.mn[k] = std::min({a, b, c});
+        p.mx[k] = std::max({a, b, c});
+        p.c[k] = ((a + b) + c) / 3.0f;
+    }
+    return p;
+}
+
+inline uint32_t expand10(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+inline uint32_t quantize(float c, float lo, float scale) {
+    float t = (c - lo) * scale;
+    if (t >= 1023.0f) return 1023u;
+    if (t > 0.0f) return uint32_t(t);
+    return 0u;
+}
+
+// 30-bit Morton code of each centroid inside the cube spanned by the centroid
+// bounds' largest extent (one scale for all three axes).
+void morton_codes(const std::vector<Prim>& prims, std::vector<uint32_t>& codes) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (const Prim& p : prims)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fmin_(lo[k], p.c[k]);
+            hi[k] = fmax_(hi[k], p.c[k]);
+        }
+    float ext = fmax_(fmax_(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
+    float scale = ext > 1e-30f ? 1024.0f / ext : 0.0f;
+    codes.resize(prims.size());
+    for (size_t i = 0; i < prims.size(); ++i) {
+        const Prim& p = prims[i];
+        codes[i] = expand10(quantize(p.c[0], lo[0], scale)) * 4u +
+                   expand10(quantize(p.c[1], lo[1], scale)) * 2u +
+                   expand10(quantize(p.c[2], lo[2], scale));
+    }
+}
+
+inline int clz32(uint32_t x) { return x ? __builtin_clz(x) : 32; }
+
+struct Karras {
+    const std::vector<uint32_t>& k;
+    int64_t n;
+    int delta(int64_t i, int64_t j) const {
+        if (j < 0 || j > n - 1) return -1;
+        uint32_t x = k[size_t(i)] ^ k[size_t(j)];
+        if (x) return clz32(x);
+        return 32 + clz32(uint32_t(i) ^ uint32_t(j));
+    }
+};
+
+struct KNode {            // Karras internal node
+    int64_t lo, hi;       // leaf range, inclusive
+    int64_t left, right;  // child indices
+    bool left_leaf, right_leaf;
+};
+
+// Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees
+// and k-d trees", Algorithm for internal node i (sorted keys, ties broken by
+// the sorted position).
+KNode karras_node(const Karras& K, int64_t i) {
+    int d = (K.delta(i, i + 1) - K.delta(i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = K.delta(i, i - d);
+    int64_t lmax = 2;
+    while (K.delta(i, i + lmax * d) > dmin) lmax <<= 1;
+    int64_t l = 0;
+    for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+        if (K.delta(i, i + (l + t) * d) > dmin) l += t;
+    int64_t j = i + l * d;
+    int dnode = K.delta(i, j);
+    int64_t s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (K.delta(i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    int64_t gamma = i + s * d + std::min(d, 0);
+    KNode kn;
+    kn.lo = std::min(i, j);
+    kn.hi = std::max(i, j);
+    kn.left = gamma;
+    kn.left_leaf = kn.lo == gamma;
+    kn.right = gamma + 1;
+    kn.right_leaf = kn.hi == gamma + 1;
+    return kn;
+}
+
+struct LbvhState {
+    std::vector<Prim> prims;        // original order
+    std::vector<uint32_t> codes;    // original order
+    std::vector<uint32_t> sorted;   // sorted position -> original id
+    std::vector<uint32_t> skeys;    // sorted keys
+    std::vector<KNode> inner;
+    std::vector<rq_bvh2_node> out;
+    uint32_t max_leaf;
+};
+
+void union_range(const LbvhState& S, int64_t lo, int64_t hi, float mn[3], float mx[3]) {
+    for (int k = 0; k < 3; ++k) {
+        mn[k] = INFINITY;
+        mx[k] = -INFINITY;
+    }
+    for (int64_t p = lo; p <= hi; ++p) {
+        const Prim& pr = S.prims[S.sorted[size_t(p)]];
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fmin_(mn[k], pr.mn[k]);
+            mx[k] = fmax_(mx[k], pr.mx[k]);
+        }
+    }
+}
+
+// Depth-first pre-order emission (left child = parent + 1, right child after
+// the left subtree, leaves as ~first / count) — the node order of
+// SoftwareBVH::recursiveBuild (common/software_bvh.hpp:90-175).
+int32_t emit(LbvhState& S, bool is_leaf, int64_t id) {
+    int64_t lo, hi;
+    if (is_leaf) {
+        lo = hi = id;
+    } else {
+        lo = S.inner[size_t(id)].lo;
+        hi = S.inner[size_t(id)].hi;
+    }
+    int32_t me = int32_t(S.out.size());
+    S.out.emplace_back();
+    float mn[3], mx[3];
+    union_range(S, lo, hi, mn, mx);
+    for (int k = 0; k < 3; ++k) {
+        S.out[me].aabb_min[k] = mn[k];
+        S.out[me].aabb_max[k] = mx[k];
+    }
+    int64_t cnt = hi - lo + 1;
+    if (cnt <= int64_t(S.max_leaf)) {
+        S.out[me].left_child = ~int32_t(lo);
+        S.out[me].right_child = int32_t(cnt);
+        return me;
+    }
+    const KNode& kn = S.inner[size_t(id)];
+    int32_t l = emit(S, kn.left_leaf, kn.left);
+    int32_t r = emit(S, kn.right_leaf, kn.right);
+    S.out[me].left_child = l;
+    S.out[me].right_child = r;
+    return me;
+}
+
+// Greedy 4-wide collapse: restates SoftwareBVH4::collapse
+// (common/software_bvh.hpp:202-291) — open the inner candidate with the
+// largest surface area (strict >, first wins) until four candidates, emit in
+// depth-first pre-order, zero-filled empty slots.
+int32_t collapse4(const rq_bvh2_node* n2, int32_t idx, std::vector<rq_bvh4_node>& out, uint32_t depth,
+                  uint32_t* max_depth) {
+    if (depth > *max_depth) *max_depth = depth;
+    const rq_bvh2_node& node = n2[idx];
+    if (node.left_child < 0) {
+        int32_t o = int32_t(out.size());
+        out.emplace_back();
+        std::memset(&out[o], 0, sizeof(rq_bvh4_node));
+        out[o].min_x[0] = node.aabb_min[0];
+        out[o].max_x[0] = node.aabb_max[0];
+        out[o].min_y[0] = node.aabb_min[1];
+        out[o].max_y[0] = node.aabb_max[1];
+        out[o].min_z[0] = node.aabb_min[2];
+        out[o].max_z[0] = node.aabb_max[2];
+        out[o].child_index[0] = node.left_child;
+        out[o].child_count[0] = node.right_child;
+        return o;
+    }
+    int32_t cand[4];
+    int nc = 2;
+    cand[0] = node.left_child;
+    cand[1] = node.right_child;
+    while (nc < 4) {
+        int best = -1;
+        float best_sa = -1.0f;
+        for (int i = 0; i < nc; ++i) {
+            const rq_bvh2_node& c = n2[cand[i]];
+            if (c.left_child >= 0) {
+                float dx = c.aabb_max[0] - c.aabb_min[0];
+                float dy = c.aabb_max[1] - c.aabb_min[1];
+                float dz = c.aabb_max[2] - c.aabb_min[2];
+                float sa = 2.0f * ((dx * dy + dy * dz) + dz * dx);
+                if (sa > best_sa) {
+                    best_sa = sa;
+                    best = i;
+                }
+            }
+        }
+        if (best < 0) break;
+        int32_t e = cand[best];
+        cand[best] = n2[e].left_child;
+        cand[nc++] = n2[e].right_child;
+    }
+    int32_t o = int32_t(out.size());
+    out.emplace_back();
+    rq_bvh4_node tmp;
+    std::memset(&tmp, 0, sizeof(tmp));
+    for (int i = 0; i < nc; ++i) {
+        const rq_bvh2_node& c = n2[cand[i]];
+        tmp.min_x[i] = c.aabb_min[0];
+        tmp.max_x[i] = c.aabb_max[0];
+        tmp.min_y[i] = c.aabb_min[1];
+        tmp.max_y[i] = c.aabb_max[1];
+        tmp.min_z[i] = c.aabb_min[2];
+        tmp.max_z[i] = c.aabb_max[2];
+        if (c.left_child < 0) {
+            tmp.child_index[i] = c.left_child;
+            tmp.child_count[i] = c.right_child;
+        } else {
+            tmp.child_count[i] = -1;
+        }
+    }
+    for (int i = 0; i < nc; ++i)
+        if (n2[cand[i]].left_child >= 0) tmp.child_index[i] = collapse4(n2, cand[i], out, depth + 1, max_depth);
+    out[o] = tmp;
+    return o;
+}
+
+// ------------------------------------------------------------- Oracle C --
+
+const uint32_t kQNaN = 0x7fc00000u;
+
+inline float bits_f(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// ------------------------------------------------------------- traversal --
+
+// Möller–Trumbore as written in software_bvh_bvh4.comp:166-178 (|a| < eps
+// rejected, u,v in [0,1], u+v <= 1).  Returns false on reject, else t.
+inline bool mt_test(V3 o, V3 d, V3 v0, V3 v1, V3 v2, float eps, float& t, float& u, float& v) {
+    V3 e1 = sub(v1, v0);
+    V3 e2 = sub(v2, v0);
+    V3 h = cross(d, e2);
+    float a = dot(e1, h);
+    if (std::fabs(a) < eps) return false;
+    float f = 1.0f / a;
+    V3 s = sub(o, v0);
+    u = f * dot(s, h);
+    if (u < 0.0f || u > 1.0f) return false;
+    V3 q = cross(s, e1);
+    v = f * dot(d, q);
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = f * dot(e2, q);
+    return true;
+}
+
+// Per-ray constants of the watertight test (Woop, Benthin, Wald 2013).
+struct WtRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+inline WtRay wt_setup(V3 d) {
+    WtRay w;
+    float ad[3] = {std::fabs(d.x), std::fabs(d.y), std::fabs(d.z)};
+    int kz = 0;
+    if (ad[1] > ad[kz]) kz = 1;
+    if (ad[2] > ad[kz]) kz = 2;
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    if (comp(d, kz) < 0.0f) std::swap(kx, ky);
+    w.kx = kx;
+    w.ky = ky;
+    w.kz = kz;
+    w.sx = comp(d, kx) / comp(d, kz);
+    w.sy = comp(d, ky) / comp(d, kz);
+    w.sz = 1.0f / comp(d, kz);
+    return w;
+}
+
+// Watertight test: edge functions in plain float products (so a shared edge
+// evaluates to exact negations), double recomputation when any is 0.0, t by
+// one IEEE division.  u, v are the weights of v1 and v2.
+inline bool wt_test(const WtRay& w, V3 o, V3 v0, V3 v1, V3 v2, float& t, float& u, float& v) {
+    V3 A = sub(v0, o), B = sub(v1, o), C = sub(v2, o);
+    float Az0 = comp(A, w.kz), Bz0 = comp(B, w.kz), Cz0 = comp(C, w.kz);
+    float Ax = std::fmaf(-w.sx, Az0, comp(A, w.kx));
+    float Ay = std::fmaf(-w.sy, Az0, comp(A, w.ky));
+    float Bx = std::fmaf(-w.sx, Bz0, comp(B, w.kx));
+    float By = std::fmaf(-w.sy, Bz0, comp(B, w.ky));
+    float Cx = std::fmaf(-w.sx, Cz0, comp(C, w.kx));
+    float Cy = std::fmaf(-w.sy, Cz0, comp(C, w.ky));
+    float U = Cx * By - Cy * Bx;
+    float V = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = (U + V) + W;
+    if (det == 0.0f) return false;
+    float Az = w.sz * Az0, Bz = w.sz * Bz0, Cz = w.sz * Cz0;
+    float T = (U * Az + V * Bz) + W * Cz;
+    t = T / det;
+    u = V / det;
+    v = W / det;
+    return true;
+}
+
+const float kTwoPow100 = 1.2676506002282294e30f;  // 2^100
+const float kTwoPowM100 = 7.888609052210118e-31f;  // 2^-100
+const float kFarScale = 1.00000095367431640625f;   // 1 + 2^-20
+
+inline float safe_inv(float d) {
+    if (std::fabs(d) < kTwoPowM100) return std::copysign(kTwoPow100, d);
+    return 1.0f / d;
+}
+
+// Slab test of the engine's traversal: fused (b*inv - o*inv), entry clamped
+// by tmin, exit by the current best, exit widened by 2^-20 relative.
+inline bool slab(const float inv[3], const float oinv[3], float tmin, float best, float mnx, float mxx,
+                 float mny, float mxy, float mnz, float mxz, float& tn) {
+    float tx0 = std::fmaf(mnx, inv[0], -oinv[0]), tx1 = std::fmaf(mxx, inv[0], -oinv[0]);
+    float ty0 = std::fmaf(mny, inv[1], -oinv[1]), ty1 = std::fmaf(mxy, inv[1], -oinv[1]);
+    float tz0 = std::fmaf(mnz, inv[2], -oinv[2]), tz1 = std::fmaf(mxz, inv[2], -oinv[2]);
+    float a = fmax_(fmax_(fmin_(tx0, tx1), fmin_(ty0, ty1)), fmax_(fmin_(tz0, tz1), tmin));
+    float b = fmin_(fmin_(fmax_(tx0, tx1), fmax_(ty0, ty1)), fmin_(fmax_(tz0, tz1), best));
+    tn = a;
+    return a <= b * kFarScale;
+}
+
+struct TraceOut {
+    bool hit;
+    float t;
+    uint32_t prim;  // leaf-order index (or RADV triangle node offset)
+    float u, v;
+    uint32_t boxes, tris;
+};
+
+// The engine's 4-wide traversal (rq_trace).  Stack of entries; inner nodes
+// and leaf children are both pushed.  Closest hit: hit children sorted by
+// entry distance (ties by slot), pushed far-first.  Any hit: hit children
+// pushed from slot 3 down to slot 0 (slot 0 on top), traversal stops at the
+// first accepted triangle.  A leaf tests its triangles in order.
+TraceOut trace_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq_ray& r, uint32_t flags) {
+    const bool any = flags & 1u;
+    const bool mt = flags & 2u;
+    V3 o{r.org[0], r.org[1], r.org[2]}, d{r.dir[0], r.dir[1], r.dir[2]};
+    float inv[3] = {safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+    float oinv[3] = {o.x * inv[0], o.y * inv[1], o.z * inv[2]};
+    WtRay w = wt_setup(d);
+    float tmin = r.tmin, best = r.tmax;
+    TraceOut res{false, -1.0f, 0xffffffffu, 0.0f, 0.0f, 0, 0};
+    struct Entry {
+        int32_t idx;   // node index, or first prim for a leaf
+        int32_t cnt;   // -1 inner, else prim count
+    };
+    std::vector<Entry> st;
+    st.reserve(64);
+    st.push_back({0, -1});
+    while (!st.empty()) {
+        Entry e = st.back();
+        st.pop_back();
+        if (e.cnt < 0) {
+            const rq_bvh4_node& n = nodes[e.idx];
+            res.boxes += 4;
+            Entry hc[4];
+            float ht[4];
+            int nh = 0;
+            for (int k = 0; k < 4; ++k) {
+                if (n.child_count[k] == 0) continue;
+                float tn;
+                if (slab(inv, oinv, tmin, best, n.min_x[k], n.max_x[k], n.min_y[k], n.max_y[k], n.min_z[k],
+                         n.max_z[k], tn)) {
+                    Entry c;
+                    if (n.child_count[k] < 0) {
+                        c = {n.child_index[k], -1};
+                    } else {
+                        c = {~n.child_index[k], n.child_count[k]};
+                    }
+                    // insertion keeps ascending distance, stable by slot
+                    int pos = nh;
+                    if (!any)
+                        while (pos > 0 && ht[pos - 1] > tn) {
+                            hc[pos] = hc[pos - 1];
+                            ht[pos] = ht[pos - 1];
+                            --pos;
+                        }
+                    hc[pos] = c;
+                    ht[pos] = tn;
+                    ++nh;
+                }
+            }
+            for (int i = nh - 1; i >= 0; --i) st.push_back(hc[i]);
+        } else {
+            for (int32_t p = 0; p < e.cnt; ++p) {
+                uint32_t pi = uint32_t(e.idx + p);
+                const rq_triangle& tr = tris[pi];
+                V3 v0{tr.v0[0], tr.v0[1], tr.v0[2]}, v1{tr.v1[0], tr.v1[1], tr.v1[2]},
+                    v2{tr.v2[0], tr.v2[1], tr.v2[2]};
+                res.tris += 1;
+                float t, u, v;
+                bool ok = mt ? mt_test(o, d, v0, v1, v2, 1e-7f, t, u, v) : wt_test(w, o, v0, v1, v2, t, u, v);
+                if (ok && t >= tmin && t < best) {
+                    best = t;
+                    res.hit = true;
+                    res.t = t;
+                    res.prim = pi;
+                    res.u = u;
+                    res.v = v;
+                    if (any) return res;
+                }
+            }
+        }
+    }
+    return res;
+}
+
+// RADV image traversal (rq_trace_radv): same ordering rules; a Box32 child is
+// either another Box32 (type 5) or a 64-B triangle node (type 0).
+TraceOut trace_radv(const uint8_t* img, const rq_ray& r, uint32_t flags) {
+    const bool any = flags & 1u;
+    const bool mt = flags & 2u;
+    V3 o{r.org[0], r.org[1], r.org[2]}, d{r.dir[0], r.dir[1], r.dir[2]};
+    float inv[3] = {safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+    float oinv[3] = {o.x * inv[0], o.y * inv[1], o.z * inv[2]};
+    WtRay w = wt_setup(d);
+    float tmin = r.tmin, best = r.tmax;
+    TraceOut res{false, -1.0f, 0xffffffffu, 0.0f, 0.0f, 0, 0};
+    const uint8_t* base = img + RQ_RADV_BVH_OFFSET;
+    std::vector<uint32_t> st;
+    st.push_back(RQ_RADV_NODE_BOX32);
+    while (!st.empty()) {
+        uint32_t id = st.back();
+        st.pop_back();
+        uint32_t type = id & 7u;
+        const uint8_t* p = base + (size_t(id & ~7u) << 3);
+        if (type == RQ_RADV_NODE_BOX32) {
+            rq_radv_box32 b;
+            std::memcpy(&b, p, sizeof(b));
+            res.boxes += 4;
+            uint32_t hc[4];
+            float ht[4];
+            int nh = 0;
+            for (int k = 0; k < 4; ++k) {
+                if (b.children[k] == RQ_RADV_INVALID_NODE) continue;
+                const float* c = b.coords[k];
+                float tn;
+                if (slab(inv, oinv, tmin, best, c[0], c[3], c[1], c[4], c[2], c[5], tn)) {
+                    int pos = nh;
+                    if (!any)
+                        while (pos > 0 && ht[pos - 1] > tn) {
+                            hc[pos] = hc[pos - 1];
+                            ht[pos] = ht[pos - 1];
+                            --pos;
+                        }
+                    hc[pos] = b.children[k];
+                    ht[pos] = tn;
+                    ++nh;
+                }
+            }
+            for (int i = nh - 1; i >= 0; --i) st.push_back(hc[i]);
+        } else if (type == RQ_RADV_NODE_TRIANGLE) {
+            rq_radv_tri tn;
+            std::memcpy(&tn, p, sizeof(tn));
+            V3 v0{tn.coords[0][0], tn.coords[0][1], tn.coords[0][2]};
+            V3 v1{tn.coords[1][0], tn.coords[1][1], tn.coords[1][2]};
+            V3 v2{tn.coords[2][0], tn.coords[2][1], tn.coords[2][2]};
+            res.tris += 1;
+            float t, u, v;
+            bool ok = mt ? mt_test(o, d, v0, v1, v2, 1e-7f, t, u, v) : wt_test(w, o, v0, v1, v2, t, u, v);
+            if (ok && t >= tmin && t < best) {
+                best = t;
+                res.hit = true;
+                res.t = t;
+                res.prim = tn.triangle_id;
+                res.u = u;
+                res.v = v;
+                if (any) return res;
+            }
+        }
+    }
+    return res;
+}
+
+// ------------------------------------------------------------ ray makers --
+
+inline uint32_t pcg_hash(uint32_t v) {
+    uint32_t state = v * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+const float kInv2Pow32 = 2.3283064365386963e-10f;  // 1/4294967295.0 evaluated in float = 2^-32
+inline float hash_float(uint32_t seed) { return float(pcg_hash(seed)) * kInv2Pow32; }
+
+// One-at-a-time style hash of rq_ao.comp:18-25.
+inline uint32_t ao_hash(uint32_t x) {
+    x += (x << 10u);
+    x ^= (x >> 6u);
+    x += (x << 3u);
+    x ^= (x >> 11u);
+    x += (x << 15u);
+    return x;
+}
+
+// sin/cos for the AO hemisphere: Cody–Waite reduction by pi/2 in three
+// parts and Taylor polynomials (coefficients 1/n!) on [-pi/4, pi/4], all
+// with explicit fused multiply-adds, so the device code can match bit for bit.
+inline void sincos_taylor(float x, float* s, float* c) {
+    float n = std::floor(std::fmaf(x, 0x1.45f306p-1f, 0.5f));
+    float r = std::fmaf(-n, 0x1.921fb6p+0f, x);
+    r = std::fmaf(-n, -0x1.777a5cp-25f, r);
+    r = std::fmaf(-n, -0x1.ee59dap-50f, r);
+    float r2 = r * r;
+    float ps = std::fmaf(r2, 0x1.71de3ap-19f, -0x1.a01a02p-13f);
+    ps = std::fmaf(r2, ps, 0x1.111112p-7f);
+    ps = std::fmaf(r2, ps, -0x1.555556p-3f);
+    ps = std::fmaf(r2 * r, ps, r);
+    float pc = std::fmaf(r2, -0x1.27e4fcp-22f, 0x1.a01a02p-16f);
+    pc = std::fmaf(r2, pc, -0x1.6c16c2p-10f);
+    pc = std::fmaf(r2, pc, 0x1.555556p-5f);
+    pc = std::fmaf(r2, pc, -0.5f);
+    pc = std::fmaf(r2, pc, 1.0f);
+    int q = int(int64_t(n) & 3);
+    float sv = q == 0 ? ps : (q == 1 ? pc : (q == 2 ? -ps : -pc));
+    float cv = q == 0 ? pc : (q == 1 ? -ps : (q == 2 ? -pc : ps));
+    *s = sv;
+    *c = cv;
+}
+
+// Matrix (column-major, GLSL convention) times (x, y, z, w).
+inline void mat4_mul(const float* m, const float in[4], float out[4]) {
+    for (int r = 0; r < 4; ++r)
+        out[r] = ((m[0 * 4 + r] * in[0] + m[1 * 4 + r] * in[1]) + m[2 * 4 + r] * in[2]) + m[3 * 4 + r] * in[3];
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+// Oracle B, stage by stage.  pos: vertex floats with stride_floats between
+// vertices; idx may be NULL (non-indexed).  Outputs sized by the caller:
+// codes/sorted/perm: n; nodes2: 2n; nodes4: max(1, n); tris: n.
+// Returns the node counts through n2/n4 and the 4-wide depth through depth4.
+int orc_lbvh_build(const float* pos, uint32_t stride_floats, const uint32_t* idx, uint32_t n,
+                   uint32_t max_leaf, uint32_t* codes_out, uint32_t* sorted_out, rq_bvh2_node* nodes2,
+                   uint32_t* n2, rq_triangle* tris, rq_bvh4_node* nodes4, uint32_t* n4, uint32_t* depth4) {
+    if (n == 0 || max_leaf == 0) return 1;
+    LbvhState S;
+    S.max_leaf = max_leaf;
+    S.prims.resize(n);
+    for (uint32_t t = 0; t < n; ++t) {
+        V3 p0, p1, p2;
+        tri_vertices(pos, stride_floats, idx, t, p0, p1, p2);
+        S.prims[t] = make_prim(p0, p1, p2);
+    }
+    morton_codes(S.prims, S.codes);
+    S.sorted.resize(n);
+    for (uint32_t i = 0; i < n; ++i) S.sorted[i] = i;
+    std::sort(S.sorted.begin(), S.sorted.end(), [&](uint32_t a, uint32_t b) {
+        return S.codes[a] != S.codes[b] ? S.codes[a] < S.codes[b] : a < b;
+    });
+    S.skeys.resize(n);
+    for (uint32_t i = 0; i < n; ++i) S.skeys[i] = S.codes[S.sorted[i]];
+    if (codes_out) std::memcpy(codes_out, S.codes.data(), 4ull * n);
+    if (sorted_out) std::memcpy(sorted_out, S.sorted.data(), 4ull * n);
+    Karras K{S.skeys, int64_t(n)};
+    if (n >= 2) {
+        S.inner.resize(n - 1);
+        for (uint32_t i = 0; i + 1 < n; ++i) S.inner[i] = karras_node(K, i);
+    }
+    S.out.reserve(2ull * n);
+    if (n == 1)
+        emit(S, true, 0);
+    else
+        emit(S, false, 0);
+    *n2 = uint32_t(S.out.size());
+    if (nodes2) std::memcpy(nodes2, S.out.data(), sizeof(rq_bvh2_node) * S.out.size());
+    if (tris) {
+        for (uint32_t k = 0; k < n; ++k) {
+            V3 p0, p1, p2;
+            tri_vertices(pos, stride_floats, idx, S.sorted[k], p0, p1, p2);
+            rq_triangle tr;
+            tr.v0[0] = p0.x; tr.v0[1] = p0.y; tr.v0[2] = p0.z; tr.v0[3] = 0.0f;
+            tr.v1[0] = p1.x; tr.v1[1] = p1.y; tr.v1[2] = p1.z; tr.v1[3] = 0.0f;
+            tr.v2[0] = p2.x; tr.v2[1] = p2.y; tr.v2[2] = p2.z; tr.v2[3] = 0.0f;
+            tris[k] = tr;
+        }
+    }
+    if (nodes4 || n4) {
+        std::vector<rq_bvh4_node> out4;
+        uint32_t md = 0;
+        collapse4(S.out.data(), 0, out4, 1, &md);
+        if (n4) *n4 = uint32_t(out4.size());
+        if (depth4) *depth4 = md;
+        if (nodes4) std::memcpy(nodes4, out4.data(), sizeof(rq_bvh4_node) * out4.size());
+    }
+    return 0;
+}
+
+// The greedy collapse alone, on any binary BVH in the GpuBvhNode layout.
+int orc_collapse4(const rq_bvh2_node* nodes2, uint32_t n2, rq_bvh4_node* nodes4, uint32_t* n4, uint32_t* depth4) {
+    if (n2 == 0) {
+        *n4 = 0;
+        return 0;
+    }
+    std::vector<rq_bvh4_node> out4;
+    uint32_t md = 0;
+    collapse4(nodes2, 0, out4, 1, &md);
+    *n4 = uint32_t(out4.size());
+    if (depth4) *depth4 = md;
+    if (nodes4) std::memcpy(nodes4, out4.data(), sizeof(rq_bvh4_node) * out4.size());
+    return 0;
+}
+
+// Oracle C: fast_bvh_builder.comp:91-257 for any n.  `img` must hold
+// 192 + 128*boxes + 64*n bytes; bytes the shader never writes (136..191
+// except the two pre-root dwords) are written as 0.
+int orc_radv_build(const float* tri9, uint32_t n, uint8_t* img) {
+    if (n == 0) return 1;
+    std::vector<uint32_t> counts{(n + 3) / 4};
+    while (counts.back() > 1) counts.push_back((counts.back() + 3) / 4);
+    std::reverse(counts.begin(), counts.end());
+    uint32_t levels = uint32_t(counts.size());
+    std::vector<uint32_t> offs(levels);
+    uint32_t total = 0;
+    for (uint32_t l = 0; l < levels; ++l) {
+        offs[l] = total;
+        total += counts[l];
+    }
+    uint64_t size = 192ull + 128ull * total + 64ull * n;
+    std::memset(img, 0, size);
+    std::vector<float> bmin(3ull * total), bmax(3ull * total);
+    uint8_t* boxes = img + 192;
+    uint8_t* trin = img + 192 + 128ull * total;
+    float qnan = bits_f(kQNaN);
+    // leaf boxes over four consecutive input triangles
+    uint32_t leaf_off = offs[levels - 1], leaf_cnt = counts[levels - 1];
+    for (uint32_t t = 0; t < leaf_cnt; ++t) {
+        rq_radv_box32 b;
+        std::memset(&b, 0, sizeof(b));
+        float umin[3] = {1e30f, 1e30f, 1e30f}, umax[3] = {-1e30f, -1e30f, -1e30f};
+        for (uint32_t c = 0; c < 4; ++c) {
+            uint32_t ti = 4 * t + c;
+            if (ti < n) {
+                const float* v = tri9 + 9ull * ti;
+                rq_radv_tri tn;
+                std::memset(&tn, 0, sizeof(tn));
+                for (int a = 0; a < 3; ++a)
+                    for (int k = 0; k < 3; ++k) tn.coords[a][k] = v[3 * a + k];
+                tn.triangle_id = ti;
+                tn.geometry_id_and_flags = RQ_RADV_GEOMETRY_OPAQUE;
+                tn.id = RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT;
+                std::memcpy(trin + 64ull * ti, &tn, 64);
+                uint32_t rel = total * 128u + ti * 64u;
+                b.children[c] = (rel >> 3) | RQ_RADV_NODE_TRIANGLE;
+                for (int k = 0; k < 3; ++k) {
+                    float mn = fmin_(v[k], fmin_(v[3 + k], v[6 + k]));
+                    float mx = fmax_(v[k], fmax_(v[3 + k], v[6 + k]));
+                    b.coords[c][k] = mn;
+                    b.coords[c][3 + k] = mx;
+                    umin[k] = fmin_(umin[k], mn);
+                    umax[k] = fmax_(umax[k], mx);
+                }
+            } else {
+                b.children[c] = RQ_RADV_INVALID_NODE;
+                for (int k = 0; k < 6; ++k) b.coords[c][k] = qnan;
+            }
+        }
+        std::memcpy(boxes + 128ull * (leaf_off + t), &b, 128);
+        for (int k = 0; k < 3; ++k) {
+            bmin[3ull * (leaf_off + t) + k] = umin[k];
+            bmax[3ull * (leaf_off + t) + k] = umax[k];
+        }
+    }
+    for (int l = int(levels) - 2; l >= 0; --l) {
+        uint32_t cnt = counts[l], off = offs[l], coff = offs[l + 1], ccnt = counts[l + 1];
+        for (uint32_t t = 0; t < cnt; ++t) {
+            rq_radv_box32 b;
+            std::memset(&b, 0, sizeof(b));
+            float umin[3] = {1e30f, 1e30f, 1e30f}, umax[3] = {-1e30f, -1e30f, -1e30f};
+            for (uint32_t c = 0; c < 4; ++c) {
+                uint32_t cl = 4 * t + c;
+                if (cl < ccnt) {
+                    uint32_t cg = coff + cl;
+                    b.children[c] = ((cg * 128u) >> 3) | RQ_RADV_NODE_BOX32;
+                    for (int k = 0; k < 3; ++k) {
+                        b.coords[c][k] = bmin[3ull * cg + k];
+                        b.coords[c][3 + k] = bmax[3ull * cg + k];
+                        umin[k] = fmin_(umin[k], bmin[3ull * cg + k]);
+                        umax[k] = fmax_(umax[k], bmax[3ull * cg + k]);
+                    }
+                } else {
+                    b.children[c] = RQ_RADV_INVALID_NODE;
+                    for (int k = 0; k < 6; ++k) b.coords[c][k] = qnan;
+                }
+            }
+            std::memcpy(boxes + 128ull * (off + t), &b, 128);
+            for (int k = 0; k < 3; ++k) {
+                bmin[3ull * (off + t) + k] = umin[k];
+                bmax[3ull * (off + t) + k] = umax[k];
+            }
+        }
+    }
+    rq_radv_header h;
+    std::memset(&h, 0, sizeof(h));
+    h.bvh_offset = 192;
+    for (int k = 0; k < 3; ++k) {
+        h.aabb_min[k] = bmin[k];
+        h.aabb_max[k] = bmax[k];
+    }
+    h.update_dispatch_size[0] = 8;
+    h.update_dispatch_size[1] = 1;
+    h.update_dispatch_size[2] = 1;
+    h.compacted_size = size;
+    h.serialization_size = size + 128;
+    h.copy_dispatch_size[0] = 1;
+    h.copy_dispatch_size[1] = 1;
+    h.copy_dispatch_size[2] = 1;
+    h.size = size;
+    h.geometry_count = 1;
+    h.leaf_nodes_offset = 192ull + 128ull * total;
+    h.primitive_count = n;
+    h.build_flags = 4;
+    h.type = 1;
+    std::memcpy(img, &h, sizeof(h));
+    uint32_t five = 5, inval = 0xffffffffu;
+    std::memcpy(img + 180, &five, 4);
+    std::memcpy(img + 188, &inval, 4);
+    return 0;
+}
+
+// Reference semantics of software_bvh_bvh4.comp:96-195 on explicit rays
+// (ray tmin/tmax replace the shader's constants 0.01 / 1000).  Hit IDs are
+// leaf-order indices (:181).
+void orc_trace_ref_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq_ray* rays, uint32_t n,
+                        rq_ray_stats* stats, rq_hit* hits, int threads) {
+    parallel_for(n, threads, [&](uint32_t idx) {
+        const rq_ray& r = rays[idx];
+        V3 o{r.org[0], r.org[1], r.org[2]}, d{r.dir[0], r.dir[1], r.dir[2]};
+        V3 inv{std::fabs(d.x) > 1e-6f ? 1.0f / d.x : 1e6f, std::fabs(d.y) > 1e-6f ? 1.0f / d.y : 1e6f,
+               std::fabs(d.z) > 1e-6f ? 1.0f / d.z : 1e6f};
+        float tmin = r.tmin, hitT = r.tmax;
+        int hitPrim = -1;
+        uint32_t boxTests = 0, triTests = 0;
+        int32_t stack[24];
+        stack[0] = 0;
+        int ptr = 1;
+        while (ptr > 0) {
+            const rq_bvh4_node& nd = nodes[stack[--ptr]];
+            boxTests += 4;
+            float tEntry[4], tExit[4];
+            for (int k = 0; k < 4; ++k) {
+                float t0x = (nd.min_x[k] - o.x) * inv.x, t1x = (nd.max_x[k] - o.x) * inv.x;
+                float t0y = (nd.min_y[k] - o.y) * inv.y, t1y = (nd.max_y[k] - o.y) * inv.y;
+                float t0z = (nd.min_z[k] - o.z) * inv.z, t1z = (nd.max_z[k] - o.z) * inv.z;
+                float tminX = fmin_(t0x, t1x), tmaxX = fmax_(t0x, t1x);
+                float tminY = fmin_(t0y, t1y), tmaxY = fmax_(t0y, t1y);
+                float tminZ = fmin_(t0z, t1z), tmaxZ = fmax_(t0z, t1z);
+                tEntry[k] = fmax_(fmax_(tminX, tminY), fmax_(tminZ, tmin));
+                tExit[k] = fmin_(fmin_(tmaxX, tmaxY), fmin_(tmaxZ, hitT));
+            }
+            int slot[4];
+            float ht[4];
+            int hc = 0;
+            for (int k = 0; k < 4; ++k)
+                if (nd.child_count[k] != 0 && tExit[k] >= tEntry[k]) {
+                    slot[hc] = k;
+                    ht[hc] = tEntry[k];
+                    ++hc;
+                }
+            if (hc == 0) continue;
+            for (int i = 0; i < hc - 1; ++i)
+                for (int j = i + 1; j < hc; ++j)
+                    if (ht[i] < ht[j]) {
+                        std::swap(ht[i], ht[j]);
+                        std::swap(slot[i], slot[j]);
+                    }
+            for (int i = 0; i < hc; ++i) {
+                int k = slot[i];
+                if (nd.child_count[k] > 0) {
+                    uint32_t first = uint32_t(~nd.child_index[k]);
+                    uint32_t cnt = uint32_t(nd.child_count[k]);
+                    triTests += cnt;
+                    for (uint32_t p = 0; p < cnt; ++p) {
+                        const rq_triangle& tr = tris[first + p];
+                        V3 v0{tr.v0[0], tr.v0[1], tr.v0[2]}, v1{tr.v1[0], tr.v1[1], tr.v1[2]},
+                            v2{tr.v2[0], tr.v2[1], tr.v2[2]};
+                        float t, u, v;
+                        if (!mt_test(o, d, v0, v1, v2, 1e-7f, t, u, v)) continue;
+                        if (t >= tmin && t < hitT) {
+                            hitT = t;
+                            hitPrim = int(first + p);
+                        }
+                    }
+                } else if (nd.child_count[k] < 0) {
+                    if (ptr < 24) stack[ptr++] = nd.child_index[k];
+                }
+            }
+        }
+        if (stats) stats[idx] = {hitPrim >= 0 ? 1u : 0u, boxTests, triTests, 0u};
+        if (hits) {
+            if (hitPrim >= 0)
+                hits[idx] = {1u, hitT, 0u, uint32_t(hitPrim)};
+            else
+                hits[idx] = {0u, -1.0f, 0xffffffffu, 0xffffffffu};
+        }
+    });
+}
+
+// Reference semantics of software_bvh_lds.comp:86-175 (t_eps 0.001) and
+// software_bvh_procedural.comp (t_eps 0.01) on explicit rays: root box test
+// against the running closest t, children tested from the parent, front-to-
+// back push, hitFound flag out.
+void orc_trace_ref_bvh2(const rq_bvh2_node* nodes, const rq_triangle* tris, const rq_ray* rays, uint32_t n,
+                        float t_eps, uint32_t* flags_out, int threads) {
+    parallel_for(n, threads, [&](uint32_t idx) {
+        const rq_ray& r = rays[idx];
+        V3 o{r.org[0], r.org[1], r.org[2]}, d{r.dir[0], r.dir[1], r.dir[2]};
+        auto clampd = [](float x) { return std::fabs(x) > 1e-8f ? x : (x >= 0.0f ? 1e-8f : -1e-8f); };
+        V3 inv{1.0f / clampd(d.x), 1.0f / clampd(d.y), 1.0f / clampd(d.z)};
+        float closestT = r.tmax;
+        uint32_t hitFound = 0;
+        auto box = [&](const rq_bvh2_node& nd, float& tb) {
+            float t0x = (nd.aabb_min[0] - o.x) * inv.x, t1x = (nd.aabb_max[0] - o.x) * inv.x;
+            float t0y = (nd.aabb_min[1] - o.y) * inv.y, t1y = (nd.aabb_max[1] - o.y) * inv.y;
+            float t0z = (nd.aabb_min[2] - o.z) * inv.z, t1z = (nd.aabb_max[2] - o.z) * inv.z;
+            float tNear = fmax_(fmax_(fmin_(t0x, t1x), fmin_(t0y, t1y)), fmin_(t0z, t1z));
+            float tFar = fmin_(fmin_(fmax_(t0x, t1x), fmax_(t0y, t1y)), fmax_(t0z, t1z));
+            tb = tNear;
+            return (tFar >= fmax_(0.0f, tNear)) && (tNear < closestT);
+        };
+        uint32_t stack[32];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const rq_bvh2_node& nd = nodes[stack[--sp]];
+            float tb;
+            if (!box(nd, tb)) continue;
+            if (nd.left_child < 0) {
+                uint32_t start = uint32_t(~nd.left_child);
+                for (int32_t i = 0; i < nd.right_child; ++i) {
+                    const rq_triangle& tr = tris[start + uint32_t(i)];
+                    V3 v0{tr.v0[0], tr.v0[1], tr.v0[2]}, v1{tr.v1[0], tr.v1[1], tr.v1[2]},
+                        v2{tr.v2[0], tr.v2[1], tr.v2[2]};
+                    float t, u, v;
+                    if (!mt_test(o, d, v0, v1, v2, 1e-8f, t, u, v)) continue;
+                    if (t > t_eps && t < closestT) {
+                        closestT = t;
+                        hitFound = 1;
+                    }
+                }
+            } else {
+                uint32_t l = uint32_t(nd.left_child), rr = uint32_t(nd.right_child);
+                float tl, tr;
+                bool hl = box(nodes[l], tl), hr = box(nodes[rr], tr);
+                if (hl && hr) {
+                    if (tl < tr) {
+                        if (sp < 32) stack[sp++] = rr;
+                        if (sp < 32) stack[sp++] = l;
+                    } else {
+                        if (sp < 32) stack[sp++] = l;
+                        if (sp < 32) stack[sp++] = rr;
+                    }
+                } else if (hl) {
+                    if (sp < 32) stack[sp++] = l;
+                } else if (hr) {
+                    if (sp < 32) stack[sp++] = rr;
+                }
+            }
+        }
+        flags_out[idx] = hitFound;
+    });
+}
+
+// The engine's 4-wide traversal specification (see trace_bvh4 above).
+// perm (may be NULL) maps leaf order to original IDs.  bary: 2 floats/ray.
+void orc_trace_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, const uint32_t* perm, const rq_ray* rays,
+                    uint32_t n, uint32_t flags, rq_hit* hits, float* bary, rq_ray_stats* stats, int threads) {
+    parallel_for(n, threads, [&](uint32_t i) {
+        TraceOut t = trace_bvh4(nodes, tris, rays[i], flags);
+        if (hits) {
+            if (t.hit)
+                hits[i] = {1u, t.t, 0u, perm ? perm[t.prim] : t.prim};
+            else
+                hits[i] = {0u, -1.0f, 0xffffffffu, 0xffffffffu};
+        }
+        if (bary) {
+            bary[2 * size_t(i)] = t.hit ? t.u : 0.0f;
+            bary[2 * size_t(i) + 1] = t.hit ? t.v : 0.0f;
+        }
+        if (stats) stats[i] = {t.hit ? 1u : 0u, t.boxes, t.tris, 0u};
+    });
+}
+
+void orc_trace_radv(const uint8_t* img, const rq_ray* rays, uint32_t n, uint32_t flags, rq_hit* hits, float* bary,
+                    int threads) {
+    parallel_for(n, threads, [&](uint32_t i) {
+        TraceOut t = trace_radv(img, rays[i], flags);
+        if (hits) {
+            if (t.hit)
+                hits[i] = {1u, t.t, 0u, t.prim};
+            else
+                hits[i] = {0u, -1.0f, 0xffffffffu, 0xffffffffu};
+        }
+        if (bary) {
+            bary[2 * size_t(i)] = t.hit ? t.u : 0.0f;
+            bary[2 * size_t(i) + 1] = t.hit ? t.v : 0.0f;
+        }
+    });
+}
+
+// software_bvh_bvh4.comp:60-94 procedural rays, tmin 0.01 / tmax 1000.
+void orc_gen_rays_procedural(const float cam[3], const float look[3], uint32_t count, uint32_t coherent,
+                             rq_ray* rays) {
+    V3 cp{cam[0], cam[1], cam[2]}, la{look[0], look[1], look[2]};
+    V3 fwd = normalize(sub(la, cp));
+    V3 right = normalize(cross(fwd, V3{0.0f, 1.0f, 0.0f}));
+    V3 up = cross(right, fwd);
+    for (uint32_t idx = 0; idx < count; ++idx) {
+        V3 o, d;
+        if (coherent) {
+            uint32_t width = 1024, height = (count + width - 1) / width;
+            uint32_t x = idx % width, y = idx / width;
+            float u = ((float(x) + 0.5f) / float(width)) * 2.0f - 1.0f;
+            float v = ((float(y) + 0.5f) / float(height)) * 2.0f - 1.0f;
+            o = cp;
+            d = normalize(add(add(fwd, mul(mul(right, u), 0.55f)), mul(mul(up, v), 0.55f)));
+        } else {
+            float rx = hash_float(idx * 6 + 0) * 80.0f - 40.0f;
+            float ry = hash_float(idx * 6 + 1) * 15.0f + 15.0f;
+            float rz = hash_float(idx * 6 + 2) * 80.0f - 40.0f;
+            o = {rx, ry, rz};
+            float dx = hash_float(idx * 6 + 3) * 0.8f - 0.4f;
+            float dy = -1.0f - hash_float(idx * 6 + 4) * 0.5f;
+            float dz = hash_float(idx * 6 + 5) * 0.8f - 0.4f;
+            d = normalize(V3{dx, dy, dz});
+        }
+        rays[idx] = {{o.x, o.y, o.z}, 0.01f, {d.x, d.y, d.z}, 1000.0f};
+    }
+}
+
+void orc_sincos(float x, float* s, float* c) { sincos_taylor(x, s, c); }
+
+}  // extern "C"

@@ -1,0 +1,277 @@
+"""ctypes bindings for the oracle — TEST INFRASTRUCTURE, not product code.
+
+Loads oracle/_build/liboracle.so (the CPU restatement in oracle.cpp) and,
+when present, oracle/_ref/libref.so (the reference's own SoftwareBVH,
+createTessellatedTerrain, compute_tree_layout and generate_dynamic_grid_mesh,
+compiled from the reference sources by oracle/Makefile).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this.
+Every array crossing the boundary is a C-contiguous numpy array.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref.so")
+
+# numpy mirrors of include/rq_layouts.h
+BVH2_NODE = np.dtype([("aabb_min", "<f4", 3), ("left_child", "<i4"), ("aabb_max", "<f4", 3), ("right_child", "<i4")])
+TRIANGLE = np.dtype([("v0", "<f4", 4), ("v1", "<f4", 4), ("v2", "<f4", 4)])
+BVH4_NODE = np.dtype([("min_x", "<f4", 4), ("max_x", "<f4", 4), ("min_y", "<f4", 4), ("max_y", "<f4", 4),
+                      ("min_z", "<f4", 4), ("max_z", "<f4", 4), ("child_index", "<i4", 4), ("child_count", "<i4", 4)])
+RAY = np.dtype([("org", "<f4", 3), ("tmin", "<f4"), ("dir", "<f4", 3), ("tmax", "<f4")])
+HIT = np.dtype([("hit", "<u4"), ("t", "<f4"), ("instance_id", "<u4"), ("primitive_id", "<u4")])
+STATS = np.dtype([("hit", "<u4"), ("box_tests", "<u4"), ("tri_tests", "<u4"), ("pad", "<u4")])
+assert BVH2_NODE.itemsize == 32 and TRIANGLE.itemsize == 48 and BVH4_NODE.itemsize == 128
+assert RAY.itemsize == 32 and HIT.itemsize == 16 and STATS.itemsize == 16
+
+_P = C.c_void_p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle library missing: run `make -C oracle`")
+        L = C.CDLL(ORACLE_SO)
+        L.orc_lbvh_build.argtypes = [_P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.orc_lbvh_build.restype = C.c_int
+        L.orc_collapse4.argtypes = [_P, C.c_uint32, _P, _P, _P]
+        L.orc_collapse4.restype = C.c_int
+        L.orc_radv_build.argtypes = [_P, C.c_uint32, _P]
+        L.orc_radv_build.restype = C.c_int
+        L.orc_trace_ref_bvh4.argtypes = [_P, _P, _P, C.c_uint32, _P, _P, C.c_int]
+        L.orc_trace_ref_bvh2.argtypes = [_P, _P, _P, C.c_uint32, C.c_float, _P, C.c_int]
+        L.orc_trace_bvh4.argtypes = [_P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, C.c_int]
+        L.orc_trace_radv.argtypes = [_P, _P, C.c_uint32, C.c_uint32, _P, _P, C.c_int]
+        L.orc_gen_rays_procedural.argtypes = [_P, _P, C.c_uint32, C.c_uint32, _P]
+        L.orc_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        _lib = L
+    return _lib
+
+
+def have_ref():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not have_ref():
+            raise RuntimeError("reference library missing: run `make -C oracle` where the reference tree exists")
+        R = C.CDLL(REF_SO)
+        R.ref_build.argtypes = [_P, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_int]
+        R.ref_build.restype = _P
+        R.ref_collapse.argtypes = [_P, C.c_uint32, _P, C.c_uint32]
+        R.ref_collapse.restype = _P
+        R.ref_counts.argtypes = [_P, _P, _P, _P]
+        R.ref_copy.argtypes = [_P, _P, _P, _P]
+        R.ref_free.argtypes = [_P]
+        R.ref_terrain.argtypes = [C.c_uint32, C.c_float, _P, _P, _P, _P]
+        R.ref_tree_layout.argtypes = [C.c_uint32, _P, _P, _P, _P, _P]
+        R.ref_dynamic_grid.argtypes = [C.c_uint32, C.c_float, C.c_float, _P, _P]
+        _ref = R
+    return _ref
+
+
+def threads():
+    return max(1, os.cpu_count() or 1)
+
+
+# ------------------------------------------------------------- Oracle B --
+
+def lbvh_build(pos, idx, max_leaf=4, stride_floats=3):
+    """Oracle B.  pos: float32 vertex array; idx: uint32 (3 per tri) or None.
+    Returns dict with codes, sorted ids, nodes2, tris, nodes4, depth4."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    if idx is not None:
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        n = idx.size // 3
+    else:
+        n = (pos.size // stride_floats) // 3
+    codes = np.empty(n, np.uint32)
+    srt = np.empty(n, np.uint32)
+    nodes2 = np.empty(2 * n, BVH2_NODE)
+    tris = np.empty(n, TRIANGLE)
+    nodes4 = np.empty(max(1, n), BVH4_NODE)
+    n2 = np.zeros(1, np.uint32)
+    n4 = np.zeros(1, np.uint32)
+    d4 = np.zeros(1, np.uint32)
+    rc = lib().orc_lbvh_build(_ptr(pos), stride_floats, _ptr(idx), n, max_leaf, _ptr(codes), _ptr(srt),
+                              _ptr(nodes2), _ptr(n2), _ptr(tris), _ptr(nodes4), _ptr(n4), _ptr(d4))
+    assert rc == 0
+    return dict(codes=codes, sorted=srt, nodes2=nodes2[: n2[0]].copy(), tris=tris,
+                nodes4=nodes4[: n4[0]].copy(), depth4=int(d4[0]))
+
+
+def collapse4(nodes2):
+    nodes2 = np.ascontiguousarray(nodes2)
+    out = np.empty(max(1, len(nodes2)), BVH4_NODE)
+    n4 = np.zeros(1, np.uint32)
+    d4 = np.zeros(1, np.uint32)
+    lib().orc_collapse4(_ptr(nodes2), len(nodes2), _ptr(out), _ptr(n4), _ptr(d4))
+    return out[: n4[0]].copy(), int(d4[0])
+
+
+# ------------------------------------------------------------- Oracle C --
+
+def radv_size(n):
+    counts = [(n + 3) // 4]
+    while counts[-1] > 1:
+        counts.append((counts[-1] + 3) // 4)
+    return 192 + 128 * sum(counts) + 64 * n
+
+
+def radv_build(tri9):
+    tri9 = np.ascontiguousarray(tri9, dtype=np.float32)
+    n = tri9.size // 9
+    img = np.empty(radv_size(n), np.uint8)
+    assert lib().orc_radv_build(_ptr(tri9), n, _ptr(img)) == 0
+    return img
+
+
+# ------------------------------------------------------------ traversal --
+
+def trace_ref_bvh4(nodes4, tris, rays):
+    rays = np.ascontiguousarray(rays)
+    stats = np.empty(len(rays), STATS)
+    hits = np.empty(len(rays), HIT)
+    lib().orc_trace_ref_bvh4(_ptr(np.ascontiguousarray(nodes4)), _ptr(np.ascontiguousarray(tris)), _ptr(rays),
+                             len(rays), _ptr(stats), _ptr(hits), threads())
+    return stats, hits
+
+
+def trace_ref_bvh2(nodes2, tris, rays, t_eps=0.001):
+    rays = np.ascontiguousarray(rays)
+    flags = np.empty(len(rays), np.uint32)
+    lib().orc_trace_ref_bvh2(_ptr(np.ascontiguousarray(nodes2)), _ptr(np.ascontiguousarray(tris)), _ptr(rays),
+                             len(rays), t_eps, _ptr(flags), threads())
+    return flags
+
+
+def trace_bvh4(nodes4, tris, perm, rays, flags=0, want_bary=False, want_stats=False):
+    rays = np.ascontiguousarray(rays)
+    hits = np.empty(len(rays), HIT)
+    bary = np.empty(2 * len(rays), np.float32) if want_bary else None
+    stats = np.empty(len(rays), STATS) if want_stats else None
+    perm = None if perm is None else np.ascontiguousarray(perm, dtype=np.uint32)
+    lib().orc_trace_bvh4(_ptr(np.ascontiguousarray(nodes4)), _ptr(np.ascontiguousarray(tris)), _ptr(perm),
+                         _ptr(rays), len(rays), flags, _ptr(hits), _ptr(bary), _ptr(stats), threads())
+    return hits, bary, stats
+
+
+def trace_radv(img, rays, flags=0, want_bary=False):
+    rays = np.ascontiguousarray(rays)
+    hits = np.empty(len(rays), HIT)
+    bary = np.empty(2 * len(rays), np.float32) if want_bary else None
+    lib().orc_trace_radv(_ptr(np.ascontiguousarray(img)), _ptr(rays), len(rays), flags, _ptr(hits), _ptr(bary),
+                         threads())
+    return hits, bary
+
+
+def gen_rays_procedural(cam, look, count, coherent):
+    rays = np.empty(count, RAY)
+    c = np.asarray(cam, np.float32)
+    l = np.asarray(look, np.float32)
+    lib().orc_gen_rays_procedural(_ptr(c), _ptr(l), count, 1 if coherent else 0, _ptr(rays))
+    return rays
+
+
+def sincos(x):
+    s, c = C.c_float(), C.c_float()
+    lib().orc_sincos(float(x), C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
+# ------------------------------------------------------------ reference --
+
+def ref_terrain(target, size=100.0):
+    R = ref()
+    nv, ni = np.zeros(1, np.uint32), np.zeros(1, np.uint32)
+    R.ref_terrain(target, size, None, None, _ptr(nv), _ptr(ni))
+    pos = np.empty(3 * int(nv[0]), np.float32)
+    idx = np.empty(int(ni[0]), np.uint32)
+    R.ref_terrain(target, size, _ptr(pos), _ptr(idx), _ptr(nv), _ptr(ni))
+    return pos, idx
+
+
+def ref_build(pos, idx, max_leaf=4, collapse=True):
+    """The reference's SoftwareBVH::build (+ SoftwareBVH4::fromBVH2)."""
+    R = ref()
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    h = R.ref_build(_ptr(pos), pos.size // 3, _ptr(idx), idx.size // 3, max_leaf, 1 if collapse else 0)
+    assert h
+    try:
+        n2, nt, n4 = np.zeros(1, np.uint32), np.zeros(1, np.uint32), np.zeros(1, np.uint32)
+        R.ref_counts(h, _ptr(n2), _ptr(nt), _ptr(n4))
+        nodes2 = np.empty(int(n2[0]), BVH2_NODE)
+        tris = np.empty(int(nt[0]), TRIANGLE)
+        nodes4 = np.empty(int(n4[0]), BVH4_NODE)
+        R.ref_copy(h, _ptr(nodes2), _ptr(tris), _ptr(nodes4) if n4[0] else None)
+    finally:
+        R.ref_free(h)
+    return nodes2, tris, nodes4
+
+
+def ref_collapse(nodes2, tris):
+    R = ref()
+    nodes2 = np.ascontiguousarray(nodes2)
+    tris = np.ascontiguousarray(tris)
+    h = R.ref_collapse(_ptr(nodes2), len(nodes2), _ptr(tris), len(tris))
+    try:
+        n2, nt, n4 = np.zeros(1, np.uint32), np.zeros(1, np.uint32), np.zeros(1, np.uint32)
+        R.ref_counts(h, _ptr(n2), _ptr(nt), _ptr(n4))
+        nodes4 = np.empty(int(n4[0]), BVH4_NODE)
+        R.ref_copy(h, None, None, _ptr(nodes4))
+    finally:
+        R.ref_free(h)
+    return nodes4
+
+
+def ref_tree_layout(n):
+    R = ref()
+    tb, nl, ts = np.zeros(1, np.uint32), np.zeros(1, np.uint32), np.zeros(1, np.uint32)
+    counts, offs = np.zeros(32, np.uint32), np.zeros(32, np.uint32)
+    R.ref_tree_layout(n, _ptr(tb), _ptr(nl), _ptr(ts), _ptr(counts), _ptr(offs))
+    L = int(nl[0])
+    return dict(total_boxes=int(tb[0]), num_levels=L, total_size=int(ts[0]),
+                counts=counts[:L].tolist(), offsets=offs[:L].tolist())
+
+
+def ref_dynamic_grid(n, time_val=0.0, extent=2.0):
+    R = ref()
+    tri9 = np.empty(9 * n, np.float32)
+    cen = np.empty(3 * n, np.float32)
+    R.ref_dynamic_grid(n, time_val, extent, _ptr(tri9), _ptr(cen))
+    return tri9, cen
+
+
+def recover_perm(tris_leaf_order, pos, idx):
+    """The reference discards the leaf-order permutation
+    (common/software_bvh.hpp:60-63); recover it by matching the 9 float bit
+    patterns of every leaf triangle to the input triangles.  Asserts unique."""
+    p = pos.reshape(-1, 3).view(np.uint32)
+    ii = idx.reshape(-1, 3)
+    inp = np.concatenate([p[ii[:, 0]], p[ii[:, 1]], p[ii[:, 2]]], axis=1)  # (n, 9)
+    lt = np.concatenate([tris_leaf_order["v0"][:, :3], tris_leaf_order["v1"][:, :3], tris_leaf_order["v2"][:, :3]],
+                        axis=1).view(np.uint32)
+    key_in = np.ascontiguousarray(inp).view([("k", "V36")]).ravel()
+    key_lt = np.ascontiguousarray(lt).view([("k", "V36")]).ravel()
+    order = np.argsort(key_in, kind="stable")
+    srt = key_in[order]
+    assert len(np.unique(srt)) == len(srt), "input triangles are not unique by vertex bits"
+    pos_in = np.searchsorted(srt, key_lt)
+    assert np.all(srt[pos_in] == key_lt)
+    return order[pos_in].astype(np.uint32)

@@ -1,0 +1,316 @@
+// k_radv.cu — the RADV image of shaders/fast_bvh_builder.comp:91-257 for any
+// triangle count, in one launch.
+//
+// The image is an implicit 4-ary tree over the triangles in input order
+// (level plan of include/radv_bvh.hpp:193-215): 64-B triangle nodes, Box32
+// leaves over four consecutive triangles, parents over four consecutive
+// children, qNaN boxes with child 0xFFFFFFFF in empty slots, the 136-B header
+// and the pre-root dwords at bytes 180 (= 5) and 188 (= 0xFFFFFFFF).  Bytes
+// the shader never writes (136..191 apart from those two dwords) are zeroed.
+//
+// Block b owns leaf boxes [1024b, 1024b+1024): 4096 triangles, one per
+// thread per round, so the four triangles of a leaf box sit in four
+// consecutive lanes and their boxes meet through warp shuffles.  The block
+// then reduces its subtree in shared memory for up to five levels.  The last
+// block to finish (atomic ticket) builds the remaining top levels and the
+// header from the per-block subtree boxes.
+#include "rq_device.cuh"
+#include "rq_internal.h"
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kLeafBoxes = 1024;  // per block
+constexpr uint32_t kQNaN = 0x7fc00000u;
+
+struct RadvArgs {
+    const float* tri9;
+    uint32_t n;
+    uint8_t* img;
+    uint32_t levels;
+    uint32_t total_boxes;
+    uint32_t counts[16];
+    uint32_t offs[16];
+    float4* top;        // 2 per block: subtree box lo, hi (then reused for the top levels)
+    uint32_t* ticket;
+    uint64_t size;
+};
+
+__device__ __forceinline__ void write_box(uint8_t* boxes, uint32_t node, const uint32_t ch[4], const float mn[4][3],
+                                          const float mx[4][3]) {
+    float4* o = reinterpret_cast<float4*>(boxes + 128ull * node);
+    float c[24];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        c[6 * k + 0] = mn[k][0];
+        c[6 * k + 1] = mn[k][1];
+        c[6 * k + 2] = mn[k][2];
+        c[6 * k + 3] = mx[k][0];
+        c[6 * k + 4] = mx[k][1];
+        c[6 * k + 5] = mx[k][2];
+    }
+    reinterpret_cast<uint4*>(o)[0] = make_uint4(ch[0], ch[1], ch[2], ch[3]);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[1 + q] = make_float4(c[4 * q], c[4 * q + 1], c[4 * q + 2], c[4 * q + 3]);
+    reinterpret_cast<uint4*>(o)[7] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// Parent box over up to four children held in (cmn, cmx); writes the Box32
+// node and returns the union through (umn, umx).
+__device__ __forceinline__ void make_parent(uint8_t* boxes, uint32_t node, uint32_t child_global0, uint32_t nvalid,
+                                            const float* cmn, const float* cmx, float umn[3], float umx[3]) {
+    uint32_t ch[4];
+    float mn[4][3], mx[4][3];
+    const float qn = __uint_as_float(kQNaN);
+    umn[0] = umn[1] = umn[2] = 1e30f;
+    umx[0] = umx[1] = umx[2] = -1e30f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (uint32_t(c) < nvalid) {
+            ch[c] = (((child_global0 + c) * 128u) >> 3) | RQ_RADV_NODE_BOX32;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                mn[c][k] = cmn[3 * c + k];
+                mx[c][k] = cmx[3 * c + k];
+                umn[k] = fminf(umn[k], mn[c][k]);
+                umx[k] = fmaxf(umx[k], mx[c][k]);
+            }
+        } else {
+            ch[c] = RQ_RADV_INVALID_NODE;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) mn[c][k] = mx[c][k] = qn;
+        }
+    }
+    write_box(boxes, node, ch, mn, mx);
+}
+
+__device__ void write_header(const RadvArgs& A, const float mn[3], const float mx[3]) {
+    uint32_t* h = reinterpret_cast<uint32_t*>(A.img);
+    // zero 0..191, then fill the fields
+    for (int i = 0; i < 48; ++i) h[i] = 0u;
+    h[0] = 192u;  // bvh_offset
+    h[1] = 0u;    // root_flags
+    for (int k = 0; k < 3; ++k) {
+        h[2 + k] = __float_as_uint(mn[k]);
+        h[5 + k] = __float_as_uint(mx[k]);
+    }
+    h[8] = 8u;  // update_dispatch_size
+    h[9] = 1u;
+    h[10] = 1u;
+    uint64_t* h64 = reinterpret_cast<uint64_t*>(A.img);
+    h64[0x30 / 8] = A.size;        // compacted_size
+    h64[0x38 / 8] = A.size + 128;  // serialization_size
+    h[0x40 / 4] = 1u;              // copy_dispatch_size
+    h[0x44 / 4] = 1u;
+    h[0x48 / 4] = 1u;
+    h64[0x50 / 8] = A.size;  // size
+    h[0x58 / 4] = 0u;        // geometry_type
+    h[0x5C / 4] = 1u;        // geometry_count
+    h64[0x60 / 8] = 192ull + 128ull * A.total_boxes;  // leaf_nodes_offset
+    h64[0x68 / 8] = A.n;                              // primitive_count
+    h64[0x70 / 8] = 0ull;                             // instance_count
+    h[0x78 / 4] = 0u;                                 // leaf_node_offsets_offset
+    h[0x7C / 4] = 4u;                                 // build_flags
+    h[0x80 / 4] = 1u;                                 // type
+    h[180 / 4] = 5u;
+    h[188 / 4] = 0xffffffffu;
+}
+
+__global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
+    // leaf-level boxes (1024) and the first parent level (256) ping-pong
+    __shared__ float s_mn0[kLeafBoxes * 3], s_mx0[kLeafBoxes * 3];
+    __shared__ float s_mn1[kLeafBoxes / 4 * 3], s_mx1[kLeafBoxes / 4 * 3];
+    __shared__ uint32_t s_last;
+    float* cmn_src = s_mn0;
+    float* cmx_src = s_mx0;
+    float* cmn_dst = s_mn1;
+    float* cmx_dst = s_mx1;
+    const uint32_t L = A.levels;
+    const uint32_t leaf_lvl = L - 1;
+    const uint32_t leaf_cnt = A.counts[leaf_lvl];
+    uint8_t* boxes = A.img + 192;
+    uint8_t* trin = A.img + 192 + 128ull * A.total_boxes;
+    const uint32_t lane = threadIdx.x & 31;
+    const float qn = __uint_as_float(kQNaN);
+
+    // ---- leaf boxes and triangle nodes
+    const uint32_t lb0 = blockIdx.x * kLeafBoxes;
+    const uint32_t nlb = min(uint32_t(kLeafBoxes), leaf_cnt - lb0);
+    for (uint32_t r = 0; r < 16; ++r) {
+        const uint32_t local = r * kT + threadIdx.x;  // triangle within block
+        const uint32_t ti = lb0 * 4u + local;
+        const bool valid = local < nlb * 4u && ti < A.n;
+        float tmn[3] = {qn, qn, qn}, tmx[3] = {qn, qn, qn};
+        if (valid) {
+            const float* v = A.tri9 + 9ull * ti;
+            float f[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) f[q] = __ldg(v + q);
+            float4* o = reinterpret_cast<float4*>(trin + 64ull * ti);
+            o[0] = make_float4(f[0], f[1], f[2], f[3]);
+            o[1] = make_float4(f[4], f[5], f[6], f[7]);
+            o[2] = make_float4(f[8], 0.0f, 0.0f, 0.0f);
+            reinterpret_cast<uint4*>(o)[3] =
+                make_uint4(ti, RQ_RADV_GEOMETRY_OPAQUE, 0u, RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                tmn[k] = fminf(f[k], fminf(f[3 + k], f[6 + k]));
+                tmx[k] = fmaxf(f[k], fmaxf(f[3 + k], f[6 + k]));
+            }
+        }
+        // gather the four triangles of this lane's leaf box (lanes 4j..4j+3)
+        const uint32_t g0 = lane & ~3u;
+        uint32_t okm = __ballot_sync(0xffffffffu, valid);
+        float cmn[4][3], cmx[4][3];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                cmn[c][k] = __shfl_sync(0xffffffffu, tmn[k], g0 + c);
+                cmx[c][k] = __shfl_sync(0xffffffffu, tmx[k], g0 + c);
+            }
+        const uint32_t lbl = local >> 2;  // leaf box within block
+        if ((lane & 3u) == 0u && lbl < nlb) {
+            uint32_t ch[4];
+            float umn[3] = {1e30f, 1e30f, 1e30f}, umx[3] = {-1e30f, -1e30f, -1e30f};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if ((okm >> (g0 + c)) & 1u) {
+                    uint32_t tic = (lb0 + lbl) * 4u + c;
+                    ch[c] = ((A.total_boxes * 128u + tic * 64u) >> 3) | RQ_RADV_NODE_TRIANGLE;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        umn[k] = fminf(umn[k], cmn[c][k]);
+                        umx[k] = fmaxf(umx[k], cmx[c][k]);
+                    }
+                } else {
+                    ch[c] = RQ_RADV_INVALID_NODE;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) cmn[c][k] = cmx[c][k] = qn;
+                }
+            }
+            write_box(boxes, A.offs[leaf_lvl] + lb0 + lbl, ch, cmn, cmx);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                s_mn0[3 * lbl + k] = umn[k];
+                s_mx0[3 * lbl + k] = umx[k];
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- in-block levels (up to five)
+    uint32_t nchild = nlb;                // children at the current level in this block
+    uint32_t child_base = lb0;            // first child index within its level
+    uint32_t lvl = leaf_lvl;              // level of the children
+    for (uint32_t j = 1; j <= 5 && lvl > 0; ++j) {
+        const uint32_t plvl = lvl - 1;
+        const uint32_t np = (nchild + 3) / 4;
+        const uint32_t pbase = child_base >> 2;
+        for (uint32_t t = threadIdx.x; t < np; t += kT) {
+            uint32_t nv = min(4u, nchild - 4 * t);
+            float umn[3], umx[3];
+            make_parent(boxes, A.offs[plvl] + pbase + t, A.offs[lvl] + child_base + 4 * t, nv, cmn_src + 12 * t,
+                        cmx_src + 12 * t, umn, umx);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                cmn_dst[3 * t + k] = umn[k];
+                cmx_dst[3 * t + k] = umx[k];
+            }
+        }
+        __syncthreads();
+        float* tn = cmn_src;
+        cmn_src = cmn_dst;
+        cmn_dst = tn;
+        float* tx = cmx_src;
+        cmx_src = cmx_dst;
+        cmx_dst = tx;
+        nchild = np;
+        child_base = pbase;
+        lvl = plvl;
+    }
+
+    if (lvl == 0) {
+        // this block built the root (single-block image)
+        if (threadIdx.x == 0) {
+            float mn[3] = {cmn_src[0], cmn_src[1], cmn_src[2]};
+            float mx[3] = {cmx_src[0], cmx_src[1], cmx_src[2]};
+            write_header(A, mn, mx);
+        }
+        return;
+    }
+
+    // ---- publish the subtree box, last block finishes the top
+    if (threadIdx.x == 0) {
+        __stcg(A.top + 2 * blockIdx.x, make_float4(cmn_src[0], cmn_src[1], cmn_src[2], 0.0f));
+        __stcg(A.top + 2 * blockIdx.x + 1, make_float4(cmx_src[0], cmx_src[1], cmx_src[2], 0.0f));
+        __threadfence();
+        s_last = atomicAdd(A.ticket, 1u) == gridDim.x - 1 ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // level `lvl` holds gridDim.x nodes whose boxes are in A.top[2b], A.top[2b+1]
+    float4* src = A.top;
+    float4* dst = A.top + 2 * gridDim.x;
+    uint32_t ncnt = A.counts[lvl];
+    while (lvl > 0) {
+        const uint32_t plvl = lvl - 1;
+        const uint32_t np = A.counts[plvl];
+        for (uint32_t t = threadIdx.x; t < np; t += kT) {
+            uint32_t nv = min(4u, ncnt - 4 * t);
+            float cmn[12], cmx[12];
+            for (uint32_t c = 0; c < nv; ++c) {
+                float4 a = __ldcg(src + 2 * (4 * t + c)), b = __ldcg(src + 2 * (4 * t + c) + 1);
+                cmn[3 * c] = a.x;
+                cmn[3 * c + 1] = a.y;
+                cmn[3 * c + 2] = a.z;
+                cmx[3 * c] = b.x;
+                cmx[3 * c + 1] = b.y;
+                cmx[3 * c + 2] = b.z;
+            }
+            float umn[3], umx[3];
+            make_parent(boxes, A.offs[plvl] + t, A.offs[lvl] + 4 * t, nv, cmn, cmx, umn, umx);
+            __stcg(dst + 2 * t, make_float4(umn[0], umn[1], umn[2], 0.0f));
+            __stcg(dst + 2 * t + 1, make_float4(umx[0], umx[1], umx[2], 0.0f));
+        }
+        __threadfence();
+        __syncthreads();
+        float4* tmp = src;
+        src = dst;
+        dst = tmp;
+        ncnt = np;
+        lvl = plvl;
+    }
+    if (threadIdx.x == 0) {
+        float4 a = __ldcg(src), b = __ldcg(src + 1);
+        float mn[3] = {a.x, a.y, a.z}, mx[3] = {b.x, b.y, b.z};
+        write_header(A, mn, mx);
+    }
+}
+
+}  // namespace
+
+int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st) {
+    const uint32_t leaf_cnt = L.level_counts[L.num_levels - 1];
+    const uint32_t blocks = (leaf_cnt + kLeafBoxes - 1) / kLeafBoxes;
+    size_t need = sizeof(float4) * 4ull * blocks + 256;
+    int rc = rq_ensure_scratch(ctx, need, st);
+    if (rc) return rc;
+    RadvArgs a;
+    a.tri9 = tri9;
+    a.n = n;
+    a.img = static_cast<uint8_t*>(img);
+    a.levels = L.num_levels;
+    a.total_boxes = L.total_boxes;
+    for (int i = 0; i < 16; ++i) {
+        a.counts[i] = L.level_counts[i];
+        a.offs[i] = L.level_offsets[i];
+    }
+    a.ticket = static_cast<uint32_t*>(ctx->scratch);
+    a.top = reinterpret_cast<float4*>(static_cast<char*>(ctx->scratch) + 256);
+    a.size = L.total_as_size;
+    cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st);
+    k_radv<<<blocks, kT, 0, st>>>(a);
+    return rq_cuda_status(ctx, cudaGetLastError(), "radv build launch");
+}

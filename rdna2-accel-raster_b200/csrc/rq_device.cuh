@@ -1,0 +1,242 @@
+// rq_device.cuh — device helpers shared by the kernels: memory-ordering
+// primitives, ordered-float encoding, the slab test, the two ray-triangle
+// tests and the hash/trigonometry used by the ray generators.
+//
+// All float arithmetic follows IEEE single precision with one rounding per
+// operation: the library is compiled with -fmad=false and fused operations
+// are written explicitly (__fmaf_rn), so results are reproducible bit for bit
+// by a CPU implementation of the same formulas.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/rq_layouts.h"
+
+namespace rq {
+
+// ------------------------------------------------------------ memory order
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// L2-coherent 16-B load (bypasses L1), for data written by other blocks in
+// the same launch.
+__device__ __forceinline__ float4 ld_cg4(const float4* p) { return __ldcg(p); }
+
+// Non-coherent read-only 16-B load through the texture path.
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ int4 ldg4i(const int4* p) { return __ldg(p); }
+
+// ---------------------------------------------------------- ordered floats
+// Monotone map float -> uint32 (-inf < ... < -0 < +0 < ... < +inf).
+__device__ __forceinline__ uint32_t f2o(float f) {
+    uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float o2f(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+// ------------------------------------------------------------------ Morton
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t quantize10(float c, float lo, float scale) {
+    float t = (c - lo) * scale;
+    if (t >= 1023.0f) return 1023u;
+    if (t > 0.0f) return (uint32_t)t;
+    return 0u;
+}
+
+// --------------------------------------------------------------- slab test
+#define RQ_TWO_POW_100 1.2676506002282294e30f
+#define RQ_TWO_POW_M100 7.888609052210118e-31f
+#define RQ_FAR_SCALE 1.00000095367431640625f
+
+// 1/d, with |d| < 2^-100 replaced by a signed 2^100 so o*inv stays exact.
+__device__ __forceinline__ float safe_inv(float d) {
+    return fabsf(d) < RQ_TWO_POW_M100 ? copysignf(RQ_TWO_POW_100, d) : 1.0f / d;
+}
+
+struct SlabRay {
+    float ix, iy, iz;  // inverse direction
+    float ox, oy, oz;  // origin * inverse direction
+};
+
+// Entry distance and hit flag of one box: fused (b*inv - o*inv) plane
+// distances, entry clamped below by tmin, exit above by best, exit widened
+// by 2^-20 relative.
+__device__ __forceinline__ bool slab(const SlabRay& r, float tmin, float best, float mnx, float mxx, float mny,
+                                     float mxy, float mnz, float mxz, float& tn) {
+    float tx0 = __fmaf_rn(mnx, r.ix, -r.ox), tx1 = __fmaf_rn(mxx, r.ix, -r.ox);
+    float ty0 = __fmaf_rn(mny, r.iy, -r.oy), ty1 = __fmaf_rn(mxy, r.iy, -r.oy);
+    float tz0 = __fmaf_rn(mnz, r.iz, -r.oz), tz1 = __fmaf_rn(mxz, r.iz, -r.oz);
+    float a = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    float b = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), best));
+    tn = a;
+    return a <= b * RQ_FAR_SCALE;
+}
+
+// ------------------------------------------------------- triangle tests
+struct F3 {
+    float x, y, z;
+};
+__device__ __forceinline__ F3 f3sub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ float f3dot(F3 a, F3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__device__ __forceinline__ F3 f3cross(F3 a, F3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ F3 f3norm(F3 v) {
+    float len = sqrtf(f3dot(v, v));
+    return {v.x / len, v.y / len, v.z / len};
+}
+__device__ __forceinline__ float f3c(F3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Moller-Trumbore in the arithmetic of software_bvh_bvh4.comp:166-178.
+__device__ __forceinline__ bool mt_test(F3 o, F3 d, F3 v0, F3 v1, F3 v2, float eps, float& t, float& u,
+                                        float& v) {
+    F3 e1 = f3sub(v1, v0);
+    F3 e2 = f3sub(v2, v0);
+    F3 h = f3cross(d, e2);
+    float a = f3dot(e1, h);
+    if (fabsf(a) < eps) return false;
+    float f = 1.0f / a;
+    F3 s = f3sub(o, v0);
+    u = f * f3dot(s, h);
+    if (u < 0.0f || u > 1.0f) return false;
+    F3 q = f3cross(s, e1);
+    v = f * f3dot(d, q);
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = f * f3dot(e2, q);
+    return true;
+}
+
+// Watertight test (Woop, Benthin, Wald 2013) with per-ray shear constants.
+struct WtRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+__device__ __forceinline__ WtRay wt_setup(F3 d) {
+    WtRay w;
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = 0;
+    float m = ax;
+    if (ay > m) {
+        kz = 1;
+        m = ay;
+    }
+    if (az > m) kz = 2;
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    float dz = f3c(d, kz);
+    if (dz < 0.0f) {
+        int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    w.kx = kx;
+    w.ky = ky;
+    w.kz = kz;
+    w.sx = f3c(d, kx) / dz;
+    w.sy = f3c(d, ky) / dz;
+    w.sz = 1.0f / dz;
+    return w;
+}
+
+// Shared-edge edge functions are exact negations of each other (plain float
+// products), exact zeros are re-evaluated in double, t = T / det rounded once.
+__device__ __forceinline__ bool wt_test(const WtRay& w, F3 o, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v) {
+    F3 A = f3sub(v0, o), B = f3sub(v1, o), C = f3sub(v2, o);
+    float Az0 = f3c(A, w.kz), Bz0 = f3c(B, w.kz), Cz0 = f3c(C, w.kz);
+    float Ax = __fmaf_rn(-w.sx, Az0, f3c(A, w.kx));
+    float Ay = __fmaf_rn(-w.sy, Az0, f3c(A, w.ky));
+    float Bx = __fmaf_rn(-w.sx, Bz0, f3c(B, w.kx));
+    float By = __fmaf_rn(-w.sy, Bz0, f3c(B, w.ky));
+    float Cx = __fmaf_rn(-w.sx, Cz0, f3c(C, w.kx));
+    float Cy = __fmaf_rn(-w.sy, Cz0, f3c(C, w.ky));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx));
+        V = (float)__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx));
+        W = (float)__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = (U + V) + W;
+    if (det == 0.0f) return false;
+    float Az = w.sz * Az0, Bz = w.sz * Bz0, Cz = w.sz * Cz0;
+    float T = (U * Az + V * Bz) + W * Cz;
+    t = T / det;
+    u = V / det;
+    v = W / det;
+    return true;
+}
+
+// ------------------------------------------------------------------ hashes
+__host__ __device__ __forceinline__ uint32_t pcg_hash(uint32_t v) {
+    uint32_t state = v * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+#define RQ_INV_2POW32 2.3283064365386963e-10f
+__device__ __forceinline__ float hash_float(uint32_t seed) { return __uint2float_rn(pcg_hash(seed)) * RQ_INV_2POW32; }
+
+// One-at-a-time style hash of shaders/rq_ao.comp:18-25.
+__device__ __forceinline__ uint32_t ao_hash(uint32_t x) {
+    x += (x << 10u);
+    x ^= (x >> 6u);
+    x += (x << 3u);
+    x ^= (x >> 11u);
+    x += (x << 15u);
+    return x;
+}
+
+// sin and cos from a Cody-Waite reduction by pi/2 (three-part constant) and
+// Taylor polynomials with coefficients 1/n! on [-pi/4, pi/4], evaluated with
+// explicit fused multiply-adds.  Used where the generated rays must be
+// reproducible bit for bit on the CPU.
+__device__ __forceinline__ void sincos_taylor(float x, float* s, float* c) {
+    float n = floorf(__fmaf_rn(x, 0x1.45f306p-1f, 0.5f));
+    float r = __fmaf_rn(-n, 0x1.921fb6p+0f, x);
+    r = __fmaf_rn(-n, -0x1.777a5cp-25f, r);
+    r = __fmaf_rn(-n, -0x1.ee59dap-50f, r);
+    float r2 = r * r;
+    float ps = __fmaf_rn(r2, 0x1.71de3ap-19f, -0x1.a01a02p-13f);
+    ps = __fmaf_rn(r2, ps, 0x1.111112p-7f);
+    ps = __fmaf_rn(r2, ps, -0x1.555556p-3f);
+    ps = __fmaf_rn(r2 * r, ps, r);
+    float pc = __fmaf_rn(r2, -0x1.27e4fcp-22f, 0x1.a01a02p-16f);
+    pc = __fmaf_rn(r2, pc, -0x1.6c16c2p-10f);
+    pc = __fmaf_rn(r2, pc, 0x1.555556p-5f);
+    pc = __fmaf_rn(r2, pc, -0.5f);
+    pc = __fmaf_rn(r2, pc, 1.0f);
+    int q = (int)((long long)n & 3);
+    *s = q == 0 ? ps : (q == 1 ? pc : (q == 2 ? -ps : -pc));
+    *c = q == 0 ? pc : (q == 1 ? -ps : (q == 2 ? -pc : ps));
+}
+
+// ------------------------------------------------------------ bounded wait
+// Iteration cap for spin-waits on flags written by other blocks of the same
+// launch: with __nanosleep(64) it is several seconds, far beyond any
+// legitimate wait, after which the waiter records an error and moves on.
+#define RQ_SPIN_LIMIT (1u << 26)
+
+__device__ __forceinline__ void set_err(uint32_t* err, uint32_t bit) { atomicOr(err, bit); }
+
+}  // namespace rq

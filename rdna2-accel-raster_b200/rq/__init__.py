@@ -1,0 +1,372 @@
+"""Python host mirror of librq's C ABI (include/rq.h), through ctypes.
+
+The engine itself is librq.so (C++ host + sm_100a CUDA kernels).  This module
+binds it for tests, benchmarks and Python callers: device buffers are torch
+CUDA tensors, passed as raw pointers.  There is no CPU or PyTorch fallback —
+loading fails loudly when librq.so is missing or no sm_100 device exists.
+
+Layouts (include/rq_layouts.h):
+  rays  float32 [n, 8]: origin xyz, tmin, direction xyz, tmax   (rq_ray)
+  hits  int32   [n, 4]: hit, t (float bits), instance id, primitive id (rq_hit)
+  stats int32   [n, 4]: hit, box tests, triangle tests, 0        (rq_ray_stats)
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "librq.so")
+
+RQ_OK = 0
+RQ_ERR_INVALID_ARG = 1
+RQ_ERR_SIZE = 2
+RQ_ERR_CUDA = 3
+RQ_ERR_OOM = 4
+RQ_ERR_DEVICE_TIMEOUT = 5
+RQ_ERR_UNSUPPORTED = 6
+RQ_ERR_BUDGET = 7
+RQ_ERR_NO_DEVICE = 8
+RQ_ERR_STATE = 9
+
+RQ_BUILD_BVH4 = 1
+RQ_TRACE_CLOSEST = 0
+RQ_TRACE_ANY = 1
+RQ_TRI_WATERTIGHT = 0
+RQ_TRI_MT = 2
+
+# numpy mirrors of the byte layouts
+BVH2_NODE = np.dtype([("aabb_min", "<f4", 3), ("left_child", "<i4"), ("aabb_max", "<f4", 3), ("right_child", "<i4")])
+TRIANGLE = np.dtype([("v0", "<f4", 4), ("v1", "<f4", 4), ("v2", "<f4", 4)])
+BVH4_NODE = np.dtype([("min_x", "<f4", 4), ("max_x", "<f4", 4), ("min_y", "<f4", 4), ("max_y", "<f4", 4),
+                      ("min_z", "<f4", 4), ("max_z", "<f4", 4), ("child_index", "<i4", 4), ("child_count", "<i4", 4)])
+RAY = np.dtype([("org", "<f4", 3), ("tmin", "<f4"), ("dir", "<f4", 3), ("tmax", "<f4")])
+HIT = np.dtype([("hit", "<u4"), ("t", "<f4"), ("instance_id", "<u4"), ("primitive_id", "<u4")])
+STATS = np.dtype([("hit", "<u4"), ("box_tests", "<u4"), ("tri_tests", "<u4"), ("pad", "<u4")])
+
+
+class RqError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"rq status {status}: {msg}")
+        self.status = status
+
+
+class BvhInfo(C.Structure):
+    _fields_ = [("num_triangles", C.c_uint32), ("num_nodes2", C.c_uint32), ("num_nodes4", C.c_uint32),
+                ("depth4", C.c_uint32), ("max_leaf", C.c_uint32), ("stack_bound", C.c_uint32),
+                ("device_bytes", C.c_uint64)]
+
+
+class RadvLayout(C.Structure):
+    _fields_ = [("num_triangles", C.c_uint32), ("total_boxes", C.c_uint32), ("num_levels", C.c_uint32),
+                ("total_as_size_lo", C.c_uint32), ("total_as_size", C.c_uint64),
+                ("level_offsets", C.c_uint32 * 16), ("level_counts", C.c_uint32 * 16)]
+
+
+_P = C.c_void_p
+_U32 = C.c_uint32
+# (name, restype, argtypes) for every entry point in include/rq.h
+SIGNATURES = [
+    ("rq_ctx_create", C.c_int, [C.c_int, C.POINTER(_P)]),
+    ("rq_ctx_destroy", C.c_int, [_P]),
+    ("rq_status_string", C.c_char_p, [C.c_int]),
+    ("rq_ctx_last_error", C.c_char_p, [_P]),
+    ("rq_ctx_check", C.c_int, [_P, _P]),
+    ("rq_ctx_scratch_bytes", C.c_uint64, [_P]),
+    ("rq_scene_grid", C.c_int, [_U32, _U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                C.c_float, C.c_uint64, _P, _P]),
+    ("rq_scene_rays_down", C.c_int, [_U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                     C.c_float, C.c_float, C.c_uint64, _P]),
+    ("rq_deform_wave", C.c_int, [_P, _P, _P, _U32, C.c_float, C.c_float, C.c_float, _P]),
+    ("rq_build", C.c_int, [_P, _P, _U32, _U32, _P, _U32, _U32, _U32, C.POINTER(_P), _P]),
+    ("rq_collapse4", C.c_int, [_P, _P, _P]),
+    ("rq_refit", C.c_int, [_P, _P, _P, _U32, _P, _P]),
+    ("rq_bvh_import2", C.c_int, [_P, _P, _U32, _P, _P, _U32, C.POINTER(_P), _P]),
+    ("rq_bvh_import4", C.c_int, [_P, _P, _U32, _P, _P, _U32, C.POINTER(_P), _P]),
+    ("rq_bvh_info_get", C.c_int, [_P, C.POINTER(BvhInfo)]),
+    ("rq_bvh_download", C.c_int, [_P, C.c_int, _P, _U32, _P, _U32, _P, _U32, _P, _U32]),
+    ("rq_bvh_download_sort", C.c_int, [_P, C.c_int, _P, _P, _U32]),
+    ("rq_bvh_destroy", C.c_int, [_P]),
+    ("rq_trace", C.c_int, [_P, _P, _P, _U32, _U32, _P, _P, _P, _P]),
+    ("rq_trace_ref_bvh4", C.c_int, [_P, _P, _P, _P, _U32, _P, _P, _P]),
+    ("rq_trace_ref_bvh2", C.c_int, [_P, _P, _P, _P, _U32, C.c_float, _P, _P]),
+    ("rq_gen_rays_procedural", C.c_int, [_P, _P, _P, _U32, _U32, _P, _P]),
+    ("rq_radv_layout_get", C.c_int, [_U32, C.POINTER(RadvLayout)]),
+    ("rq_radv_size", C.c_uint64, [_U32]),
+    ("rq_build_radv", C.c_int, [_P, _P, _U32, _P, C.c_uint64, _P]),
+    ("rq_trace_radv", C.c_int, [_P, _P, C.c_uint64, _P, _U32, _U32, _P, _P, _P]),
+]
+
+_lib = None
+
+
+def lib():
+    """Load librq.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"librq.so not built at {LIB_PATH}: run `make -C rdna2-accel-raster_b200/csrc`")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(t):
+    """Raw pointer of a torch tensor or numpy array (None -> NULL)."""
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data_as(_P)
+    return _P(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return _P(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return _P(stream)
+    return _P(stream.cuda_stream)
+
+
+class Context:
+    """An rq_ctx on one CUDA device (owns scratch memory)."""
+
+    def __init__(self, device=0):
+        h = _P()
+        rc = lib().rq_ctx_create(device, C.byref(h))
+        if rc != RQ_OK:
+            raise RqError(rc, lib().rq_status_string(rc).decode())
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().rq_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc, what=""):
+        if rc != RQ_OK:
+            msg = lib().rq_ctx_last_error(self.h).decode() if self.h else ""
+            raise RqError(rc, f"{what}: {lib().rq_status_string(rc).decode()} ({msg})")
+
+    def sync_check(self, stream=None):
+        """Synchronise and raise if a device-side bounded wait failed."""
+        self.check(lib().rq_ctx_check(self.h, _stream(stream)), "device error word")
+
+    def scratch_bytes(self):
+        return int(lib().rq_ctx_scratch_bytes(self.h))
+
+
+class Bvh:
+    """An rq_bvh handle (device-resident BVH in the reference layouts)."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = handle
+
+    @staticmethod
+    def build(ctx, pos, idx=None, max_leaf=4, bvh4=True, stride_bytes=12, stream=None, into=None):
+        """pos: float32 CUDA tensor of vertices; idx: int32/uint32 CUDA tensor
+        [T, 3] or None (non-indexed: 3 consecutive vertices per triangle)."""
+        nverts = pos.numel() * 4 // stride_bytes
+        ntri = idx.numel() // 3 if idx is not None else nverts // 3
+        h = _P(into.h.value) if into is not None else _P()
+        rc = lib().rq_build(ctx.h, _ptr(pos), stride_bytes, nverts, _ptr(idx), ntri, max_leaf,
+                            RQ_BUILD_BVH4 if bvh4 else 0, C.byref(h), _stream(stream))
+        ctx.check(rc, "rq_build")
+        if into is not None:
+            into.h = h
+            return into
+        return Bvh(ctx, h)
+
+    @staticmethod
+    def import2(ctx, nodes2, tris, perm=None, stream=None):
+        h = _P()
+        rc = lib().rq_bvh_import2(ctx.h, _ptr(nodes2), nodes2.numel() // 8, _ptr(tris), _ptr(perm),
+                                  tris.numel() // 12, C.byref(h), _stream(stream))
+        ctx.check(rc, "rq_bvh_import2")
+        return Bvh(ctx, h)
+
+    @staticmethod
+    def import4(ctx, nodes4, tris, perm=None, stream=None):
+        h = _P()
+        rc = lib().rq_bvh_import4(ctx.h, _ptr(nodes4), nodes4.numel() // 32, _ptr(tris), _ptr(perm),
+                                  tris.numel() // 12, C.byref(h), _stream(stream))
+        ctx.check(rc, "rq_bvh_import4")
+        return Bvh(ctx, h)
+
+    def collapse4(self, stream=None):
+        self.ctx.check(lib().rq_collapse4(self.ctx.h, self.h, _stream(stream)), "rq_collapse4")
+
+    def refit(self, pos, idx=None, stride_bytes=12, stream=None):
+        self.ctx.check(lib().rq_refit(self.ctx.h, self.h, _ptr(pos), stride_bytes, _ptr(idx), _stream(stream)),
+                       "rq_refit")
+
+    def info(self):
+        inf = BvhInfo()
+        self.ctx.check(lib().rq_bvh_info_get(self.h, C.byref(inf)), "rq_bvh_info_get")
+        return {k: getattr(inf, k) for k, _ in BvhInfo._fields_}
+
+    def download(self):
+        """Host copies: nodes2, tris, nodes4, perm as numpy structured arrays."""
+        inf = self.info()
+        n2 = np.empty(inf["num_nodes2"], BVH2_NODE)
+        tr = np.empty(inf["num_triangles"], TRIANGLE)
+        n4 = np.empty(inf["num_nodes4"], BVH4_NODE)
+        pm = np.empty(inf["num_triangles"], np.uint32)
+        rc = lib().rq_bvh_download(self.h, 1, _ptr(n2), len(n2), _ptr(tr), len(tr), _ptr(n4), len(n4), _ptr(pm),
+                                   len(pm))
+        self.ctx.check(rc, "rq_bvh_download")
+        return n2, tr, n4, pm
+
+    def download_sort(self):
+        inf = self.info()
+        keys = np.empty(inf["num_triangles"], np.uint32)
+        ids = np.empty(inf["num_triangles"], np.uint32)
+        self.ctx.check(lib().rq_bvh_download_sort(self.h, 1, _ptr(keys), _ptr(ids), len(keys)), "download_sort")
+        return keys, ids
+
+    def destroy(self):
+        if self.h:
+            lib().rq_bvh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def _empty_i32(n, cols, device):
+    import torch
+    return torch.empty((n, cols), dtype=torch.int32, device=device)
+
+
+def trace(ctx, bvh, rays, flags=0, bary=False, stats=False, hits=None, stream=None):
+    """rays: float32 CUDA tensor [n, 8].  Returns (hits int32 [n,4], bary, stats)."""
+    import torch
+    n = rays.shape[0]
+    dev = rays.device
+    hits = hits if hits is not None else _empty_i32(n, 4, dev)
+    b = torch.empty((n, 2), dtype=torch.float32, device=dev) if bary else None
+    s = _empty_i32(n, 4, dev) if stats else None
+    rc = lib().rq_trace(ctx.h, bvh.h, _ptr(rays), n, flags, _ptr(hits), _ptr(b), _ptr(s), _stream(stream))
+    ctx.check(rc, "rq_trace")
+    return hits, b, s
+
+
+def trace_ref_bvh4(ctx, nodes4, tris, rays, stream=None):
+    n = rays.shape[0]
+    st = _empty_i32(n, 4, rays.device)
+    hits = _empty_i32(n, 4, rays.device)
+    rc = lib().rq_trace_ref_bvh4(ctx.h, _ptr(nodes4), _ptr(tris), _ptr(rays), n, _ptr(st), _ptr(hits),
+                                 _stream(stream))
+    ctx.check(rc, "rq_trace_ref_bvh4")
+    return st, hits
+
+
+def trace_ref_bvh2(ctx, nodes2, tris, rays, t_eps=0.001, stream=None):
+    import torch
+    n = rays.shape[0]
+    flags = torch.empty(n, dtype=torch.int32, device=rays.device)
+    rc = lib().rq_trace_ref_bvh2(ctx.h, _ptr(nodes2), _ptr(tris), _ptr(rays), n, t_eps, _ptr(flags),
+                                 _stream(stream))
+    ctx.check(rc, "rq_trace_ref_bvh2")
+    return flags
+
+
+def gen_rays_procedural(ctx, cam, look, count, coherent, device="cuda", stream=None):
+    import torch
+    rays = torch.empty((count, 8), dtype=torch.float32, device=device)
+    c = (C.c_float * 3)(*cam)
+    l = (C.c_float * 3)(*look)
+    rc = lib().rq_gen_rays_procedural(ctx.h, C.cast(c, _P), C.cast(l, _P), count, 1 if coherent else 0,
+                                      _ptr(rays), _stream(stream))
+    ctx.check(rc, "rq_gen_rays_procedural")
+    return rays
+
+
+def radv_layout(n):
+    L = RadvLayout()
+    rc = lib().rq_radv_layout_get(n, C.byref(L))
+    if rc != RQ_OK:
+        raise RqError(rc, "rq_radv_layout_get")
+    lv = L.num_levels
+    return dict(total_boxes=L.total_boxes, num_levels=lv, total_size=int(L.total_as_size),
+                counts=list(L.level_counts[:lv]), offsets=list(L.level_offsets[:lv]))
+
+
+def radv_size(n):
+    return int(lib().rq_radv_size(n))
+
+
+def build_radv(ctx, tri9, image=None, stream=None):
+    import torch
+    n = tri9.numel() // 9
+    size = radv_size(n)
+    if image is None:
+        image = torch.empty(size, dtype=torch.uint8, device=tri9.device)
+    rc = lib().rq_build_radv(ctx.h, _ptr(tri9), n, _ptr(image), image.numel(), _stream(stream))
+    ctx.check(rc, "rq_build_radv")
+    return image
+
+
+def trace_radv(ctx, image, rays, flags=0, bary=False, stream=None):
+    import torch
+    n = rays.shape[0]
+    hits = _empty_i32(n, 4, rays.device)
+    b = torch.empty((n, 2), dtype=torch.float32, device=rays.device) if bary else None
+    rc = lib().rq_trace_radv(ctx.h, _ptr(image), image.numel(), _ptr(rays), n, flags, _ptr(hits), _ptr(b),
+                             _stream(stream))
+    ctx.check(rc, "rq_trace_radv")
+    return hits, b
+
+
+def scene_grid(qx, qy, x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, amp=0.2, freq=3.0, sigma=0.01, seed=0):
+    """Height-field grid on the host: float32 [V,3] positions, uint32 [T,3] indices."""
+    pos = np.empty(((qx + 1) * (qy + 1), 3), np.float32)
+    idx = np.empty((2 * qx * qy, 3), np.uint32)
+    rc = lib().rq_scene_grid(qx, qy, x0, x1, y0, y1, amp, freq, sigma, seed, _ptr(pos), _ptr(idx))
+    if rc != RQ_OK:
+        raise RqError(rc, "rq_scene_grid")
+    return pos, idx
+
+
+def scene_rays_down(n, x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, z=2.0, spread=0.3, tmin=0.01, tmax=1000.0, seed=0):
+    """Downward rays on the host as float32 [n, 8] (the plain workload's rays)."""
+    rays = np.empty((n, 8), np.float32)
+    rc = lib().rq_scene_rays_down(n, x0, x1, y0, y1, z, spread, tmin, tmax, seed, _ptr(rays))
+    if rc != RQ_OK:
+        raise RqError(rc, "rq_scene_rays_down")
+    return rays
+
+
+def deform_wave(ctx, base, out, t, amp=0.05, freq=1.0, stream=None):
+    rc = lib().rq_deform_wave(ctx.h, _ptr(base), _ptr(out), base.numel() // 3, t, amp, freq, _stream(stream))
+    ctx.check(rc, "rq_deform_wave")
+    return out
+
+
+def hits_numpy(hits_tensor):
+    """int32 [n,4] CUDA tensor -> numpy HIT structured array."""
+    return hits_tensor.cpu().numpy().view(HIT).reshape(-1)
+
+
+def stats_numpy(stats_tensor):
+    return stats_tensor.cpu().numpy().view(STATS).reshape(-1)
+
+
+def rays_numpy(rays_tensor):
+    return rays_tensor.cpu().numpy().view(RAY).reshape(-1)

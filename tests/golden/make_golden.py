@@ -1,0 +1,63 @@
+"""Regenerate the golden fixtures in tests/golden/ from the reference.
+
+Run in a container that has the reference tree (default /root/reference) and
+the oracle built (`make -C oracle`).  The GPU box never needs the reference:
+the tests read only the files this script writes.
+
+  exp0_ray_stats.json   published SW BVH4 statistics, results/exp0_ray_stats.csv
+  radv_layouts.json     compute_tree_layout (include/radv_bvh.hpp:193-215)
+  ref_terrain1000.npz   createTessellatedTerrain(1000) and the reference's
+                        SoftwareBVH / SoftwareBVH4 bytes for it
+  ref_dynamic_grids.npz generate_dynamic_grid_mesh(N, 1.25) for the builder
+                        verification sizes N = 64, 256, 1024, 4096
+"""
+import csv
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import pyoracle as O  # noqa: E402
+
+REF = os.environ.get("RQ_REFERENCE", "/root/reference")
+
+
+def main():
+    rows = []
+    with open(os.path.join(REF, "results", "exp0_ray_stats.csv")) as f:
+        for r in csv.DictReader(f):
+            if r["HitRate_SW_pct"] == "N/A":
+                continue
+            rows.append(dict(tris=int(r["Triangles"]), pattern=r["RayPattern"],
+                             hw_hit_pct=float(r["HitRate_HW_pct"]), sw_hit_pct=float(r["HitRate_SW_pct"]),
+                             box_tests=float(r["AvgBoxTests_PerRay"]), tri_tests=float(r["AvgTriTests_PerRay"])))
+    with open(os.path.join(HERE, "exp0_ray_stats.json"), "w") as f:
+        json.dump({"source": "results/exp0_ray_stats.csv", "rays": 1048576, "camera": [0, 50, -45],
+                   "look_at": [0, 0, 5], "rows": rows}, f, indent=1)
+
+    lay = {}
+    for n in (1, 3, 4, 5, 16, 17, 64, 256, 1024, 4096, 4097, 65536, 100000):
+        lay[str(n)] = O.ref_tree_layout(n)
+    with open(os.path.join(HERE, "radv_layouts.json"), "w") as f:
+        json.dump(lay, f, indent=1)
+
+    pos, idx = O.ref_terrain(1000)
+    n2, tris, n4 = O.ref_build(pos, idx)
+    np.savez_compressed(os.path.join(HERE, "ref_terrain1000.npz"), pos=pos, idx=idx, nodes2=n2.view(np.uint8),
+                        tris=tris.view(np.uint8), nodes4=n4.view(np.uint8))
+
+    grids = {}
+    for n in (64, 256, 1024, 4096):
+        tri9, cen = O.ref_dynamic_grid(n, 1.25)
+        grids[f"tri9_{n}"] = tri9
+        grids[f"cen_{n}"] = cen
+    np.savez_compressed(os.path.join(HERE, "ref_dynamic_grids.npz"), **grids)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
