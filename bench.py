@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark of the ray-query engine on one B200 (or N replicas).
+
+Default workload — the 1080p shadows + AO frame: a 2,499,848-triangle
+height-field grid (1118x1118 quads, seed 1), per step a full LBVH rebuild
+(Morton codes, onesweep radix sort, Karras hierarchy, refit, 4-wide
+collapse), 2,073,600 primary closest-hit rays into a G-buffer, then 16
+any-hit shadow rays and 1 cosine AO ray per pixel generated and traced in one
+kernel.  value = rays traced per step / step time (Mrays/s); the per-frame
+build rate (Mtris/s) and the any-hit rate are reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the frame:
+the path has no exchange step, so there is no collective on the data path;
+the barrier and the max-over-ranks step time use the process group only.
+
+--impl reference times the reference's CPU implementation of the path on the
+host cores: the reference's own SoftwareBVH::build + SoftwareBVH4::fromBVH2
+(compiled from its sources into oracle/_ref, single-threaded as written) and
+the CPU statement of the frame's rays (the reference has no CPU traversal)
+on all host threads, over a bounded pixel sample, projected to the frame.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rdna2-accel-raster_b200"))
+
+WIDTH, HEIGHT = 1920, 1080
+METRIC = "Mrays/s + BVH Mtris/s on 1 B200; p50/p99 request latency batched vs plain"
+# kernels launched by one step of the default workload: build = centroids,
+# morton, hist, hist_scan, 4 onesweep passes, karras, leaves, scan, emit,
+# collapse (13); then gbuffer and shadow/AO
+KERNELS_PER_STEP = 15
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=6000, help="pixels in the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x):
+    import torch
+    if pg is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, x):
+    import torch
+    if pg is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def read_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.md)."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    for ln in open(path):
+        if ln.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_frame_baseline(pos, idx, sample, threads):
+    """CPU time of one frame: the reference's SoftwareBVH build (+ fromBVH2,
+    single-threaded as written) on the full mesh and the CPU statement of the
+    frame's rays over `sample` pixels on `threads` threads, projected to all
+    pixels.  Returns dict(value Mrays/s, build_s, trace_s, rays, ...)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    from rq import workloads as W
+
+    ntri = len(idx)
+    t0 = time.perf_counter()
+    if O.have_ref():
+        n2, tr, n4 = O.ref_build(pos.reshape(-1), idx.reshape(-1))
+        kind = "reference"
+    else:
+        b = O.lbvh_build(pos.reshape(-1), idx.reshape(-1))
+        n2, tr, n4 = b["nodes2"], b["tris"], b["nodes4"]
+        kind = "port"
+    build_s = time.perf_counter() - t0
+    cam = W.shadow_camera()
+    params = W.shadow_params()
+    rng = np.random.default_rng(123)
+    pixels = np.sort(rng.choice(WIDTH * HEIGHT, sample, replace=False)).astype(np.uint32)
+    t0 = time.perf_counter()
+    g = O.render_gbuffer(n4, tr, None, cam, pixels)
+    gfull = np.zeros(WIDTH * HEIGHT, O.GBUFFER_PX)
+    gfull[pixels] = g
+    _, _, sec_rays = O.render_shadow_ao(n4, tr, gfull, params, pixels)
+    trace_s = time.perf_counter() - t0
+    rays_sample = sample + sec_rays
+    frame_rays = rays_sample * (WIDTH * HEIGHT) / sample
+    frame_s = build_s + trace_s * (WIDTH * HEIGHT) / sample
+    return dict(value=frame_rays / frame_s / 1e6, build_s=build_s, trace_s=trace_s, rays_sample=rays_sample,
+                frame_s=frame_s, kind=kind, cores=threads, triangles=ntri,
+                build_mtris=ntri / build_s / 1e6, trace_mrays=rays_sample / trace_s / 1e6)
+
+
+def run_reference(args, world, rank, pg):
+    """The reference arm: CPU implementation of the path, rank 0 only."""
+    if rank != 0:
+        return
+    import numpy as np
+    from rq import workloads as W
+
+    pos, idx = W.shadow_mesh()
+    threads = os.cpu_count() or 1
+    steps_done, vals, frame_s = 0, [], []
+    budget_s = 150.0
+    t_start = time.perf_counter()
+    for s in range(args.warmup + args.steps):
+        r = cpu_frame_baseline(pos, idx, args.cpu_sample, threads)
+        if s >= args.warmup:
+            vals.append(r["value"])
+            frame_s.append(r["frame_s"])
+            steps_done += 1
+        if time.perf_counter() - t_start > budget_s and steps_done >= 1:
+            break
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Mrays/s", "n_gpus": world,
+        "steps": steps_done, "warmup": args.warmup, "ms_per_step": round(1000 * statistics.median(frame_s), 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "1080p shadows + AO (2,499,848 triangles, 1920x1080, 16 lights, 1 SPP AO)",
+                   "parallelism": "cpu"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "Mrays/s", "cores": threads, "kind": r["kind"],
+                         "sample": (f"per step: reference SoftwareBVH::build+fromBVH2 on the full mesh "
+                                    f"({r['build_s']:.2f}s, 1 thread) + {args.cpu_sample} random pixels' primary, "
+                                    f"shadow and AO rays ({r['rays_sample']} rays, {threads} threads), projected to "
+                                    f"{WIDTH}x{HEIGHT}")},
+        "e2e": {"value": round(v, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+    import rq
+    from rq import workloads as W
+
+    ctx = rq.Context(local)
+    pos, idx = W.shadow_mesh()
+    ntri = len(idx)
+    cam = W.shadow_camera()
+    params = W.shadow_params()
+    npx = WIDTH * HEIGHT
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    # device-resident inputs and outputs
+    p_d = torch.from_numpy(pos).to(dev)
+    i_d = torch.from_numpy(idx.view(np.int32)).to(dev)
+    gbuf = torch.empty((npx, 8), dtype=torch.int32, device=dev)
+    mask = torch.empty(npx, dtype=torch.int32, device=dev)
+    ao = torch.empty(npx, dtype=torch.float32, device=dev)
+    counters = torch.zeros(4, dtype=torch.int64, device=dev)
+    bvh = rq.Bvh.build(ctx, p_d, i_d)
+
+    def step(count=None):
+        rq.Bvh.build(ctx, p_d, i_d, into=bvh)
+        rq.render_gbuffer(ctx, bvh, cam, gbuf)
+        rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao, count)
+
+    # ray count of one frame (deterministic): primary + shadow + AO
+    counters.zero_()
+    step(counters)
+    ctx.sync_check()
+    sec_rays = int(counters[0].item())
+    frame_rays = npx + sec_rays
+    hits = int((gbuf[:, 3] != 0).sum().item())
+
+    # node / triangle tests per any-hit ray, for the algorithmic bytes
+    cp = rq.shade_params(WIDTH, HEIGHT, W.shadow_lights(16), ao_spp=1, ao_tmax=0.5,
+                         flags=rq.RQ_SHADE_COUNT_TESTS)
+    counters.zero_()
+    rq.render_shadow_ao(ctx, bvh, gbuf, cp, mask, ao, counters)
+    ctx.sync_check()
+    c = counters.cpu().numpy()
+    v_node = c[1] / 4.0 / max(1, c[0])
+    v_tri = c[2] / max(1, c[0])
+    info = bvh.info()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4 * args.steps + 2)]
+    barrier(pg)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        ev[0].record(stream)
+        for s in range(args.steps):
+            e0, e1, e2, e3 = ev[1 + 4 * s: 5 + 4 * s]
+            e0.record(stream)
+            rq.Bvh.build(ctx, p_d, i_d, into=bvh)
+            e1.record(stream)
+            rq.render_gbuffer(ctx, bvh, cam, gbuf)
+            e2.record(stream)
+            rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao, None)
+            e3.record(stream)
+        ev[-1].record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(pg)
+    ctx.sync_check()
+    total_ms = ev[0].elapsed_time(ev[-1])
+    build_ms = [ev[1 + 4 * s].elapsed_time(ev[2 + 4 * s]) for s in range(args.steps)]
+    prim_ms = [ev[2 + 4 * s].elapsed_time(ev[3 + 4 * s]) for s in range(args.steps)]
+    shade_ms = [ev[3 + 4 * s].elapsed_time(ev[4 + 4 * s]) for s in range(args.steps)]
+    ms_step = max_over_ranks(pg, total_ms / args.steps)
+    value = sum_over_ranks(pg, frame_rays) / (ms_step * 1e-3) / 1e6
+
+    # end to end through the C ABI with host buffers: H2D of the mesh from
+    # pinned memory, the frame, D2H of the light masks and AO values
+    pos_h = torch.from_numpy(pos).pin_memory()
+    idx_h = torch.from_numpy(idx.view(np.int32)).pin_memory()
+    mask_h = torch.empty(npx, dtype=torch.int32).pin_memory()
+    ao_h = torch.empty(npx, dtype=torch.float32).pin_memory()
+    h2d = pos_h.numel() * 4 + idx_h.numel() * 4
+    d2h = mask_h.numel() * 4 + ao_h.numel() * 4
+
+    def e2e_step():
+        p_d.copy_(pos_h, non_blocking=True)
+        i_d.copy_(idx_h, non_blocking=True)
+        step()
+        mask_h.copy_(mask, non_blocking=True)
+        ao_h.copy_(ao, non_blocking=True)
+
+    for _ in range(max(3, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier(pg)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(pg)
+    e2e_ms = max_over_ranks(pg, a.elapsed_time(b) / args.steps)
+    e2e_value = sum_over_ranks(pg, frame_rays) / (e2e_ms * 1e-3) / 1e6
+
+    if rank != 0:
+        return
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    shade_med = statistics.median(shade_ms)
+    # algorithmic bytes of the shadow/AO launch: G-buffer read (32 B/pixel),
+    # mask + AO written (8 B/pixel), per ray the 128-B nodes and 48-B
+    # triangles its traversal visits (mean counts measured above)
+    alg_bytes = npx * (32 + 8) + sec_rays * (128.0 * v_node + 48.0 * v_tri)
+    achieved = alg_bytes / (shade_med * 1e-3) / 1e9
+    traffic = read_traffic("k_shadow_ao_1080p.md")
+    clocks = clk.summary()
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        r = cpu_frame_baseline(pos, idx, args.cpu_sample, os.cpu_count() or 1)
+        cpu = {"value": round(r["value"], 3), "unit": "Mrays/s", "cores": r["cores"], "kind": r["kind"],
+               "sample": (f"reference SoftwareBVH::build+fromBVH2 on the full mesh ({r['build_s']:.2f}s, 1 thread, "
+                          f"{r['build_mtris']:.2f} Mtris/s) + {args.cpu_sample} random pixels' primary, shadow and AO "
+                          f"rays ({r['rays_sample']} rays, {r['trace_mrays']:.2f} Mrays/s on {r['cores']} threads), "
+                          f"projected to {WIDTH}x{HEIGHT}")}
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": ("1080p shadows + AO: 2,499,848-triangle grid (1118x1118 quads, seed 1), per-frame LBVH "
+                         "rebuild, 1920x1080 primary rays, 16 any-hit shadow rays + 1 SPP AO (tmax 0.5) per pixel"),
+            "triangles": ntri, "width": WIDTH, "height": HEIGHT, "lights": 16, "ao_spp": 1,
+            "rays_per_step": frame_rays, "primary_rays": npx, "secondary_rays": sec_rays, "primary_hits": hits,
+            "l2": "inputs larger than L2: the per-step rebuild writes ~0.2 GB of nodes and triangles",
+            "parallelism": "replicas" if world > 1 else "single",
+        },
+        "build_mtris_per_s": round(ntri / statistics.median(build_ms) / 1e3, 1),
+        "build_ms": round(statistics.median(build_ms), 4),
+        "primary_mrays_per_s": round(npx / statistics.median(prim_ms) / 1e3, 1),
+        "anyhit_mrays_per_s": round(sec_rays / shade_med / 1e3, 1),
+        "shadow_ao_ms": round(shade_med, 4),
+        "bvh": {"nodes4": info["num_nodes4"], "depth4": info["depth4"], "nodes2": info["num_nodes2"],
+                "node_visits_per_anyhit_ray": round(v_node, 3), "tri_tests_per_anyhit_ray": round(v_tri, 3)},
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 4)},
+        "roofline": {"bound": "hbm", "kernel": "k_shadow_ao", "achieved": round(achieved, 1), "peak": hbm,
+                     "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback",
+                     "algorithmic_bytes_per_launch": round(alg_bytes)},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": KERNELS_PER_STEP * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    bvh.destroy()
+    ctx.close()
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, pg)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

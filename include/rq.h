@@ -193,6 +193,88 @@ int rq_gen_rays_procedural(rq_ctx* ctx, const float cam_pos[3], const float look
                            uint32_t count, uint32_t coherent, rq_ray* rays, rq_stream stream);
 
 /* ------------------------------------------------------------------ */
+/* Frames: rays generated inside the traversal kernels                 */
+/* ------------------------------------------------------------------ */
+
+/* Pinhole camera of benchmarks/exp1_visbuf/shaders/visbuf_raycast.comp:15-51:
+ * pixel (x, y) looks through NDC ((x+jx)/W*2-1, (y+jy)/H*2-1, 1) mapped to
+ * the world by inv_view_proj (column-major, GLSL convention) and divided by
+ * w; the ray leaves cam_pos toward that point.  jx = jy = 0.5 without
+ * jitter; with jitter they are per-pixel U(0,1) draws from `seed`. */
+typedef struct rq_camera {
+    float inv_view_proj[16];
+    float cam_pos[3];
+    uint32_t width;
+    uint32_t height;
+    uint32_t jitter;
+    uint32_t seed;
+    float tmin; /* 0.01 in visbuf_raycast.comp:295 */
+    float tmax; /* 10000 in visbuf_raycast.comp:297 */
+    uint32_t flags; /* RQ_TRI_* */
+} rq_camera;
+
+/* One G-buffer pixel (32 B): hit position, visibility value (primitive
+ * id + 1, 0 for a miss, as visbuf_raycast.comp:304-310 writes it), unit face
+ * normal turned toward the camera (rq_ao.comp:67-68), hit distance. */
+typedef struct rq_gbuffer_px {
+    float pos[3];
+    uint32_t vis;
+    float nrm[3];
+    float t;
+} rq_gbuffer_px;
+
+typedef struct rq_light {
+    float pos[3];
+    float radius;
+} rq_light;
+
+#define RQ_MAX_LIGHTS 32
+
+/* Shadow and ambient-occlusion parameters.  Per pixel with a hit, light k
+ * casts an any-hit shadow ray when dist in [0.001, radius] and N.L > 0, from
+ * P + shadow_bias*N with [shadow_tmin, dist - shadow_bias]
+ * (shaders/tiled_lighting_ra.comp:223-253); ao_spp cosine-weighted any-hit
+ * rays from P + ao_bias*N with [ao_tmin, ao_tmax], seeded y*W + x + 5544
+ * (shaders/rq_ao.comp:18-94). */
+typedef struct rq_shade_params {
+    uint32_t width;
+    uint32_t height;
+    uint32_t num_lights; /* <= RQ_MAX_LIGHTS */
+    uint32_t ao_spp;     /* 0: no AO rays (ao gets 1.0) */
+    float ao_tmax;       /* maxAoDistance */
+    float ao_tmin;       /* 0.01 */
+    float ao_bias;       /* 0.03 */
+    float shadow_tmin;   /* 0.01 */
+    float shadow_bias;   /* 0.04 */
+    uint32_t flags;      /* RQ_TRI_* */
+    rq_light lights[RQ_MAX_LIGHTS];
+} rq_shade_params;
+
+/* Camera from eye / target / up (right-handed look-at), vertical field of
+ * view in degrees and image size: fills inv_view_proj (Vulkan clip space,
+ * y flipped as the reference's projection) and cam_pos; jitter off, tmin
+ * 0.01, tmax 10000, watertight triangles.  Host only. */
+int rq_camera_look_at(const float eye[3], const float target[3], const float up[3], float fovy_deg,
+                      uint32_t width, uint32_t height, rq_camera* out);
+
+/* Primary closest-hit rays for every pixel into `gbuf` (width*height
+ * entries, device).  The visibility-buffer pass of visbuf_raycast.comp and
+ * the G-buffer the lighting passes read.  `cam` is a host pointer. */
+int rq_render_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera* cam, rq_gbuffer_px* gbuf, rq_stream stream);
+
+/* params->flags bit: also count node and triangle tests into counters[1..2] */
+#define RQ_SHADE_COUNT_TESTS 16u
+
+/* Shadow and AO rays for every G-buffer pixel, generated and traced in one
+ * kernel.  light_mask[p] bit k = light k cast a shadow ray that reached it;
+ * ao[p] = unoccluded fraction (1.0 for empty pixels).  `counters` (device,
+ * may be NULL) accumulates [0] rays cast and, with RQ_SHADE_COUNT_TESTS,
+ * [1] box tests (4 per node visited) and [2] triangle tests.  `params` is a
+ * host pointer; the other buffers are device pointers. */
+int rq_render_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_shade_params* params,
+                        uint32_t* light_mask, float* ao, unsigned long long* counters, rq_stream stream);
+
+/* ------------------------------------------------------------------ */
 /* RADV image (fast_bvh_builder.comp)                                  */
 /* ------------------------------------------------------------------ */
 

@@ -35,7 +35,7 @@
 #include <thread>
 #include <vector>
 
-#include "../include/rq_layouts.h"
+#include "../include/rq.h"
 
 namespace {
 
@@ -79,6 +79,20 @@ void parallel_for(uint32_t n, int threads, F&& f) {
     for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
     for (auto& th : pool) th.join();
 }
+
+// Traversal stack without heap traffic: 1024 entries, far above the
+// 3*depth+1 a 4-wide traversal can need for any tree the engine accepts.
+template <class T>
+struct FixedStack {
+    T v[1024];
+    int n = 0;
+    void push_back(const T& x) {
+        if (n < 1024) v[n++] = x;
+    }
+    bool empty() const { return n == 0; }
+    T back() const { return v[n - 1]; }
+    void pop_back() { --n; }
+};
 
 inline V3 load_vertex(const float* pos, uint32_t stride_floats, uint32_t v) {
     const float* p = pos + size_t(v) * stride_floats;
@@ -460,8 +474,7 @@ TraceOut trace_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq
         int32_t idx;   // node index, or first prim for a leaf
         int32_t cnt;   // -1 inner, else prim count
     };
-    std::vector<Entry> st;
-    st.reserve(64);
+    FixedStack<Entry> st;
     st.push_back({0, -1});
     while (!st.empty()) {
         Entry e = st.back();
@@ -533,7 +546,7 @@ TraceOut trace_radv(const uint8_t* img, const rq_ray& r, uint32_t flags) {
     float tmin = r.tmin, best = r.tmax;
     TraceOut res{false, -1.0f, 0xffffffffu, 0.0f, 0.0f, 0, 0};
     const uint8_t* base = img + RQ_RADV_BVH_OFFSET;
-    std::vector<uint32_t> st;
+    FixedStack<uint32_t> st;
     st.push_back(RQ_RADV_NODE_BOX32);
     while (!st.empty()) {
         uint32_t id = st.back();
@@ -1048,5 +1061,107 @@ void orc_gen_rays_procedural(const float cam[3], const float look[3], uint32_t c
 }
 
 void orc_sincos(float x, float* s, float* c) { sincos_taylor(x, s, c); }
+
+// Primary rays of visbuf_raycast.comp:15-51 (optional per-pixel jitter),
+// closest hit with the engine traversal, G-buffer pixel as rq_render_gbuffer
+// writes it.  `pixels` lists the pixel indices to evaluate (NULL = all);
+// out[i] receives pixel pixels[i].
+void orc_render_gbuffer(const rq_bvh4_node* nodes, const rq_triangle* tris, const uint32_t* perm, const rq_camera* cam,
+                        const uint32_t* pixels, uint32_t npix, rq_gbuffer_px* out, int threads) {
+    const rq_camera c = *cam;
+    parallel_for(npix, threads, [&](uint32_t i) {
+        uint32_t pixel = pixels ? pixels[i] : i;
+        uint32_t px = pixel % c.width, py = pixel / c.width;
+        float jx = 0.5f, jy = 0.5f;
+        if (c.jitter) {
+            uint32_t h = pcg_hash(c.seed ^ pcg_hash(pixel));
+            jx = float(h) * kInv2Pow32;
+            jy = float(pcg_hash(h)) * kInv2Pow32;
+        }
+        float u = (float(px) + jx) / float(c.width);
+        float v = (float(py) + jy) / float(c.height);
+        float cl[4] = {u * 2.0f - 1.0f, v * 2.0f - 1.0f, 1.0f, 1.0f};
+        float wt[4];
+        mat4_mul(c.inv_view_proj, cl, wt);
+        V3 o{c.cam_pos[0], c.cam_pos[1], c.cam_pos[2]};
+        V3 target{wt[0] / wt[3], wt[1] / wt[3], wt[2] / wt[3]};
+        V3 d = normalize(sub(target, o));
+        rq_ray r{{o.x, o.y, o.z}, c.tmin, {d.x, d.y, d.z}, c.tmax};
+        TraceOut t = trace_bvh4(nodes, tris, r, c.flags & 2u);
+        rq_gbuffer_px g;
+        if (!t.hit) {
+            g = {{0.0f, 0.0f, 0.0f}, 0u, {0.0f, 0.0f, 0.0f}, -1.0f};
+        } else {
+            V3 p{o.x + t.t * d.x, o.y + t.t * d.y, o.z + t.t * d.z};
+            const rq_triangle& tr = tris[t.prim];
+            V3 e1{tr.v1[0] - tr.v0[0], tr.v1[1] - tr.v0[1], tr.v1[2] - tr.v0[2]};
+            V3 e2{tr.v2[0] - tr.v0[0], tr.v2[1] - tr.v0[1], tr.v2[2] - tr.v0[2]};
+            V3 n = normalize(cross(e1, e2));
+            if (dot(n, sub(o, p)) < 0.0f) n = {-n.x, -n.y, -n.z};
+            uint32_t pid = perm ? perm[t.prim] : t.prim;
+            g = {{p.x, p.y, p.z}, pid + 1u, {n.x, n.y, n.z}, t.t};
+        }
+        out[i] = g;
+    });
+}
+
+// Shadow rays of tiled_lighting_ra.comp:223-253 and AO rays of
+// rq_ao.comp:18-94 for the listed pixels of a full-size G-buffer.
+void orc_render_shadow_ao(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq_gbuffer_px* gbuf,
+                          const rq_shade_params* prm, const uint32_t* pixels, uint32_t npix, uint32_t* mask, float* ao,
+                          uint64_t* rays_out, int threads) {
+    const rq_shade_params p = *prm;
+    std::atomic<uint64_t> total{0};
+    parallel_for(npix, threads, [&](uint32_t i) {
+        uint32_t pixel = pixels ? pixels[i] : i;
+        const rq_gbuffer_px& g = gbuf[pixel];
+        uint32_t m = 0, rays = 0;
+        float occl = 1.0f;
+        if (g.vis != 0u) {
+            V3 P{g.pos[0], g.pos[1], g.pos[2]}, N{g.nrm[0], g.nrm[1], g.nrm[2]};
+            V3 os{P.x + N.x * p.shadow_bias, P.y + N.y * p.shadow_bias, P.z + N.z * p.shadow_bias};
+            for (uint32_t k = 0; k < p.num_lights; ++k) {
+                const rq_light& L0 = p.lights[k];
+                V3 tl{L0.pos[0] - P.x, L0.pos[1] - P.y, L0.pos[2] - P.z};
+                float dist = std::sqrt(dot(tl, tl));
+                if (dist > L0.radius || dist < 0.001f) continue;
+                V3 L{tl.x / dist, tl.y / dist, tl.z / dist};
+                if (fmax_(0.0f, dot(N, L)) <= 0.0f) continue;
+                ++rays;
+                rq_ray r{{os.x, os.y, os.z}, p.shadow_tmin, {L.x, L.y, L.z}, dist - p.shadow_bias};
+                if (!trace_bvh4(nodes, tris, r, 1u | (p.flags & 2u)).hit) m |= 1u << k;
+            }
+            if (p.ao_spp) {
+                uint32_t seed = pixel + 5544u;
+                V3 oa{P.x + N.x * p.ao_bias, P.y + N.y * p.ao_bias, P.z + N.z * p.ao_bias};
+                float unocc = 0.0f;
+                for (uint32_t s = 0; s < p.ao_spp; ++s) {
+                    seed = ao_hash(seed);
+                    float u1 = float(seed) * kInv2Pow32;
+                    seed = ao_hash(seed);
+                    float u2 = float(seed) * kInv2Pow32;
+                    float rr = std::sqrt(u1);
+                    float theta = 6.2831853f * u2;
+                    float sn, cs;
+                    sincos_taylor(theta, &sn, &cs);
+                    float x = rr * cs, y = rr * sn, z = std::sqrt(fmax_(0.0f, 1.0f - u1));
+                    V3 up = std::fabs(N.z) < 0.999f ? V3{0.0f, 0.0f, 1.0f} : V3{1.0f, 0.0f, 0.0f};
+                    V3 tg = normalize(cross(up, N));
+                    V3 bt = cross(N, tg);
+                    V3 dir = normalize(V3{(tg.x * x + bt.x * y) + N.x * z, (tg.y * x + bt.y * y) + N.y * z,
+                                          (tg.z * x + bt.z * y) + N.z * z});
+                    ++rays;
+                    rq_ray r{{oa.x, oa.y, oa.z}, p.ao_tmin, {dir.x, dir.y, dir.z}, p.ao_tmax};
+                    if (!trace_bvh4(nodes, tris, r, 1u | (p.flags & 2u)).hit) unocc += 1.0f;
+                }
+                occl = unocc / float(p.ao_spp);
+            }
+        }
+        mask[i] = m;
+        ao[i] = occl;
+        total += rays;
+    });
+    if (rays_out) *rays_out = total;
+}
 
 }  // extern "C"

@@ -188,6 +188,38 @@ def gen_rays_procedural(cam, look, count, coherent):
     return rays
 
 
+GBUFFER_PX = np.dtype([("pos", "<f4", 3), ("vis", "<u4"), ("nrm", "<f4", 3), ("t", "<f4")])
+
+
+def render_gbuffer(nodes4, tris, perm, cam, pixels=None):
+    """cam: an rq.Camera ctypes structure; pixels: uint32 indices or None."""
+    import ctypes as CC
+    L = lib()
+    L.orc_render_gbuffer.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, C.c_int]
+    npix = cam.width * cam.height if pixels is None else len(pixels)
+    out = np.empty(npix, GBUFFER_PX)
+    px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    L.orc_render_gbuffer(_ptr(np.ascontiguousarray(nodes4)), _ptr(np.ascontiguousarray(tris)),
+                         _ptr(None if perm is None else np.ascontiguousarray(perm, np.uint32)),
+                         CC.cast(CC.byref(cam), _P), _ptr(px), npix, _ptr(out), threads())
+    return out
+
+
+def render_shadow_ao(nodes4, tris, gbuf_full, params, pixels=None):
+    import ctypes as CC
+    L = lib()
+    L.orc_render_shadow_ao.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, _P, _P, C.c_int]
+    npix = params.width * params.height if pixels is None else len(pixels)
+    mask = np.empty(npix, np.uint32)
+    ao = np.empty(npix, np.float32)
+    rays = np.zeros(1, np.uint64)
+    px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    L.orc_render_shadow_ao(_ptr(np.ascontiguousarray(nodes4)), _ptr(np.ascontiguousarray(tris)),
+                           _ptr(np.ascontiguousarray(gbuf_full)), CC.cast(CC.byref(params), _P), _ptr(px), npix,
+                           _ptr(mask), _ptr(ao), _ptr(rays), threads())
+    return mask, ao, int(rays[0])
+
+
 def sincos(x):
     s, c = C.c_float(), C.c_float()
     lib().orc_sincos(float(x), C.byref(s), C.byref(c))

@@ -468,6 +468,45 @@ int rq_gen_rays_procedural(rq_ctx* ctx, const float cam_pos[3], const float look
     return rq_launch_gen_procedural(ctx, cam_pos, look_at, count, coherent, rays, S(stream));
 }
 
+// ---------------------------------------------------------------- frames
+
+static int frame_checks(rq_ctx* ctx, const rq_bvh* bvh) {
+    if (!bvh->built || !bvh->has4) return rq_set_error(ctx, RQ_ERR_STATE, "handle has no 4-wide BVH");
+    if (!bvh->counts_valid) {
+        int rc = sync_counts(const_cast<rq_bvh*>(bvh));
+        if (rc) return rc;
+    }
+    if (bvh->h_counts[3] > 16) return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "leaf with more than 16 primitives");
+    if (3u * bvh->h_counts[2] + 1u > 128u)
+        return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "4-wide tree deeper than 42 levels");
+    return RQ_OK;
+}
+
+int rq_render_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera* cam, rq_gbuffer_px* gbuf, rq_stream stream) {
+    if (!ctx || !bvh || !cam || !gbuf) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (cam->width == 0 || cam->height == 0 || (cam->flags & ~2u))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad camera");
+    if (!aligned(gbuf, 16)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "misaligned G-buffer");
+    cudaSetDevice(ctx->device);
+    int rc = frame_checks(ctx, bvh);
+    if (rc) return rc;
+    return rq_launch_gbuffer(ctx, bvh, *cam, gbuf, S(stream));
+}
+
+int rq_render_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_shade_params* params,
+                        uint32_t* light_mask, float* ao, unsigned long long* counters, rq_stream stream) {
+    if (!ctx || !bvh || !gbuf || !params || !light_mask || !ao)
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (params->num_lights > RQ_MAX_LIGHTS || params->width == 0 || params->height == 0 || (params->flags & ~(RQ_TRI_MT | RQ_SHADE_COUNT_TESTS)))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad shading parameters");
+    if (!aligned(gbuf, 16) || (counters && !aligned(counters, 8)))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "misaligned buffer");
+    cudaSetDevice(ctx->device);
+    int rc = frame_checks(ctx, bvh);
+    if (rc) return rc;
+    return rq_launch_shadow_ao(ctx, bvh, gbuf, *params, light_mask, ao, counters, S(stream));
+}
+
 // ---------------------------------------------------------------- RADV
 
 int rq_radv_layout_get(uint32_t n, rq_radv_layout* out) {

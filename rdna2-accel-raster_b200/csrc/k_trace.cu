@@ -14,11 +14,11 @@
 //  k_ref2     software_bvh_lds.comp:86-175 as published (hitFound flag).
 #include "rq_device.cuh"
 #include "rq_internal.h"
+#include "trace_core.cuh"
 
 namespace {
 
 constexpr int kT = 128;
-constexpr uint32_t kLeafBit = 0x80000000u;
 
 __device__ __forceinline__ void store_miss(rq_hit* hits, uint32_t i) {
     reinterpret_cast<uint4*>(hits)[i] = make_uint4(0u, __float_as_uint(-1.0f), 0xffffffffu, 0xffffffffu);
@@ -37,104 +37,20 @@ __global__ void __launch_bounds__(kT) k_trace4(const rq_bvh4_node* __restrict__ 
     // the stack variant was picked from the host's copy of the depth; the
     // live depth (after an in-place rebuild) must still fit
     if (i == 0 && 3u * __ldg(counts + 2) + 1u > uint32_t(STACK)) rq::set_err(err, RQ_DERR_STACK);
-    int32_t* stk = s_stack + threadIdx.x;
-
     const float4* rp = reinterpret_cast<const float4*>(rays + i);
-    float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-    rq::F3 o{r0.x, r0.y, r0.z}, d{r1.x, r1.y, r1.z};
-    const float tmin = r0.w;
-    float best = r1.w;
-    rq::SlabRay sr;
-    sr.ix = rq::safe_inv(d.x);
-    sr.iy = rq::safe_inv(d.y);
-    sr.iz = rq::safe_inv(d.z);
-    sr.ox = o.x * sr.ix;
-    sr.oy = o.y * sr.iy;
-    sr.oz = o.z * sr.iz;
-    rq::WtRay w;
-    if (!MT) w = rq::wt_setup(d);
-
-    uint32_t hit_idx = 0xffffffffu;
-    float hu = 0.0f, hv = 0.0f;
-    uint32_t boxes = 0, ntris = 0;
-    stk[0] = 0;
-    int sp = 1;
-    while (sp > 0) {
-        const int32_t e = stk[(--sp) * kT];
-        if (e >= 0) {
-            const float4* np = reinterpret_cast<const float4*>(nodes + e);
-            const float4 mnx = rq::ldg4(np + 0), mxx = rq::ldg4(np + 1);
-            const float4 mny = rq::ldg4(np + 2), mxy = rq::ldg4(np + 3);
-            const float4 mnz = rq::ldg4(np + 4), mxz = rq::ldg4(np + 5);
-            const int4 cix = rq::ldg4i(reinterpret_cast<const int4*>(np + 6));
-            const int4 cnt = rq::ldg4i(reinterpret_cast<const int4*>(np + 7));
-            if (STATS) boxes += 4;
-            const float amnx[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, amxx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
-            const float amny[4] = {mny.x, mny.y, mny.z, mny.w}, amxy[4] = {mxy.x, mxy.y, mxy.z, mxy.w};
-            const float amnz[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, amxz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
-            const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
-            int32_t he[4];
-            float ht[4];
-            int nh = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (acc[k] == 0) continue;
-                float tn;
-                if (rq::slab(sr, tmin, best, amnx[k], amxx[k], amny[k], amxy[k], amnz[k], amxz[k], tn)) {
-                    int32_t ent = acc[k] < 0 ? aci[k]
-                                             : int32_t(kLeafBit | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
-                    int pos = nh;
-                    if (!ANY) {
-                        while (pos > 0 && ht[pos - 1] > tn) {
-                            he[pos] = he[pos - 1];
-                            ht[pos] = ht[pos - 1];
-                            --pos;
-                        }
-                    }
-                    he[pos] = ent;
-                    ht[pos] = tn;
-                    ++nh;
-                }
-            }
-            if (sp + nh > STACK) {
-                rq::set_err(err, RQ_DERR_STACK);
-                nh = STACK - sp;
-            }
-            for (int j = nh - 1; j >= 0; --j) stk[(sp++) * kT] = he[j];
-        } else {
-            const uint32_t first = uint32_t(e) & 0x07ffffffu;
-            const uint32_t cntl = ((uint32_t(e) >> 27) & 15u) + 1u;
-            bool done = false;
-            for (uint32_t p = first; p < first + cntl; ++p) {
-                const float4* tp = reinterpret_cast<const float4*>(tris + p);
-                float4 a = rq::ldg4(tp), b = rq::ldg4(tp + 1), c = rq::ldg4(tp + 2);
-                rq::F3 v0{a.x, a.y, a.z}, v1{b.x, b.y, b.z}, v2{c.x, c.y, c.z};
-                if (STATS) ++ntris;
-                float t, u, v;
-                bool ok = MT ? rq::mt_test(o, d, v0, v1, v2, 1e-7f, t, u, v) : rq::wt_test(w, o, v0, v1, v2, t, u, v);
-                if (ok && t >= tmin && t < best) {
-                    best = t;
-                    hit_idx = p;
-                    hu = u;
-                    hv = v;
-                    if (ANY) {
-                        done = true;
-                        break;
-                    }
-                }
-            }
-            if (ANY && done) break;
-        }
-    }
-    if (hit_idx != 0xffffffffu) {
-        uint32_t pid = perm ? __ldg(perm + hit_idx) : hit_idx;
-        reinterpret_cast<uint4*>(hits)[i] = make_uint4(1u, __float_as_uint(best), 0u, pid);
+    const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+    rq::TraceResult res;
+    rq::trace_ray<ANY, MT, STATS, STACK, kT>(nodes, tris, s_stack + threadIdx.x, rq::F3{r0.x, r0.y, r0.z},
+                                            rq::F3{r1.x, r1.y, r1.z}, r0.w, r1.w, res, err);
+    const bool hit = res.idx != rq::kNoHit;
+    if (hit) {
+        uint32_t pid = perm ? __ldg(perm + res.idx) : res.idx;
+        reinterpret_cast<uint4*>(hits)[i] = make_uint4(1u, __float_as_uint(res.t), 0u, pid);
     } else {
         store_miss(hits, i);
     }
-    if (BARY) reinterpret_cast<float2*>(bary)[i] = hit_idx != 0xffffffffu ? make_float2(hu, hv) : make_float2(0.f, 0.f);
-    if (STATS)
-        reinterpret_cast<uint4*>(stats)[i] = make_uint4(hit_idx != 0xffffffffu ? 1u : 0u, boxes, ntris, 0u);
+    if (BARY) reinterpret_cast<float2*>(bary)[i] = hit ? make_float2(res.u, res.v) : make_float2(0.f, 0.f);
+    if (STATS) reinterpret_cast<uint4*>(stats)[i] = make_uint4(hit ? 1u : 0u, res.boxes, res.tris, 0u);
 }
 
 template <bool ANY, bool MT, bool BARY>

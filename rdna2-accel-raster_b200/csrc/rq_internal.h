@@ -135,6 +135,11 @@ int rq_launch_trace_ref2(rq_ctx* ctx, const rq_bvh2_node* nodes, const rq_triang
 int rq_launch_trace_radv(rq_ctx* ctx, const void* img, uint64_t bytes, const rq_ray* rays, uint32_t n,
                          uint32_t flags, rq_hit* hits, float* bary, cudaStream_t st);
 
+// ---------------------------------------------------------------- k_frame
+int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_gbuffer_px* gbuf, cudaStream_t st);
+int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_shade_params& p,
+                        uint32_t* mask, float* ao, unsigned long long* counter, cudaStream_t st);
+
 // ---------------------------------------------------------------- k_radv
 int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st);
 

@@ -8,6 +8,7 @@
 // from SplitMix64 (seeded) through Box-Muller, all in double precision and
 // rounded to float once per coordinate.  Each quad (i, j) contributes the two
 // triangles (v00, v10, v01) and (v10, v11, v01), quads in row-major order.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -101,5 +102,79 @@ extern "C" int rq_scene_rays_down(uint32_t n, float x0, float x1, float y0, floa
         r.dir[2] = float(dz / len);
         r.tmax = tmax;
     }
+    return RQ_OK;
+}
+
+// Right-handed look-at view and a Vulkan-style perspective (depth 0..1, y
+// flipped), combined and inverted in double precision, stored column-major.
+extern "C" int rq_camera_look_at(const float eye[3], const float target[3], const float up[3], float fovy_deg,
+                                 uint32_t width, uint32_t height, rq_camera* out) {
+    if (!eye || !target || !up || !out || width == 0 || height == 0 || !(fovy_deg > 0.0f && fovy_deg < 180.0f))
+        return RQ_ERR_INVALID_ARG;
+    double e[3] = {eye[0], eye[1], eye[2]}, t[3] = {target[0], target[1], target[2]}, u0[3] = {up[0], up[1], up[2]};
+    auto norm = [](double* v) {
+        double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        v[0] /= l;
+        v[1] /= l;
+        v[2] /= l;
+    };
+    auto cross = [](const double* a, const double* b, double* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    double f[3] = {t[0] - e[0], t[1] - e[1], t[2] - e[2]};
+    norm(f);
+    double sx[3], ux[3];
+    cross(f, u0, sx);
+    norm(sx);
+    cross(sx, f, ux);
+    // view (column-major M[col][row])
+    double V[4][4] = {{sx[0], ux[0], -f[0], 0}, {sx[1], ux[1], -f[1], 0}, {sx[2], ux[2], -f[2], 0},
+                      {-(sx[0] * e[0] + sx[1] * e[1] + sx[2] * e[2]), -(ux[0] * e[0] + ux[1] * e[1] + ux[2] * e[2]),
+                       f[0] * e[0] + f[1] * e[1] + f[2] * e[2], 1}};
+    const double aspect = double(width) / double(height);
+    const double th = std::tan(double(fovy_deg) * 3.14159265358979323846 / 360.0);
+    const double zn = 0.1, zf = 100.0;
+    double Pm[4][4] = {{1.0 / (aspect * th), 0, 0, 0},
+                       {0, -1.0 / th, 0, 0},
+                       {0, 0, zf / (zn - zf), -1},
+                       {0, 0, -(zf * zn) / (zf - zn), 0}};
+    // VP = P * V  (column-major: VP[c][r] = sum_k P[k][r] * V[c][k])
+    double A[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            double acc = 0;
+            for (int k = 0; k < 4; ++k) acc += Pm[k][r] * V[c][k];
+            A[r][c] = acc;  // row-major copy for the inversion
+            A[r][4 + c] = r == c ? 1.0 : 0.0;
+        }
+    for (int col = 0; col < 4; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 4; ++r)
+            if (std::fabs(A[r][col]) > std::fabs(A[piv][col])) piv = r;
+        if (std::fabs(A[piv][col]) < 1e-300) return RQ_ERR_INVALID_ARG;
+        if (piv != col)
+            for (int k = 0; k < 8; ++k) std::swap(A[piv][k], A[col][k]);
+        const double d = A[col][col];
+        for (int k = 0; k < 8; ++k) A[col][k] /= d;
+        for (int r = 0; r < 4; ++r)
+            if (r != col) {
+                const double m = A[r][col];
+                for (int k = 0; k < 8; ++k) A[r][k] -= m * A[col][k];
+            }
+    }
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r) out->inv_view_proj[4 * c + r] = float(A[r][4 + c]);
+    out->cam_pos[0] = eye[0];
+    out->cam_pos[1] = eye[1];
+    out->cam_pos[2] = eye[2];
+    out->width = width;
+    out->height = height;
+    out->jitter = 0;
+    out->seed = 0;
+    out->tmin = 0.01f;
+    out->tmax = 10000.0f;
+    out->flags = 0;
     return RQ_OK;
 }

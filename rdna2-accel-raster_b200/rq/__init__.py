@@ -63,6 +63,27 @@ class RadvLayout(C.Structure):
                 ("level_offsets", C.c_uint32 * 16), ("level_counts", C.c_uint32 * 16)]
 
 
+class Camera(C.Structure):
+    _fields_ = [("inv_view_proj", C.c_float * 16), ("cam_pos", C.c_float * 3), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("jitter", C.c_uint32), ("seed", C.c_uint32), ("tmin", C.c_float),
+                ("tmax", C.c_float), ("flags", C.c_uint32)]
+
+
+class Light(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("radius", C.c_float)]
+
+
+MAX_LIGHTS = 32
+
+
+class ShadeParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("num_lights", C.c_uint32), ("ao_spp", C.c_uint32),
+                ("ao_tmax", C.c_float), ("ao_tmin", C.c_float), ("ao_bias", C.c_float), ("shadow_tmin", C.c_float),
+                ("shadow_bias", C.c_float), ("flags", C.c_uint32), ("lights", Light * MAX_LIGHTS)]
+
+
+GBUFFER_PX = np.dtype([("pos", "<f4", 3), ("vis", "<u4"), ("nrm", "<f4", 3), ("t", "<f4")])
+
 _P = C.c_void_p
 _U32 = C.c_uint32
 # (name, restype, argtypes) for every entry point in include/rq.h
@@ -91,6 +112,9 @@ SIGNATURES = [
     ("rq_trace_ref_bvh4", C.c_int, [_P, _P, _P, _P, _U32, _P, _P, _P]),
     ("rq_trace_ref_bvh2", C.c_int, [_P, _P, _P, _P, _U32, C.c_float, _P, _P]),
     ("rq_gen_rays_procedural", C.c_int, [_P, _P, _P, _U32, _U32, _P, _P]),
+    ("rq_camera_look_at", C.c_int, [_P, _P, _P, C.c_float, _U32, _U32, C.POINTER(Camera)]),
+    ("rq_render_gbuffer", C.c_int, [_P, _P, C.POINTER(Camera), _P, _P]),
+    ("rq_render_shadow_ao", C.c_int, [_P, _P, _P, C.POINTER(ShadeParams), _P, _P, _P, _P]),
     ("rq_radv_layout_get", C.c_int, [_U32, C.POINTER(RadvLayout)]),
     ("rq_radv_size", C.c_uint64, [_U32]),
     ("rq_build_radv", C.c_int, [_P, _P, _U32, _P, C.c_uint64, _P]),
@@ -122,6 +146,14 @@ def _ptr(t):
     if isinstance(t, np.ndarray):
         return t.ctypes.data_as(_P)
     return _P(t.data_ptr())
+
+
+def _count(t, item_bytes):
+    """Number of `item_bytes` records in a tensor/array, whatever its dtype."""
+    nbytes = t.nbytes if isinstance(t, np.ndarray) else t.numel() * t.element_size()
+    if nbytes % item_bytes:
+        raise ValueError(f"buffer of {nbytes} bytes is not a whole number of {item_bytes}-byte records")
+    return nbytes // item_bytes
 
 
 def _stream(stream):
@@ -179,8 +211,8 @@ class Bvh:
     def build(ctx, pos, idx=None, max_leaf=4, bvh4=True, stride_bytes=12, stream=None, into=None):
         """pos: float32 CUDA tensor of vertices; idx: int32/uint32 CUDA tensor
         [T, 3] or None (non-indexed: 3 consecutive vertices per triangle)."""
-        nverts = pos.numel() * 4 // stride_bytes
-        ntri = idx.numel() // 3 if idx is not None else nverts // 3
+        nverts = _count(pos, 4) * 4 // stride_bytes
+        ntri = _count(idx, 12) if idx is not None else nverts // 3
         h = _P(into.h.value) if into is not None else _P()
         rc = lib().rq_build(ctx.h, _ptr(pos), stride_bytes, nverts, _ptr(idx), ntri, max_leaf,
                             RQ_BUILD_BVH4 if bvh4 else 0, C.byref(h), _stream(stream))
@@ -193,16 +225,16 @@ class Bvh:
     @staticmethod
     def import2(ctx, nodes2, tris, perm=None, stream=None):
         h = _P()
-        rc = lib().rq_bvh_import2(ctx.h, _ptr(nodes2), nodes2.numel() // 8, _ptr(tris), _ptr(perm),
-                                  tris.numel() // 12, C.byref(h), _stream(stream))
+        rc = lib().rq_bvh_import2(ctx.h, _ptr(nodes2), _count(nodes2, 32), _ptr(tris), _ptr(perm),
+                                  _count(tris, 48), C.byref(h), _stream(stream))
         ctx.check(rc, "rq_bvh_import2")
         return Bvh(ctx, h)
 
     @staticmethod
     def import4(ctx, nodes4, tris, perm=None, stream=None):
         h = _P()
-        rc = lib().rq_bvh_import4(ctx.h, _ptr(nodes4), nodes4.numel() // 32, _ptr(tris), _ptr(perm),
-                                  tris.numel() // 12, C.byref(h), _stream(stream))
+        rc = lib().rq_bvh_import4(ctx.h, _ptr(nodes4), _count(nodes4, 128), _ptr(tris), _ptr(perm),
+                                  _count(tris, 48), C.byref(h), _stream(stream))
         ctx.check(rc, "rq_bvh_import4")
         return Bvh(ctx, h)
 
@@ -257,7 +289,7 @@ def _empty_i32(n, cols, device):
 def trace(ctx, bvh, rays, flags=0, bary=False, stats=False, hits=None, stream=None):
     """rays: float32 CUDA tensor [n, 8].  Returns (hits int32 [n,4], bary, stats)."""
     import torch
-    n = rays.shape[0]
+    n = _count(rays, 32)
     dev = rays.device
     hits = hits if hits is not None else _empty_i32(n, 4, dev)
     b = torch.empty((n, 2), dtype=torch.float32, device=dev) if bary else None
@@ -268,7 +300,7 @@ def trace(ctx, bvh, rays, flags=0, bary=False, stats=False, hits=None, stream=No
 
 
 def trace_ref_bvh4(ctx, nodes4, tris, rays, stream=None):
-    n = rays.shape[0]
+    n = _count(rays, 32)
     st = _empty_i32(n, 4, rays.device)
     hits = _empty_i32(n, 4, rays.device)
     rc = lib().rq_trace_ref_bvh4(ctx.h, _ptr(nodes4), _ptr(tris), _ptr(rays), n, _ptr(st), _ptr(hits),
@@ -279,7 +311,7 @@ def trace_ref_bvh4(ctx, nodes4, tris, rays, stream=None):
 
 def trace_ref_bvh2(ctx, nodes2, tris, rays, t_eps=0.001, stream=None):
     import torch
-    n = rays.shape[0]
+    n = _count(rays, 32)
     flags = torch.empty(n, dtype=torch.int32, device=rays.device)
     rc = lib().rq_trace_ref_bvh2(ctx.h, _ptr(nodes2), _ptr(tris), _ptr(rays), n, t_eps, _ptr(flags),
                                  _stream(stream))
@@ -314,18 +346,18 @@ def radv_size(n):
 
 def build_radv(ctx, tri9, image=None, stream=None):
     import torch
-    n = tri9.numel() // 9
+    n = _count(tri9, 36)
     size = radv_size(n)
     if image is None:
         image = torch.empty(size, dtype=torch.uint8, device=tri9.device)
-    rc = lib().rq_build_radv(ctx.h, _ptr(tri9), n, _ptr(image), image.numel(), _stream(stream))
+    rc = lib().rq_build_radv(ctx.h, _ptr(tri9), n, _ptr(image), _count(image, 1), _stream(stream))
     ctx.check(rc, "rq_build_radv")
     return image
 
 
 def trace_radv(ctx, image, rays, flags=0, bary=False, stream=None):
     import torch
-    n = rays.shape[0]
+    n = _count(rays, 32)
     hits = _empty_i32(n, 4, rays.device)
     b = torch.empty((n, 2), dtype=torch.float32, device=rays.device) if bary else None
     rc = lib().rq_trace_radv(ctx.h, _ptr(image), image.numel(), _ptr(rays), n, flags, _ptr(hits), _ptr(b),
@@ -357,6 +389,50 @@ def deform_wave(ctx, base, out, t, amp=0.05, freq=1.0, stream=None):
     rc = lib().rq_deform_wave(ctx.h, _ptr(base), _ptr(out), base.numel() // 3, t, amp, freq, _stream(stream))
     ctx.check(rc, "rq_deform_wave")
     return out
+
+
+def camera_look_at(eye, target, up, fovy_deg, width, height, jitter=False, seed=0, flags=0):
+    cam = Camera()
+    f3 = C.c_float * 3
+    rc = lib().rq_camera_look_at(C.cast(f3(*eye), _P), C.cast(f3(*target), _P), C.cast(f3(*up), _P), fovy_deg,
+                                 width, height, C.byref(cam))
+    if rc != RQ_OK:
+        raise RqError(rc, "rq_camera_look_at")
+    cam.jitter = 1 if jitter else 0
+    cam.seed = seed
+    cam.flags = flags
+    return cam
+
+
+def shade_params(width, height, lights, ao_spp=1, ao_tmax=0.5, flags=0):
+    """lights: sequence of (x, y, z, radius)."""
+    p = ShadeParams()
+    p.width, p.height, p.num_lights, p.ao_spp = width, height, len(lights), ao_spp
+    p.ao_tmax, p.ao_tmin, p.ao_bias = ao_tmax, 0.01, 0.03
+    p.shadow_tmin, p.shadow_bias, p.flags = 0.01, 0.04, flags
+    for k, (x, y, z, r) in enumerate(lights):
+        p.lights[k].pos[0], p.lights[k].pos[1], p.lights[k].pos[2], p.lights[k].radius = x, y, z, r
+    return p
+
+
+def render_gbuffer(ctx, bvh, cam, gbuf=None, stream=None):
+    """Primary rays -> G-buffer as int32 [H*W, 8] CUDA tensor (rq_gbuffer_px)."""
+    import torch
+    if gbuf is None:
+        gbuf = torch.empty((cam.width * cam.height, 8), dtype=torch.int32, device="cuda")
+    ctx.check(lib().rq_render_gbuffer(ctx.h, bvh.h, C.byref(cam), _ptr(gbuf), _stream(stream)), "rq_render_gbuffer")
+    return gbuf
+
+
+def render_shadow_ao(ctx, bvh, gbuf, params, mask=None, ao=None, counter=None, stream=None):
+    import torch
+    n = params.width * params.height
+    mask = mask if mask is not None else torch.empty(n, dtype=torch.int32, device="cuda")
+    ao = ao if ao is not None else torch.empty(n, dtype=torch.float32, device="cuda")
+    rc = lib().rq_render_shadow_ao(ctx.h, bvh.h, _ptr(gbuf), C.byref(params), _ptr(mask), _ptr(ao), _ptr(counter),
+                                   _stream(stream))
+    ctx.check(rc, "rq_render_shadow_ao")
+    return mask, ao
 
 
 def hits_numpy(hits_tensor):

@@ -1,0 +1,85 @@
+"""GPU parity of the fused ray-generation kernels (G-buffer primary rays,
+shadow rays, AO rays) against the oracle's statement of the same frame:
+bit-exact G-buffer, light masks, AO values and ray counts, on a full small
+frame and on a pixel sample of the full 1080p shadows + AO workload."""
+import numpy as np
+import pytest
+import torch
+
+import pyoracle as O
+import rq
+from rq import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def build(ctx, pos, idx):
+    return rq.Bvh.build(ctx, torch.from_numpy(pos).cuda(), torch.from_numpy(idx.view(np.int32)).cuda())
+
+
+def frame(ctx, b, cam, params):
+    gb = rq.render_gbuffer(ctx, b, cam)
+    counter = torch.zeros(4, dtype=torch.int64, device="cuda")
+    mask, ao = rq.render_shadow_ao(ctx, b, gb, params, counter=counter)
+    ctx.sync_check()
+    return gb, mask, ao, int(counter[0])
+
+
+@pytest.mark.parametrize("flags", [0, rq.RQ_TRI_MT])
+def test_small_frame_bit_exact(ctx, flags):
+    pos, idx = rq.scene_grid(128, 128, seed=1)
+    b = build(ctx, pos, idx)
+    n2, tr, n4, perm = b.download()
+    w, h = 320, 180
+    cam = W.shadow_camera(w, h, flags=flags)
+    params = rq.shade_params(w, h, W.shadow_lights(16), ao_spp=2, ao_tmax=0.5, flags=flags)
+    gb, mask, ao, rays = frame(ctx, b, cam, params)
+    og = O.render_gbuffer(n4, tr, perm, cam)
+    gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    assert gbn.tobytes() == og.tobytes()
+    assert (gbn["vis"] > 0).all(), "the camera sees only the mesh"
+    om, oa, orays = O.render_shadow_ao(n4, tr, og, params)
+    assert np.array_equal(mask.cpu().numpy().astype(np.uint32), om)
+    assert ao.cpu().numpy().tobytes() == oa.tobytes()
+    assert rays == orays
+    # some pixels are shadowed or occluded, most are lit
+    lit = np.unpackbits(om.view(np.uint8)).mean() * 32 / 16
+    assert 0.5 < lit < 1.0 and 0.0 < oa.mean() < 1.0
+    b.destroy()
+
+
+def test_jittered_primary_rays_bit_exact(ctx):
+    pos, idx = rq.scene_grid(256, 256, seed=3)
+    b = build(ctx, pos, idx)
+    n2, tr, n4, perm = b.download()
+    cam = W.visibility_camera(400, 240, jitter=True, seed=3)
+    gb = rq.render_gbuffer(ctx, b, cam)
+    og = O.render_gbuffer(n4, tr, perm, cam)
+    assert gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1).tobytes() == og.tobytes()
+    cam0 = W.visibility_camera(400, 240, jitter=False)
+    gb0 = rq.render_gbuffer(ctx, b, cam0).cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    assert not np.array_equal(gb0["vis"], og["vis"])  # jitter moves the samples
+    b.destroy()
+
+
+def test_full_1080p_workload_sampled(ctx):
+    # the benchmarked frame: 2,499,848 triangles, 1920x1080, 16 lights, AO
+    pos, idx = W.shadow_mesh()
+    assert len(idx) == 2499848
+    b = build(ctx, pos, idx)
+    cam = W.shadow_camera()
+    params = W.shadow_params()
+    gb, mask, ao, rays = frame(ctx, b, cam, params)
+    n2, tr, n4, perm = b.download()
+    rng = np.random.default_rng(0)
+    pixels = rng.choice(1920 * 1080, 4000, replace=False).astype(np.uint32)
+    og = O.render_gbuffer(n4, tr, perm, cam, pixels)
+    gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    assert gbn[pixels].tobytes() == og.tobytes()
+    assert (gbn["vis"] > 0).all()
+    om, oa, _ = O.render_shadow_ao(n4, tr, gbn, params, pixels)
+    assert np.array_equal(mask.cpu().numpy().astype(np.uint32)[pixels], om)
+    assert ao.cpu().numpy()[pixels].tobytes() == oa.tobytes()
+    # ray count: every pixel casts its primary ray, up to 16 shadow rays and one AO ray
+    assert 0.9 * 16 * 1920 * 1080 < rays <= 17 * 1920 * 1080
+    b.destroy()
