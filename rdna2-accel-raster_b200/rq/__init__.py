@@ -34,6 +34,7 @@ RQ_TRACE_CLOSEST = 0
 RQ_TRACE_ANY = 1
 RQ_TRI_WATERTIGHT = 0
 RQ_TRI_MT = 2
+RQ_SHADE_COUNT_TESTS = 16
 
 # numpy mirrors of the byte layouts
 BVH2_NODE = np.dtype([("aabb_min", "<f4", 3), ("left_child", "<i4"), ("aabb_max", "<f4", 3), ("right_child", "<i4")])

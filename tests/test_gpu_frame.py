@@ -80,6 +80,8 @@ def test_full_1080p_workload_sampled(ctx):
     om, oa, _ = O.render_shadow_ao(n4, tr, gbn, params, pixels)
     assert np.array_equal(mask.cpu().numpy().astype(np.uint32)[pixels], om)
     assert ao.cpu().numpy()[pixels].tobytes() == oa.tobytes()
-    # ray count: every pixel casts its primary ray, up to 16 shadow rays and one AO ray
-    assert 0.9 * 16 * 1920 * 1080 < rays <= 17 * 1920 * 1080
+    # ray count: up to 16 shadow rays (lights behind the local surface are
+    # skipped; the sigma-0.01 jitter on a 0.0018-spaced grid makes the surface
+    # rough) and one AO ray per pixel
+    assert 0.6 * 16 * 1920 * 1080 < rays <= 17 * 1920 * 1080
     b.destroy()
