@@ -1,0 +1,146 @@
+// rq_software_bvh.hpp — C++ host wrapper over librq's C ABI that keeps the
+// call shape of the reference's CPU builder:
+//
+//   SoftwareBVH  bvh  = SoftwareBVH::build(mesh, maxPrimsPerLeaf);   // common/software_bvh.hpp:35
+//   SoftwareBVH4 bvh4 = SoftwareBVH4::fromBVH2(bvh);                // common/software_bvh.hpp:193
+//
+// becomes
+//
+//   rq::Engine eng;                                   // one context per device / thread
+//   rq::SoftwareBVH  bvh  = rq::SoftwareBVH::build(eng, mesh, maxPrimsPerLeaf);
+//   rq::SoftwareBVH4 bvh4 = rq::SoftwareBVH4::fromBVH2(eng, bvh);
+//
+// The mesh type is any type with `vertices[i].pos[3]` floats and a
+// `std::vector<uint32_t> indices` (the reference's SceneMesh qualifies).
+// nodes / triangles come back in the byte layouts of GpuBvhNode, GpuTriangle
+// and GpuBvh4Node (rq_layouts.h), so they upload unchanged to the reference's
+// traversal shaders.  Unlike the reference, `perm` keeps the leaf-order ->
+// original triangle id map.  Errors throw rq::Error (C++ side only; the C ABI
+// itself never throws).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "rq.h"
+
+namespace rq {
+
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string& what) : std::runtime_error(what), status(s) {}
+};
+
+inline void check(int status, rq_ctx* ctx, const char* what) {
+    if (status != RQ_OK)
+        throw Error(status, std::string(what) + ": " + rq_status_string(status) + " " +
+                                (ctx ? rq_ctx_last_error(ctx) : ""));
+}
+
+// Owns an rq_ctx on one device.
+class Engine {
+   public:
+    explicit Engine(int device = 0) { check(rq_ctx_create(device, &ctx_), nullptr, "rq_ctx_create"); }
+    ~Engine() {
+        if (ctx_) rq_ctx_destroy(ctx_);
+    }
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+    rq_ctx* get() const { return ctx_; }
+
+   private:
+    rq_ctx* ctx_ = nullptr;
+};
+
+struct SoftwareBVH {
+    std::vector<rq_bvh2_node> nodes;
+    std::vector<rq_triangle> triangles;
+    std::vector<uint32_t> perm;  // leaf order -> original triangle id
+
+    template <class Mesh>
+    static SoftwareBVH build(Engine& eng, const Mesh& mesh, uint32_t maxPrimsPerLeaf = 4) {
+        const size_t nv = mesh.vertices.size();
+        const uint32_t nt = uint32_t(mesh.indices.size() / 3);
+        std::vector<float> pos(3 * nv);
+        for (size_t v = 0; v < nv; ++v)
+            for (int c = 0; c < 3; ++c) pos[3 * v + c] = mesh.vertices[v].pos[c];
+        float* d_pos = nullptr;
+        uint32_t* d_idx = nullptr;
+        auto fail = [&](cudaError_t e) {
+            if (e != cudaSuccess) {
+                cudaFree(d_pos);
+                cudaFree(d_idx);
+                throw Error(RQ_ERR_CUDA, cudaGetErrorString(e));
+            }
+        };
+        fail(cudaMalloc(&d_pos, pos.size() * sizeof(float)));
+        fail(cudaMalloc(&d_idx, mesh.indices.size() * sizeof(uint32_t)));
+        fail(cudaMemcpy(d_pos, pos.data(), pos.size() * sizeof(float), cudaMemcpyHostToDevice));
+        fail(cudaMemcpy(d_idx, mesh.indices.data(), mesh.indices.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        rq_bvh* h = nullptr;
+        int st = rq_build(eng.get(), d_pos, 12, uint32_t(nv), d_idx, nt, maxPrimsPerLeaf, 0, &h, nullptr);
+        cudaFree(d_pos);
+        cudaFree(d_idx);
+        check(st, eng.get(), "rq_build");
+        SoftwareBVH out;
+        rq_bvh_info info;
+        st = rq_bvh_info_get(h, &info);
+        if (st == RQ_OK) {
+            out.nodes.resize(info.num_nodes2);
+            out.triangles.resize(nt);
+            out.perm.resize(nt);
+            st = rq_bvh_download(h, 1, out.nodes.data(), info.num_nodes2, out.triangles.data(), nt, nullptr, 0,
+                                 out.perm.data(), nt);
+        }
+        rq_bvh_destroy(h);
+        check(st, eng.get(), "rq_bvh_download");
+        return out;
+    }
+};
+
+struct SoftwareBVH4 {
+    std::vector<rq_bvh4_node> nodes;
+    std::vector<rq_triangle> triangles;
+
+    static SoftwareBVH4 fromBVH2(Engine& eng, const SoftwareBVH& b2) {
+        SoftwareBVH4 out;
+        out.triangles = b2.triangles;
+        if (b2.nodes.empty()) return out;
+        rq_bvh2_node* d_n = nullptr;
+        rq_triangle* d_t = nullptr;
+        cudaError_t e = cudaMalloc(&d_n, b2.nodes.size() * sizeof(rq_bvh2_node));
+        if (e == cudaSuccess) e = cudaMalloc(&d_t, b2.triangles.size() * sizeof(rq_triangle));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_n, b2.nodes.data(), b2.nodes.size() * sizeof(rq_bvh2_node), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_t, b2.triangles.data(), b2.triangles.size() * sizeof(rq_triangle),
+                           cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(d_n);
+            cudaFree(d_t);
+            throw Error(RQ_ERR_CUDA, cudaGetErrorString(e));
+        }
+        rq_bvh* h = nullptr;
+        int st = rq_bvh_import2(eng.get(), d_n, uint32_t(b2.nodes.size()), d_t, nullptr,
+                                uint32_t(b2.triangles.size()), &h, nullptr);
+        cudaFree(d_n);
+        cudaFree(d_t);
+        check(st, eng.get(), "rq_bvh_import2");
+        st = rq_collapse4(eng.get(), h, nullptr);
+        rq_bvh_info info;
+        if (st == RQ_OK) st = rq_bvh_info_get(h, &info);
+        if (st == RQ_OK) {
+            out.nodes.resize(info.num_nodes4);
+            st = rq_bvh_download(h, 1, nullptr, 0, nullptr, 0, out.nodes.data(), info.num_nodes4, nullptr, 0);
+        }
+        rq_bvh_destroy(h);
+        check(st, eng.get(), "rq_collapse4");
+        return out;
+    }
+};
+
+}  // namespace rq
