@@ -292,6 +292,20 @@ uint64_t rq_radv_size(uint32_t num_triangles);
 int rq_build_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* as_image,
                   uint64_t as_bytes, rq_stream stream);
 
+/* Allocation-free variant of rq_build_radv, with no counterpart in the
+ * reference.  For callers that own all of their device memory and cannot let
+ * a library call cudaMalloc/cudaFree (which synchronise the device and can
+ * fail under a fixed budget): it takes no context, allocates nothing, and
+ * keeps its scratch in a static device array inside librq.so, so it accepts
+ * at most RQ_RADV_NOALLOC_MAX_TRIANGLES triangles (RQ_ERR_UNSUPPORTED
+ * beyond).  Runs on the current device.  Its first call on a device looks up
+ * the array's device address; make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * race, so order them on one stream.  Output bytes equal rq_build_radv's. */
+#define RQ_RADV_NOALLOC_MAX_TRIANGLES (1u << 24)
+int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, void* as_image, uint64_t as_bytes,
+                          rq_stream stream);
+
 /* Trace rays through a RADV image (the rayQueryEXT role of
  * shaders/verify_rayquery.comp:41-59): primitive IDs are the nodes'
  * triangle_id; `bary` as in rq_trace. */

@@ -14,6 +14,8 @@
 // then reduces its subtree in shared memory for up to five levels.  The last
 // block to finish (atomic ticket) builds the remaining top levels and the
 // header from the per-block subtree boxes.
+#include <mutex>
+
 #include "rq_device.cuh"
 #include "rq_internal.h"
 
@@ -290,6 +292,74 @@ __global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Allocation-free RADV build.  Some callers own every byte of device memory
+// they use — they size their buffers up front from their own pool or budget
+// and cannot let a library call cudaMalloc / cudaFree, which synchronise the
+// whole device and can fail mid-frame.  This variant takes only the vertex
+// buffer and the image buffer from the caller; its scratch (the finishing
+// ticket and two boxes per block for the top levels) lives in the static
+// device array below, sized for at most RQ_RADV_NOALLOC_MAX_TRIANGLES
+// triangles.  Every GPU that loads librq.so holds the array until the
+// process exits.
+static __device__ __align__(256) unsigned char rq_radv_noalloc_scratch
+    [256 + 4 * sizeof(float4) * ((RQ_RADV_NOALLOC_MAX_TRIANGLES / 4 + kLeafBoxes - 1) / kLeafBoxes)];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[256] = {};  // device address of the array, per device ordinal
+}  // namespace
+
+extern "C" int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, void* as_image, uint64_t as_bytes,
+                                     rq_stream stream) {
+    if (!tri9 || !as_image || num_triangles == 0) return RQ_ERR_INVALID_ARG;
+    if (num_triangles > RQ_RADV_NOALLOC_MAX_TRIANGLES) return RQ_ERR_UNSUPPORTED;
+    if (reinterpret_cast<uintptr_t>(as_image) & 15u) return RQ_ERR_INVALID_ARG;
+    rq_radv_layout L;
+    if (rq_radv_layout_get(num_triangles, &L) != RQ_OK) return RQ_ERR_UNSUPPORTED;
+    if (as_bytes < L.total_as_size) return RQ_ERR_SIZE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return RQ_ERR_NO_DEVICE;
+    void* base = nullptr;
+    {
+        // set-up once per device, with that device current: the host-side
+        // name of the array is not a device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, rq_radv_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return RQ_ERR_CUDA;
+            }
+            g_noalloc_ptr[dev] = p;
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RadvArgs a;
+    a.tri9 = tri9;
+    a.n = num_triangles;
+    a.img = static_cast<uint8_t*>(as_image);
+    a.levels = L.num_levels;
+    a.total_boxes = L.total_boxes;
+    for (int i = 0; i < 16; ++i) {
+        a.counts[i] = L.level_counts[i];
+        a.offs[i] = L.level_offsets[i];
+    }
+    a.ticket = static_cast<uint32_t*>(base);
+    a.top = reinterpret_cast<float4*>(static_cast<char*>(base) + 256);
+    a.size = L.total_as_size;
+    // the array keeps the previous call's contents: the ticket must start at 0
+    if (cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st) != cudaSuccess) {
+        cudaGetLastError();
+        return RQ_ERR_CUDA;
+    }
+    const uint32_t leaf_cnt = L.level_counts[L.num_levels - 1];
+    k_radv<<<(leaf_cnt + kLeafBoxes - 1) / kLeafBoxes, kT, 0, st>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return RQ_ERR_CUDA;
+    return RQ_OK;
+}
 
 int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st) {
     const uint32_t leaf_cnt = L.level_counts[L.num_levels - 1];

@@ -120,7 +120,10 @@ SIGNATURES = [
     ("rq_radv_size", C.c_uint64, [_U32]),
     ("rq_build_radv", C.c_int, [_P, _P, _U32, _P, C.c_uint64, _P]),
     ("rq_trace_radv", C.c_int, [_P, _P, C.c_uint64, _P, _U32, _U32, _P, _P, _P]),
+    ("rq_build_radv_noalloc", C.c_int, [_P, _U32, _P, C.c_uint64, _P]),
 ]
+
+RADV_NOALLOC_MAX_TRIANGLES = 1 << 24
 
 _lib = None
 
