@@ -143,7 +143,8 @@ int rq_ctx_create(int device, rq_ctx** out) {
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
     cudaSetDevice(device);
-    if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess || cudaMallocHost(&ctx->h_err, 256) != cudaSuccess) {
+    if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess || cudaMallocHost(&ctx->h_err, 256) != cudaSuccess ||
+        cudaMalloc(&ctx->d_ctr, 256) != cudaSuccess) {
         cudaGetLastError();
         rq_ctx_destroy(ctx);
         return RQ_ERR_OOM;
@@ -159,6 +160,7 @@ int rq_ctx_destroy(rq_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->d_ctr) cudaFree(ctx->d_ctr);
     if (ctx->h_err) cudaFreeHost(ctx->h_err);
     delete ctx;
     return RQ_OK;
@@ -497,7 +499,8 @@ int rq_render_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
                         uint32_t* light_mask, float* ao, unsigned long long* counters, rq_stream stream) {
     if (!ctx || !bvh || !gbuf || !params || !light_mask || !ao)
         return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
-    if (params->num_lights > RQ_MAX_LIGHTS || params->width == 0 || params->height == 0 || (params->flags & ~(RQ_TRI_MT | RQ_SHADE_COUNT_TESTS)))
+    if (params->num_lights > RQ_MAX_LIGHTS || params->ao_spp > 32 || params->width == 0 || params->height == 0 ||
+        (params->flags & ~(RQ_TRI_MT | RQ_SHADE_COUNT_TESTS)))
         return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad shading parameters");
     if (!aligned(gbuf, 16) || (counters && !aligned(counters, 8)))
         return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "misaligned buffer");

@@ -1,22 +1,29 @@
-// k_frame.cu — traversal kernels that generate their own rays.
+// k_frame.cu — traversal kernels that generate their own rays, on the
+// persistent engine of trace_engine.cuh.
 //
 //  k_gbuffer    one primary closest-hit ray per pixel
 //               (benchmarks/exp1_visbuf/shaders/visbuf_raycast.comp:15-51,
-//               optional per-pixel jitter), writing position, visibility
-//               value, camera-facing face normal and t;
-//  k_shadow_ao  per G-buffer pixel, the any-hit shadow rays of
-//               shaders/tiled_lighting_ra.comp:223-253 and the cosine
-//               hemisphere AO rays of shaders/rq_ao.comp:18-94, traced in the
-//               same thread one after another — no ray or hit buffers touch
-//               HBM.  Blocks are 16x8 pixel tiles, so a warp's rays toward one
-//               light start side by side and walk the same nodes.
+//               optional per-pixel jitter) -> position, visibility value,
+//               camera-facing face normal, t.
+//  k_shadow_ao  the any-hit shadow rays of shaders/tiled_lighting_ra.comp:
+//               223-253 and the cosine-hemisphere AO rays of
+//               shaders/rq_ao.comp:18-94, generated from the G-buffer inside
+//               the kernel.  A ray id names (8x4 pixel tile, ray kind k, pixel
+//               in tile): the 32 ids of one chunk are the 32 pixels of a tile
+//               casting toward the same light (or the same AO sample), the
+//               most coherent batch a warp can trace.  A ray that reaches its
+//               light / escapes sets bit k of its pixel's 64-bit result word
+//               (lights in bits 0..31, AO samples in bits 32..63).
+//  k_shade_finish  result words -> light mask and AO fraction per pixel.
+// No ray or hit buffer touches HBM.
 #include "rq_device.cuh"
 #include "rq_internal.h"
-#include "trace_core.cuh"
+#include "trace_engine.cuh"
 
 namespace {
 
-constexpr int kTX = 16, kTY = 8, kT = kTX * kTY;
+constexpr int kT = 128;
+constexpr uint32_t kTileW = 8, kTileH = 4;
 
 struct CamArgs {
     float m[16];
@@ -25,6 +32,15 @@ struct CamArgs {
     float tmin, tmax;
 };
 
+__device__ __forceinline__ bool tile_pixel(uint32_t tile, uint32_t j, uint32_t tiles_x, uint32_t w, uint32_t h,
+                                           uint32_t& pixel) {
+    const uint32_t px = (tile % tiles_x) * kTileW + (j & 7u);
+    const uint32_t py = (tile / tiles_x) * kTileH + (j >> 3);
+    if (px >= w || py >= h) return false;
+    pixel = py * w + px;
+    return true;
+}
+
 // Per-pixel jitter draws in [0, 1].
 __device__ __forceinline__ void jitter2(uint32_t seed, uint32_t pixel, float& jx, float& jy) {
     uint32_t h = rq::pcg_hash(seed ^ rq::pcg_hash(pixel));
@@ -32,46 +48,57 @@ __device__ __forceinline__ void jitter2(uint32_t seed, uint32_t pixel, float& jx
     jy = __uint2float_rn(rq::pcg_hash(h)) * RQ_INV_2POW32;
 }
 
-template <bool MT, int STACK>
-__global__ void __launch_bounds__(kT) k_gbuffer(const rq_bvh4_node* __restrict__ nodes,
-                                                const rq_triangle* __restrict__ tris,
-                                                const uint32_t* __restrict__ perm, CamArgs c,
-                                                rq_gbuffer_px* __restrict__ gbuf, uint32_t* err) {
-    extern __shared__ int32_t s_stack[];
-    const uint32_t px = blockIdx.x * kTX + threadIdx.x % kTX;
-    const uint32_t py = blockIdx.y * kTY + threadIdx.x / kTX;
-    if (px >= c.w || py >= c.h) return;
-    const uint32_t pixel = py * c.w + px;
-    float jx = 0.5f, jy = 0.5f;
-    if (c.jitter) jitter2(c.seed, pixel, jx, jy);
-    const float u = (__uint2float_rn(px) + jx) / __uint2float_rn(c.w);
-    const float v = (__uint2float_rn(py) + jy) / __uint2float_rn(c.h);
-    const float cl[4] = {u * 2.0f - 1.0f, v * 2.0f - 1.0f, 1.0f, 1.0f};
-    float wt[4];
+struct GbufSrc {
+    struct Meta {
+        uint32_t pixel;
+    };
+    uint32_t total;
+    uint32_t tiles_x;
+    CamArgs c;
+    const rq_triangle* tris;
+    const uint32_t* perm;
+    rq_gbuffer_px* gbuf;
+
+    __device__ bool make(uint32_t id, rq::Ray& r, Meta& m) const {
+        uint32_t pixel;
+        if (!tile_pixel(id >> 5, id & 31u, tiles_x, c.w, c.h, pixel)) return false;
+        m.pixel = pixel;
+        const uint32_t px = pixel % c.w, py = pixel / c.w;
+        float jx = 0.5f, jy = 0.5f;
+        if (c.jitter) jitter2(c.seed, pixel, jx, jy);
+        const float u = (__uint2float_rn(px) + jx) / __uint2float_rn(c.w);
+        const float v = (__uint2float_rn(py) + jy) / __uint2float_rn(c.h);
+        const float cl[4] = {u * 2.0f - 1.0f, v * 2.0f - 1.0f, 1.0f, 1.0f};
+        float wt[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-        wt[r] = ((c.m[r] * cl[0] + c.m[4 + r] * cl[1]) + c.m[8 + r] * cl[2]) + c.m[12 + r] * cl[3];
-    const rq::F3 o{c.cx, c.cy, c.cz};
-    const rq::F3 target{wt[0] / wt[3], wt[1] / wt[3], wt[2] / wt[3]};
-    const rq::F3 d = rq::f3norm(rq::f3sub(target, o));
-    rq::TraceResult res;
-    rq::trace_ray<false, MT, false, STACK, kT>(nodes, tris, s_stack + threadIdx.x, o, d, c.tmin, c.tmax, res, err);
-    float4* out = reinterpret_cast<float4*>(gbuf + pixel);
-    if (res.idx == rq::kNoHit) {
-        out[0] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
-        out[1] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-        return;
+        for (int k = 0; k < 4; ++k)
+            wt[k] = ((c.m[k] * cl[0] + c.m[4 + k] * cl[1]) + c.m[8 + k] * cl[2]) + c.m[12 + k] * cl[3];
+        r.o = rq::F3{c.cx, c.cy, c.cz};
+        const rq::F3 target{wt[0] / wt[3], wt[1] / wt[3], wt[2] / wt[3]};
+        r.d = rq::f3norm(rq::f3sub(target, r.o));
+        r.tmin = c.tmin;
+        r.tmax = c.tmax;
+        return true;
     }
-    const rq::F3 p{o.x + res.t * d.x, o.y + res.t * d.y, o.z + res.t * d.z};
-    const float4* tp = reinterpret_cast<const float4*>(tris + res.idx);
-    const float4 a = rq::ldg4(tp), b = rq::ldg4(tp + 1), cc = rq::ldg4(tp + 2);
-    const rq::F3 e1{b.x - a.x, b.y - a.y, b.z - a.z}, e2{cc.x - a.x, cc.y - a.y, cc.z - a.z};
-    rq::F3 n = rq::f3norm(rq::f3cross(e1, e2));
-    if (rq::f3dot(n, rq::f3sub(o, p)) < 0.0f) n = {-n.x, -n.y, -n.z};
-    const uint32_t pid = perm ? __ldg(perm + res.idx) : res.idx;
-    out[0] = make_float4(p.x, p.y, p.z, __uint_as_float(pid + 1u));
-    out[1] = make_float4(n.x, n.y, n.z, res.t);
-}
+
+    __device__ void finish(uint32_t, const Meta& m, const rq::Ray& r, const rq::Hit& h) const {
+        float4* out = reinterpret_cast<float4*>(gbuf + m.pixel);
+        if (!h.hit) {
+            out[0] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
+            out[1] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+            return;
+        }
+        const rq::F3 p{r.o.x + h.t * r.d.x, r.o.y + h.t * r.d.y, r.o.z + h.t * r.d.z};
+        const float4* tp = reinterpret_cast<const float4*>(tris + h.idx);
+        const float4 a = rq::ldg4(tp), b = rq::ldg4(tp + 1), cc = rq::ldg4(tp + 2);
+        const rq::F3 e1{b.x - a.x, b.y - a.y, b.z - a.z}, e2{cc.x - a.x, cc.y - a.y, cc.z - a.z};
+        rq::F3 n = rq::f3norm(rq::f3cross(e1, e2));
+        if (rq::f3dot(n, rq::f3sub(r.o, p)) < 0.0f) n = {-n.x, -n.y, -n.z};
+        const uint32_t pid = perm ? __ldg(perm + h.idx) : h.idx;
+        out[0] = make_float4(p.x, p.y, p.z, __uint_as_float(pid + 1u));
+        out[1] = make_float4(n.x, n.y, n.z, h.t);
+    }
+};
 
 struct ShadeArgs {
     uint32_t w, h, nl, spp;
@@ -79,14 +106,16 @@ struct ShadeArgs {
     float lx[RQ_MAX_LIGHTS], ly[RQ_MAX_LIGHTS], lz[RQ_MAX_LIGHTS], lr[RQ_MAX_LIGHTS];
 };
 
-// rq_ao.comp:27-45: rand() advances the hash state; cosine-weighted
-// direction around N with the tangent frame of the shader.
 __device__ __forceinline__ float ao_rand(uint32_t& seed) {
     seed = rq::ao_hash(seed);
     return __uint2float_rn(seed) * RQ_INV_2POW32;
 }
 
-__device__ __forceinline__ rq::F3 hemisphere(rq::F3 N, uint32_t& seed) {
+// rq_ao.comp:32-45 for sample s of the pixel: the hash state advances two
+// draws per sample from y*W + x + 5544.
+__device__ __forceinline__ rq::F3 hemisphere(rq::F3 N, uint32_t pixel, uint32_t s) {
+    uint32_t seed = pixel + 5544u;
+    for (uint32_t i = 0; i < 2 * s; ++i) seed = rq::ao_hash(seed);
     const float u1 = ao_rand(seed);
     const float u2 = ao_rand(seed);
     const float r = sqrtf(u1);
@@ -101,75 +130,109 @@ __device__ __forceinline__ rq::F3 hemisphere(rq::F3 N, uint32_t& seed) {
                              (tg.z * x + bt.z * y) + N.z * z});
 }
 
+template <bool STATS>
+struct ShadeSrc {
+    struct Meta {
+        uint32_t pixel, bit;
+    };
+    uint32_t total;
+    uint32_t tiles_x;
+    uint32_t kinds;  // lights + AO samples
+    const ShadeArgs* s;
+    const rq_gbuffer_px* gbuf;
+    unsigned long long* words;
+    uint32_t rays = 0, boxes = 0, tris = 0;
+
+    __device__ bool make(uint32_t id, rq::Ray& r, Meta& m) {
+        const uint32_t q = id >> 5, k = q % kinds;
+        uint32_t pixel;
+        if (!tile_pixel(q / kinds, id & 31u, tiles_x, s->w, s->h, pixel)) return false;
+        const float4* gp = reinterpret_cast<const float4*>(gbuf + pixel);
+        const float4 g0 = __ldg(gp);
+        if (__float_as_uint(g0.w) == 0u) return false;
+        const float4 g1 = __ldg(gp + 1);
+        const rq::F3 P{g0.x, g0.y, g0.z}, N{g1.x, g1.y, g1.z};
+        m.pixel = pixel;
+        m.bit = k;
+        if (k < s->nl) {
+            const rq::F3 tl{s->lx[k] - P.x, s->ly[k] - P.y, s->lz[k] - P.z};
+            const float dist = sqrtf(rq::f3dot(tl, tl));
+            if (dist > s->lr[k] || dist < 0.001f) return false;
+            const rq::F3 L{tl.x / dist, tl.y / dist, tl.z / dist};
+            if (fmaxf(0.0f, rq::f3dot(N, L)) <= 0.0f) return false;
+            r.o = rq::F3{P.x + N.x * s->sh_bias, P.y + N.y * s->sh_bias, P.z + N.z * s->sh_bias};
+            r.d = L;
+            r.tmin = s->sh_tmin;
+            r.tmax = dist - s->sh_bias;
+        } else {
+            m.bit = 32u + (k - s->nl);
+            r.o = rq::F3{P.x + N.x * s->ao_bias, P.y + N.y * s->ao_bias, P.z + N.z * s->ao_bias};
+            r.d = hemisphere(N, pixel, k - s->nl);
+            r.tmin = s->ao_tmin;
+            r.tmax = s->ao_tmax;
+        }
+        ++rays;
+        return true;
+    }
+
+    __device__ void finish(uint32_t, const Meta& m, const rq::Ray&, const rq::Hit& h) {
+        if (STATS) {
+            boxes += h.boxes;
+            tris += h.tris;
+        }
+        if (!h.hit) atomicOr(words + m.pixel, 1ull << m.bit);
+    }
+};
+
+template <bool MT, int STACK>
+__global__ void __launch_bounds__(kT) k_gbuffer(const rq_bvh4_node* __restrict__ nodes,
+                                                const rq_triangle* __restrict__ tris,
+                                                const __grid_constant__ GbufSrc src, uint32_t* ctr,
+                                                uint32_t* err) {
+    extern __shared__ int32_t s_stack[];
+    rq::trace_persistent<false, MT, false, STACK, kT>(nodes, tris, src, ctr, s_stack + threadIdx.x, err);
+}
+
 template <bool MT, bool STATS, int STACK>
 __global__ void __launch_bounds__(kT) k_shadow_ao(const rq_bvh4_node* __restrict__ nodes,
                                                   const rq_triangle* __restrict__ tris,
-                                                  const rq_gbuffer_px* __restrict__ gbuf, ShadeArgs s,
-                                                  uint32_t* __restrict__ mask, float* __restrict__ ao,
-                                                  unsigned long long* counters, uint32_t* err) {
+                                                  const rq_gbuffer_px* __restrict__ gbuf,
+                                                  const __grid_constant__ ShadeArgs sa,
+                                                  unsigned long long* words, unsigned long long* counters,
+                                                  uint32_t* ctr, uint32_t* err) {
     extern __shared__ int32_t s_stack[];
-    const uint32_t px = blockIdx.x * kTX + threadIdx.x % kTX;
-    const uint32_t py = blockIdx.y * kTY + threadIdx.x / kTX;
-    const bool inside = px < s.w && py < s.h;
-    uint32_t rays = 0, boxes = 0, ntris = 0;
-    if (inside) {
-        const uint32_t pixel = py * s.w + px;
-        const float4* gp = reinterpret_cast<const float4*>(gbuf + pixel);
-        const float4 g0 = __ldg(gp), g1 = __ldg(gp + 1);
-        uint32_t m = 0;
-        float occl = 1.0f;
-        if (__float_as_uint(g0.w) != 0u) {
-            const rq::F3 P{g0.x, g0.y, g0.z}, N{g1.x, g1.y, g1.z};
-            rq::TraceResult res;
-            const rq::F3 os{P.x + N.x * s.sh_bias, P.y + N.y * s.sh_bias, P.z + N.z * s.sh_bias};
-            for (uint32_t k = 0; k < s.nl; ++k) {
-                const rq::F3 tl{s.lx[k] - P.x, s.ly[k] - P.y, s.lz[k] - P.z};
-                const float dist = sqrtf(rq::f3dot(tl, tl));
-                if (dist > s.lr[k] || dist < 0.001f) continue;
-                const rq::F3 L{tl.x / dist, tl.y / dist, tl.z / dist};
-                if (fmaxf(0.0f, rq::f3dot(N, L)) <= 0.0f) continue;
-                ++rays;
-                rq::trace_ray<true, MT, STATS, STACK, kT>(nodes, tris, s_stack + threadIdx.x, os, L, s.sh_tmin,
-                                                          dist - s.sh_bias, res, err);
-                if (STATS) {
-                    boxes += res.boxes;
-                    ntris += res.tris;
-                }
-                if (res.idx == rq::kNoHit) m |= 1u << k;
-            }
-            if (s.spp) {
-                uint32_t seed = pixel + 5544u;
-                const rq::F3 oa{P.x + N.x * s.ao_bias, P.y + N.y * s.ao_bias, P.z + N.z * s.ao_bias};
-                float unocc = 0.0f;
-                for (uint32_t i = 0; i < s.spp; ++i) {
-                    const rq::F3 dir = hemisphere(N, seed);
-                    ++rays;
-                    rq::trace_ray<true, MT, STATS, STACK, kT>(nodes, tris, s_stack + threadIdx.x, oa, dir, s.ao_tmin,
-                                                              s.ao_tmax, res, err);
-                    if (STATS) {
-                        boxes += res.boxes;
-                        ntris += res.tris;
-                    }
-                    if (res.idx == rq::kNoHit) unocc += 1.0f;
-                }
-                occl = unocc / __uint2float_rn(s.spp);
-            }
-        }
-        mask[pixel] = m;
-        ao[pixel] = occl;
-    }
+    ShadeSrc<STATS> src;
+    src.kinds = sa.nl + sa.spp;
+    src.tiles_x = (sa.w + kTileW - 1) / kTileW;
+    src.total = src.tiles_x * ((sa.h + kTileH - 1) / kTileH) * src.kinds * 32u;
+    src.s = &sa;
+    src.gbuf = gbuf;
+    src.words = words;
+    rq::trace_persistent<true, MT, STATS, STACK, kT>(nodes, tris, src, ctr, s_stack + threadIdx.x, err);
     if (counters) {
-        const uint32_t wsum = __reduce_add_sync(0xffffffffu, rays);
-        if ((threadIdx.x & 31) == 0 && wsum) atomicAdd(counters, (unsigned long long)wsum);
+        const uint32_t r = __reduce_add_sync(rq::kFull, src.rays);
+        if ((threadIdx.x & 31u) == 0 && r) atomicAdd(counters, (unsigned long long)r);
         if (STATS) {
-            const uint32_t bsum = __reduce_add_sync(0xffffffffu, boxes);
-            const uint32_t tsum = __reduce_add_sync(0xffffffffu, ntris);
-            if ((threadIdx.x & 31) == 0) {
-                atomicAdd(counters + 1, (unsigned long long)bsum);
-                atomicAdd(counters + 2, (unsigned long long)tsum);
+            const uint32_t b = __reduce_add_sync(rq::kFull, src.boxes);
+            const uint32_t t = __reduce_add_sync(rq::kFull, src.tris);
+            if ((threadIdx.x & 31u) == 0) {
+                atomicAdd(counters + 1, (unsigned long long)b);
+                atomicAdd(counters + 2, (unsigned long long)t);
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(256) k_shade_finish(const rq_gbuffer_px* __restrict__ gbuf,
+                                                      const unsigned long long* __restrict__ words, uint32_t npix,
+                                                      uint32_t spp, uint32_t* __restrict__ mask,
+                                                      float* __restrict__ ao) {
+    const uint32_t p = blockIdx.x * 256 + threadIdx.x;
+    if (p >= npix) return;
+    const unsigned long long w = words[p];
+    const bool vis = reinterpret_cast<const uint4*>(gbuf + p)->w != 0u;
+    mask[p] = uint32_t(w);
+    ao[p] = (vis && spp) ? __uint2float_rn(uint32_t(__popcll(w >> 32))) / __uint2float_rn(spp) : 1.0f;
 }
 
 template <class F>
@@ -179,17 +242,25 @@ cudaError_t with_stack(uint32_t bound, F&& f) {
     return f(std::integral_constant<int, 128>{});
 }
 
+// Grid of a persistent kernel: every SM filled to its occupancy.
 template <class K>
-cudaError_t prep(K kern, int stack) {
-    size_t smem = size_t(stack) * kT * sizeof(int32_t);
-    if (smem > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+cudaError_t persistent_grid(K kern, int stack, int sms, int* blocks) {
+    const size_t smem = size_t(stack) * kT * sizeof(int32_t);
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, smem);
+    if (e != cudaSuccess) return e;
+    *blocks = sms * (per_sm > 0 ? per_sm : 1);
     return cudaSuccess;
 }
 
 }  // namespace
 
 int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_gbuffer_px* gbuf, cudaStream_t st) {
-    CamArgs c;
+    GbufSrc src;
+    CamArgs& c = src.c;
     for (int i = 0; i < 16; ++i) c.m[i] = cam.inv_view_proj[i];
     c.cx = cam.cam_pos[0];
     c.cy = cam.cam_pos[1];
@@ -200,17 +271,25 @@ int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_g
     c.seed = cam.seed;
     c.tmin = cam.tmin;
     c.tmax = cam.tmax;
+    src.tiles_x = (cam.width + kTileW - 1) / kTileW;
+    src.total = src.tiles_x * ((cam.height + kTileH - 1) / kTileH) * 32u;
+    src.tris = bvh->tris;
+    src.perm = bvh->perm;
+    src.gbuf = gbuf;
     const uint32_t bound = 3u * (bvh->h_counts[2] + 2u) + 1u;
     const bool mt = cam.flags & RQ_TRI_MT;
-    dim3 grid((cam.width + kTX - 1) / kTX, (cam.height + kTY - 1) / kTY);
-    cudaError_t e = with_stack(bound, [&](auto S) {
-        constexpr int STACK = decltype(S)::value;
-        auto k = mt ? k_gbuffer<true, STACK> : k_gbuffer<false, STACK>;
-        cudaError_t r = prep(k, STACK);
-        if (r != cudaSuccess) return r;
-        k<<<grid, kT, size_t(STACK) * kT * 4, st>>>(bvh->nodes4, bvh->tris, bvh->perm, c, gbuf, ctx->d_err);
-        return cudaGetLastError();
-    });
+    uint32_t* ctr = ctx->d_ctr;
+    cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess)
+        e = with_stack(bound, [&](auto S) {
+            constexpr int STACK = decltype(S)::value;
+            auto k = mt ? k_gbuffer<true, STACK> : k_gbuffer<false, STACK>;
+            int blocks = 0;
+            cudaError_t r = persistent_grid(k, STACK, ctx->num_sms, &blocks);
+            if (r != cudaSuccess) return r;
+            k<<<blocks, kT, size_t(STACK) * kT * 4, st>>>(bvh->nodes4, bvh->tris, src, ctr, ctx->d_err);
+            return cudaGetLastError();
+        });
     return rq_cuda_status(ctx, e, "gbuffer launch");
 }
 
@@ -233,18 +312,31 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
         s.lz[k] = on ? p.lights[k].pos[2] : 0.0f;
         s.lr[k] = on ? p.lights[k].radius : 0.0f;
     }
+    const uint32_t npix = p.width * p.height;
+    int rc = rq_ensure_scratch(ctx, sizeof(unsigned long long) * size_t(npix) + 256, st);
+    if (rc) return rc;
+    unsigned long long* words = static_cast<unsigned long long*>(ctx->scratch);
     const uint32_t bound = 3u * (bvh->h_counts[2] + 2u) + 1u;
     const bool mt = p.flags & RQ_TRI_MT;
     const bool stats = (p.flags & RQ_SHADE_COUNT_TESTS) && counter;
-    dim3 grid((p.width + kTX - 1) / kTX, (p.height + kTY - 1) / kTY);
-    cudaError_t e = with_stack(bound, [&](auto S) {
-        constexpr int STACK = decltype(S)::value;
-        auto k = mt ? (stats ? k_shadow_ao<true, true, STACK> : k_shadow_ao<true, false, STACK>)
-                    : (stats ? k_shadow_ao<false, true, STACK> : k_shadow_ao<false, false, STACK>);
-        cudaError_t r = prep(k, STACK);
-        if (r != cudaSuccess) return r;
-        k<<<grid, kT, size_t(STACK) * kT * 4, st>>>(bvh->nodes4, bvh->tris, gbuf, s, mask, ao, counter, ctx->d_err);
-        return cudaGetLastError();
-    });
+    uint32_t* ctr = ctx->d_ctr;
+    cudaError_t e = cudaMemsetAsync(words, 0, sizeof(unsigned long long) * size_t(npix), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess && p.num_lights + p.ao_spp > 0)
+        e = with_stack(bound, [&](auto S) {
+            constexpr int STACK = decltype(S)::value;
+            auto k = mt ? (stats ? k_shadow_ao<true, true, STACK> : k_shadow_ao<true, false, STACK>)
+                        : (stats ? k_shadow_ao<false, true, STACK> : k_shadow_ao<false, false, STACK>);
+            int blocks = 0;
+            cudaError_t r = persistent_grid(k, STACK, ctx->num_sms, &blocks);
+            if (r != cudaSuccess) return r;
+            k<<<blocks, kT, size_t(STACK) * kT * 4, st>>>(bvh->nodes4, bvh->tris, gbuf, s, words, counter, ctr,
+                                                          ctx->d_err);
+            return cudaGetLastError();
+        });
+    if (e == cudaSuccess) {
+        k_shade_finish<<<(npix + 255) / 256, 256, 0, st>>>(gbuf, words, npix, p.ao_spp, mask, ao);
+        e = cudaGetLastError();
+    }
     return rq_cuda_status(ctx, e, "shadow/AO launch");
 }

@@ -14,7 +14,7 @@
 //  k_ref2     software_bvh_lds.comp:86-175 as published (hitFound flag).
 #include "rq_device.cuh"
 #include "rq_internal.h"
-#include "trace_core.cuh"
+#include "trace_engine.cuh"
 
 namespace {
 
@@ -24,33 +24,50 @@ __device__ __forceinline__ void store_miss(rq_hit* hits, uint32_t i) {
     reinterpret_cast<uint4*>(hits)[i] = make_uint4(0u, __float_as_uint(-1.0f), 0xffffffffu, 0xffffffffu);
 }
 
+// Ray source of rq_trace: rays from a buffer, hits to a buffer.
+template <bool STATS, bool BARY>
+struct BufSrc {
+    struct Meta {};
+    uint32_t total;
+    const rq_ray* rays;
+    const uint32_t* perm;
+    rq_hit* hits;
+    float* bary;
+    rq_ray_stats* stats;
+
+    __device__ bool make(uint32_t id, rq::Ray& r, Meta&) const {
+        const float4* rp = reinterpret_cast<const float4*>(rays + id);
+        const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+        r.o = rq::F3{r0.x, r0.y, r0.z};
+        r.d = rq::F3{r1.x, r1.y, r1.z};
+        r.tmin = r0.w;
+        r.tmax = r1.w;
+        return true;
+    }
+
+    __device__ void finish(uint32_t id, const Meta&, const rq::Ray&, const rq::Hit& h) const {
+        if (h.hit) {
+            const uint32_t pid = perm ? __ldg(perm + h.idx) : h.idx;
+            reinterpret_cast<uint4*>(hits)[id] = make_uint4(1u, __float_as_uint(h.t), 0u, pid);
+        } else {
+            store_miss(hits, id);
+        }
+        if (BARY) reinterpret_cast<float2*>(bary)[id] = h.hit ? make_float2(h.u, h.v) : make_float2(0.f, 0.f);
+        if (STATS) reinterpret_cast<uint4*>(stats)[id] = make_uint4(h.hit ? 1u : 0u, h.boxes, h.tris, 0u);
+    }
+};
+
 template <bool ANY, bool MT, bool STATS, bool BARY, int STACK>
 __global__ void __launch_bounds__(kT) k_trace4(const rq_bvh4_node* __restrict__ nodes,
                                                const rq_triangle* __restrict__ tris,
-                                               const uint32_t* __restrict__ perm, const rq_ray* __restrict__ rays,
-                                               uint32_t n, rq_hit* __restrict__ hits, float* __restrict__ bary,
-                                               rq_ray_stats* __restrict__ stats, const uint32_t* __restrict__ counts,
-                                               uint32_t* err) {
+                                               const __grid_constant__ BufSrc<STATS, BARY> src,
+                                               const uint32_t* __restrict__ counts, uint32_t* ctr, uint32_t* err) {
     extern __shared__ int32_t s_stack[];
-    const uint32_t i = blockIdx.x * kT + threadIdx.x;
-    if (i >= n) return;
     // the stack variant was picked from the host's copy of the depth; the
     // live depth (after an in-place rebuild) must still fit
-    if (i == 0 && 3u * __ldg(counts + 2) + 1u > uint32_t(STACK)) rq::set_err(err, RQ_DERR_STACK);
-    const float4* rp = reinterpret_cast<const float4*>(rays + i);
-    const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-    rq::TraceResult res;
-    rq::trace_ray<ANY, MT, STATS, STACK, kT>(nodes, tris, s_stack + threadIdx.x, rq::F3{r0.x, r0.y, r0.z},
-                                            rq::F3{r1.x, r1.y, r1.z}, r0.w, r1.w, res, err);
-    const bool hit = res.idx != rq::kNoHit;
-    if (hit) {
-        uint32_t pid = perm ? __ldg(perm + res.idx) : res.idx;
-        reinterpret_cast<uint4*>(hits)[i] = make_uint4(1u, __float_as_uint(res.t), 0u, pid);
-    } else {
-        store_miss(hits, i);
-    }
-    if (BARY) reinterpret_cast<float2*>(bary)[i] = hit ? make_float2(res.u, res.v) : make_float2(0.f, 0.f);
-    if (STATS) reinterpret_cast<uint4*>(stats)[i] = make_uint4(hit ? 1u : 0u, res.boxes, res.tris, 0u);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && 3u * __ldg(counts + 2) + 1u > uint32_t(STACK))
+        rq::set_err(err, RQ_DERR_STACK);
+    rq::trace_persistent<ANY, MT, STATS, STACK, kT>(nodes, tris, src, ctr, s_stack + threadIdx.x, err);
 }
 
 template <bool ANY, bool MT, bool BARY>
@@ -295,32 +312,45 @@ __global__ void __launch_bounds__(kT) k_ref2(const rq_bvh2_node* __restrict__ no
 }
 
 template <bool ANY, bool MT, bool STATS, bool BARY, int STACK>
-cudaError_t launch4(const rq_bvh* b, const rq_ray* rays, uint32_t n, rq_hit* hits, float* bary, rq_ray_stats* stats,
-                    uint32_t* err, cudaStream_t st) {
+cudaError_t launch4(rq_ctx* ctx, const rq_bvh* b, const rq_ray* rays, uint32_t n, rq_hit* hits, float* bary,
+                    rq_ray_stats* stats, cudaStream_t st) {
     auto kern = k_trace4<ANY, MT, STATS, BARY, STACK>;
-    size_t smem = size_t(STACK) * kT * sizeof(int32_t);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess) return e;
-    }
-    kern<<<(n + kT - 1) / kT, kT, smem, st>>>(b->nodes4, b->tris, b->perm, rays, n, hits, bary, stats, b->d_counts,
-                                              err);
+    const size_t smem = size_t(STACK) * kT * sizeof(int32_t);
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, smem);
+    if (e != cudaSuccess) return e;
+    // persistent grid: every SM filled, never more blocks than 32-ray chunks
+    uint32_t blocks = uint32_t(ctx->num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+    const uint32_t need = (n + kT - 1) / kT;
+    if (blocks > need) blocks = need;
+    BufSrc<STATS, BARY> src;
+    src.total = n;
+    src.rays = rays;
+    src.perm = b->perm;
+    src.hits = hits;
+    src.bary = bary;
+    src.stats = stats;
+    e = cudaMemsetAsync(ctx->d_ctr, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    kern<<<blocks, kT, smem, st>>>(b->nodes4, b->tris, src, b->d_counts, ctx->d_ctr, ctx->d_err);
     return cudaGetLastError();
 }
 
 template <bool ANY, bool MT, bool STATS, bool BARY>
-cudaError_t launch4_stack(uint32_t bound, const rq_bvh* b, const rq_ray* rays, uint32_t n, rq_hit* hits, float* bary,
-                          rq_ray_stats* stats, uint32_t* err, cudaStream_t st) {
-    if (bound <= 32) return launch4<ANY, MT, STATS, BARY, 32>(b, rays, n, hits, bary, stats, err, st);
-    if (bound <= 64) return launch4<ANY, MT, STATS, BARY, 64>(b, rays, n, hits, bary, stats, err, st);
-    return launch4<ANY, MT, STATS, BARY, 128>(b, rays, n, hits, bary, stats, err, st);
+cudaError_t launch4_stack(uint32_t bound, rq_ctx* ctx, const rq_bvh* b, const rq_ray* rays, uint32_t n,
+                          rq_hit* hits, float* bary, rq_ray_stats* stats, cudaStream_t st) {
+    if (bound <= 32) return launch4<ANY, MT, STATS, BARY, 32>(ctx, b, rays, n, hits, bary, stats, st);
+    if (bound <= 64) return launch4<ANY, MT, STATS, BARY, 64>(ctx, b, rays, n, hits, bary, stats, st);
+    return launch4<ANY, MT, STATS, BARY, 128>(ctx, b, rays, n, hits, bary, stats, st);
 }
 
 template <bool ANY, bool MT>
-cudaError_t launch4_opts(uint32_t bound, bool stats_on, bool bary_on, const rq_bvh* b, const rq_ray* rays,
-                         uint32_t n, rq_hit* hits, float* bary, rq_ray_stats* stats, uint32_t* err, cudaStream_t st) {
-    if (stats_on || bary_on) return launch4_stack<ANY, MT, true, true>(bound, b, rays, n, hits, bary, stats, err, st);
-    return launch4_stack<ANY, MT, false, false>(bound, b, rays, n, hits, bary, stats, err, st);
+cudaError_t launch4_opts(uint32_t bound, bool ex, rq_ctx* ctx, const rq_bvh* b, const rq_ray* rays, uint32_t n,
+                         rq_hit* hits, float* bary, rq_ray_stats* stats, cudaStream_t st) {
+    if (ex) return launch4_stack<ANY, MT, true, true>(bound, ctx, b, rays, n, hits, bary, stats, st);
+    return launch4_stack<ANY, MT, false, false>(bound, ctx, b, rays, n, hits, bary, stats, st);
 }
 
 }  // namespace
@@ -348,13 +378,13 @@ int rq_launch_trace(rq_ctx* ctx, const rq_bvh* bvh, const rq_ray* rays, uint32_t
     const bool ex = stats || bary;
     cudaError_t e;
     if (any && mt)
-        e = launch4_opts<true, true>(bound, ex, ex, bvh, rays, n, hits, ba_out, st_out, ctx->d_err, st);
+        e = launch4_opts<true, true>(bound, ex, ctx, bvh, rays, n, hits, ba_out, st_out, st);
     else if (any)
-        e = launch4_opts<true, false>(bound, ex, ex, bvh, rays, n, hits, ba_out, st_out, ctx->d_err, st);
+        e = launch4_opts<true, false>(bound, ex, ctx, bvh, rays, n, hits, ba_out, st_out, st);
     else if (mt)
-        e = launch4_opts<false, true>(bound, ex, ex, bvh, rays, n, hits, ba_out, st_out, ctx->d_err, st);
+        e = launch4_opts<false, true>(bound, ex, ctx, bvh, rays, n, hits, ba_out, st_out, st);
     else
-        e = launch4_opts<false, false>(bound, ex, ex, bvh, rays, n, hits, ba_out, st_out, ctx->d_err, st);
+        e = launch4_opts<false, false>(bound, ex, ctx, bvh, rays, n, hits, ba_out, st_out, st);
     return rq_cuda_status(ctx, e, "trace launch");
 }
 

@@ -15,6 +15,9 @@
 
 namespace rq {
 
+// Primitive index of "no hit".
+constexpr uint32_t kNoHit = 0xffffffffu;
+
 // ------------------------------------------------------------ memory order
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
     uint32_t v;

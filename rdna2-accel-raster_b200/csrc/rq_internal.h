@@ -28,6 +28,7 @@ struct rq_ctx {
     size_t scratch_bytes = 0;
     uint32_t* d_err = nullptr;      // device error word
     uint32_t* h_err = nullptr;      // pinned mirror
+    uint32_t* d_ctr = nullptr;      // work counters of persistent launches (zeroed per launch)
     std::string last_error;
     int collapse_blocks = 0;        // co-resident blocks of the collapse kernel
 };

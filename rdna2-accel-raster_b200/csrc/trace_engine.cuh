@@ -1,0 +1,209 @@
+// trace_engine.cuh — persistent traversal with per-lane ray refill.
+//
+// Every lane of a warp owns one ray at a time.  Ray ids come from a global
+// counter in chunks of 32 (one atomic per chunk); whenever lanes are idle,
+// a ballot and a rank within the idle mask hand them the next ids, so a warp
+// keeps 32 rays in flight until the ids run out.  Each round:
+//   1. inner phase — lanes without a pending leaf pop stack entries; an inner
+//      node is box-tested and its hit children pushed (closest hit: sorted
+//      near-to-far and pushed far-first; any hit: slot 3..0), a leaf entry is
+//      parked as the lane's pending leaf; the phase ends when no lane wants
+//      another inner node (every lane parked a leaf or ran out of entries);
+//   2. leaf phase — lanes test their parked leaf's triangles in order;
+//   3. lanes whose stack is empty, or whose any-hit ray found a hit, report
+//      the result to the ray source and become idle.
+// Per ray this visits stack entries in exactly the order of a sequential
+// pop-process-push traversal, so results do not depend on which lane or
+// round a ray runs in and match the oracle's traversal bit for bit.
+//
+// A ray source provides:
+//   uint32_t total;                                 number of ray ids
+//   bool make(uint32_t id, Ray& r, Meta& m);        false = no ray for this id
+//   void finish(uint32_t id, const Meta& m, const Hit& h);
+#pragma once
+
+#include "rq_device.cuh"
+#include "rq_internal.h"
+
+namespace rq {
+
+constexpr int32_t kNoLeaf = 0;  // leaf entries always have bit 31 set
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr uint32_t kChunk = 32;
+
+struct Ray {
+    F3 o, d;
+    float tmin, tmax;
+};
+
+struct Hit {
+    bool hit;
+    float t;
+    uint32_t idx;  // leaf-order primitive index
+    float u, v;
+    uint32_t boxes, tris;
+};
+
+template <bool ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src>
+__device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict__ nodes,
+                                                 const rq_triangle* __restrict__ tris, Src& src, uint32_t* ctr,
+                                                 int32_t* stk, uint32_t* err) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    // warp-uniform chunk of ray ids
+    uint32_t next = 0, end = 0;
+    bool exhausted = false;
+    // lane state
+    bool active = false;
+    uint32_t rid = 0;
+    typename Src::Meta meta;
+    Ray ray;
+    SlabRay sr;
+    WtRay w;
+    float best = 0.0f;
+    int sp = 0;
+    Hit h;
+    h.hit = false;
+    h.t = 0.0f;
+    h.idx = kNoHit;
+    h.u = h.v = 0.0f;
+    h.boxes = h.tris = 0;
+
+    for (;;) {
+        // ---- refill idle lanes
+        uint32_t idle = __ballot_sync(kFull, !active);
+        while (idle && !exhausted) {
+            if (next == end) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(ctr, kChunk);
+                base = __shfl_sync(kFull, base, 0);
+                if (base >= src.total) {
+                    exhausted = true;
+                    break;
+                }
+                next = base;
+                end = min(base + kChunk, src.total);
+            }
+            const uint32_t take = min(uint32_t(__popc(idle)), end - next);
+            const uint32_t rank = __popc(idle & lt_mask);
+            const bool mine = ((idle >> lane) & 1u) && rank < take;
+            if (mine) {
+                rid = next + rank;
+                if (src.make(rid, ray, meta)) {
+                    active = true;
+                    sr.ix = safe_inv(ray.d.x);
+                    sr.iy = safe_inv(ray.d.y);
+                    sr.iz = safe_inv(ray.d.z);
+                    sr.ox = ray.o.x * sr.ix;
+                    sr.oy = ray.o.y * sr.iy;
+                    sr.oz = ray.o.z * sr.iz;
+                    if (!MT) w = wt_setup(ray.d);
+                    best = ray.tmax;
+                    h.hit = false;
+                    h.idx = kNoHit;
+                    h.u = h.v = 0.0f;
+                    h.boxes = h.tris = 0;
+                    stk[0] = 0;
+                    sp = 1;
+                }
+            }
+            next += take;
+            // lanes whose id made no ray (a light behind the surface, an
+            // empty pixel) take the next id at once
+            idle = __ballot_sync(kFull, !active);
+        }
+        if (!__any_sync(kFull, active)) {
+            if (exhausted) break;
+            continue;
+        }
+
+        // ---- inner phase
+        int32_t leaf = kNoLeaf;
+        for (;;) {
+            const bool want = active && sp > 0 && leaf == kNoLeaf;
+            if (!__any_sync(kFull, want)) break;
+            if (!want) continue;
+            const int32_t e = stk[(--sp) * STRIDE];
+            if (e < 0) {
+                leaf = e;
+                continue;
+            }
+            const float4* np = reinterpret_cast<const float4*>(nodes + e);
+            const float4 mnx = ldg4(np + 0), mxx = ldg4(np + 1);
+            const float4 mny = ldg4(np + 2), mxy = ldg4(np + 3);
+            const float4 mnz = ldg4(np + 4), mxz = ldg4(np + 5);
+            const int4 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
+            const int4 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
+            if (STATS) h.boxes += 4;
+            const float amnx[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, amxx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
+            const float amny[4] = {mny.x, mny.y, mny.z, mny.w}, amxy[4] = {mxy.x, mxy.y, mxy.z, mxy.w};
+            const float amnz[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, amxz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
+            const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
+            int32_t he[4];
+            float ht[4];
+            int nh = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (acc[k] == 0) continue;
+                float tn;
+                if (slab(sr, ray.tmin, best, amnx[k], amxx[k], amny[k], amxy[k], amnz[k], amxz[k], tn)) {
+                    const int32_t ent = acc[k] < 0
+                                            ? aci[k]
+                                            : int32_t(0x80000000u | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
+                    int pos = nh;
+                    if (!ANY) {
+                        while (pos > 0 && ht[pos - 1] > tn) {
+                            he[pos] = he[pos - 1];
+                            ht[pos] = ht[pos - 1];
+                            --pos;
+                        }
+                    }
+                    he[pos] = ent;
+                    ht[pos] = tn;
+                    ++nh;
+                }
+            }
+            if (sp + nh > STACK) {
+                set_err(err, RQ_DERR_STACK);
+                nh = STACK - sp;
+            }
+            for (int j = nh - 1; j >= 0; --j) stk[(sp++) * STRIDE] = he[j];
+        }
+
+        // ---- leaf phase
+        bool done = false;
+        if (active && leaf != kNoLeaf) {
+            const uint32_t first = uint32_t(leaf) & 0x07ffffffu;
+            const uint32_t cntl = ((uint32_t(leaf) >> 27) & 15u) + 1u;
+            for (uint32_t p = first; p < first + cntl; ++p) {
+                const float4* tp = reinterpret_cast<const float4*>(tris + p);
+                const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+                const F3 v0{a.x, a.y, a.z}, v1{b.x, b.y, b.z}, v2{c.x, c.y, c.z};
+                if (STATS) ++h.tris;
+                float t, u, v;
+                const bool ok = MT ? mt_test(ray.o, ray.d, v0, v1, v2, 1e-7f, t, u, v)
+                                   : wt_test(w, ray.o, v0, v1, v2, t, u, v);
+                if (ok && t >= ray.tmin && t < best) {
+                    best = t;
+                    h.hit = true;
+                    h.idx = p;
+                    h.u = u;
+                    h.v = v;
+                    if (ANY) {
+                        done = true;
+                        break;
+                    }
+                }
+            }
+        }
+
+        // ---- report finished rays
+        if (active && (done || sp == 0)) {
+            h.t = best;
+            src.finish(rid, meta, ray, h);
+            active = false;
+        }
+    }
+}
+
+}  // namespace rq
