@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=6000, help="pixels in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the visibility / batched / serving workloads")
     return ap.parse_args()
 
 
@@ -343,6 +344,10 @@ def run_ours(args, world, rank, local, pg):
     e2e_ms = max_over_ranks(pg, a.elapsed_time(b) / args.steps)
     e2e_value = sum_over_ranks(pg, frame_rays) / (e2e_ms * 1e-3) / 1e6
 
+    bvh.destroy()
+    del p_d, i_d, gbuf, mask, ao
+    vis = run_visibility(ctx, dev, stream) if not args.no_extra else None
+
     if rank != 0:
         return
     peaks = {}
@@ -403,10 +408,64 @@ def run_ours(args, world, rank, local, pg):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "visibility": vis,
     }
     print(json.dumps(line), flush=True)
-    bvh.destroy()
     ctx.close()
+
+
+def run_visibility(ctx, dev, stream, frames=200):
+    """Subpixel visibility: 8,323,200 triangles (2040x2040 quads, seed 3) deforming
+    every frame (z = z0 + 0.05 sin(0.1 f + x)); 1920x1080 jittered primary rays
+    per frame; the BVH either fully rebuilt or refitted each frame."""
+    import numpy as np
+    import torch
+    import rq
+    from rq import workloads as W
+
+    pos, idx = W.visibility_mesh()
+    ntri = len(idx)
+    base = torch.from_numpy(pos).to(dev)
+    cur = torch.empty_like(base)
+    i_d = torch.from_numpy(idx.view(np.int32)).to(dev)
+    gbuf = torch.empty((WIDTH * HEIGHT, 8), dtype=torch.int32, device=dev)
+    rq.deform_wave(ctx, base, cur, W.deform_time(0), W.DEFORM_AMP, W.DEFORM_FREQ)
+    bvh = rq.Bvh.build(ctx, cur, i_d)
+    out = {"workload": ("subpixel visibility: 8,323,200-triangle grid (2040x2040 quads, seed 3) deformed every "
+                        "frame, 1920x1080 jittered closest-hit primary rays, 200 frames per mode"),
+           "triangles": ntri, "frames": frames}
+    for mode in ("rebuild", "refit"):
+        rq.deform_wave(ctx, base, cur, W.deform_time(0), W.DEFORM_AMP, W.DEFORM_FREQ)
+        rq.Bvh.build(ctx, cur, i_d, into=bvh)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * frames + 1)]
+        torch.cuda.synchronize(dev)
+        ev[0].record(stream)
+        for f in range(frames):
+            rq.deform_wave(ctx, base, cur, W.deform_time(f), W.DEFORM_AMP, W.DEFORM_FREQ)
+            if mode == "rebuild":
+                rq.Bvh.build(ctx, cur, i_d, into=bvh)
+            else:
+                bvh.refit(cur, i_d)
+            ev[3 * f + 1].record(stream)
+            cam = W.visibility_camera(seed=3 + f)
+            rq.render_gbuffer(ctx, bvh, cam, gbuf)
+            ev[3 * f + 2].record(stream)
+            ev[3 * f + 3].record(stream)
+        torch.cuda.synchronize(dev)
+        ctx.sync_check()
+        total = ev[0].elapsed_time(ev[-1])
+        upd = [(ev[3 * f].elapsed_time(ev[3 * f + 1])) for f in range(1, frames)]
+        trc = [ev[3 * f + 1].elapsed_time(ev[3 * f + 2]) for f in range(frames)]
+        hits = int((gbuf[:, 3] != 0).sum().item())
+        out[mode] = {"ms_per_frame": round(total / frames, 4),
+                     "update_ms": round(statistics.median(upd), 4),
+                     "trace_ms": round(statistics.median(trc), 4),
+                     "trace_ms_last_frame": round(trc[-1], 4),
+                     "mrays_per_s": round(WIDTH * HEIGHT / (total / frames) / 1e3, 1),
+                     "update_mtris_per_s": round(ntri / statistics.median(upd) / 1e3, 1),
+                     "primary_hits_last_frame": hits}
+    bvh.destroy()
+    return out
 
 
 def main():

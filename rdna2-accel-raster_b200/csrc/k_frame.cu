@@ -1,14 +1,16 @@
-// k_frame.cu — traversal kernels that generate their own rays, on the
-// persistent engine of trace_engine.cuh.
+// k_frame.cu — traversal kernels that generate their own rays.
 //
-//  k_gbuffer    one primary closest-hit ray per pixel
+//  k_gbuffer_seq  one primary closest-hit ray per pixel and thread
 //               (benchmarks/exp1_visbuf/shaders/visbuf_raycast.comp:15-51,
 //               optional per-pixel jitter) -> position, visibility value,
-//               camera-facing face normal, t.
+//               camera-facing face normal, t.  Camera rays are coherent, so
+//               the one-ray-per-thread schedule of trace_core.cuh wins.
 //  k_shadow_ao  the any-hit shadow rays of shaders/tiled_lighting_ra.comp:
 //               223-253 and the cosine-hemisphere AO rays of
 //               shaders/rq_ao.comp:18-94, generated from the G-buffer inside
-//               the kernel.  A ray id names (8x4 pixel tile, ray kind k, pixel
+//               the kernel, on the refilling schedule of trace_engine.cuh
+//               (a pixel's rays differ in length, so lanes must not wait for
+//               one another).  A ray id names (8x4 pixel tile, ray kind k, pixel
 //               in tile): the 32 ids of one chunk are the 32 pixels of a tile
 //               casting toward the same light (or the same AO sample), the
 //               most coherent batch a warp can trace.  A ray that reaches its
@@ -18,6 +20,7 @@
 // No ray or hit buffer touches HBM.
 #include "rq_device.cuh"
 #include "rq_internal.h"
+#include "trace_core.cuh"
 #include "trace_engine.cuh"
 
 namespace {
@@ -184,13 +187,32 @@ struct ShadeSrc {
     }
 };
 
+// One camera ray per thread, 16x8 pixels per block: primary rays are
+// coherent, so lanes stay together without refilling.
 template <bool MT, int STACK>
-__global__ void __launch_bounds__(kT) k_gbuffer(const rq_bvh4_node* __restrict__ nodes,
-                                                const rq_triangle* __restrict__ tris,
-                                                const __grid_constant__ GbufSrc src, uint32_t* ctr,
-                                                uint32_t* err) {
+__global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restrict__ nodes,
+                                                    const rq_triangle* __restrict__ tris,
+                                                    const __grid_constant__ GbufSrc src, uint32_t* err) {
     extern __shared__ int32_t s_stack[];
-    rq::trace_persistent<false, MT, false, STACK, kT>(nodes, tris, src, ctr, s_stack + threadIdx.x, err);
+    const uint32_t px = blockIdx.x * 16 + threadIdx.x % 16;
+    const uint32_t py = blockIdx.y * 8 + threadIdx.x / 16;
+    if (px >= src.c.w || py >= src.c.h) return;
+    const uint32_t id = ((py / kTileH) * src.tiles_x + px / kTileW) * 32u + (py % kTileH) * kTileW + px % kTileW;
+    rq::Ray r;
+    GbufSrc::Meta m;
+    src.make(id, r, m);
+    rq::TraceResult res;
+    rq::trace_ray<false, MT, false, STACK, kT>(nodes, tris, s_stack + threadIdx.x, r.o, r.d, r.tmin, r.tmax, res,
+                                               err);
+    rq::Hit h;
+    h.hit = res.idx != rq::kNoHit;
+    h.t = res.t;
+    h.idx = res.idx;
+    h.u = res.u;
+    h.v = res.v;
+    h.boxes = res.boxes;
+    h.tris = res.tris;
+    src.finish(id, m, r, h);
 }
 
 template <bool MT, bool STATS, int STACK>
@@ -278,18 +300,18 @@ int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_g
     src.gbuf = gbuf;
     const uint32_t bound = 3u * (bvh->h_counts[2] + 2u) + 1u;
     const bool mt = cam.flags & RQ_TRI_MT;
-    uint32_t* ctr = ctx->d_ctr;
-    cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
-    if (e == cudaSuccess)
-        e = with_stack(bound, [&](auto S) {
-            constexpr int STACK = decltype(S)::value;
-            auto k = mt ? k_gbuffer<true, STACK> : k_gbuffer<false, STACK>;
-            int blocks = 0;
-            cudaError_t r = persistent_grid(k, STACK, ctx->num_sms, &blocks);
+    dim3 grid((cam.width + 15) / 16, (cam.height + 7) / 8);
+    cudaError_t e = with_stack(bound, [&](auto S) {
+        constexpr int STACK = decltype(S)::value;
+        auto k = mt ? k_gbuffer_seq<true, STACK> : k_gbuffer_seq<false, STACK>;
+        const size_t smem = size_t(STACK) * kT * 4;
+        if (smem > 48 * 1024) {
+            cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             if (r != cudaSuccess) return r;
-            k<<<blocks, kT, size_t(STACK) * kT * 4, st>>>(bvh->nodes4, bvh->tris, src, ctr, ctx->d_err);
-            return cudaGetLastError();
-        });
+        }
+        k<<<grid, kT, smem, st>>>(bvh->nodes4, bvh->tris, src, ctx->d_err);
+        return cudaGetLastError();
+    });
     return rq_cuda_status(ctx, e, "gbuffer launch");
 }
 

@@ -1,0 +1,116 @@
+// trace_core.cuh — the engine's 4-wide traversal of one ray by one thread
+// from start to end (the schedule for one coherent ray per thread, such as
+// camera rays; trace_engine.cuh is the schedule that refills lanes).
+//
+// Stack entries are int32: >= 0 an inner node index; bit 31 set a leaf
+// (bits 27..30 = count-1, bits 0..26 = first primitive).  Each thread's
+// stack lives in shared memory with a stride of the block size, so the
+// entries of one warp fall in distinct banks.  3*depth+1 entries suffice.
+// The visit order is the one of trace_engine.cuh: results are identical.
+#pragma once
+
+#include "rq_device.cuh"
+#include "rq_internal.h"
+
+namespace rq {
+
+constexpr uint32_t kLeafBit = 0x80000000u;
+
+struct TraceResult {
+    float t;        // nearest accepted distance (tmax when nothing was hit)
+    uint32_t idx;   // leaf-order primitive index, kNoHit for a miss
+    float u, v;     // barycentrics of v1 and v2
+    uint32_t boxes; // 4 per inner node visited
+    uint32_t tris;  // triangles tested
+};
+
+template <bool ANY, bool MT, bool STATS, int STACK, int STRIDE>
+__device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes,
+                                          const rq_triangle* __restrict__ tris, int32_t* stk, F3 o, F3 d,
+                                          float tmin, float tmax, TraceResult& res, uint32_t* err) {
+    SlabRay sr;
+    sr.ix = safe_inv(d.x);
+    sr.iy = safe_inv(d.y);
+    sr.iz = safe_inv(d.z);
+    sr.ox = o.x * sr.ix;
+    sr.oy = o.y * sr.iy;
+    sr.oz = o.z * sr.iz;
+    WtRay w;
+    if (!MT) w = wt_setup(d);
+    float best = tmax;
+    res.idx = kNoHit;
+    res.u = res.v = 0.0f;
+    res.boxes = res.tris = 0;
+    stk[0] = 0;
+    int sp = 1;
+    while (sp > 0) {
+        const int32_t e = stk[(--sp) * STRIDE];
+        if (e >= 0) {
+            const float4* np = reinterpret_cast<const float4*>(nodes + e);
+            const float4 mnx = ldg4(np + 0), mxx = ldg4(np + 1);
+            const float4 mny = ldg4(np + 2), mxy = ldg4(np + 3);
+            const float4 mnz = ldg4(np + 4), mxz = ldg4(np + 5);
+            const int4 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
+            const int4 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
+            if (STATS) res.boxes += 4;
+            const float amnx[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, amxx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
+            const float amny[4] = {mny.x, mny.y, mny.z, mny.w}, amxy[4] = {mxy.x, mxy.y, mxy.z, mxy.w};
+            const float amnz[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, amxz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
+            const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
+            int32_t he[4];
+            float ht[4];
+            int nh = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (acc[k] == 0) continue;
+                float tn;
+                if (slab(sr, tmin, best, amnx[k], amxx[k], amny[k], amxy[k], amnz[k], amxz[k], tn)) {
+                    const int32_t ent =
+                        acc[k] < 0 ? aci[k] : int32_t(kLeafBit | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
+                    int pos = nh;
+                    if (!ANY) {
+                        while (pos > 0 && ht[pos - 1] > tn) {
+                            he[pos] = he[pos - 1];
+                            ht[pos] = ht[pos - 1];
+                            --pos;
+                        }
+                    }
+                    he[pos] = ent;
+                    ht[pos] = tn;
+                    ++nh;
+                }
+            }
+            if (sp + nh > STACK) {
+                set_err(err, RQ_DERR_STACK);
+                nh = STACK - sp;
+            }
+            for (int j = nh - 1; j >= 0; --j) stk[(sp++) * STRIDE] = he[j];
+        } else {
+            const uint32_t first = uint32_t(e) & 0x07ffffffu;
+            const uint32_t cntl = ((uint32_t(e) >> 27) & 15u) + 1u;
+            bool done = false;
+            for (uint32_t p = first; p < first + cntl; ++p) {
+                const float4* tp = reinterpret_cast<const float4*>(tris + p);
+                const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+                const F3 v0{a.x, a.y, a.z}, v1{b.x, b.y, b.z}, v2{c.x, c.y, c.z};
+                if (STATS) ++res.tris;
+                float t, u, v;
+                const bool ok = MT ? mt_test(o, d, v0, v1, v2, 1e-7f, t, u, v) : wt_test(w, o, v0, v1, v2, t, u, v);
+                if (ok && t >= tmin && t < best) {
+                    best = t;
+                    res.idx = p;
+                    res.u = u;
+                    res.v = v;
+                    if (ANY) {
+                        done = true;
+                        break;
+                    }
+                }
+            }
+            if (ANY && done) break;
+        }
+    }
+    res.t = best;
+}
+
+}  // namespace rq

@@ -58,8 +58,19 @@ def visibility_mesh(q=2040):
 
 
 def visibility_camera(width=1920, height=1080, jitter=True, seed=3, flags=0):
-    return camera_look_at((0.0, -0.6, 2.6), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 20.0, width, height, jitter=jitter,
+    """Straight down from z=3 with a 19.5 degree vertical field: every pixel
+    stays on the mesh even where it dips to z=-0.25, and about 47 % of the
+    grid (1.9 triangles per pixel at 2040x2040 quads) is in view."""
+    return camera_look_at((0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 19.5, width, height, jitter=jitter,
                           seed=seed, flags=flags)
+
+
+DEFORM_AMP, DEFORM_FREQ, DEFORM_DT = 0.05, 1.0, 0.1
+
+
+def deform_time(frame):
+    """Frame f of a deformation sequence: z = z0 + 0.05*sin(0.1*f + x)."""
+    return DEFORM_DT * frame
 
 
 def log_uniform_int(rng, lo, hi, size):
