@@ -80,6 +80,11 @@ int rq_scene_rays_down(uint32_t n, float x0, float x1, float y0, float y1, float
  * per-frame deformation step (benchmarks/expA_async/shaders/mesh_deform.comp:25-34). */
 int rq_deform_wave(rq_ctx* ctx, const float* base, float* out, uint32_t num_vertices,
                    float t, float amp, float freq, rq_stream stream);
+/* The same with the time in device memory: `state` (device, 2 uint32) holds
+ * t as float bits and a zeroed work word; after the launch t has advanced
+ * by dt.  A recorded sequence of frames then animates without host input. */
+int rq_deform_wave_step(rq_ctx* ctx, const float* base, float* out, uint32_t num_vertices,
+                        uint32_t* state, float dt, float amp, float freq, rq_stream stream);
 
 /* ------------------------------------------------------------------ */
 /* BVH build (LBVH: Morton codes, onesweep radix sort, Karras emission, */
@@ -191,6 +196,48 @@ int rq_trace_ref_bvh2(rq_ctx* ctx, const rq_bvh2_node* nodes, const rq_triangle*
  * origins in [-40,40]x[15,30]x[-40,40] heading down.  tmin 0.01, tmax 1000. */
 int rq_gen_rays_procedural(rq_ctx* ctx, const float cam_pos[3], const float look_at[3],
                            uint32_t count, uint32_t coherent, rq_ray* rays, rq_stream stream);
+
+/* ------------------------------------------------------------------ */
+/* Batches: many meshes built in one launch and traced in one launch   */
+/* ------------------------------------------------------------------ */
+
+typedef struct rq_batch rq_batch;
+
+/* One mesh of a batch inside shared vertex and index buffers: its vertices
+ * start at vertex_offset, its triangles (3 mesh-local uint32 indices each) at
+ * triangle_offset.  At most 2^20 triangles per mesh. */
+typedef struct rq_mesh_desc {
+    uint32_t vertex_offset;
+    uint32_t num_vertices;
+    uint32_t triangle_offset;
+    uint32_t num_triangles;
+} rq_mesh_desc;
+
+/* Allocate a batch for the given meshes (host array; copied).  Triangle
+ * ranges must not overlap.  The batch owns its arrays and build scratch. */
+int rq_batch_create(rq_ctx* ctx, const rq_mesh_desc* meshes, uint32_t num_meshes, uint32_t max_leaf,
+                    rq_batch** out);
+/* Build every mesh's binary and 4-wide BVH in ONE persistent launch: each
+ * thread block builds one mesh at a time (largest first) with the same steps
+ * as rq_build, so each mesh's bytes equal a separate rq_build of it.  Device
+ * pointers; stride as in rq_build.  The first build synchronises once to
+ * read the depths; later builds stay asynchronous. */
+int rq_batch_build(rq_ctx* ctx, rq_batch* batch, const float* positions, uint32_t stride_bytes,
+                   const uint32_t* indices, rq_stream stream);
+/* Trace rays of any meshes of the batch in ONE persistent launch.  ray_mesh[i]
+ * names ray i's mesh; ray_flags[i] (may be NULL: `flags` for all) selects any
+ * hit (RQ_TRACE_ANY) per ray; RQ_TRI_MT in `flags` selects the triangle
+ * test.  Primitive IDs are mesh-local original triangle ids.  stats may be NULL. */
+int rq_batch_trace(rq_ctx* ctx, const rq_batch* batch, const rq_ray* rays, const uint32_t* ray_mesh,
+                   const uint32_t* ray_flags, uint32_t n, uint32_t flags, rq_hit* hits, rq_ray_stats* stats,
+                   rq_stream stream);
+/* Per-mesh counts (synchronises) and downloads, as rq_bvh_info_get /
+ * rq_bvh_download for one mesh of the batch. */
+int rq_batch_info_get(rq_batch* batch, uint32_t mesh, rq_bvh_info* info);
+int rq_batch_download(rq_batch* batch, uint32_t mesh, int host, rq_bvh2_node* nodes2, uint32_t cap_nodes2,
+                      rq_triangle* tris, uint32_t cap_tris, rq_bvh4_node* nodes4, uint32_t cap_nodes4,
+                      uint32_t* perm, uint32_t cap_perm);
+int rq_batch_destroy(rq_batch* batch);
 
 /* ------------------------------------------------------------------ */
 /* Frames: rays generated inside the traversal kernels                 */

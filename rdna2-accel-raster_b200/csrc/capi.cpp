@@ -197,6 +197,12 @@ int rq_deform_wave(rq_ctx* ctx, const float* base, float* out, uint32_t num_vert
     return rq_launch_deform(ctx, base, out, num_vertices, t, amp, freq, S(stream));
 }
 
+int rq_deform_wave_step(rq_ctx* ctx, const float* base, float* out, uint32_t num_vertices, uint32_t* state, float dt,
+                        float amp, float freq, rq_stream stream) {
+    if (!ctx || !base || !out || !state) return RQ_ERR_INVALID_ARG;
+    return rq_launch_deform_step(ctx, base, out, num_vertices, state, dt, amp, freq, S(stream));
+}
+
 // ---------------------------------------------------------------- build
 
 int rq_build(rq_ctx* ctx, const float* positions, uint32_t stride_bytes, uint32_t num_vertices,

@@ -1,13 +1,13 @@
 // k_build.cu — LBVH build of a binary BVH in the layouts of
-// common/software_bvh.hpp:
+// common/software_bvh.hpp, one mesh per launch sequence:
 //   1. per-triangle centroid ((p0+p1)+p2)/3 (software_bvh.hpp:53) and
 //      centroid bounds (ordered-uint atomics);
 //   2. 30-bit Morton code in the cube of the largest centroid extent;
 //   3. onesweep radix sort of (code, triangle id)              [k_sort.cu]
 //   4. Karras 2012 internal nodes, parent links;
 //   5. one thread per sorted leaf: leaf-ordered triangle copy, permutation,
-//      leaf box, atomic bottom-up box refit, and the depth-first emission
-//      count of the leaf starting there;
+//      leaf box, the depth-first emission count of the leaf starting there,
+//      then the atomic bottom-up box refit;
 //   6. exclusive scan of the emission counts                    [k_sort.cu]
 //   7. depth-first pre-order node writes: every emitted node v sits at
 //      A[lo(v)] + L(v), where lo(v) is its first primitive, A the scan and
@@ -15,35 +15,17 @@
 //      SoftwareBVH::recursiveBuild (software_bvh.hpp:90-175): left child at
 //      parent + 1, right child after the left subtree;
 //   8. the greedy 4-wide collapse                               [k_collapse.cu]
+// The per-element steps live in build_core.cuh (shared with k_batch.cu).
+// Also the refit of an existing handle (k_parents2, k_refit2, k_refit4).
 #include <algorithm>
 
+#include "build_core.cuh"
 #include "rq_device.cuh"
 #include "rq_internal.h"
 
 namespace {
 
-constexpr uint32_t kNone = 0xffffffffu;
 constexpr int kT = 256;
-
-__device__ __forceinline__ void load_tri(const float* __restrict__ pos, uint32_t sf, const uint32_t* __restrict__ idx,
-                                         uint32_t t, rq::F3& p0, rq::F3& p1, rq::F3& p2) {
-    uint32_t i0, i1, i2;
-    if (idx) {
-        i0 = __ldg(idx + 3ull * t);
-        i1 = __ldg(idx + 3ull * t + 1);
-        i2 = __ldg(idx + 3ull * t + 2);
-    } else {
-        i0 = 3 * t;
-        i1 = 3 * t + 1;
-        i2 = 3 * t + 2;
-    }
-    const float* a = pos + size_t(i0) * sf;
-    const float* b = pos + size_t(i1) * sf;
-    const float* c = pos + size_t(i2) * sf;
-    p0 = {__ldg(a), __ldg(a + 1), __ldg(a + 2)};
-    p1 = {__ldg(b), __ldg(b + 1), __ldg(b + 2)};
-    p2 = {__ldg(c), __ldg(c + 1), __ldg(c + 2)};
-}
 
 __global__ void __launch_bounds__(kT) k_centroids(const float* __restrict__ pos, uint32_t sf,
                                                   const uint32_t* __restrict__ idx, uint32_t n,
@@ -51,17 +33,15 @@ __global__ void __launch_bounds__(kT) k_centroids(const float* __restrict__ pos,
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (uint32_t t = blockIdx.x * kT + threadIdx.x; t < n; t += gridDim.x * kT) {
         rq::F3 p0, p1, p2;
-        load_tri(pos, sf, idx, t, p0, p1, p2);
-        float cx = ((p0.x + p1.x) + p2.x) / 3.0f;
-        float cy = ((p0.y + p1.y) + p2.y) / 3.0f;
-        float cz = ((p0.z + p1.z) + p2.z) / 3.0f;
-        cent[t] = make_float4(cx, cy, cz, 0.0f);
-        mn[0] = fminf(mn[0], cx);
-        mn[1] = fminf(mn[1], cy);
-        mn[2] = fminf(mn[2], cz);
-        mx[0] = fmaxf(mx[0], cx);
-        mx[1] = fmaxf(mx[1], cy);
-        mx[2] = fmaxf(mx[2], cz);
+        rq::load_tri(pos, sf, idx, t, p0, p1, p2);
+        const float4 c = rq::centroid(p0, p1, p2);
+        cent[t] = c;
+        mn[0] = fminf(mn[0], c.x);
+        mn[1] = fminf(mn[1], c.y);
+        mn[2] = fminf(mn[2], c.z);
+        mx[0] = fmaxf(mx[0], c.x);
+        mx[1] = fmaxf(mx[1], c.y);
+        mx[2] = fmaxf(mx[2], c.z);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -83,74 +63,24 @@ __global__ void __launch_bounds__(kT) k_centroids(const float* __restrict__ pos,
 __global__ void __launch_bounds__(kT) k_morton(const float4* __restrict__ cent, uint32_t n,
                                                const uint32_t* __restrict__ bounds, uint32_t* __restrict__ keys,
                                                uint32_t* __restrict__ vals) {
-    float lx = rq::o2f(bounds[0]), ly = rq::o2f(bounds[1]), lz = rq::o2f(bounds[2]);
-    float hx = rq::o2f(bounds[3]), hy = rq::o2f(bounds[4]), hz = rq::o2f(bounds[5]);
-    float ext = fmaxf(fmaxf(hx - lx, hy - ly), hz - lz);
-    float scale = ext > 1e-30f ? 1024.0f / ext : 0.0f;
+    const float lx = rq::o2f(bounds[0]), ly = rq::o2f(bounds[1]), lz = rq::o2f(bounds[2]);
+    const float scale = rq::morton_scale(lx, ly, lz, rq::o2f(bounds[3]), rq::o2f(bounds[4]), rq::o2f(bounds[5]));
     for (uint32_t t = blockIdx.x * kT + threadIdx.x; t < n; t += gridDim.x * kT) {
-        float4 c = cent[t];
-        keys[t] = rq::expand10(rq::quantize10(c.x, lx, scale)) * 4u +
-                  rq::expand10(rq::quantize10(c.y, ly, scale)) * 2u + rq::expand10(rq::quantize10(c.z, lz, scale));
+        keys[t] = rq::morton30(cent[t], lx, ly, lz, scale);
         vals[t] = t;
     }
 }
 
-__device__ __forceinline__ int kdelta(const uint32_t* __restrict__ k, int n, int i, int j) {
-    if (j < 0 || j > n - 1) return -1;
-    uint32_t x = __ldg(k + i) ^ __ldg(k + j);
-    if (x) return __clz(x);
-    return 32 + __clz(uint32_t(i) ^ uint32_t(j));
-}
-
-// Karras 2012: range and split of internal node i over sorted keys.
 __global__ void __launch_bounds__(kT) k_karras(const uint32_t* __restrict__ keys, uint32_t n32,
                                                int32_t* __restrict__ kl, int32_t* __restrict__ kr,
                                                uint32_t* __restrict__ klo, uint32_t* __restrict__ khi,
                                                uint32_t* __restrict__ par_in, uint32_t* __restrict__ par_lf) {
     const int n = int(n32);
-    for (int i = blockIdx.x * kT + threadIdx.x; i < n - 1; i += gridDim.x * kT) {
-        int d = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
-        int dmin = kdelta(keys, n, i, i - d);
-        int lmax = 2;
-        while (kdelta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
-        int l = 0;
-        for (int t = lmax >> 1; t >= 1; t >>= 1)
-            if (kdelta(keys, n, i, i + (l + t) * d) > dmin) l += t;
-        int j = i + l * d;
-        int dnode = kdelta(keys, n, i, j);
-        int s = 0, t = l;
-        do {
-            t = (t + 1) >> 1;
-            if (kdelta(keys, n, i, i + (s + t) * d) > dnode) s += t;
-        } while (t > 1);
-        int gamma = i + s * d + min(d, 0);
-        int lo = min(i, j), hi = max(i, j);
-        bool lleaf = lo == gamma, rleaf = hi == gamma + 1;
-        kl[i] = lleaf ? int32_t(0x80000000u | uint32_t(gamma)) : gamma;
-        kr[i] = rleaf ? int32_t(0x80000000u | uint32_t(gamma + 1)) : gamma + 1;
-        klo[i] = uint32_t(lo);
-        khi[i] = uint32_t(hi);
-        uint32_t pl = uint32_t(i) << 1, pr = (uint32_t(i) << 1) | 1u;
-        if (lleaf)
-            par_lf[gamma] = pl;
-        else
-            par_in[gamma] = pl;
-        if (rleaf)
-            par_lf[gamma + 1] = pr;
-        else
-            par_in[gamma + 1] = pr;
-        if (i == 0) par_in[0] = kNone;
-    }
-    if (n == 1 && blockIdx.x == 0 && threadIdx.x == 0) par_lf[0] = kNone;
+    for (int i = blockIdx.x * kT + threadIdx.x; i < n - 1; i += gridDim.x * kT)
+        rq::karras_node(keys, n, i, kl, kr, klo, khi, par_in, par_lf);
+    if (n == 1 && blockIdx.x == 0 && threadIdx.x == 0) par_lf[0] = rq::kNoParent;
 }
 
-__device__ __forceinline__ uint32_t count_in(const uint32_t* klo, const uint32_t* khi, uint32_t i) {
-    return khi[i] - klo[i] + 1u;
-}
-
-// One thread per sorted leaf k: triangle copy, permutation, leaf box,
-// emission count c[k], then the atomic bottom-up refit (the second child to
-// arrive at a node computes its box and continues upward).
 __global__ void __launch_bounds__(kT) k_leaves(const float* __restrict__ pos, uint32_t sf,
                                                const uint32_t* __restrict__ idx, uint32_t n, uint32_t max_leaf,
                                                const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
@@ -162,116 +92,22 @@ __global__ void __launch_bounds__(kT) k_leaves(const float* __restrict__ pos, ui
                                                uint32_t* __restrict__ perm, uint32_t* __restrict__ keys_out,
                                                uint32_t* err) {
     for (uint32_t k = blockIdx.x * kT + threadIdx.x; k < n; k += gridDim.x * kT) {
-        uint32_t id = sids[k];
-        rq::F3 p0, p1, p2;
-        load_tri(pos, sf, idx, id, p0, p1, p2);
-        float4* tp = reinterpret_cast<float4*>(tris + k);
-        tp[0] = make_float4(p0.x, p0.y, p0.z, 0.0f);
-        tp[1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
-        tp[2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
-        perm[k] = id;
-        keys_out[k] = skeys[k];
-        float4 lo = make_float4(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)),
-                                fminf(p0.z, fminf(p1.z, p2.z)), 0.0f);
-        float4 hi = make_float4(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)),
-                                fmaxf(p0.z, fmaxf(p1.z, p2.z)), 0.0f);
-        box_lf[2 * size_t(k)] = lo;
-        box_lf[2 * size_t(k) + 1] = hi;
-
-        // emission count: the emitted leaf holding k is its highest ancestor
-        // with count <= max_leaf; if that leaf starts at k, c = 1 + L(leaf).
-        uint32_t par = par_lf[k];
-        uint32_t ulo = k;
-        while (par != kNone) {
-            uint32_t pp = par >> 1;
-            if (count_in(klo, khi, pp) > max_leaf) break;
-            ulo = klo[pp];
-            par = par_in[pp];
-        }
-        uint32_t c = 0;
-        if (ulo == k) {
-            uint32_t L = 0;
-            while (par != kNone && (par & 1u) == 0u) {
-                ++L;
-                par = par_in[par >> 1];
-            }
-            c = 1u + L;
-        }
-        c_out[k] = c;
-
-        // bottom-up refit
+        rq::leaf_step(k, pos, sf, idx, max_leaf, skeys, sids, klo, khi, par_in, par_lf, box_lf, c_out, tris, perm,
+                      keys_out);
         __threadfence();
-        par = par_lf[k];
-        uint32_t guard = 0;
-        while (par != kNone) {
-            uint32_t p = par >> 1;
-            uint32_t old = atomicAdd(&refit_flag[p], 1u);
-            if (old == 0u) break;
-            __threadfence();
-            int32_t a = kl[p], b = kr[p];
-            const float4* ba = a < 0 ? box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : box_in + 2 * size_t(a);
-            const float4* bb = b < 0 ? box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : box_in + 2 * size_t(b);
-            float4 alo = rq::ld_cg4(ba), ahi = rq::ld_cg4(ba + 1);
-            float4 blo = rq::ld_cg4(bb), bhi = rq::ld_cg4(bb + 1);
-            float4 ulo4 = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f);
-            float4 uhi4 = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f);
-            __stcg(box_in + 2 * size_t(p), ulo4);
-            __stcg(box_in + 2 * size_t(p) + 1, uhi4);
-            __threadfence();
-            par = par_in[p];
-            if (++guard > 128u) {
-                rq::set_err(err, RQ_DERR_REFIT);
-                break;
-            }
-        }
+        rq::refit_walk(k, kl, kr, par_in, par_lf, box_in, box_lf, refit_flag, err);
     }
 }
 
-// Node writes in depth-first pre-order.  Thread p handles internal node p
-// (if emitted) and the emitted leaf starting at primitive p (if any).
-__global__ void __launch_bounds__(kT) k_emit2(uint32_t n, uint32_t max_leaf, const int32_t* __restrict__ kl,
-                                              const int32_t* __restrict__ kr, const uint32_t* __restrict__ klo,
-                                              const uint32_t* __restrict__ khi, const uint32_t* __restrict__ par_in,
+__global__ void __launch_bounds__(kT) k_emit2(uint32_t n, uint32_t max_leaf, const int32_t* __restrict__ kr,
+                                              const uint32_t* __restrict__ klo, const uint32_t* __restrict__ khi,
+                                              const uint32_t* __restrict__ par_in,
                                               const uint32_t* __restrict__ par_lf, const float4* __restrict__ box_in,
                                               const float4* __restrict__ box_lf, const uint32_t* __restrict__ c,
                                               const uint32_t* __restrict__ A, rq_bvh2_node* __restrict__ out,
                                               uint32_t* __restrict__ counts) {
     for (uint32_t p = blockIdx.x * kT + threadIdx.x; p < n; p += gridDim.x * kT) {
-        if (p + 1 < n && count_in(klo, khi, p) > max_leaf) {
-            uint32_t L = 0, par = par_in[p];
-            while (par != kNone && (par & 1u) == 0u) {
-                ++L;
-                par = par_in[par >> 1];
-            }
-            uint32_t pre = A[klo[p]] + L;
-            int32_t r = kr[p];
-            uint32_t rlo = r < 0 ? (uint32_t(r) & 0x7fffffffu) : klo[r];
-            float4 lo = box_in[2 * size_t(p)], hi = box_in[2 * size_t(p) + 1];
-            float4* o = reinterpret_cast<float4*>(out + pre);
-            o[0] = make_float4(lo.x, lo.y, lo.z, __int_as_float(int32_t(pre + 1)));
-            o[1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(int32_t(A[rlo])));
-        }
-        uint32_t cp = c[p];
-        if (cp) {
-            // re-find the emitted leaf starting at p
-            uint32_t par = par_lf[p];
-            uint32_t node = p;
-            bool is_leaf = true;
-            while (par != kNone) {
-                uint32_t pp = par >> 1;
-                if (count_in(klo, khi, pp) > max_leaf) break;
-                node = pp;
-                is_leaf = false;
-                par = par_in[pp];
-            }
-            uint32_t cnt = is_leaf ? 1u : count_in(klo, khi, node);
-            const float4* b = is_leaf ? box_lf + 2 * size_t(node) : box_in + 2 * size_t(node);
-            float4 lo = b[0], hi = b[1];
-            uint32_t pre = A[p] + cp - 1u;
-            float4* o = reinterpret_cast<float4*>(out + pre);
-            o[0] = make_float4(lo.x, lo.y, lo.z, __int_as_float(~int32_t(p)));
-            o[1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(int32_t(cnt)));
-        }
+        const uint32_t cp = rq::emit_step(p, n, max_leaf, kr, klo, khi, par_in, par_lf, box_in, box_lf, c, A, out);
         if (p == n - 1) {
             counts[0] = A[p] + cp;  // binary node count
             counts[3] = max_leaf;
@@ -283,11 +119,11 @@ __global__ void __launch_bounds__(kT) k_emit2(uint32_t n, uint32_t max_leaf, con
 // Parent links of an emitted binary BVH (any layout with the root at 0).
 __global__ void __launch_bounds__(kT) k_parents2(const rq_bvh2_node* __restrict__ nodes, const uint32_t* counts,
                                                  uint32_t* __restrict__ parent, uint32_t* __restrict__ flag) {
-    uint32_t n2 = counts[0];
+    const uint32_t n2 = counts[0];
     for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < n2; i += gridDim.x * kT) {
         const rq_bvh2_node nd = nodes[i];
         flag[i] = 0u;
-        if (i == 0) parent[0] = kNone;
+        if (i == 0) parent[0] = rq::kNoParent;
         if (nd.left_child >= 0) {
             parent[nd.left_child] = i;
             parent[nd.right_child] = i;
@@ -302,15 +138,15 @@ __global__ void __launch_bounds__(kT) k_refit2(const float* __restrict__ pos, ui
                                                const uint32_t* __restrict__ perm, rq_bvh2_node* nodes,
                                                rq_triangle* __restrict__ tris, const uint32_t* __restrict__ parent,
                                                uint32_t* flag, uint32_t* err) {
-    uint32_t n2 = counts[0];
+    const uint32_t n2 = counts[0];
     for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < n2; i += gridDim.x * kT) {
-        rq_bvh2_node nd = nodes[i];
+        const rq_bvh2_node nd = nodes[i];
         if (nd.left_child >= 0) continue;
-        uint32_t first = uint32_t(~nd.left_child), cnt = uint32_t(nd.right_child);
+        const uint32_t first = uint32_t(~nd.left_child), cnt = uint32_t(nd.right_child);
         float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (uint32_t q = first; q < first + cnt; ++q) {
             rq::F3 p0, p1, p2;
-            load_tri(pos, sf, idx, perm[q], p0, p1, p2);
+            rq::load_tri(pos, sf, idx, perm[q], p0, p1, p2);
             float4* tp = reinterpret_cast<float4*>(tris + q);
             tp[0] = make_float4(p0.x, p0.y, p0.z, 0.0f);
             tp[1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
@@ -328,15 +164,15 @@ __global__ void __launch_bounds__(kT) k_refit2(const float* __restrict__ pos, ui
         __threadfence();
         uint32_t p = parent[i];
         uint32_t guard = 0;
-        while (p != kNone) {
+        while (p != rq::kNoParent) {
             if (atomicAdd(&flag[p], 1u) == 0u) break;
             __threadfence();
             const float4* pn = reinterpret_cast<const float4*>(nodes + p);
-            float4 pa = rq::ld_cg4(pn), pb = rq::ld_cg4(pn + 1);
-            int32_t l = __float_as_int(pa.w), r = __float_as_int(pb.w);
+            const float4 pa = rq::ld_cg4(pn), pb = rq::ld_cg4(pn + 1);
+            const int32_t l = __float_as_int(pa.w), r = __float_as_int(pb.w);
             const float4* ln = reinterpret_cast<const float4*>(nodes + l);
             const float4* rn = reinterpret_cast<const float4*>(nodes + r);
-            float4 la = rq::ld_cg4(ln), lb = rq::ld_cg4(ln + 1), ra = rq::ld_cg4(rn), rb = rq::ld_cg4(rn + 1);
+            const float4 la = rq::ld_cg4(ln), lb = rq::ld_cg4(ln + 1), ra = rq::ld_cg4(rn), rb = rq::ld_cg4(rn + 1);
             __stcg(reinterpret_cast<float4*>(nodes + p),
                    make_float4(fminf(la.x, ra.x), fminf(la.y, ra.y), fminf(la.z, ra.z), pa.w));
             __stcg(reinterpret_cast<float4*>(nodes + p) + 1,
@@ -355,11 +191,11 @@ __global__ void __launch_bounds__(kT) k_refit2(const float* __restrict__ pos, ui
 // by the collapse.
 __global__ void __launch_bounds__(kT) k_refit4(const rq_bvh2_node* __restrict__ n2, const uint32_t* counts,
                                                const int32_t* __restrict__ map4, rq_bvh4_node* __restrict__ n4) {
-    uint32_t m = counts[1];
+    const uint32_t m = counts[1];
     for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < 4 * m; i += gridDim.x * kT) {
-        int32_t s = map4[i];
+        const int32_t s = map4[i];
         if (s < 0) continue;
-        uint32_t node = i >> 2, k = i & 3u;
+        const uint32_t node = i >> 2, k = i & 3u;
         const rq_bvh2_node c = n2[s];
         n4[node].min_x[k] = c.aabb_min[0];
         n4[node].max_x[k] = c.aabb_max[0];
@@ -371,8 +207,8 @@ __global__ void __launch_bounds__(kT) k_refit4(const rq_bvh2_node* __restrict__ 
 }
 
 inline uint32_t grid_for(uint32_t n, int sms) {
-    uint32_t b = (n + kT - 1) / kT;
-    uint32_t cap = uint32_t(sms) * 8u;
+    const uint32_t b = (n + kT - 1) / kT;
+    const uint32_t cap = uint32_t(sms) * 8u;
     return std::max(1u, std::min(b, cap));
 }
 
@@ -380,8 +216,8 @@ inline uint32_t grid_for(uint32_t n, int sms) {
 
 size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s) {
     Carve c{reinterpret_cast<uintptr_t>(base), 0};
-    size_t N = n ? n : 1;
-    uint32_t tiles = rq_sort_tiles(uint32_t(N)), stiles = rq_scan_tiles(uint32_t(N));
+    const size_t N = n ? n : 1;
+    const uint32_t tiles = rq_sort_tiles(uint32_t(N)), stiles = rq_scan_tiles(uint32_t(N));
     s.cent = c.take<float4>(N);
     s.bounds = c.take<uint32_t>(8);
     s.keys[0] = c.take<uint32_t>(N);
@@ -415,7 +251,7 @@ size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s) {
 int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
                     uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t st) {
     BuildScratch s;
-    size_t need = rq_build_scratch_carve(nullptr, n, s);
+    const size_t need = rq_build_scratch_carve(nullptr, n, s);
     int rc = rq_ensure_scratch(ctx, need, st);
     if (rc) return rc;
     rq_build_scratch_carve(ctx->scratch, n, s);
@@ -440,8 +276,8 @@ int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_
                                               s.par_in, s.par_lf, s.box_in, s.box_lf, s.refit_flag, s.c, bvh->tris,
                                               bvh->perm, bvh->skeys, ctx->d_err);
     rq_launch_scan(ctx, s.c, s.a, n, s.scan_status, s.tile_ctr + 8, st);
-    k_emit2<<<grid_for(n, sms), kT, 0, st>>>(n, max_leaf, s.kl, s.kr, s.klo, s.khi, s.par_in, s.par_lf, s.box_in,
-                                             s.box_lf, s.c, s.a, bvh->nodes2, bvh->d_counts);
+    k_emit2<<<grid_for(n, sms), kT, 0, st>>>(n, max_leaf, s.kr, s.klo, s.khi, s.par_in, s.par_lf, s.box_in, s.box_lf,
+                                             s.c, s.a, bvh->nodes2, bvh->d_counts);
     rc = rq_cuda_status(ctx, cudaGetLastError(), "build launch");
     if (rc) return rc;
     if (collapse) return rq_launch_collapse(ctx, bvh, s, st);
@@ -450,8 +286,8 @@ int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_
 
 int rq_launch_refit(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
                     cudaStream_t st) {
-    uint32_t n2cap = bvh->cap_nodes2;
-    size_t need = sizeof(uint32_t) * (2ull * n2cap + 64);
+    const uint32_t n2cap = bvh->cap_nodes2;
+    const size_t need = sizeof(uint32_t) * (2ull * n2cap + 64);
     int rc = rq_ensure_scratch(ctx, need, st);
     if (rc) return rc;
     uint32_t* parent = static_cast<uint32_t*>(ctx->scratch);

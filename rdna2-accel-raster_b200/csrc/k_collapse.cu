@@ -17,6 +17,7 @@
 // RQ_DERR_GRID_BARRIER and every block leaves the kernel.
 #include <algorithm>
 
+#include "build_core.cuh"
 #include "rq_device.cuh"
 #include "rq_internal.h"
 
@@ -72,161 +73,24 @@ __device__ bool grid_sync(uint32_t* ctl, uint32_t* err) {
     return s_ok != 0u;
 }
 
-struct N2 {
-    float mn[3], mx[3];
-    int32_t l, r;
-};
-__device__ __forceinline__ N2 load2(const rq_bvh2_node* n2, int32_t i) {
-    const float4* p = reinterpret_cast<const float4*>(n2 + i);
-    float4 a = __ldg(p), b = __ldg(p + 1);
-    N2 o;
-    o.mn[0] = a.x;
-    o.mn[1] = a.y;
-    o.mn[2] = a.z;
-    o.l = __float_as_int(a.w);
-    o.mx[0] = b.x;
-    o.mx[1] = b.y;
-    o.mx[2] = b.z;
-    o.r = __float_as_int(b.w);
-    return o;
-}
-
 __global__ void __launch_bounds__(kT) k_collapse(CollapseArgs A) {
     __shared__ uint32_t s_lvl[kMaxLevels + 2];
-    const uint32_t tid = blockIdx.x * kT + threadIdx.x;
-    const uint32_t nthreads = gridDim.x * kT;
-    const bool root_leaf = load2(A.n2, 0).l < 0;
-    if (tid == 0) {
-        A.q[0] = 0u;
-        A.pre[0] = 0u;
-        A.ctl[0] = 1u;
-    }
-    if (!grid_sync(A.ctl, A.err)) return;
-
-    // ---- phase 1: levels, candidates, queue
-    uint32_t start = 0, end = 1, depth = 0;
-    while (start < end) {
-        if (threadIdx.x == 0) s_lvl[depth] = start;
-        for (uint32_t e = start + tid; e < end; e += nthreads) {
-            int32_t u = int32_t(__ldcg(A.q + e));
-            int32_t c[4] = {-1, -1, -1, -1};
-            int nc;
-            if (root_leaf) {
-                c[0] = 0;
-                nc = 1;
-            } else {
-                N2 nd = load2(A.n2, u);
-                c[0] = nd.l;
-                c[1] = nd.r;
-                nc = 2;
-                while (nc < 4) {
-                    int best = -1;
-                    float best_sa = -1.0f;
-                    for (int i = 0; i < nc; ++i) {
-                        N2 ci = load2(A.n2, c[i]);
-                        if (ci.l >= 0) {
-                            float dx = ci.mx[0] - ci.mn[0];
-                            float dy = ci.mx[1] - ci.mn[1];
-                            float dz = ci.mx[2] - ci.mn[2];
-                            float sa = 2.0f * ((dx * dy + dy * dz) + dz * dx);
-                            if (sa > best_sa) {
-                                best_sa = sa;
-                                best = i;
-                            }
-                        }
-                    }
-                    if (best < 0) break;
-                    N2 ex = load2(A.n2, c[best]);
-                    c[best] = ex.l;
-                    c[nc++] = ex.r;
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                int32_t cq = -1;
-                if (c[k] >= 0 && !root_leaf && load2(A.n2, c[k]).l >= 0) {
-                    uint32_t pos = atomicAdd(A.ctl, 1u);
-                    __stcg(A.q + pos, uint32_t(c[k]));
-                    cq = int32_t(pos);
-                }
-                __stcg(A.cand + 4 * size_t(e) + k, c[k]);
-                __stcg(A.child_q + 4 * size_t(e) + k, cq);
-            }
-        }
-        if (!grid_sync(A.ctl, A.err)) return;
-        ++depth;
-        start = end;
-        end = __ldcg(A.ctl);
-        if (depth >= kMaxLevels) {
-            if (tid == 0) rq::set_err(A.err, RQ_DERR_QUEUE);
-            return;
-        }
-    }
-    if (threadIdx.x == 0) s_lvl[depth] = end;
-    __syncthreads();
-    const uint32_t total = end;
-
-    // ---- phase 2: subtree sizes, deepest level first
-    for (int lv = int(depth) - 1; lv >= 0; --lv) {
-        for (uint32_t e = s_lvl[lv] + tid; e < s_lvl[lv + 1]; e += nthreads) {
-            uint32_t s = 1;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                int32_t cq = __ldcg(A.child_q + 4 * size_t(e) + k);
-                if (cq >= 0) s += __ldcg(A.sz + cq);
-            }
-            __stcg(A.sz + e, s);
-        }
-        if (!grid_sync(A.ctl, A.err)) return;
-    }
-
-    // ---- phase 3: pre-order positions and node writes, top-down
-    for (uint32_t lv = 0; lv < depth; ++lv) {
-        for (uint32_t e = s_lvl[lv] + tid; e < s_lvl[lv + 1]; e += nthreads) {
-            uint32_t p = __ldcg(A.pre + e);
-            uint32_t off = p + 1u;
-            float mnx[4], mxx[4], mny[4], mxy[4], mnz[4], mxz[4];
-            int32_t ci[4], cc[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                int32_t c = __ldcg(A.cand + 4 * size_t(e) + k);
-                mnx[k] = mxx[k] = mny[k] = mxy[k] = mnz[k] = mxz[k] = 0.0f;
-                ci[k] = 0;
-                cc[k] = 0;
-                if (c >= 0) {
-                    N2 nd = load2(A.n2, c);
-                    mnx[k] = nd.mn[0];
-                    mxx[k] = nd.mx[0];
-                    mny[k] = nd.mn[1];
-                    mxy[k] = nd.mx[1];
-                    mnz[k] = nd.mn[2];
-                    mxz[k] = nd.mx[2];
-                    int32_t cq = __ldcg(A.child_q + 4 * size_t(e) + k);
-                    if (cq >= 0) {
-                        __stcg(A.pre + cq, off);
-                        ci[k] = int32_t(off);
-                        cc[k] = -1;
-                        off += __ldcg(A.sz + cq);
-                    } else {
-                        ci[k] = nd.l;
-                        cc[k] = nd.r;
-                    }
-                }
-                A.map4[4 * size_t(p) + k] = c;
-            }
-            float4* o = reinterpret_cast<float4*>(A.out4 + p);
-            o[0] = make_float4(mnx[0], mnx[1], mnx[2], mnx[3]);
-            o[1] = make_float4(mxx[0], mxx[1], mxx[2], mxx[3]);
-            o[2] = make_float4(mny[0], mny[1], mny[2], mny[3]);
-            o[3] = make_float4(mxy[0], mxy[1], mxy[2], mxy[3]);
-            o[4] = make_float4(mnz[0], mnz[1], mnz[2], mnz[3]);
-            o[5] = make_float4(mxz[0], mxz[1], mxz[2], mxz[3]);
-            reinterpret_cast<int4*>(o)[6] = make_int4(ci[0], ci[1], ci[2], ci[3]);
-            reinterpret_cast<int4*>(o)[7] = make_int4(cc[0], cc[1], cc[2], cc[3]);
-        }
-        if (!grid_sync(A.ctl, A.err)) return;
-    }
-    if (tid == 0) {
+    rq::CollapseIO io;
+    io.n2 = A.n2;
+    io.q = A.q;
+    io.cand = A.cand;
+    io.child_q = A.child_q;
+    io.sz = A.sz;
+    io.pre = A.pre;
+    io.tail = A.ctl;
+    io.out4 = A.out4;
+    io.map4 = A.map4;
+    uint32_t total = 0, depth = 0;
+    auto sync = [&]() { return grid_sync(A.ctl, A.err); };
+    if (!rq::collapse_levels<true>(io, blockIdx.x * kT + threadIdx.x, gridDim.x * kT, s_lvl, kMaxLevels, sync, A.err,
+                                   &total, &depth))
+        return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.counts[1] = total;
         A.counts[2] = depth;
     }

@@ -62,7 +62,43 @@ __global__ void __launch_bounds__(kT) k_deform_wave(const float* __restrict__ ba
     out[3 * size_t(v) + 2] = z + amp * s;
 }
 
+// Same deformation with the time in device memory: state[0] = t (float
+// bits), state[1] = block ticket.  Every block reads t first; the last block
+// to take a ticket advances t by dt and clears the ticket, so a captured
+// graph moves the mesh forward on every replay.
+__global__ void __launch_bounds__(kT) k_deform_wave_step(const float* __restrict__ base, float* __restrict__ out,
+                                                         uint32_t nv, uint32_t* state, float dt, float amp,
+                                                         float freq) {
+    __shared__ float s_t;
+    __shared__ bool s_last;
+    if (threadIdx.x == 0) s_t = __uint_as_float(rq::ld_acquire(state));
+    __syncthreads();
+    const float t = s_t;
+    const uint32_t v = blockIdx.x * kT + threadIdx.x;
+    if (v < nv) {
+        const float x = base[3 * size_t(v)], y = base[3 * size_t(v) + 1], z = base[3 * size_t(v) + 2];
+        float s, c;
+        rq::sincos_taylor(t + freq * x, &s, &c);
+        out[3 * size_t(v)] = x;
+        out[3 * size_t(v) + 1] = y;
+        out[3 * size_t(v) + 2] = z + amp * s;
+    }
+    if (threadIdx.x == 0) s_last = atomicAdd(state + 1, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        state[1] = 0u;
+        rq::st_release(state, __float_as_uint(t + dt));
+    }
+}
+
 }  // namespace
+
+int rq_launch_deform_step(rq_ctx* ctx, const float* base, float* out, uint32_t nv, uint32_t* state, float dt,
+                          float amp, float freq, cudaStream_t st) {
+    if (nv == 0) return RQ_OK;
+    k_deform_wave_step<<<(nv + kT - 1) / kT, kT, 0, st>>>(base, out, nv, state, dt, amp, freq);
+    return rq_cuda_status(ctx, cudaGetLastError(), "deform step launch");
+}
 
 int rq_launch_gen_procedural(rq_ctx* ctx, const float cam[3], const float look[3], uint32_t count,
                              uint32_t coherent, rq_ray* rays, cudaStream_t st) {

@@ -63,7 +63,7 @@ struct Carve {
     uintptr_t base;
     size_t off = 0;
     template <class T>
-    T* take(size_t n) {
+    __host__ __device__ T* take(size_t n) {
         off = (off + 255) & ~size_t(255);
         T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
         off += n * sizeof(T);
@@ -149,3 +149,5 @@ int rq_launch_gen_procedural(rq_ctx* ctx, const float cam[3], const float look[3
                              uint32_t coherent, rq_ray* rays, cudaStream_t st);
 int rq_launch_deform(rq_ctx* ctx, const float* base, float* out, uint32_t nv, float t, float amp, float freq,
                      cudaStream_t st);
+int rq_launch_deform_step(rq_ctx* ctx, const float* base, float* out, uint32_t nv, uint32_t* state, float dt,
+                          float amp, float freq, cudaStream_t st);

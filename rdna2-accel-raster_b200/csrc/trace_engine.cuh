@@ -34,6 +34,22 @@ constexpr uint32_t kChunk = 32;
 struct Ray {
     F3 o, d;
     float tmin, tmax;
+    // set by sources that trace many BVHs in one launch (Src::kMulti)
+    const rq_bvh4_node* nodes;
+    const rq_triangle* tris;
+    bool any;  // per-ray any hit (ANY == kAnyPerRay)
+};
+
+// ANY template argument: 0 closest hit, 1 any hit, kAnyPerRay = Ray::any.
+constexpr int kAnyPerRay = 2;
+
+template <class Src, class = void>
+struct IsMulti {
+    static constexpr bool value = false;
+};
+template <class Src>
+struct IsMulti<Src, decltype(void(Src::kMulti))> {
+    static constexpr bool value = Src::kMulti;
 };
 
 struct Hit {
@@ -44,7 +60,7 @@ struct Hit {
     uint32_t boxes, tris;
 };
 
-template <bool ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src>
+template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src>
 __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict__ nodes,
                                                  const rq_triangle* __restrict__ tris, Src& src, uint32_t* ctr,
                                                  int32_t* stk, uint32_t* err) {
@@ -128,7 +144,8 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                 leaf = e;
                 continue;
             }
-            const float4* np = reinterpret_cast<const float4*>(nodes + e);
+            const rq_bvh4_node* nb = IsMulti<Src>::value ? ray.nodes : nodes;
+            const float4* np = reinterpret_cast<const float4*>(nb + e);
             const float4 mnx = ldg4(np + 0), mxx = ldg4(np + 1);
             const float4 mny = ldg4(np + 2), mxy = ldg4(np + 3);
             const float4 mnz = ldg4(np + 4), mxz = ldg4(np + 5);
@@ -151,7 +168,7 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                                             ? aci[k]
                                             : int32_t(0x80000000u | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
                     int pos = nh;
-                    if (!ANY) {
+                    if (ANY == 0 || (ANY == kAnyPerRay && !ray.any)) {
                         while (pos > 0 && ht[pos - 1] > tn) {
                             he[pos] = he[pos - 1];
                             ht[pos] = ht[pos - 1];
@@ -176,7 +193,7 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
             const uint32_t first = uint32_t(leaf) & 0x07ffffffu;
             const uint32_t cntl = ((uint32_t(leaf) >> 27) & 15u) + 1u;
             for (uint32_t p = first; p < first + cntl; ++p) {
-                const float4* tp = reinterpret_cast<const float4*>(tris + p);
+                const float4* tp = reinterpret_cast<const float4*>((IsMulti<Src>::value ? ray.tris : tris) + p);
                 const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
                 const F3 v0{a.x, a.y, a.z}, v1{b.x, b.y, b.z}, v2{c.x, c.y, c.z};
                 if (STATS) ++h.tris;
@@ -189,7 +206,7 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                     h.idx = p;
                     h.u = u;
                     h.v = v;
-                    if (ANY) {
+                    if (ANY == 1 || (ANY == kAnyPerRay && ray.any)) {
                         done = true;
                         break;
                     }

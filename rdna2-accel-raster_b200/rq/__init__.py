@@ -85,6 +85,12 @@ class ShadeParams(C.Structure):
 
 GBUFFER_PX = np.dtype([("pos", "<f4", 3), ("vis", "<u4"), ("nrm", "<f4", 3), ("t", "<f4")])
 
+
+class MeshDesc(C.Structure):
+    _fields_ = [("vertex_offset", C.c_uint32), ("num_vertices", C.c_uint32), ("triangle_offset", C.c_uint32),
+                ("num_triangles", C.c_uint32)]
+
+
 _P = C.c_void_p
 _U32 = C.c_uint32
 # (name, restype, argtypes) for every entry point in include/rq.h
@@ -100,6 +106,7 @@ SIGNATURES = [
     ("rq_scene_rays_down", C.c_int, [_U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                      C.c_float, C.c_float, C.c_uint64, _P]),
     ("rq_deform_wave", C.c_int, [_P, _P, _P, _U32, C.c_float, C.c_float, C.c_float, _P]),
+    ("rq_deform_wave_step", C.c_int, [_P, _P, _P, _U32, _P, C.c_float, C.c_float, C.c_float, _P]),
     ("rq_build", C.c_int, [_P, _P, _U32, _U32, _P, _U32, _U32, _U32, C.POINTER(_P), _P]),
     ("rq_collapse4", C.c_int, [_P, _P, _P]),
     ("rq_refit", C.c_int, [_P, _P, _P, _U32, _P, _P]),
@@ -121,6 +128,12 @@ SIGNATURES = [
     ("rq_build_radv", C.c_int, [_P, _P, _U32, _P, C.c_uint64, _P]),
     ("rq_trace_radv", C.c_int, [_P, _P, C.c_uint64, _P, _U32, _U32, _P, _P, _P]),
     ("rq_build_radv_noalloc", C.c_int, [_P, _U32, _P, C.c_uint64, _P]),
+    ("rq_batch_create", C.c_int, [_P, C.POINTER(MeshDesc), _U32, _U32, C.POINTER(_P)]),
+    ("rq_batch_build", C.c_int, [_P, _P, _P, _U32, _P, _P]),
+    ("rq_batch_trace", C.c_int, [_P, _P, _P, _P, _P, _U32, _U32, _P, _P, _P]),
+    ("rq_batch_info_get", C.c_int, [_P, _U32, C.POINTER(BvhInfo)]),
+    ("rq_batch_download", C.c_int, [_P, _U32, C.c_int, _P, _U32, _P, _U32, _P, _U32, _P, _U32]),
+    ("rq_batch_destroy", C.c_int, [_P]),
 ]
 
 RADV_NOALLOC_MAX_TRIANGLES = 1 << 24
@@ -285,6 +298,58 @@ class Bvh:
             pass
 
 
+class Batch:
+    """An rq_batch handle: many meshes' BVHs, built by one launch."""
+
+    def __init__(self, ctx, meshes, max_leaf=4):
+        """meshes: sequence of (vertex_offset, num_vertices, triangle_offset, num_triangles)."""
+        arr = (MeshDesc * len(meshes))(*[MeshDesc(*m) for m in meshes])
+        h = _P()
+        ctx.check(lib().rq_batch_create(ctx.h, arr, len(meshes), max_leaf, C.byref(h)), "rq_batch_create")
+        self.ctx, self.h, self.meshes = ctx, h, list(meshes)
+
+    def build(self, pos, idx, stride_bytes=12, stream=None):
+        self.ctx.check(lib().rq_batch_build(self.ctx.h, self.h, _ptr(pos), stride_bytes, _ptr(idx), _stream(stream)),
+                       "rq_batch_build")
+
+    def trace(self, rays, ray_mesh, ray_flags=None, flags=0, hits=None, stats=False, stream=None):
+        import torch
+        n = _count(rays, 32)
+        hits = hits if hits is not None else _empty_i32(n, 4, rays.device)
+        s = _empty_i32(n, 4, rays.device) if stats else None
+        rc = lib().rq_batch_trace(self.ctx.h, self.h, _ptr(rays), _ptr(ray_mesh), _ptr(ray_flags), n, flags,
+                                  _ptr(hits), _ptr(s), _stream(stream))
+        self.ctx.check(rc, "rq_batch_trace")
+        return hits, s
+
+    def info(self, m):
+        inf = BvhInfo()
+        self.ctx.check(lib().rq_batch_info_get(self.h, m, C.byref(inf)), "rq_batch_info_get")
+        return {k: getattr(inf, k) for k, _ in BvhInfo._fields_}
+
+    def download(self, m):
+        inf = self.info(m)
+        n2 = np.empty(inf["num_nodes2"], BVH2_NODE)
+        tr = np.empty(inf["num_triangles"], TRIANGLE)
+        n4 = np.empty(inf["num_nodes4"], BVH4_NODE)
+        pm = np.empty(inf["num_triangles"], np.uint32)
+        rc = lib().rq_batch_download(self.h, m, 1, _ptr(n2), len(n2), _ptr(tr), len(tr), _ptr(n4), len(n4),
+                                     _ptr(pm), len(pm))
+        self.ctx.check(rc, "rq_batch_download")
+        return n2, tr, n4, pm
+
+    def destroy(self):
+        if self.h:
+            lib().rq_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
 def _empty_i32(n, cols, device):
     import torch
     return torch.empty((n, cols), dtype=torch.int32, device=device)
@@ -437,6 +502,14 @@ def render_shadow_ao(ctx, bvh, gbuf, params, mask=None, ao=None, counter=None, s
                                    _stream(stream))
     ctx.check(rc, "rq_render_shadow_ao")
     return mask, ao
+
+
+def deform_wave_step(ctx, base, out, state, dt, amp=0.05, freq=1.0, stream=None):
+    """state: int32 CUDA tensor of 2 (t as float bits, work word)."""
+    rc = lib().rq_deform_wave_step(ctx.h, _ptr(base), _ptr(out), base.numel() // 3, _ptr(state), dt, amp, freq,
+                                   _stream(stream))
+    ctx.check(rc, "rq_deform_wave_step")
+    return out
 
 
 def hits_numpy(hits_tensor):

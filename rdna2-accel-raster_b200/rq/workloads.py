@@ -90,3 +90,32 @@ def grid_for_triangles(t):
     qx = max(1, int(math.sqrt(q)))
     qy = max(1, q // qx)
     return qx, qy
+
+
+def batched_meshes(sizes, seed=2):
+    """Concatenate one height-field grid per requested triangle count (mesh m
+    seeded seed*100003 + m).  Returns float32 [V,3] positions, uint32 [T,3]
+    mesh-local indices and the (vertex_offset, num_vertices, triangle_offset,
+    num_triangles) of every mesh."""
+    pos_l, idx_l, descs = [], [], []
+    v_off = t_off = 0
+    for m, t in enumerate(sizes):
+        qx, qy = grid_for_triangles(t)
+        p, i = scene_grid(qx, qy, seed=seed * 100003 + m)
+        pos_l.append(p)
+        idx_l.append(i)
+        descs.append((v_off, len(p), t_off, len(i)))
+        v_off += len(p)
+        t_off += len(i)
+    return np.concatenate(pos_l), np.concatenate(idx_l), descs
+
+
+def batched_rays(descs, per_mesh_any=4096, per_mesh_closest=4096, seed=2):
+    """Downward random rays per mesh (as the plain workload's): the first
+    per_mesh_any of each mesh are any-hit, the rest closest-hit.  Returns
+    float32 [R,8] rays, uint32 mesh index per ray, uint32 flags per ray."""
+    k = per_mesh_any + per_mesh_closest
+    rays = scene_rays_down(len(descs) * k, -1.0, 1.0, -1.0, 1.0, 2.0, 0.3, 0.01, 1000.0, seed)
+    mesh = np.repeat(np.arange(len(descs), dtype=np.uint32), k)
+    flags = np.tile(np.r_[np.ones(per_mesh_any, np.uint32), np.zeros(per_mesh_closest, np.uint32)], len(descs))
+    return rays, mesh, flags

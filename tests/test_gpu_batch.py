@@ -1,0 +1,98 @@
+"""GPU parity of the batched form: one persistent launch builds many meshes,
+one launch traces rays of all of them.  Every mesh's bytes must equal a
+separate rq_build of that mesh (itself bit-exact with the oracle), and every
+hit must equal a separate rq_trace on that mesh."""
+import numpy as np
+import pytest
+import torch
+
+import pyoracle as O
+import rq
+from rq import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def make_batch(ctx, sizes, seed=5):
+    pos, idx, descs = W.batched_meshes(sizes, seed=seed)
+    p = torch.from_numpy(pos).cuda()
+    i = torch.from_numpy(idx.view(np.int32)).cuda()
+    b = rq.Batch(ctx, descs)
+    b.build(p, i)
+    ctx.sync_check()
+    return pos, idx, descs, p, i, b
+
+
+SIZES = [2, 4, 6, 64, 100, 998, 4096, 20000, 65536, 3, 130]
+
+
+def test_batch_bytes_equal_separate_builds(ctx):
+    pos, idx, descs, p, i, b = make_batch(ctx, SIZES)
+    for m, (vo, nv, to, nt) in enumerate(descs):
+        pm, im = pos[vo:vo + nv], idx[to:to + nt]
+        s = rq.Bvh.build(ctx, torch.from_numpy(pm).cuda(), torch.from_numpy(im.view(np.int32)).cuda())
+        got = b.download(m)
+        want = s.download()
+        for g, w, name in zip(got, want, ("nodes2", "tris", "nodes4", "perm")):
+            assert g.tobytes() == w.tobytes(), f"mesh {m} ({nt} triangles): {name} differs"
+        assert b.info(m)["depth4"] == s.info()["depth4"]
+        s.destroy()
+    # and one mesh against the oracle directly
+    vo, nv, to, nt = descs[7]
+    o = O.lbvh_build(pos[vo:vo + nv].reshape(-1), idx[to:to + nt].reshape(-1))
+    n2, tr, n4, pm = b.download(7)
+    assert n2.tobytes() == o["nodes2"].tobytes() and n4.tobytes() == o["nodes4"].tobytes()
+    b.destroy()
+
+
+def test_batch_rebuild_is_stable(ctx):
+    pos, idx, descs, p, i, b = make_batch(ctx, SIZES)
+    first = [b.download(m) for m in range(len(descs))]
+    b.build(p, i)
+    ctx.sync_check()
+    for m in range(len(descs)):
+        assert all(x.tobytes() == y.tobytes() for x, y in zip(first[m], b.download(m)))
+    b.destroy()
+
+
+@pytest.mark.parametrize("tri_flags", [0, rq.RQ_TRI_MT])
+def test_batch_trace_equals_separate_traces(ctx, tri_flags):
+    pos, idx, descs, p, i, b = make_batch(ctx, SIZES)
+    rays, mesh, flags = W.batched_rays(descs, 500, 700, seed=11)
+    rays_t = torch.from_numpy(rays).cuda()
+    hits, stats = b.trace(rays_t, torch.from_numpy(mesh.view(np.int32)).cuda(),
+                          torch.from_numpy(flags.view(np.int32)).cuda(), flags=tri_flags, stats=True)
+    h = rq.hits_numpy(hits)
+    st = rq.stats_numpy(stats)
+    for m, (vo, nv, to, nt) in enumerate(descs):
+        s = rq.Bvh.build(ctx, torch.from_numpy(pos[vo:vo + nv]).cuda(),
+                         torch.from_numpy(idx[to:to + nt].view(np.int32)).cuda())
+        sel = np.nonzero(mesh == m)[0]
+        for f in (0, 1):
+            part = sel[flags[sel] == f]
+            hh, _, ss = rq.trace(ctx, s, torch.from_numpy(rays[part]).cuda(), flags=f | tri_flags, stats=True)
+            assert rq.hits_numpy(hh).tobytes() == h[part].tobytes(), (m, f)
+            assert rq.stats_numpy(ss).tobytes() == st[part].tobytes(), (m, f)
+        s.destroy()
+    assert 0.3 < h["hit"].mean() < 0.9
+    b.destroy()
+
+
+def test_batched_workload_sampled(ctx):
+    # the batched configuration's 512 meshes (log-uniform 64..65,536), one build
+    sizes = W.batched_sizes(512, seed=2)
+    pos, idx, descs, p, i, b = make_batch(ctx, sizes, seed=2)
+    rng = np.random.default_rng(1)
+    for m in rng.choice(len(descs), 6, replace=False):
+        vo, nv, to, nt = descs[m]
+        o = O.lbvh_build(pos[vo:vo + nv].reshape(-1), idx[to:to + nt].reshape(-1))
+        n2, tr, n4, pm = b.download(int(m))
+        assert n2.tobytes() == o["nodes2"].tobytes() and n4.tobytes() == o["nodes4"].tobytes(), m
+    b.destroy()
+
+
+def test_batch_rejects_bad_descriptors(ctx):
+    with pytest.raises(rq.RqError):
+        rq.Batch(ctx, [(0, 3, 0, 2), (0, 3, 1, 2)])  # overlapping triangle ranges
+    with pytest.raises(rq.RqError):
+        rq.Batch(ctx, [(0, 3, 0, 0)])  # empty mesh

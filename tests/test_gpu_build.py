@@ -173,6 +173,23 @@ def test_deform_matches_oracle_sin(ctx):
     assert np.array_equal(got[:, 2], want) and np.array_equal(got[:, :2], pos[:, :2])
 
 
+def test_deform_step_advances_device_time(ctx):
+    pos, _ = rq.scene_grid(100, 100, seed=2)
+    p = torch.from_numpy(pos).cuda()
+    q = torch.empty_like(p)
+    want = torch.empty_like(p)
+    state = torch.zeros(2, dtype=torch.int32, device="cuda")
+    state[0] = int(np.float32(0.3).view(np.int32))
+    for k in range(3):
+        rq.deform_wave_step(ctx, p, q, state, 0.1)
+        t = np.float32(0.3)
+        for _ in range(k):
+            t = np.float32(t + np.float32(0.1))
+        rq.deform_wave(ctx, p, want, float(t), 0.05, 1.0)
+        assert torch.equal(q, want), k
+    assert int(state[1].item()) == 0
+
+
 def test_bad_arguments_fail_loudly(ctx):
     p = torch.zeros(9, dtype=torch.float32, device="cuda")
     with pytest.raises(rq.RqError) as e:
