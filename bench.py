@@ -348,6 +348,7 @@ def run_ours(args, world, rank, local, pg):
     del p_d, i_d, gbuf, mask, ao
     vis = run_visibility(ctx, dev, stream) if not args.no_extra else None
     batched = run_batched(ctx, dev) if not args.no_extra else None
+    serving = run_serving(dev) if not args.no_extra else None
 
     if rank != 0:
         return
@@ -411,6 +412,7 @@ def run_ours(args, world, rank, local, pg):
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "visibility": vis,
         "batched": batched,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
@@ -538,6 +540,97 @@ def run_batched(ctx, dev, steps=200, plain_steps=20):
         h.destroy()
     batch.destroy()
     return out
+
+
+def run_serving(dev, duration_s=2.0, catalogue=256):
+    """Serving: Poisson 2,000 requests/s for `duration_s` (seed 4) over a
+    catalogue of 256 height-field meshes with triangle counts log-uniform in
+    [64, 1M]; rays per request log-uniform in [1k, 2M]; 50 % shadow, 30 % AO,
+    20 % closest hit, rays generated inside the traversal launch.  BVHs stay
+    resident (120 GB budget, LRU eviction); every mesh is built once before
+    the timed stream.  Batched: up to 1,024 requests / 16M rays per launch,
+    4 launches in flight.  Plain: one request per launch, one in flight.
+    Latency = completion seen by the host - submission at the arrival time.
+    Also a saturation run (every request at t=0) for throughput."""
+    import numpy as np
+    import torch
+    import rq
+    from rq import workloads as W
+
+    sizes = W.serving_catalogue(catalogue, seed=4)
+    meshes = [W.serving_mesh(sizes, m, seed=4) for m in range(catalogue)]
+    t_arr, mesh, kind, nrays, seeds = W.serving_requests(catalogue, duration_s, seed=4)
+    n = len(t_arr)
+    ring = 1 << 27  # hit slots reused round-robin (results are left on the device)
+    hits = torch.empty((ring, 4), dtype=torch.int32, device=dev)
+    offs, o = [], 0
+    for c in nrays:
+        if o + c > ring:
+            o = 0
+        offs.append(o)
+        o += int(c)
+    base = hits.data_ptr()
+
+    def make_reqs(srv, ids):
+        return [rq.Request(ids[int(mesh[i])], int(kind[i]), int(nrays[i]), int(seeds[i]), 0, 0, None,
+                           base + 16 * offs[i], i) for i in range(n)]
+
+    def one(mode):
+        cfg = dict(mode=mode, budget_bytes=120 << 30, slots=4, max_wave_rays=1 << 24, max_wave_requests=1024)
+        srv = rq.Server(**cfg)
+        ids = [srv.add_mesh(p, i) for p, i in meshes]
+        # warm the resident cache: one 1,000-ray request per mesh
+        t0 = srv.now()
+        for m in range(catalogue):
+            srv.submit(rq.Request(ids[m], 3, 1000, 1, 0, 0, None, base, 0))
+        warm = srv.completions()
+        t_warm = srv.now() - t0
+        st0 = srv.stats()
+        reqs = make_reqs(srv, ids)
+        tickets = srv.replay(reqs, t_arr)
+        comp = srv.completions()
+        st1 = srv.stats()
+        lat = np.array([comp[t]["t_done"] - comp[t]["t_submit"] for t in tickets])
+        ok = all(comp[t]["status"] == 0 for t in tickets) and all(c["status"] == 0 for c in warm.values())
+        t_first = min(comp[t]["t_submit"] for t in tickets)
+        t_last = max(comp[t]["t_done"] for t in tickets)
+        stream = {"p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                  "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                  "mean_ms": round(float(lat.mean()) * 1e3, 3),
+                  "mrays_per_s": round(float(nrays.sum()) / (t_last - t_first) / 1e6, 1),
+                  "requests_per_s": round(n / (t_last - t_first), 1),
+                  "launches": int(st1["launches"] - st0["launches"]),
+                  "requests_per_launch": round(n / max(1, st1["launches"] - st0["launches"]), 2),
+                  "all_ok": bool(ok)}
+        # saturation: the same requests, all at t = 0
+        tickets = srv.replay(reqs, np.zeros(n))
+        comp = srv.completions()
+        t_first = min(comp[t]["t_submit"] for t in tickets)
+        t_last = max(comp[t]["t_done"] for t in tickets)
+        lat = np.array([comp[t]["t_done"] - comp[t]["t_submit"] for t in tickets])
+        sat = {"makespan_ms": round((t_last - t_first) * 1e3, 2),
+               "mrays_per_s": round(float(nrays.sum()) / (t_last - t_first) / 1e6, 1),
+               "requests_per_s": round(n / (t_last - t_first), 1),
+               "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+               "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3)}
+        st = srv.stats()
+        srv.close()
+        return {"stream": stream, "saturation": sat, "warm_build_s": round(t_warm, 3),
+                "resident_gb": round(st["peak_resident_bytes"] / 1e9, 2), "builds": int(st["builds"])}
+
+    b = one(rq.RQ_SERVE_BATCHED)
+    p = one(rq.RQ_SERVE_PLAIN)
+    torch.cuda.synchronize(dev)
+    return {
+        "workload": (f"serving: Poisson {W.SERVE_RATE:.0f} req/s for {duration_s:g} s (seed 4, {n} requests), "
+                     f"{catalogue} resident height-field meshes with triangle counts log-uniform in [64, 1M] "
+                     f"(mean {sizes.mean() / 1e3:.1f}k), rays log-uniform in [1k, 2M] (mean {nrays.mean() / 1e3:.1f}k), "
+                     "50% shadow / 30% AO / 20% closest hit generated in the launch; 120 GB budget"),
+        "requests": n, "rays": int(nrays.sum()), "catalogue_triangles": int(sizes.sum()),
+        "batched": b, "plain": p,
+        "stream_p99_ratio_plain_over_batched": round(p["stream"]["p99_ms"] / b["stream"]["p99_ms"], 2),
+        "saturation_throughput_ratio": round(b["saturation"]["mrays_per_s"] / p["saturation"]["mrays_per_s"], 2),
+    }
 
 
 def run_visibility(ctx, dev, stream, frames=200):

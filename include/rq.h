@@ -280,7 +280,7 @@ typedef struct rq_light {
 /* Shadow and ambient-occlusion parameters.  Per pixel with a hit, light k
  * casts an any-hit shadow ray when dist in [0.001, radius] and N.L > 0, from
  * P + shadow_bias*N with [shadow_tmin, dist - shadow_bias]
- * (shaders/tiled_lighting_ra.comp:223-253); ao_spp cosine-weighted any-hit
+ * (shaders/tiled_lighting_ra.comp:118-148); ao_spp cosine-weighted any-hit
  * rays from P + ao_bias*N with [ao_tmin, ao_tmax], seeded y*W + x + 5544
  * (shaders/rq_ao.comp:18-94). */
 typedef struct rq_shade_params {

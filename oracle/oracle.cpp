@@ -1062,6 +1062,66 @@ void orc_gen_rays_procedural(const float cam[3], const float look[3], uint32_t c
 
 void orc_sincos(float x, float* s, float* c) { sincos_taylor(x, s, c); }
 
+// The generated rays of the serving requests (kind 1 shadow, 2 AO, 3
+// closest), ray i from draws pcg_hash(base + k) / 2^32 with
+// base = pcg_hash(seed ^ pcg_hash(i)).  Shadow and AO rays start on a point
+// of triangle pcg_hash(base + 7) % ntri (folded barycentrics, face normal
+// turned to +z): shadow toward a light in [-1,1]^2 x [2,2.5] from P + 0.04 N
+// over [0.01, dist - 0.04] (shaders/tiled_lighting_ra.comp:118-148); AO a
+// cosine-hemisphere direction from P + 0.03 N over [0.01, 0.5]
+// (shaders/rq_ao.comp:32-45, 77-86).  any[i] = 1 for any-hit rays.
+void orc_gen_mesh_rays(const float* pos, const uint32_t* idx, uint32_t ntri, uint32_t kind, uint32_t seed,
+                       uint32_t n, rq_ray* rays, uint32_t* any) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t base = pcg_hash(seed ^ pcg_hash(i));
+        auto draw = [&](uint32_t k) { return float(pcg_hash(base + k)) * kInv2Pow32; };
+        V3 o, d;
+        float tmin = 0.01f, tmax;
+        if (kind == 3u) {
+            o = {-1.0f + 2.0f * draw(0), -1.0f + 2.0f * draw(1), 2.0f};
+            d = normalize(V3{-0.3f + 0.6f * draw(2), -0.3f + 0.6f * draw(3), -1.0f});
+            tmax = 1000.0f;
+        } else {
+            const uint32_t t = pcg_hash(base + 7u) % ntri;
+            auto vtx = [&](uint32_t v) { return V3{pos[3ull * v], pos[3ull * v + 1], pos[3ull * v + 2]}; };
+            const V3 v0 = vtx(idx[3ull * t]), v1 = vtx(idx[3ull * t + 1]), v2 = vtx(idx[3ull * t + 2]);
+            float a = draw(0), b = draw(1);
+            if (a + b > 1.0f) {
+                a = 1.0f - a;
+                b = 1.0f - b;
+            }
+            const V3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+            const V3 P{v0.x + (e1.x * a + e2.x * b), v0.y + (e1.y * a + e2.y * b), v0.z + (e1.z * a + e2.z * b)};
+            V3 N = normalize(cross(e1, e2));
+            if (N.z < 0.0f) N = {-N.x, -N.y, -N.z};
+            if (kind == 1u) {
+                const V3 L{-1.0f + 2.0f * draw(2), -1.0f + 2.0f * draw(3), 2.0f + 0.5f * draw(4)};
+                const V3 tl = sub(L, P);
+                const float dist = std::sqrt(dot(tl, tl));
+                d = {tl.x / dist, tl.y / dist, tl.z / dist};
+                o = {P.x + N.x * 0.04f, P.y + N.y * 0.04f, P.z + N.z * 0.04f};
+                tmax = dist - 0.04f;
+            } else {
+                const float u1 = draw(2), u2 = draw(3);
+                const float rr = std::sqrt(u1);
+                const float theta = 6.2831853f * u2;
+                float sn, cs;
+                sincos_taylor(theta, &sn, &cs);
+                const float x = rr * cs, y = rr * sn, z = std::sqrt(fmax_(0.0f, 1.0f - u1));
+                const V3 up = std::fabs(N.z) < 0.999f ? V3{0.0f, 0.0f, 1.0f} : V3{1.0f, 0.0f, 0.0f};
+                const V3 tg = normalize(cross(up, N));
+                const V3 bt = cross(N, tg);
+                d = normalize(V3{(tg.x * x + bt.x * y) + N.x * z, (tg.y * x + bt.y * y) + N.y * z,
+                                 (tg.z * x + bt.z * y) + N.z * z});
+                o = {P.x + N.x * 0.03f, P.y + N.y * 0.03f, P.z + N.z * 0.03f};
+                tmax = 0.5f;
+            }
+        }
+        rays[i] = rq_ray{{o.x, o.y, o.z}, tmin, {d.x, d.y, d.z}, tmax};
+        if (any) any[i] = kind == 3u ? 0u : 1u;
+    }
+}
+
 // Primary rays of visbuf_raycast.comp:15-51 (optional per-pixel jitter),
 // closest hit with the engine traversal, G-buffer pixel as rq_render_gbuffer
 // writes it.  `pixels` lists the pixel indices to evaluate (NULL = all);
@@ -1105,7 +1165,7 @@ void orc_render_gbuffer(const rq_bvh4_node* nodes, const rq_triangle* tris, cons
     });
 }
 
-// Shadow rays of tiled_lighting_ra.comp:223-253 and AO rays of
+// Shadow rays of shaders/tiled_lighting_ra.comp:118-148 and AO rays of
 // rq_ao.comp:18-94 for the listed pixels of a full-size G-buffer.
 void orc_render_shadow_ao(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq_gbuffer_px* gbuf,
                           const rq_shade_params* prm, const uint32_t* pixels, uint32_t npix, uint32_t* mask, float* ao,

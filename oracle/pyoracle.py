@@ -57,6 +57,7 @@ def lib():
         L.orc_trace_radv.argtypes = [_P, _P, C.c_uint32, C.c_uint32, _P, _P, C.c_int]
         L.orc_gen_rays_procedural.argtypes = [_P, _P, C.c_uint32, C.c_uint32, _P]
         L.orc_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.orc_gen_mesh_rays.argtypes = [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]
         _lib = L
     return _lib
 
@@ -178,6 +179,18 @@ def trace_radv(img, rays, flags=0, want_bary=False):
     lib().orc_trace_radv(_ptr(np.ascontiguousarray(img)), _ptr(rays), len(rays), flags, _ptr(hits), _ptr(bary),
                          threads())
     return hits, bary
+
+
+def gen_mesh_rays(pos, idx, kind, seed, count):
+    """Rays of a generated serving request (kind 1 shadow, 2 AO, 3 closest)
+    and their any-hit flags."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    rays = np.empty(count, RAY)
+    anyf = np.empty(count, np.uint32)
+    lib().orc_gen_mesh_rays(_ptr(pos), _ptr(idx), len(idx.reshape(-1)) // 3, kind, seed, count, _ptr(rays),
+                            _ptr(anyf))
+    return rays, anyf
 
 
 def gen_rays_procedural(cam, look, count, coherent):

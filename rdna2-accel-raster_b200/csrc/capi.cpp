@@ -41,9 +41,11 @@ void free_arrays(rq_bvh* b) {
     b->capacity = 0;
 }
 
-// One allocation carved into the layouts: capacity N triangles, node2_cap
-// binary nodes, node4_cap 4-wide nodes.
-int alloc_arrays(rq_ctx* ctx, rq_bvh* b, uint32_t n, uint32_t node2_cap, uint32_t node4_cap) {
+}  // namespace
+
+// Bytes of the one allocation behind a handle: capacity N triangles,
+// node2_cap binary nodes, node4_cap 4-wide nodes.
+size_t rq_bvh_alloc_bytes(uint32_t n, uint32_t node2_cap, uint32_t node4_cap) {
     Carve c{0, 0};
     c.take<rq_bvh2_node>(node2_cap);
     c.take<rq_triangle>(n);
@@ -52,7 +54,14 @@ int alloc_arrays(rq_ctx* ctx, rq_bvh* b, uint32_t n, uint32_t node2_cap, uint32_
     c.take<rq_bvh4_node>(node4_cap);
     c.take<int32_t>(4ull * node4_cap);
     c.take<uint32_t>(4);
-    size_t bytes = c.off + 256;
+    return c.off + 256;
+}
+
+namespace {
+
+// One allocation carved into the layouts.
+int alloc_arrays(rq_ctx* ctx, rq_bvh* b, uint32_t n, uint32_t node2_cap, uint32_t node4_cap) {
+    size_t bytes = rq_bvh_alloc_bytes(n, node2_cap, node4_cap);
     void* mem = nullptr;
     cudaError_t e = cudaMalloc(&mem, bytes);
     if (e != cudaSuccess) {

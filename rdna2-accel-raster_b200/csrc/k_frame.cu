@@ -6,7 +6,7 @@
 //               camera-facing face normal, t.  Camera rays are coherent, so
 //               the one-ray-per-thread schedule of trace_core.cuh wins.
 //  k_shadow_ao  the any-hit shadow rays of shaders/tiled_lighting_ra.comp:
-//               223-253 and the cosine-hemisphere AO rays of
+//               118-148 and the cosine-hemisphere AO rays of
 //               shaders/rq_ao.comp:18-94, generated from the G-buffer inside
 //               the kernel, on the refilling schedule of trace_engine.cuh
 //               (a pixel's rays differ in length, so lanes must not wait for
@@ -121,16 +121,7 @@ __device__ __forceinline__ rq::F3 hemisphere(rq::F3 N, uint32_t pixel, uint32_t 
     for (uint32_t i = 0; i < 2 * s; ++i) seed = rq::ao_hash(seed);
     const float u1 = ao_rand(seed);
     const float u2 = ao_rand(seed);
-    const float r = sqrtf(u1);
-    const float theta = 6.2831853f * u2;
-    float sn, cs;
-    rq::sincos_taylor(theta, &sn, &cs);
-    const float x = r * cs, y = r * sn, z = sqrtf(fmaxf(0.0f, 1.0f - u1));
-    const rq::F3 up = fabsf(N.z) < 0.999f ? rq::F3{0.0f, 0.0f, 1.0f} : rq::F3{1.0f, 0.0f, 0.0f};
-    const rq::F3 tg = rq::f3norm(rq::f3cross(up, N));
-    const rq::F3 bt = rq::f3cross(N, tg);
-    return rq::f3norm(rq::F3{(tg.x * x + bt.x * y) + N.x * z, (tg.y * x + bt.y * y) + N.y * z,
-                             (tg.z * x + bt.z * y) + N.z * z});
+    return rq::cosine_hemisphere(N, u1, u2);
 }
 
 template <bool STATS>

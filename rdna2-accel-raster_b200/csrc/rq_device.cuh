@@ -234,6 +234,22 @@ __device__ __forceinline__ void sincos_taylor(float x, float* s, float* c) {
     *c = q == 0 ? pc : (q == 1 ? -ps : (q == 2 ? -pc : ps));
 }
 
+// Cosine-weighted direction about the unit normal N from two draws in [0,1]
+// (the hemisphere sample of shaders/rq_ao.comp:32-45: r = sqrt(u1),
+// theta = 2 pi u2, tangent frame from the cross product with z or x).
+__device__ __forceinline__ F3 cosine_hemisphere(F3 N, float u1, float u2) {
+    const float r = sqrtf(u1);
+    const float theta = 6.2831853f * u2;
+    float sn, cs;
+    sincos_taylor(theta, &sn, &cs);
+    const float x = r * cs, y = r * sn, z = sqrtf(fmaxf(0.0f, 1.0f - u1));
+    const F3 up = fabsf(N.z) < 0.999f ? F3{0.0f, 0.0f, 1.0f} : F3{1.0f, 0.0f, 0.0f};
+    const F3 tg = f3norm(f3cross(up, N));
+    const F3 bt = f3cross(N, tg);
+    return f3norm(F3{(tg.x * x + bt.x * y) + N.x * z, (tg.y * x + bt.y * y) + N.y * z,
+                     (tg.z * x + bt.z * y) + N.z * z});
+}
+
 // ------------------------------------------------------------ bounded wait
 // Iteration cap for spin-waits on flags written by other blocks of the same
 // launch: with __nanosleep(64) it is several seconds, far beyond any

@@ -19,7 +19,8 @@
 // A ray source provides:
 //   uint32_t total;                                 number of ray ids
 //   bool make(uint32_t id, Ray& r, Meta& m);        false = no ray for this id
-//   void finish(uint32_t id, const Meta& m, const Hit& h);
+//   void finish(uint32_t id, const Meta& m, const Ray& r, const Hit& h);
+//   optional: kRoundEnd = true and void round_end(bool finished, const Meta& m).
 #pragma once
 
 #include "rq_device.cuh"
@@ -50,6 +51,18 @@ struct IsMulti {
 template <class Src>
 struct IsMulti<Src, decltype(void(Src::kMulti))> {
     static constexpr bool value = Src::kMulti;
+};
+
+// Sources with kRoundEnd get round_end(finished, meta) once per round from
+// all 32 lanes together (finished: this lane reported a ray this round;
+// meta: that ray's), e.g. to count completions with one atomic per group.
+template <class Src, class = void>
+struct HasRoundEnd {
+    static constexpr bool value = false;
+};
+template <class Src>
+struct HasRoundEnd<Src, decltype(void(Src::kRoundEnd))> {
+    static constexpr bool value = Src::kRoundEnd;
 };
 
 struct Hit {
@@ -215,10 +228,16 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
         }
 
         // ---- report finished rays
+        bool fin = false;
         if (active && (done || sp == 0)) {
             h.t = best;
             src.finish(rid, meta, ray, h);
             active = false;
+            fin = true;
+        }
+        if constexpr (HasRoundEnd<Src>::value) {
+            __syncwarp();
+            src.round_end(fin, meta);
         }
     }
 }

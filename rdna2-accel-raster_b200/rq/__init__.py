@@ -91,6 +91,29 @@ class MeshDesc(C.Structure):
                 ("num_triangles", C.c_uint32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("mode", C.c_uint32), ("slots", C.c_uint32),
+                ("max_wave_rays", C.c_uint32), ("max_wave_requests", C.c_uint32), ("max_leaf", C.c_uint32),
+                ("trace_flags", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("mesh", C.c_uint32), ("kind", C.c_uint32), ("num_rays", C.c_uint32), ("seed", C.c_uint32),
+                ("flags", C.c_uint32), ("reserved", C.c_uint32), ("rays", C.c_void_p), ("hits", C.c_void_p),
+                ("user", C.c_uint64)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("user", C.c_uint64), ("status", C.c_int32), ("built", C.c_uint32),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "failed", "launches", "builds", "evictions",
+                                          "rays", "resident_bytes", "peak_resident_bytes",
+                                          "max_requests_per_launch", "max_launches_in_flight")]
+
+
 _P = C.c_void_p
 _U32 = C.c_uint32
 # (name, restype, argtypes) for every entry point in include/rq.h
@@ -134,7 +157,27 @@ SIGNATURES = [
     ("rq_batch_info_get", C.c_int, [_P, _U32, C.POINTER(BvhInfo)]),
     ("rq_batch_download", C.c_int, [_P, _U32, C.c_int, _P, _U32, _P, _U32, _P, _U32, _P, _U32]),
     ("rq_batch_destroy", C.c_int, [_P]),
+    # include/rq_serve.h
+    ("rq_server_create", C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_P)]),
+    ("rq_server_destroy", C.c_int, [_P]),
+    ("rq_server_add_mesh", C.c_int, [_P, _P, _U32, _P, _U32, C.POINTER(_U32)]),
+    ("rq_server_mesh_bytes", C.c_uint64, [_U32, _U32]),
+    ("rq_server_submit", C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    ("rq_server_replay", C.c_int, [_P, C.POINTER(Request), _P, _U32, _P]),
+    ("rq_server_poll", C.c_int, [_P, C.POINTER(Completion), _U32, C.POINTER(_U32)]),
+    ("rq_server_drain", C.c_int, [_P, _U32]),
+    ("rq_server_now", C.c_double, [_P]),
+    ("rq_server_stats_get", C.c_int, [_P, C.POINTER(ServerStats)]),
+    ("rq_server_last_error", C.c_char_p, [_P]),
+    ("rq_gen_mesh_rays", C.c_int, [_P, _P, _P, _U32, _U32, _U32, _U32, _P, _P, _P]),
 ]
+
+RQ_RAYS_BUFFER = 0
+RQ_RAYS_SHADOW = 1
+RQ_RAYS_AO = 2
+RQ_RAYS_CLOSEST = 3
+RQ_SERVE_BATCHED = 0
+RQ_SERVE_PLAIN = 1
 
 RADV_NOALLOC_MAX_TRIANGLES = 1 << 24
 
@@ -523,3 +566,114 @@ def stats_numpy(stats_tensor):
 
 def rays_numpy(rays_tensor):
     return rays_tensor.cpu().numpy().view(RAY).reshape(-1)
+
+
+def gen_mesh_rays(ctx, pos, idx, kind, seed, count, stream=None):
+    """The rays a generated serving request of `kind` traces on the mesh
+    (pos float32 [V,3], idx int32/uint32 [T,3] CUDA tensors): float32 [count,8]
+    rays and int32 [count] any-hit flags."""
+    import torch
+    rays = torch.empty((count, 8), dtype=torch.float32, device=pos.device)
+    anyf = torch.empty(count, dtype=torch.int32, device=pos.device)
+    ntri = _count(idx, 12) if idx is not None else 0
+    rc = lib().rq_gen_mesh_rays(ctx.h, _ptr(pos), _ptr(idx), ntri, kind, seed, count, _ptr(rays), _ptr(anyf),
+                                _stream(stream))
+    ctx.check(rc, "rq_gen_mesh_rays")
+    return rays, anyf
+
+
+class ServeError(RqError):
+    pass
+
+
+class Server:
+    """An rq_server (include/rq_serve.h): a request loop with resident BVHs,
+    a memory budget and coalesced traversal launches."""
+
+    def __init__(self, device=0, budget_bytes=120 << 30, mode=RQ_SERVE_BATCHED, slots=4, max_wave_rays=1 << 24,
+                 max_wave_requests=1024, max_leaf=4, trace_flags=0):
+        cfg = ServerConfig(budget_bytes, mode, slots, max_wave_rays, max_wave_requests, max_leaf, trace_flags)
+        h = _P()
+        rc = lib().rq_server_create(device, C.byref(cfg), C.byref(h))
+        if rc:
+            raise ServeError(rc, f"rq_server_create: {lib().rq_status_string(rc).decode()}")
+        self.h = h
+        self._keep = []
+
+    def _check(self, rc, what):
+        if rc:
+            err = lib().rq_server_last_error(self.h).decode()
+            raise ServeError(rc, f"{what}: {lib().rq_status_string(rc).decode()} {err}")
+
+    @staticmethod
+    def mesh_bytes(num_vertices, num_triangles):
+        return int(lib().rq_server_mesh_bytes(num_vertices, num_triangles))
+
+    def add_mesh(self, pos, idx):
+        """pos float32 [V,3], idx uint32 [T,3] host arrays -> mesh id."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        idx = np.ascontiguousarray(idx, np.uint32)
+        mid = _U32()
+        self._check(lib().rq_server_add_mesh(self.h, _ptr(pos), len(pos.reshape(-1)) // 3, _ptr(idx),
+                                             len(idx.reshape(-1)) // 3, C.byref(mid)), "rq_server_add_mesh")
+        return mid.value
+
+    @staticmethod
+    def request(mesh, kind, num_rays, hits, seed=0, rays=None, flags=0, user=0):
+        """hits: int32 [num_rays,4] CUDA tensor (kept alive by the caller)."""
+        return Request(mesh, kind, num_rays, seed, flags, 0, _ptr(rays).value if rays is not None else None,
+                       _ptr(hits).value, user)
+
+    def submit(self, req):
+        t = C.c_uint64()
+        self._check(lib().rq_server_submit(self.h, C.byref(req), C.byref(t)), "rq_server_submit")
+        return t.value
+
+    def replay(self, reqs, arrival):
+        """Submit reqs[i] at arrival[i] seconds from now (ascending); returns tickets."""
+        n = len(reqs)
+        arr = (Request * n)(*reqs)
+        at = np.ascontiguousarray(arrival, np.float64)
+        tickets = np.zeros(n, np.uint64)
+        self._check(lib().rq_server_replay(self.h, arr, _ptr(at), n, _ptr(tickets)), "rq_server_replay")
+        return tickets
+
+    def poll(self, capacity=4096):
+        out = (Completion * capacity)()
+        n = _U32()
+        self._check(lib().rq_server_poll(self.h, out, capacity, C.byref(n)), "rq_server_poll")
+        return [out[i] for i in range(n.value)]
+
+    def drain(self, timeout_ms=120000):
+        self._check(lib().rq_server_drain(self.h, timeout_ms), "rq_server_drain")
+
+    def completions(self):
+        """Drain, then every completion as a dict keyed by ticket."""
+        self.drain()
+        res = {}
+        while True:
+            got = self.poll()
+            if not got:
+                break
+            for c in got:
+                res[c.ticket] = {k: getattr(c, k) for k, _ in Completion._fields_}
+        return res
+
+    def now(self):
+        return lib().rq_server_now(self.h)
+
+    def stats(self):
+        s = ServerStats()
+        self._check(lib().rq_server_stats_get(self.h, C.byref(s)), "rq_server_stats_get")
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().rq_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

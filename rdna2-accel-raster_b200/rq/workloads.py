@@ -119,3 +119,37 @@ def batched_rays(descs, per_mesh_any=4096, per_mesh_closest=4096, seed=2):
     mesh = np.repeat(np.arange(len(descs), dtype=np.uint32), k)
     flags = np.tile(np.r_[np.ones(per_mesh_any, np.uint32), np.zeros(per_mesh_closest, np.uint32)], len(descs))
     return rays, mesh, flags
+
+
+# ------------------------------------------------------------------ serving
+SERVE_RATE = 2000.0          # requests per second (Poisson)
+SERVE_MIX = (0.5, 0.3, 0.2)  # shadow, AO, closest hit
+
+
+def serving_catalogue(count=256, seed=4):
+    """Triangle counts of the served meshes, log-uniform in [64, 1M]; mesh m
+    is the height-field grid seeded seed*100003 + m.  A request draws its mesh
+    uniformly from the catalogue, so request meshes are log-uniform in
+    [64, 1M] too, and each mesh is reused by many requests."""
+    rng = np.random.default_rng(seed)
+    return np.maximum(64, log_uniform_int(rng, 64, 1 << 20, count) // 2 * 2)
+
+
+def serving_mesh(sizes, m, seed=4):
+    qx, qy = grid_for_triangles(sizes[m])
+    return scene_grid(qx, qy, seed=seed * 100003 + m)
+
+
+def serving_requests(n_meshes, duration_s=2.0, rate=SERVE_RATE, seed=4):
+    """Poisson arrivals at `rate` over `duration_s`: arrival times (s), mesh
+    index, kind (1 shadow, 2 AO, 3 closest), ray count log-uniform in
+    [1000, 2M], per-request seed."""
+    rng = np.random.default_rng(seed + 1)
+    gaps = rng.exponential(1.0 / rate, size=int(rate * duration_s * 1.5) + 16)
+    t = np.cumsum(gaps)
+    t = t[t < duration_s]
+    n = len(t)
+    mesh = rng.integers(0, n_meshes, n)
+    kind = rng.choice([1, 2, 3], size=n, p=list(SERVE_MIX))
+    rays = log_uniform_int(rng, 1000, 2_000_000, n)
+    return t, mesh, kind, rays, np.arange(n, dtype=np.uint32) + 1
