@@ -452,6 +452,17 @@ def run_batched(ctx, dev, steps=200, plain_steps=20):
     dt = W.DEFORM_DT
 
     batch = rq.Batch(ctx, descs)
+    # launch shapes: the committed autotuner table, else tune now (untimed)
+    from rq import tune as T
+    key = T.workload_key(descs, 8192)
+    shape = T.lookup(key)
+    if shape is not None:
+        batch.set_tuning(shape)
+        tuning = {"source": "committed table rq/tuning_b200.json", **shape}
+    else:
+        got, trials = batch.autotune(base, i_d, rays_d, mesh_d, flags_d, hits=hits_b, reps=3)
+        tuning = {"source": f"autotuned in this run ({len(trials)} shapes timed)",
+                  **{k: got[k] for k in rq.Batch.TUNING_KEYS}}
 
     def bstep():
         rq.deform_wave_step(ctx, base, cur, state, dt, W.DEFORM_AMP, W.DEFORM_FREQ)
@@ -534,6 +545,7 @@ def run_batched(ctx, dev, steps=200, plain_steps=20):
                   "mode": plain_mode},
         "speedup_p50": round(percentile(pms, 50) / percentile(bms, 50), 2),
         "hits_equal": equal,
+        "tuning": tuning,
     }
     del gb
     for h in handles:

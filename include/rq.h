@@ -239,6 +239,37 @@ int rq_batch_download(rq_batch* batch, uint32_t mesh, int host, rq_bvh2_node* no
                       uint32_t* perm, uint32_t cap_perm);
 int rq_batch_destroy(rq_batch* batch);
 
+/* Launch shapes of a batch's two kernels.  Results do not depend on them. */
+typedef struct rq_batch_tuning {
+    uint32_t build_threads;       /* threads per build block: 256, 512 or 1024 */
+    uint32_t build_blocks;        /* persistent build blocks (clamped to max_build_blocks) */
+    uint32_t trace_threads;       /* threads per traversal block: 64, 128 or 256 */
+    uint32_t trace_chunk;         /* ray ids a warp takes per refill: 32 or 64 */
+    uint32_t trace_reg_cap;       /* 1: launch bounds that hold the kernel to 64 registers */
+    uint32_t trace_blocks_per_sm; /* 0: as many as fit */
+    uint32_t stack_entries;       /* stack entries per lane; 0 or anything below
+                                     3 * (depth + 2) + 1 means that bound */
+    uint32_t max_build_blocks;    /* read only: build scratch slices the batch holds */
+    float build_ms;               /* rq_batch_autotune: measured time of this shape */
+    float trace_ms;
+} rq_batch_tuning;
+
+int rq_batch_tuning_get(const rq_batch* batch, rq_batch_tuning* out);
+/* Validates the shape (RQ_ERR_INVALID_ARG for one that has no kernel). */
+int rq_batch_tuning_set(rq_batch* batch, const rq_batch_tuning* t);
+/* Autotuner: builds the batch and traces the given rays once per candidate
+ * shape — every build block size with 1..occupancy blocks per SM, every
+ * traversal block size x refill chunk x register cap — timing each with CUDA
+ * events (median of `reps`), and keeps the fastest build and traversal shape.
+ * The stack depth is the smallest safe one for the batch's deepest tree.
+ * Writes up to `cap` measured candidates to `trials` (build_ms set for build
+ * shapes, trace_ms for traversal shapes) and their number to *count.
+ * Synchronous; overwrites the batch and `hits`. */
+int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint32_t stride_bytes,
+                      const uint32_t* indices, const rq_ray* rays, const uint32_t* ray_mesh,
+                      const uint32_t* ray_flags, uint32_t n, rq_hit* hits, uint32_t reps, rq_batch_tuning* trials,
+                      uint32_t cap, uint32_t* count, rq_stream stream);
+
 /* ------------------------------------------------------------------ */
 /* Frames: rays generated inside the traversal kernels                 */
 /* ------------------------------------------------------------------ */

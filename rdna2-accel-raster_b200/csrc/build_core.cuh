@@ -143,8 +143,11 @@ __device__ __forceinline__ void leaf_step(uint32_t k, const float* __restrict__ 
 }
 
 // Atomic bottom-up refit from sorted leaf k: at each node the second child
-// to arrive computes the union box and continues upward.  The caller fences
-// the leaf box before the walk.
+// to arrive computes the union box and continues upward.  The arrival count
+// is an acquire-release add: it publishes the box this thread wrote last
+// (the leaf box, then each union) and, for the second arrival, makes the
+// sibling's box visible.  CTA: all leaves of the tree are in this block.
+template <bool CTA = false>
 __device__ __forceinline__ void refit_walk(uint32_t k, const int32_t* kl, const int32_t* kr, const uint32_t* par_in,
                                            const uint32_t* par_lf, float4* box_in, const float4* box_lf,
                                            uint32_t* refit_flag, uint32_t* err) {
@@ -152,8 +155,7 @@ __device__ __forceinline__ void refit_walk(uint32_t k, const int32_t* kl, const 
     uint32_t guard = 0;
     while (par != kNoParent) {
         const uint32_t p = par >> 1;
-        if (atomicAdd(&refit_flag[p], 1u) == 0u) break;
-        __threadfence();
+        if (atom_add_acq_rel<CTA>(&refit_flag[p], 1u) == 0u) break;
         const int32_t a = kl[p], b = kr[p];
         const float4* ba = a < 0 ? box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : box_in + 2 * size_t(a);
         const float4* bb = b < 0 ? box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : box_in + 2 * size_t(b);
@@ -162,7 +164,6 @@ __device__ __forceinline__ void refit_walk(uint32_t k, const int32_t* kl, const 
         __stcg(box_in + 2 * size_t(p), make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f));
         __stcg(box_in + 2 * size_t(p) + 1,
                make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f));
-        __threadfence();
         par = par_in[p];
         if (++guard > 128u) {
             set_err(err, RQ_DERR_REFIT);

@@ -6,6 +6,7 @@
 #include <new>
 #include <numeric>
 #include <string>
+#include <vector>
 
 #include "rq_batch.h"
 
@@ -33,9 +34,163 @@ int sync_batch_counts(rq_batch* b) {
     return RQ_OK;
 }
 
+// Default shapes: 512-thread build blocks, as many as fit; 128-thread
+// traversal blocks, 32-id refills, no register cap.
+rq_batch_tuning default_tuning(rq_ctx* ctx, uint32_t slices) {
+    rq_batch_tuning t{};
+    t.build_threads = 512;
+    t.build_blocks = std::min<uint32_t>(slices, uint32_t(ctx->num_sms) *
+                                                    uint32_t(std::max(1, rq_batch_build_occupancy(512))));
+    t.trace_threads = 128;
+    t.trace_chunk = 32;
+    t.trace_reg_cap = 0;
+    t.trace_blocks_per_sm = 0;
+    t.stack_entries = 0;
+    t.max_build_blocks = slices;
+    return t;
+}
+
+// Median time of `reps` runs of f() on stream st (after one warm-up run).
+template <class F>
+int time_median(rq_ctx* ctx, cudaStream_t st, uint32_t reps, F&& f, float* ms) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
+        return rq_cuda_status(ctx, cudaGetLastError(), "tuning events");
+    std::vector<float> t;
+    int rc = f();
+    for (uint32_t r = 0; r < reps && rc == RQ_OK; ++r) {
+        cudaEventRecord(a, st);
+        rc = f();
+        cudaEventRecord(b, st);
+        if (rc == RQ_OK) {
+            cudaError_t e = cudaEventSynchronize(b);
+            float x = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&x, a, b);
+            if (e != cudaSuccess) rc = rq_cuda_status(ctx, e, "tuning timing");
+            t.push_back(x);
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    std::sort(t.begin(), t.end());
+    *ms = t.empty() ? 0.0f : t[t.size() / 2];
+    return RQ_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int rq_batch_tuning_get(const rq_batch* batch, rq_batch_tuning* out) {
+    if (!batch || !out) return RQ_ERR_INVALID_ARG;
+    *out = batch->tune;
+    out->max_build_blocks = batch->build_slices;
+    return RQ_OK;
+}
+
+int rq_batch_tuning_set(rq_batch* batch, const rq_batch_tuning* t) {
+    if (!batch || !t) return RQ_ERR_INVALID_ARG;
+    if ((t->build_threads != 256 && t->build_threads != 512 && t->build_threads != 1024) || t->build_blocks == 0 ||
+        !rq_batch_trace_shape_ok(t->trace_threads, t->trace_chunk, t->trace_reg_cap) || t->stack_entries > 128)
+        return rq_set_error(batch->ctx, RQ_ERR_INVALID_ARG, "no kernel for this batch shape");
+    const float bm = batch->tune.build_ms, tm = batch->tune.trace_ms;
+    batch->tune = *t;
+    batch->tune.build_ms = bm;
+    batch->tune.trace_ms = tm;
+    batch->tune.max_build_blocks = batch->build_slices;
+    return RQ_OK;
+}
+
+int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint32_t stride_bytes,
+                      const uint32_t* indices, const rq_ray* rays, const uint32_t* ray_mesh,
+                      const uint32_t* ray_flags, uint32_t n, rq_hit* hits, uint32_t reps, rq_batch_tuning* trials,
+                      uint32_t cap, uint32_t* count, rq_stream stream) {
+    if (!ctx || !batch || !positions || !indices || (n && (!rays || !ray_mesh || !hits)) || (cap && !trials) ||
+        !count)
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    reps = std::max(1u, std::min(reps, 50u));
+    *count = 0;
+    int rc = rq_batch_build(ctx, batch, positions, stride_bytes, indices, stream);
+    if (rc == RQ_OK && !batch->counts_valid) rc = sync_batch_counts(batch);
+    if (rc) return rc;
+    const rq_batch_tuning start = batch->tune;
+    auto record = [&](const rq_batch_tuning& t) {
+        if (*count < cap) trials[*count] = t;
+        ++*count;
+    };
+    // build shapes
+    rq_batch_tuning best_b = start;
+    float best_bms = -1.0f;
+    for (uint32_t bt : {256u, 512u, 1024u}) {
+        const int occ = rq_batch_build_occupancy(bt);
+        for (int k = 1; k <= occ; ++k) {
+            rq_batch_tuning t = start;
+            t.build_threads = bt;
+            t.build_blocks = std::min<uint32_t>(batch->build_slices, uint32_t(ctx->num_sms) * uint32_t(k));
+            if (k > 1 && t.build_blocks == std::min<uint32_t>(batch->build_slices, uint32_t(ctx->num_sms) * (k - 1)))
+                continue;  // clamped to the same grid as k - 1
+            batch->tune = t;
+            float ms = 0.0f;
+            rc = time_median(ctx, st, reps,
+                             [&] { return rq_launch_batch_build(ctx, batch, positions, stride_bytes, indices, st); },
+                             &ms);
+            if (rc) break;
+            t.build_ms = ms;
+            t.trace_ms = 0.0f;
+            record(t);
+            if (best_bms < 0.0f || ms < best_bms) {
+                best_bms = ms;
+                best_b = t;
+            }
+        }
+        if (rc) break;
+    }
+    // traversal shapes (on the batch as built)
+    rq_batch_tuning best_t = start;
+    float best_tms = -1.0f;
+    if (rc == RQ_OK && n) {
+        for (uint32_t tt : {64u, 128u, 256u})
+            for (uint32_t chunk : {32u, 64u})
+                for (uint32_t cap64 : {0u, 1u}) {
+                    rq_batch_tuning t = best_b;
+                    t.trace_threads = tt;
+                    t.trace_chunk = chunk;
+                    t.trace_reg_cap = cap64;
+                    t.trace_blocks_per_sm = 0;
+                    t.stack_entries = 0;
+                    batch->tune = t;
+                    float ms = 0.0f;
+                    rc = time_median(ctx, st, reps,
+                                     [&] {
+                                         return rq_launch_batch_trace(ctx, batch, rays, ray_mesh, ray_flags, n, 0u,
+                                                                      hits, nullptr, ctx->d_ctr, st);
+                                     },
+                                     &ms);
+                    if (rc) break;
+                    t.build_ms = 0.0f;
+                    t.trace_ms = ms;
+                    record(t);
+                    if (best_tms < 0.0f || ms < best_tms) {
+                        best_tms = ms;
+                        best_t = t;
+                    }
+                }
+    }
+    rq_batch_tuning fin = best_b;
+    fin.trace_threads = best_t.trace_threads;
+    fin.trace_chunk = best_t.trace_chunk;
+    fin.trace_reg_cap = best_t.trace_reg_cap;
+    fin.trace_blocks_per_sm = best_t.trace_blocks_per_sm;
+    fin.stack_entries = (3u * (batch->max_depth + 2u) + 1u + 3u) & ~3u;
+    fin.build_ms = std::max(0.0f, best_bms);
+    fin.trace_ms = std::max(0.0f, best_tms);
+    fin.max_build_blocks = batch->build_slices;
+    batch->tune = rc == RQ_OK ? fin : start;
+    return rc;
+}
 
 int rq_batch_create(rq_ctx* ctx, const rq_mesh_desc* meshes, uint32_t num_meshes, uint32_t max_leaf,
                     rq_batch** out) {
@@ -86,12 +241,17 @@ int rq_batch_create(rq_ctx* ctx, const rq_mesh_desc* meshes, uint32_t num_meshes
     c.take<uint32_t>(64);
     b->mem_bytes = c.off + 256;
     b->scratch_stride = rq_batch_block_scratch(maxt);
-    uint32_t blocks = uint32_t(rq_batch_build_blocks(ctx->num_sms));
+    // scratch slices: enough for the most resident build blocks of any
+    // block size, within the scratch budget and the mesh count
+    int occ = 0;
+    for (uint32_t t : {256u, 512u, 1024u}) occ = std::max(occ, rq_batch_build_occupancy(t));
+    uint32_t blocks = uint32_t(ctx->num_sms) * uint32_t(std::max(1, occ));
     blocks = std::min<uint32_t>(blocks, uint32_t(std::max<size_t>(1, kScratchBudget / b->scratch_stride)));
     blocks = std::max(1u, std::min(blocks, num_meshes));
-    b->build_blocks = blocks;
+    b->build_slices = blocks;
+    b->tune = default_tuning(ctx, blocks);
     if (cudaMalloc(&b->mem, b->mem_bytes) != cudaSuccess ||
-        cudaMalloc(&b->scratch, b->scratch_stride * blocks) != cudaSuccess) {
+        cudaMalloc(&b->scratch, b->scratch_stride * b->build_slices) != cudaSuccess) {
         cudaGetLastError();
         free_batch(b);
         delete b;

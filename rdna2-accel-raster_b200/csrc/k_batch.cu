@@ -23,12 +23,10 @@
 
 namespace {
 
-constexpr int kBT = 512;              // build block
-constexpr int kBW = kBT / 32;         // warps per build block
+// Build blocks of BT threads (256, 512 or 1024: a tuned shape); the sort
+// ranks kSortItems keys per thread per tile.
 constexpr int kSortItems = 8;
-constexpr int kSortTile = kBT * kSortItems;
 constexpr uint32_t kMaxLevels = 120;
-constexpr int kTT = 128;              // trace block
 
 struct BlockScratch {
     float4* cent;
@@ -94,7 +92,9 @@ struct BuildArgs {
 };
 
 // Block-wide exclusive scan of one value per thread; *total = sum.
+template <int BT>
 __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+    constexpr int kBW = BT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t x = v;
 #pragma unroll
@@ -122,12 +122,14 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* s_warp, uin
 
 // Stable LSD radix sort of n (key, value) pairs by the low 30 key bits, four
 // 8-bit passes between (keys[0], vals[0]) and (keys[1], vals[1]); the result
-// ends in buffer 0.  Each pass: a digit histogram, then tiles of 4,096 keys
+// ends in buffer 0.  Each pass: a digit histogram, then tiles of BT x 8 keys
 // ranked per warp with match_any (peers in lane order) and scattered at
 // digit base + running tile offset — the same stable order as the onesweep
 // kernels of k_sort.cu.
+template <int BT>
 __device__ void block_sort(BlockScratch& s, uint32_t n, uint32_t* s_hist, uint32_t* s_off, uint32_t (*s_wcnt)[256],
                            uint32_t* s_warp) {
+    constexpr int kBW = BT / 32, kBT = BT, kSortTile = BT * kSortItems;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int pass = 0; pass < 4; ++pass) {
         const uint32_t shift = 8u * pass;
@@ -141,7 +143,7 @@ __device__ void block_sort(BlockScratch& s, uint32_t n, uint32_t* s_hist, uint32
         __syncthreads();
         uint32_t tot;
         const uint32_t hv = threadIdx.x < 256 ? s_hist[threadIdx.x] : 0u;
-        const uint32_t ex = block_scan(hv, s_warp, &tot);
+        const uint32_t ex = block_scan<BT>(hv, s_warp, &tot);
         if (threadIdx.x < 256) s_off[threadIdx.x] = ex;
         __syncthreads();
         for (uint32_t base = 0; base < n; base += kSortTile) {
@@ -200,10 +202,11 @@ __device__ void block_sort(BlockScratch& s, uint32_t n, uint32_t* s_hist, uint32
     }
 }
 
-// Exclusive scan of c[0..n) into a[0..n), tiles of 512 x 8 with a carry.
+// Exclusive scan of c[0..n) into a[0..n), tiles of BT x 8 with a carry.
+template <int BT>
 __device__ void block_scan_array(const uint32_t* c, uint32_t* a, uint32_t n, uint32_t* s_warp) {
     uint32_t carry = 0;
-    for (uint32_t base = 0; base < n; base += kBT * 8) {
+    for (uint32_t base = 0; base < n; base += BT * 8) {
         const uint32_t i0 = base + threadIdx.x * 8;
         uint32_t v[8], sum = 0;
 #pragma unroll
@@ -212,7 +215,7 @@ __device__ void block_scan_array(const uint32_t* c, uint32_t* a, uint32_t n, uin
             sum += v[k];
         }
         uint32_t tot;
-        uint32_t run = carry + block_scan(sum, s_warp, &tot);
+        uint32_t run = carry + block_scan<BT>(sum, s_warp, &tot);
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (i0 + k < n) a[i0 + k] = run;
@@ -223,7 +226,9 @@ __device__ void block_scan_array(const uint32_t* c, uint32_t* a, uint32_t n, uin
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBT) k_batch_build(BuildArgs A) {
+template <int BT>
+__global__ void __launch_bounds__(BT) k_batch_build(BuildArgs A) {
+    constexpr int kBT = BT, kBW = BT / 32;
     __shared__ uint32_t s_hist[256], s_off[256];
     __shared__ uint32_t s_wcnt[kBW][256];
     __shared__ uint32_t s_warp[32];
@@ -299,7 +304,7 @@ __global__ void __launch_bounds__(kBT) k_batch_build(BuildArgs A) {
         __syncthreads();
 
         // ---- sort, hierarchy, leaves + refit
-        block_sort(S, n, s_hist, s_off, s_wcnt, s_warp);
+        block_sort<BT>(S, n, s_hist, s_off, s_wcnt, s_warp);
         for (uint32_t i = threadIdx.x; i + 1 < n; i += kBT)
             rq::karras_node(S.keys[0], int(n), int(i), S.kl, S.kr, S.klo, S.khi, S.par_in, S.par_lf);
         if (n == 1 && threadIdx.x == 0) S.par_lf[0] = rq::kNoParent;
@@ -307,13 +312,12 @@ __global__ void __launch_bounds__(kBT) k_batch_build(BuildArgs A) {
         for (uint32_t k = threadIdx.x; k < n; k += kBT) {
             rq::leaf_step(k, pos, A.sf, idx, A.max_leaf, S.keys[0], S.vals[0], S.klo, S.khi, S.par_in, S.par_lf,
                           S.box_lf, S.c, tris, perm, skeys);
-            __threadfence();
-            rq::refit_walk(k, S.kl, S.kr, S.par_in, S.par_lf, S.box_in, S.box_lf, S.refit_flag, A.err);
+            rq::refit_walk<true>(k, S.kl, S.kr, S.par_in, S.par_lf, S.box_in, S.box_lf, S.refit_flag, A.err);
         }
         __syncthreads();
 
         // ---- depth-first binary nodes
-        block_scan_array(S.c, S.a, n, s_warp);
+        block_scan_array<BT>(S.c, S.a, n, s_warp);
         for (uint32_t p = threadIdx.x; p < n; p += kBT) {
             const uint32_t cp = rq::emit_step(p, n, A.max_leaf, S.kr, S.klo, S.khi, S.par_in, S.par_lf, S.box_in,
                                               S.box_lf, S.c, S.a, out2);
@@ -391,19 +395,48 @@ struct BatchSrc {
     }
 };
 
-template <bool MT, bool STATS, int STACK>
-__global__ void __launch_bounds__(kTT) k_batch_trace(const __grid_constant__ BatchSrc<STATS> src, uint32_t* ctr,
-                                                     uint32_t* err) {
+// Traversal blocks of TT threads, ray ids taken CHUNK at a time, and (CAP64)
+// launch bounds that hold registers to 64 per thread: the tuned shapes.
+// The stack has `stack` rows (runtime, from the batch's deepest tree).
+template <bool MT, bool STATS, int TT, int CHUNK, bool CAP64>
+__global__ void __launch_bounds__(TT, CAP64 ? 65536 / (TT * 64) : 1)
+    k_batch_trace(const __grid_constant__ BatchSrc<STATS> src, uint32_t* ctr, uint32_t* err, int stack) {
     extern __shared__ int32_t s_stack[];
-    rq::trace_persistent<rq::kAnyPerRay, MT, STATS, STACK, kTT>(nullptr, nullptr, src, ctr, s_stack + threadIdx.x,
-                                                                 err);
+    rq::trace_persistent<rq::kAnyPerRay, MT, STATS, 128, TT, const BatchSrc<STATS>, CHUNK>(
+        nullptr, nullptr, src, ctr, s_stack + threadIdx.x, err, stack);
+}
+
+template <int BT>
+int build_occupancy() {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_build<BT>, BT, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per_sm;
 }
 
 template <class F>
-cudaError_t with_stack(uint32_t bound, F&& f) {
-    if (bound <= 32) return f(std::integral_constant<int, 32>{});
-    if (bound <= 64) return f(std::integral_constant<int, 64>{});
-    return f(std::integral_constant<int, 128>{});
+cudaError_t with_build_shape(uint32_t bt, F&& f) {
+    if (bt == 256) return f(std::integral_constant<int, 256>{});
+    if (bt == 1024) return f(std::integral_constant<int, 1024>{});
+    return f(std::integral_constant<int, 512>{});
+}
+
+// Kernel of a traversal shape (only the default shape has the counting and
+// reference-arithmetic variants).
+template <bool MT, bool STATS>
+const void* trace_kernel(uint32_t tt, uint32_t chunk, uint32_t cap64) {
+#define RQ_SHAPE(T, C, L) \
+    if (tt == T && chunk == C && (cap64 != 0) == L) return reinterpret_cast<const void*>(k_batch_trace<MT, STATS, T, C, L>);
+    if constexpr (!MT && !STATS) {
+        RQ_SHAPE(64, 32, false) RQ_SHAPE(64, 32, true) RQ_SHAPE(64, 64, false) RQ_SHAPE(64, 64, true)
+        RQ_SHAPE(128, 32, true) RQ_SHAPE(128, 64, false) RQ_SHAPE(128, 64, true)
+        RQ_SHAPE(256, 32, false) RQ_SHAPE(256, 32, true) RQ_SHAPE(256, 64, false) RQ_SHAPE(256, 64, true)
+    }
+    RQ_SHAPE(128, 32, false)
+#undef RQ_SHAPE
+    return nullptr;
 }
 
 }  // namespace
@@ -413,10 +446,15 @@ size_t rq_batch_block_scratch(uint32_t max_tris) {
     return carve_block(0, max_tris, s);
 }
 
-int rq_batch_build_blocks(int num_sms) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_build, kBT, 0) != cudaSuccess) return 0;
-    return num_sms * (per_sm > 0 ? per_sm : 1);
+int rq_batch_build_occupancy(uint32_t threads) {
+    if (threads == 256) return build_occupancy<256>();
+    if (threads == 1024) return build_occupancy<1024>();
+    if (threads == 512) return build_occupancy<512>();
+    return 0;
+}
+
+bool rq_batch_trace_shape_ok(uint32_t threads, uint32_t chunk, uint32_t cap64) {
+    return trace_kernel<false, false>(threads, chunk, cap64) != nullptr;
 }
 
 int rq_launch_batch_build(rq_ctx* ctx, rq_batch* b, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
@@ -441,11 +479,14 @@ int rq_launch_batch_build(rq_ctx* ctx, rq_batch* b, const float* pos, uint32_t s
     a.map4 = b->map4;
     a.counts = b->d_counts;
     a.err = ctx->d_err;
+    const uint32_t blocks = std::min(b->tune.build_blocks, b->build_slices);
     cudaError_t e = cudaMemsetAsync(b->d_ctr, 0, sizeof(uint32_t), st);
-    if (e == cudaSuccess) {
-        k_batch_build<<<b->build_blocks, kBT, 0, st>>>(a);
-        e = cudaGetLastError();
-    }
+    if (e == cudaSuccess)
+        e = with_build_shape(b->tune.build_threads, [&](auto T) {
+            constexpr int BT = decltype(T)::value;
+            k_batch_build<BT><<<blocks, BT, 0, st>>>(a);
+            return cudaGetLastError();
+        });
     return rq_cuda_status(ctx, e, "batch build launch");
 }
 
@@ -453,32 +494,41 @@ int rq_launch_batch_trace(rq_ctx* ctx, const rq_batch* b, const rq_ray* rays, co
                           const uint32_t* ray_flags, uint32_t n, uint32_t flags, rq_hit* hits, rq_ray_stats* stats,
                           uint32_t* ctr, cudaStream_t st) {
     const uint32_t bound = 3u * (b->max_depth + 2u) + 1u;
+    if (bound > 128u) return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "4-wide tree deeper than 40 levels");
     const bool mt = flags & RQ_TRI_MT;
+    // the counting and reference-arithmetic variants run in the default shape
+    const bool tuned = !mt && !stats;
+    const uint32_t tt = tuned ? b->tune.trace_threads : 128u;
+    const uint32_t chunk = tuned ? b->tune.trace_chunk : 32u;
+    const uint32_t cap64 = tuned ? b->tune.trace_reg_cap : 0u;
+    // stack rows: the bound, rounded up to a multiple of 4 (16-B rows)
+    const int stack = int((std::max(bound, b->tune.stack_entries) + 3u) & ~3u);
+    const void* kern = mt ? (stats ? trace_kernel<true, true>(tt, chunk, cap64) : trace_kernel<true, false>(tt, chunk, cap64))
+                          : (stats ? trace_kernel<false, true>(tt, chunk, cap64) : trace_kernel<false, false>(tt, chunk, cap64));
+    if (!kern) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
+    const size_t smem = size_t(stack) * tt * sizeof(int32_t);
     cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
-    if (e == cudaSuccess)
-        e = with_stack(bound, [&](auto S) {
-            constexpr int STACK = decltype(S)::value;
-            const size_t smem = size_t(STACK) * kTT * sizeof(int32_t);
-            auto launch = [&](auto kern, auto src) {
-                cudaError_t r = cudaSuccess;
-                if (smem > 48 * 1024) r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                               int(smem));
-                int per_sm = 0;
-                if (r == cudaSuccess) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTT, smem);
-                if (r != cudaSuccess) return r;
-                uint32_t blocks = uint32_t(ctx->num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
-                blocks = std::min(blocks, (n + kTT - 1) / kTT);
-                kern<<<blocks, kTT, smem, st>>>(src, ctr, ctx->d_err);
-                return cudaGetLastError();
-            };
-            if (stats) {
-                BatchSrc<true> src{n, rays, ray_mesh, ray_flags, flags, b->d_meshes, b->nodes4, b->tris, b->perm,
-                                   hits, stats};
-                return mt ? launch(k_batch_trace<true, true, STACK>, src) : launch(k_batch_trace<false, true, STACK>, src);
-            }
-            BatchSrc<false> src{n, rays, ray_mesh, ray_flags, flags, b->d_meshes, b->nodes4, b->tris, b->perm,
-                                hits, nullptr};
-            return mt ? launch(k_batch_trace<true, false, STACK>, src) : launch(k_batch_trace<false, false, STACK>, src);
-        });
+    if (e == cudaSuccess && smem > 48 * 1024)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(tt), smem);
+    if (e == cudaSuccess) {
+        if (b->tune.trace_blocks_per_sm && int(b->tune.trace_blocks_per_sm) < per_sm)
+            per_sm = int(b->tune.trace_blocks_per_sm);
+        uint32_t blocks = uint32_t(ctx->num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+        blocks = std::max(1u, std::min(blocks, (n + tt - 1) / tt));
+        uint32_t* err = ctx->d_err;
+        if (stats) {
+            BatchSrc<true> src{n, rays, ray_mesh, ray_flags, flags, b->d_meshes, b->nodes4, b->tris, b->perm, hits,
+                               stats};
+            void* args[] = {&src, &ctr, &err, const_cast<int*>(&stack)};
+            e = cudaLaunchKernel(kern, dim3(blocks), dim3(tt), args, smem, st);
+        } else {
+            BatchSrc<false> src{n, rays, ray_mesh, ray_flags, flags, b->d_meshes, b->nodes4, b->tris, b->perm, hits,
+                                nullptr};
+            void* args[] = {&src, &ctr, &err, const_cast<int*>(&stack)};
+            e = cudaLaunchKernel(kern, dim3(blocks), dim3(tt), args, smem, st);
+        }
+    }
     return rq_cuda_status(ctx, e, "batch trace launch");
 }

@@ -94,7 +94,6 @@ __global__ void __launch_bounds__(kT) k_leaves(const float* __restrict__ pos, ui
     for (uint32_t k = blockIdx.x * kT + threadIdx.x; k < n; k += gridDim.x * kT) {
         rq::leaf_step(k, pos, sf, idx, max_leaf, skeys, sids, klo, khi, par_in, par_lf, box_lf, c_out, tris, perm,
                       keys_out);
-        __threadfence();
         rq::refit_walk(k, kl, kr, par_in, par_lf, box_in, box_lf, refit_flag, err);
     }
 }
@@ -161,12 +160,11 @@ __global__ void __launch_bounds__(kT) k_refit2(const float* __restrict__ pos, ui
         float4* o = reinterpret_cast<float4*>(nodes + i);
         __stcg(o, make_float4(mn[0], mn[1], mn[2], __int_as_float(nd.left_child)));
         __stcg(o + 1, make_float4(mx[0], mx[1], mx[2], __int_as_float(nd.right_child)));
-        __threadfence();
         uint32_t p = parent[i];
         uint32_t guard = 0;
         while (p != rq::kNoParent) {
-            if (atomicAdd(&flag[p], 1u) == 0u) break;
-            __threadfence();
+            // publishes this thread's last box; the second arrival sees the sibling's
+            if (rq::atom_add_acq_rel(&flag[p], 1u) == 0u) break;
             const float4* pn = reinterpret_cast<const float4*>(nodes + p);
             const float4 pa = rq::ld_cg4(pn), pb = rq::ld_cg4(pn + 1);
             const int32_t l = __float_as_int(pa.w), r = __float_as_int(pb.w);
@@ -177,7 +175,6 @@ __global__ void __launch_bounds__(kT) k_refit2(const float* __restrict__ pos, ui
                    make_float4(fminf(la.x, ra.x), fminf(la.y, ra.y), fminf(la.z, ra.z), pa.w));
             __stcg(reinterpret_cast<float4*>(nodes + p) + 1,
                    make_float4(fmaxf(lb.x, rb.x), fmaxf(lb.y, rb.y), fmaxf(lb.z, rb.z), pb.w));
-            __threadfence();
             p = parent[p];
             if (++guard > 256u) {
                 rq::set_err(err, RQ_DERR_REFIT);

@@ -34,7 +34,8 @@ struct rq_batch {
     // per-block build scratch, sized for the largest mesh
     void* scratch = nullptr;
     size_t scratch_stride = 0;
-    uint32_t build_blocks = 0;
+    uint32_t build_slices = 0;     // scratch slices: the most build blocks a launch may use
+    rq_batch_tuning tune{};        // launch shapes
     std::vector<uint32_t> h_counts;
     bool counts_valid = false;
     uint32_t max_depth = 0;
@@ -43,7 +44,10 @@ struct rq_batch {
 };
 
 size_t rq_batch_block_scratch(uint32_t max_tris);
-int rq_batch_build_blocks(int num_sms);
+// Resident build blocks per SM for a build block size (0 if none).
+int rq_batch_build_occupancy(uint32_t threads);
+// Whether a traversal kernel exists for this shape.
+bool rq_batch_trace_shape_ok(uint32_t threads, uint32_t chunk, uint32_t cap64);
 int rq_launch_batch_build(rq_ctx* ctx, rq_batch* b, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
                           cudaStream_t st);
 int rq_launch_batch_trace(rq_ctx* ctx, const rq_batch* b, const rq_ray* rays, const uint32_t* ray_mesh,

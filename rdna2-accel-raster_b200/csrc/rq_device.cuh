@@ -32,6 +32,18 @@ __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Fetch-and-add with acquire-release semantics: releases this thread's
+// earlier stores and acquires those released by earlier adds on the same
+// word (the hand-off of a bottom-up refit, without separate fences).
+template <bool CTA = false>
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    if (CTA)
+        asm volatile("atom.acq_rel.cta.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    else
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 // L2-coherent 16-B load (bypasses L1), for data written by other blocks in
 // the same launch.
 __device__ __forceinline__ float4 ld_cg4(const float4* p) { return __ldcg(p); }

@@ -30,7 +30,7 @@ namespace rq {
 
 constexpr int32_t kNoLeaf = 0;  // leaf entries always have bit 31 set
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr uint32_t kChunk = 32;
+constexpr uint32_t kChunk = 32;  // default ray ids per refill atomic
 
 struct Ray {
     F3 o, d;
@@ -73,10 +73,13 @@ struct Hit {
     uint32_t boxes, tris;
 };
 
-template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src>
+// STACK bounds the entries per lane (stk has STACK rows of STRIDE words);
+// stack_cap, if smaller, is the bound actually allocated.  CHUNK: ray ids
+// taken per atomic.
+template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src, int CHUNK = int(kChunk)>
 __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict__ nodes,
                                                  const rq_triangle* __restrict__ tris, Src& src, uint32_t* ctr,
-                                                 int32_t* stk, uint32_t* err) {
+                                                 int32_t* stk, uint32_t* err, int stack_cap = STACK) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     // warp-uniform chunk of ray ids
@@ -104,14 +107,14 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
         while (idle && !exhausted) {
             if (next == end) {
                 uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(ctr, kChunk);
+                if (lane == 0) base = atomicAdd(ctr, uint32_t(CHUNK));
                 base = __shfl_sync(kFull, base, 0);
                 if (base >= src.total) {
                     exhausted = true;
                     break;
                 }
                 next = base;
-                end = min(base + kChunk, src.total);
+                end = min(base + uint32_t(CHUNK), src.total);
             }
             const uint32_t take = min(uint32_t(__popc(idle)), end - next);
             const uint32_t rank = __popc(idle & lt_mask);
@@ -193,9 +196,9 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                     ++nh;
                 }
             }
-            if (sp + nh > STACK) {
+            if (sp + nh > stack_cap) {
                 set_err(err, RQ_DERR_STACK);
-                nh = STACK - sp;
+                nh = stack_cap - sp;
             }
             for (int j = nh - 1; j >= 0; --j) stk[(sp++) * STRIDE] = he[j];
         }

@@ -91,6 +91,13 @@ class MeshDesc(C.Structure):
                 ("num_triangles", C.c_uint32)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("build_threads", C.c_uint32), ("build_blocks", C.c_uint32), ("trace_threads", C.c_uint32),
+                ("trace_chunk", C.c_uint32), ("trace_reg_cap", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
+                ("stack_entries", C.c_uint32), ("max_build_blocks", C.c_uint32), ("build_ms", C.c_float),
+                ("trace_ms", C.c_float)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("mode", C.c_uint32), ("slots", C.c_uint32),
                 ("max_wave_rays", C.c_uint32), ("max_wave_requests", C.c_uint32), ("max_leaf", C.c_uint32),
@@ -157,6 +164,10 @@ SIGNATURES = [
     ("rq_batch_info_get", C.c_int, [_P, _U32, C.POINTER(BvhInfo)]),
     ("rq_batch_download", C.c_int, [_P, _U32, C.c_int, _P, _U32, _P, _U32, _P, _U32, _P, _U32]),
     ("rq_batch_destroy", C.c_int, [_P]),
+    ("rq_batch_tuning_get", C.c_int, [_P, C.POINTER(BatchTuning)]),
+    ("rq_batch_tuning_set", C.c_int, [_P, C.POINTER(BatchTuning)]),
+    ("rq_batch_autotune", C.c_int, [_P, _P, _P, _U32, _P, _P, _P, _P, _U32, _P, _U32, C.POINTER(BatchTuning), _U32,
+                                    C.POINTER(_U32), _P]),
     # include/rq_serve.h
     ("rq_server_create", C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_P)]),
     ("rq_server_destroy", C.c_int, [_P]),
@@ -364,6 +375,38 @@ class Batch:
                                   _ptr(hits), _ptr(s), _stream(stream))
         self.ctx.check(rc, "rq_batch_trace")
         return hits, s
+
+    TUNING_KEYS = ("build_threads", "build_blocks", "trace_threads", "trace_chunk", "trace_reg_cap",
+                   "trace_blocks_per_sm", "stack_entries")
+
+    def tuning(self):
+        t = BatchTuning()
+        self.ctx.check(lib().rq_batch_tuning_get(self.h, C.byref(t)), "rq_batch_tuning_get")
+        return {k: getattr(t, k) for k, _ in BatchTuning._fields_}
+
+    def set_tuning(self, shape):
+        """shape: dict with (a subset of) TUNING_KEYS."""
+        t = BatchTuning()
+        lib().rq_batch_tuning_get(self.h, C.byref(t))
+        for k in self.TUNING_KEYS:
+            if k in shape:
+                setattr(t, k, int(shape[k]))
+        self.ctx.check(lib().rq_batch_tuning_set(self.h, C.byref(t)), "rq_batch_tuning_set")
+
+    def autotune(self, pos, idx, rays, ray_mesh, ray_flags=None, hits=None, reps=5, stride_bytes=12, stream=None):
+        """Time every build and traversal shape on these inputs; keep the
+        fastest.  Returns (chosen shape, list of measured candidates)."""
+        n = _count(rays, 32)
+        hits = hits if hits is not None else _empty_i32(n, 4, rays.device)
+        cap = 256
+        trials = (BatchTuning * cap)()
+        cnt = _U32()
+        rc = lib().rq_batch_autotune(self.ctx.h, self.h, _ptr(pos), stride_bytes, _ptr(idx), _ptr(rays),
+                                     _ptr(ray_mesh), _ptr(ray_flags), n, _ptr(hits), reps, trials, cap,
+                                     C.byref(cnt), _stream(stream))
+        self.ctx.check(rc, "rq_batch_autotune")
+        tr = [{k: getattr(trials[i], k) for k, _ in BatchTuning._fields_} for i in range(min(cap, cnt.value))]
+        return self.tuning(), tr
 
     def info(self, m):
         inf = BvhInfo()

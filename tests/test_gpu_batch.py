@@ -96,3 +96,50 @@ def test_batch_rejects_bad_descriptors(ctx):
         rq.Batch(ctx, [(0, 3, 0, 2), (0, 3, 1, 2)])  # overlapping triangle ranges
     with pytest.raises(rq.RqError):
         rq.Batch(ctx, [(0, 3, 0, 0)])  # empty mesh
+
+
+def test_every_launch_shape_gives_identical_results(ctx):
+    pos, idx, descs, p, i, b = make_batch(ctx, SIZES)
+    rays, mesh, flags = W.batched_rays(descs, 300, 300, seed=12)
+    rays_t = torch.from_numpy(rays).cuda()
+    mesh_t = torch.from_numpy(mesh.view(np.int32)).cuda()
+    flags_t = torch.from_numpy(flags.view(np.int32)).cuda()
+    want_tree = [b.download(m) for m in range(len(descs))]
+    want_hits = b.trace(rays_t, mesh_t, flags_t)[0].cpu().numpy()
+    base = b.tuning()
+    assert base["build_threads"] == 512 and base["trace_threads"] == 128 and base["max_build_blocks"] >= 1
+    for bt, blocks in ((256, 1), (1024, 3), (512, base["max_build_blocks"])):
+        b.set_tuning({"build_threads": bt, "build_blocks": blocks})
+        b.build(p, i)
+        ctx.sync_check()
+        for m in range(len(descs)):
+            assert all(x.tobytes() == y.tobytes() for x, y in zip(want_tree[m], b.download(m))), (bt, blocks, m)
+    for tt in (64, 128, 256):
+        for chunk in (32, 64):
+            for cap in (0, 1):
+                b.set_tuning({"trace_threads": tt, "trace_chunk": chunk, "trace_reg_cap": cap, "stack_entries": 128})
+                got = b.trace(rays_t, mesh_t, flags_t)[0].cpu().numpy()
+                ctx.sync_check()
+                assert got.tobytes() == want_hits.tobytes(), (tt, chunk, cap)
+    with pytest.raises(rq.RqError):
+        b.set_tuning({"trace_threads": 96})
+    b.destroy()
+
+
+def test_autotune_keeps_a_measured_shape(ctx):
+    pos, idx, descs, p, i, b = make_batch(ctx, SIZES)
+    rays, mesh, flags = W.batched_rays(descs, 200, 200, seed=13)
+    rays_t = torch.from_numpy(rays).cuda()
+    mesh_t = torch.from_numpy(mesh.view(np.int32)).cuda()
+    flags_t = torch.from_numpy(flags.view(np.int32)).cuda()
+    want = b.trace(rays_t, mesh_t, flags_t)[0].cpu().numpy()
+    shape, trials = b.autotune(p, i, rays_t, mesh_t, flags_t, reps=2)
+    builds = [t for t in trials if t["build_ms"] > 0]
+    traces = [t for t in trials if t["trace_ms"] > 0]
+    assert len(traces) == 12 and len(builds) >= 3
+    assert shape["build_ms"] == min(t["build_ms"] for t in builds)
+    assert shape["trace_ms"] == min(t["trace_ms"] for t in traces)
+    assert shape["stack_entries"] >= 3 * (max(b.info(m)["depth4"] for m in range(len(descs))) + 2) + 1
+    got = b.trace(rays_t, mesh_t, flags_t)[0].cpu().numpy()
+    assert got.tobytes() == want.tobytes()
+    b.destroy()
