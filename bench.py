@@ -274,6 +274,18 @@ def run_ours(args, world, rank, local, pg):
     frame_rays = npx + sec_rays
     hits = int((gbuf[:, 3] != 0).sum().item())
 
+    # launch shape of the shadow/AO traversal: committed autotuner table,
+    # else tuned now (untimed)
+    from rq import tune as T
+    skey = T.shadow_key(len(idx), params)
+    sshape = T.lookup_shadow(skey)
+    if sshape is not None:
+        ctx.set_trace_tuning(**sshape)
+        shade_tuning = {"source": "committed table rq/tuning_b200.json", **sshape}
+    else:
+        sshape, strials = T.tune_shadow(ctx, bvh, gbuf, params, reps=3)
+        shade_tuning = {"source": f"autotuned in this run ({len(strials)} shapes timed)", **sshape}
+
     # node / triangle tests per any-hit ray, for the algorithmic bytes
     cp = rq.shade_params(WIDTH, HEIGHT, W.shadow_lights(16), ao_spp=1, ao_tmax=0.5,
                          flags=rq.RQ_SHADE_COUNT_TESTS)
@@ -410,6 +422,7 @@ def run_ours(args, world, rank, local, pg):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "shadow_tuning": shade_tuning,
         "visibility": vis,
         "batched": batched,
         "serving": serving,

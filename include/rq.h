@@ -54,6 +54,18 @@ int rq_ctx_check(rq_ctx* ctx, rq_stream stream);
 /* Bytes of device scratch the context currently holds. */
 uint64_t rq_ctx_scratch_bytes(const rq_ctx* ctx);
 
+/* Launch shape of the context's persistent shadow/AO traversal
+ * (rq_render_shadow_ao).  Results do not depend on it. */
+typedef struct rq_trace_tuning {
+    uint32_t threads;  /* per block: 64, 128 or 256 (default 128) */
+    uint32_t chunk;    /* ray ids a warp takes per refill: 32 or 64 (default 32) */
+    uint32_t reg_cap;  /* registers per thread the launch bounds allow: 0 (no bound), 64 or 80 (default) */
+    uint32_t reserved;
+} rq_trace_tuning;
+int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out);
+/* RQ_ERR_INVALID_ARG for a shape that has no kernel. */
+int rq_ctx_trace_tuning_set(rq_ctx* ctx, const rq_trace_tuning* t);
+
 /* ------------------------------------------------------------------ */
 /* Mesh generation and deformation (inputs of the BVH path)            */
 /* ------------------------------------------------------------------ */
@@ -245,7 +257,7 @@ typedef struct rq_batch_tuning {
     uint32_t build_blocks;        /* persistent build blocks (clamped to max_build_blocks) */
     uint32_t trace_threads;       /* threads per traversal block: 64, 128 or 256 */
     uint32_t trace_chunk;         /* ray ids a warp takes per refill: 32 or 64 */
-    uint32_t trace_reg_cap;       /* 1: launch bounds that hold the kernel to 64 registers */
+    uint32_t trace_reg_cap;       /* registers per thread the launch bounds allow: 0 (none), 64 or 80 */
     uint32_t trace_blocks_per_sm; /* 0: as many as fit */
     uint32_t stack_entries;       /* stack entries per lane; 0 or anything below
                                      3 * (depth + 2) + 1 means that bound */

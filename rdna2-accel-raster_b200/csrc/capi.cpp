@@ -198,6 +198,20 @@ int rq_ctx_check(rq_ctx* ctx, rq_stream stream) {
 
 uint64_t rq_ctx_scratch_bytes(const rq_ctx* ctx) { return ctx ? ctx->scratch_bytes : 0; }
 
+int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out) {
+    if (!ctx || !out) return RQ_ERR_INVALID_ARG;
+    *out = ctx->shade_shape;
+    return RQ_OK;
+}
+
+int rq_ctx_trace_tuning_set(rq_ctx* ctx, const rq_trace_tuning* t) {
+    if (!ctx || !t) return RQ_ERR_INVALID_ARG;
+    if (!rq_shade_shape_ok(*t)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
+    ctx->shade_shape = *t;
+    ctx->shade_shape.reserved = 0;
+    return RQ_OK;
+}
+
 // ---------------------------------------------------------------- meshes
 
 int rq_deform_wave(rq_ctx* ctx, const float* base, float* out, uint32_t num_vertices, float t, float amp,

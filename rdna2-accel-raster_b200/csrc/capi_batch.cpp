@@ -154,11 +154,11 @@ int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint
     if (rc == RQ_OK && n) {
         for (uint32_t tt : {64u, 128u, 256u})
             for (uint32_t chunk : {32u, 64u})
-                for (uint32_t cap64 : {0u, 1u}) {
+                for (uint32_t regs : {0u, 64u, 80u}) {
                     rq_batch_tuning t = best_b;
                     t.trace_threads = tt;
                     t.trace_chunk = chunk;
-                    t.trace_reg_cap = cap64;
+                    t.trace_reg_cap = regs;
                     t.trace_blocks_per_sm = 0;
                     t.stack_entries = 0;
                     batch->tune = t;

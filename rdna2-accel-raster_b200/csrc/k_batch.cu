@@ -395,11 +395,11 @@ struct BatchSrc {
     }
 };
 
-// Traversal blocks of TT threads, ray ids taken CHUNK at a time, and (CAP64)
-// launch bounds that hold registers to 64 per thread: the tuned shapes.
+// Traversal blocks of TT threads, ray ids taken CHUNK at a time, and (REGS)
+// launch bounds that hold registers to REGS per thread: the tuned shapes.
 // The stack has `stack` rows (runtime, from the batch's deepest tree).
-template <bool MT, bool STATS, int TT, int CHUNK, bool CAP64>
-__global__ void __launch_bounds__(TT, CAP64 ? 65536 / (TT * 64) : 1)
+template <bool MT, bool STATS, int TT, int CHUNK, int REGS>
+__global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     k_batch_trace(const __grid_constant__ BatchSrc<STATS> src, uint32_t* ctr, uint32_t* err, int stack) {
     extern __shared__ int32_t s_stack[];
     rq::trace_persistent<rq::kAnyPerRay, MT, STATS, 128, TT, const BatchSrc<STATS>, CHUNK>(
@@ -426,15 +426,16 @@ cudaError_t with_build_shape(uint32_t bt, F&& f) {
 // Kernel of a traversal shape (only the default shape has the counting and
 // reference-arithmetic variants).
 template <bool MT, bool STATS>
-const void* trace_kernel(uint32_t tt, uint32_t chunk, uint32_t cap64) {
-#define RQ_SHAPE(T, C, L) \
-    if (tt == T && chunk == C && (cap64 != 0) == L) return reinterpret_cast<const void*>(k_batch_trace<MT, STATS, T, C, L>);
+const void* trace_kernel(uint32_t tt, uint32_t chunk, uint32_t regs) {
+#define RQ_SHAPE(T, C, R) \
+    if (tt == T && chunk == C && regs == R) return reinterpret_cast<const void*>(k_batch_trace<MT, STATS, T, C, R>);
+#define RQ_SHAPES(T, C) RQ_SHAPE(T, C, 0) RQ_SHAPE(T, C, 64) RQ_SHAPE(T, C, 80)
     if constexpr (!MT && !STATS) {
-        RQ_SHAPE(64, 32, false) RQ_SHAPE(64, 32, true) RQ_SHAPE(64, 64, false) RQ_SHAPE(64, 64, true)
-        RQ_SHAPE(128, 32, true) RQ_SHAPE(128, 64, false) RQ_SHAPE(128, 64, true)
-        RQ_SHAPE(256, 32, false) RQ_SHAPE(256, 32, true) RQ_SHAPE(256, 64, false) RQ_SHAPE(256, 64, true)
+        RQ_SHAPES(64, 32) RQ_SHAPES(64, 64) RQ_SHAPES(128, 64) RQ_SHAPES(256, 32) RQ_SHAPES(256, 64)
+        RQ_SHAPE(128, 32, 64) RQ_SHAPE(128, 32, 80)
     }
-    RQ_SHAPE(128, 32, false)
+    RQ_SHAPE(128, 32, 0)
+#undef RQ_SHAPES
 #undef RQ_SHAPE
     return nullptr;
 }
@@ -453,8 +454,8 @@ int rq_batch_build_occupancy(uint32_t threads) {
     return 0;
 }
 
-bool rq_batch_trace_shape_ok(uint32_t threads, uint32_t chunk, uint32_t cap64) {
-    return trace_kernel<false, false>(threads, chunk, cap64) != nullptr;
+bool rq_batch_trace_shape_ok(uint32_t threads, uint32_t chunk, uint32_t regs) {
+    return trace_kernel<false, false>(threads, chunk, regs) != nullptr;
 }
 
 int rq_launch_batch_build(rq_ctx* ctx, rq_batch* b, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
@@ -500,11 +501,11 @@ int rq_launch_batch_trace(rq_ctx* ctx, const rq_batch* b, const rq_ray* rays, co
     const bool tuned = !mt && !stats;
     const uint32_t tt = tuned ? b->tune.trace_threads : 128u;
     const uint32_t chunk = tuned ? b->tune.trace_chunk : 32u;
-    const uint32_t cap64 = tuned ? b->tune.trace_reg_cap : 0u;
+    const uint32_t regs = tuned ? b->tune.trace_reg_cap : 0u;
     // stack rows: the bound, rounded up to a multiple of 4 (16-B rows)
     const int stack = int((std::max(bound, b->tune.stack_entries) + 3u) & ~3u);
-    const void* kern = mt ? (stats ? trace_kernel<true, true>(tt, chunk, cap64) : trace_kernel<true, false>(tt, chunk, cap64))
-                          : (stats ? trace_kernel<false, true>(tt, chunk, cap64) : trace_kernel<false, false>(tt, chunk, cap64));
+    const void* kern = mt ? (stats ? trace_kernel<true, true>(tt, chunk, regs) : trace_kernel<true, false>(tt, chunk, regs))
+                          : (stats ? trace_kernel<false, true>(tt, chunk, regs) : trace_kernel<false, false>(tt, chunk, regs));
     if (!kern) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
     const size_t smem = size_t(stack) * tt * sizeof(int32_t);
     cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);

@@ -206,13 +206,13 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
     src.finish(id, m, r, h);
 }
 
-template <bool MT, bool STATS, int STACK>
-__global__ void __launch_bounds__(kT) k_shadow_ao(const rq_bvh4_node* __restrict__ nodes,
-                                                  const rq_triangle* __restrict__ tris,
-                                                  const rq_gbuffer_px* __restrict__ gbuf,
-                                                  const __grid_constant__ ShadeArgs sa,
-                                                  unsigned long long* words, unsigned long long* counters,
-                                                  uint32_t* ctr, uint32_t* err) {
+// TT threads per block, CHUNK ray ids per refill, REGS: launch bounds that
+// hold registers to REGS (0: none) — the tuned shapes; `stack` rows per lane.
+template <bool MT, bool STATS, int TT, int CHUNK, int REGS>
+__global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
+    k_shadow_ao(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
+                const rq_gbuffer_px* __restrict__ gbuf, const __grid_constant__ ShadeArgs sa,
+                unsigned long long* words, unsigned long long* counters, uint32_t* ctr, uint32_t* err, int stack) {
     extern __shared__ int32_t s_stack[];
     ShadeSrc<STATS> src;
     src.kinds = sa.nl + sa.spp;
@@ -221,7 +221,8 @@ __global__ void __launch_bounds__(kT) k_shadow_ao(const rq_bvh4_node* __restrict
     src.s = &sa;
     src.gbuf = gbuf;
     src.words = words;
-    rq::trace_persistent<true, MT, STATS, STACK, kT>(nodes, tris, src, ctr, s_stack + threadIdx.x, err);
+    rq::trace_persistent<true, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK>(nodes, tris, src, ctr,
+                                                                         s_stack + threadIdx.x, err, stack);
     if (counters) {
         const uint32_t r = __reduce_add_sync(rq::kFull, src.rays);
         if ((threadIdx.x & 31u) == 0 && r) atomicAdd(counters, (unsigned long long)r);
@@ -255,21 +256,26 @@ cudaError_t with_stack(uint32_t bound, F&& f) {
     return f(std::integral_constant<int, 128>{});
 }
 
-// Grid of a persistent kernel: every SM filled to its occupancy.
-template <class K>
-cudaError_t persistent_grid(K kern, int stack, int sms, int* blocks) {
-    const size_t smem = size_t(stack) * kT * sizeof(int32_t);
-    cudaError_t e = cudaSuccess;
-    if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, smem);
-    if (e != cudaSuccess) return e;
-    *blocks = sms * (per_sm > 0 ? per_sm : 1);
-    return cudaSuccess;
+// Shadow/AO kernel of a launch shape (only the default shape has the
+// counting and reference-arithmetic variants).
+template <bool MT, bool STATS>
+const void* shade_kernel(const rq_trace_tuning& t) {
+#define RQ_SHAPE(T, C, R) \
+    if (t.threads == T && t.chunk == C && t.reg_cap == R) return reinterpret_cast<const void*>(k_shadow_ao<MT, STATS, T, C, R>);
+#define RQ_SHAPES(T, C) RQ_SHAPE(T, C, 0) RQ_SHAPE(T, C, 64) RQ_SHAPE(T, C, 80)
+    if constexpr (!MT && !STATS) {
+        RQ_SHAPES(64, 32) RQ_SHAPES(64, 64) RQ_SHAPES(128, 64) RQ_SHAPES(256, 32) RQ_SHAPES(256, 64)
+        RQ_SHAPE(128, 32, 64) RQ_SHAPE(128, 32, 80)
+    }
+    RQ_SHAPE(128, 32, 0)
+#undef RQ_SHAPES
+#undef RQ_SHAPE
+    return nullptr;
 }
 
 }  // namespace
+
+bool rq_shade_shape_ok(const rq_trace_tuning& t) { return shade_kernel<false, false>(t) != nullptr; }
 
 int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_gbuffer_px* gbuf, cudaStream_t st) {
     GbufSrc src;
@@ -335,18 +341,27 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
     uint32_t* ctr = ctx->d_ctr;
     cudaError_t e = cudaMemsetAsync(words, 0, sizeof(unsigned long long) * size_t(npix), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
-    if (e == cudaSuccess && p.num_lights + p.ao_spp > 0)
-        e = with_stack(bound, [&](auto S) {
-            constexpr int STACK = decltype(S)::value;
-            auto k = mt ? (stats ? k_shadow_ao<true, true, STACK> : k_shadow_ao<true, false, STACK>)
-                        : (stats ? k_shadow_ao<false, true, STACK> : k_shadow_ao<false, false, STACK>);
-            int blocks = 0;
-            cudaError_t r = persistent_grid(k, STACK, ctx->num_sms, &blocks);
-            if (r != cudaSuccess) return r;
-            k<<<blocks, kT, size_t(STACK) * kT * 4, st>>>(bvh->nodes4, bvh->tris, gbuf, s, words, counter, ctr,
-                                                          ctx->d_err);
-            return cudaGetLastError();
-        });
+    if (e == cudaSuccess && p.num_lights + p.ao_spp > 0) {
+        // the counting and reference-arithmetic variants run in the default shape
+        const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0} : ctx->shade_shape;
+        const void* k = mt ? (stats ? shade_kernel<true, true>(shape) : shade_kernel<true, false>(shape))
+                           : (stats ? shade_kernel<false, true>(shape) : shade_kernel<false, false>(shape));
+        if (!k) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
+        // stack rows: the bound for the tree's depth, rounded up to 4
+        const int stack = int((bound + 3u) & ~3u);
+        const size_t smem = size_t(stack) * shape.threads * sizeof(int32_t);
+        if (smem > 48 * 1024) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        int per_sm = 0;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, int(shape.threads), smem);
+        if (e == cudaSuccess) {
+            const uint32_t blocks = uint32_t(ctx->num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+            const rq_bvh4_node* nodes = bvh->nodes4;
+            const rq_triangle* tris = bvh->tris;
+            uint32_t* err = ctx->d_err;
+            void* args[] = {&nodes, &tris, &gbuf, &s, &words, &counter, &ctr, &err, const_cast<int*>(&stack)};
+            e = cudaLaunchKernel(k, dim3(blocks), dim3(shape.threads), args, smem, st);
+        }
+    }
     if (e == cudaSuccess) {
         k_shade_finish<<<(npix + 255) / 256, 256, 0, st>>>(gbuf, words, npix, p.ao_spp, mask, ao);
         e = cudaGetLastError();

@@ -47,7 +47,7 @@ size_t rq_batch_block_scratch(uint32_t max_tris);
 // Resident build blocks per SM for a build block size (0 if none).
 int rq_batch_build_occupancy(uint32_t threads);
 // Whether a traversal kernel exists for this shape.
-bool rq_batch_trace_shape_ok(uint32_t threads, uint32_t chunk, uint32_t cap64);
+bool rq_batch_trace_shape_ok(uint32_t threads, uint32_t chunk, uint32_t regs);
 int rq_launch_batch_build(rq_ctx* ctx, rq_batch* b, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
                           cudaStream_t st);
 int rq_launch_batch_trace(rq_ctx* ctx, const rq_batch* b, const rq_ray* rays, const uint32_t* ray_mesh,

@@ -31,6 +31,7 @@ struct rq_ctx {
     uint32_t* d_ctr = nullptr;      // work counters of persistent launches (zeroed per launch)
     std::string last_error;
     int collapse_blocks = 0;        // co-resident blocks of the collapse kernel
+    rq_trace_tuning shade_shape{128, 32, 80, 0};  // shadow/AO traversal launch shape
 };
 
 struct rq_bvh {
@@ -138,6 +139,7 @@ int rq_launch_trace_radv(rq_ctx* ctx, const void* img, uint64_t bytes, const rq_
 
 // ---------------------------------------------------------------- k_frame
 int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_gbuffer_px* gbuf, cudaStream_t st);
+bool rq_shade_shape_ok(const rq_trace_tuning& t);
 int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_shade_params& p,
                         uint32_t* mask, float* ao, unsigned long long* counter, cudaStream_t st);
 

@@ -91,6 +91,10 @@ class MeshDesc(C.Structure):
                 ("num_triangles", C.c_uint32)]
 
 
+class TraceTuning(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("chunk", C.c_uint32), ("reg_cap", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class BatchTuning(C.Structure):
     _fields_ = [("build_threads", C.c_uint32), ("build_blocks", C.c_uint32), ("trace_threads", C.c_uint32),
                 ("trace_chunk", C.c_uint32), ("trace_reg_cap", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
@@ -131,6 +135,8 @@ SIGNATURES = [
     ("rq_ctx_last_error", C.c_char_p, [_P]),
     ("rq_ctx_check", C.c_int, [_P, _P]),
     ("rq_ctx_scratch_bytes", C.c_uint64, [_P]),
+    ("rq_ctx_trace_tuning_get", C.c_int, [_P, C.POINTER(TraceTuning)]),
+    ("rq_ctx_trace_tuning_set", C.c_int, [_P, C.POINTER(TraceTuning)]),
     ("rq_scene_grid", C.c_int, [_U32, _U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                 C.c_float, C.c_uint64, _P, _P]),
     ("rq_scene_rays_down", C.c_int, [_U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
@@ -269,6 +275,16 @@ class Context:
 
     def scratch_bytes(self):
         return int(lib().rq_ctx_scratch_bytes(self.h))
+
+    def trace_tuning(self):
+        """Launch shape of the shadow/AO traversal (rq_trace_tuning)."""
+        t = TraceTuning()
+        self.check(lib().rq_ctx_trace_tuning_get(self.h, C.byref(t)), "rq_ctx_trace_tuning_get")
+        return {"threads": t.threads, "chunk": t.chunk, "reg_cap": t.reg_cap}
+
+    def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80):
+        t = TraceTuning(threads, chunk, reg_cap, 0)
+        self.check(lib().rq_ctx_trace_tuning_set(self.h, C.byref(t)), "rq_ctx_trace_tuning_set")
 
 
 class Bvh:

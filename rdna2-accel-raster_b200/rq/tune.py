@@ -1,12 +1,15 @@
-"""Launch-shape table of the batched form, written by the autotuner.
+"""Launch-shape table written by the autotuner.
 
-`python -m rq.tune --out FILE` builds the batched workload (512 deforming
-grids, 4,096 any-hit + 4,096 closest-hit rays per mesh), runs
-rq_batch_autotune on it (every build block size x blocks per SM, every
-traversal block size x refill chunk x register cap, median of 5 timed runs
-each) and writes the chosen shapes and all measured candidates as JSON.  The
+`python -m rq.tune --out FILE` times, on the device:
+  - the 1080p shadows + AO frame's traversal (rq_render_shadow_ao) in every
+    block size x refill chunk x register budget (median of 5 runs each);
+  - the batched workload (512 deforming grids, 4,096 any-hit + 4,096
+    closest-hit rays per mesh) through rq_batch_autotune: every build block
+    size x blocks per SM, every traversal block size x chunk x register budget;
+and writes the chosen shapes and every measured candidate as JSON.  The
 committed copy (tuning_b200.json beside this file) is what the benchmark and
-callers load with `lookup`; a workload missing from it is tuned at run time.
+callers load with `lookup` / `lookup_shadow`; a workload missing from it is
+tuned at run time.
 """
 import argparse
 import json
@@ -36,6 +39,48 @@ def lookup(key, path=TABLE):
     return e["shape"] if e else None
 
 
+SHADE_SHAPES = [(t, c, r) for t in (64, 128, 256) for c in (32, 64) for r in (0, 64, 80)]
+
+
+def shadow_key(ntri, params):
+    return (f"shadow_ao:tris={ntri},{params.width}x{params.height},lights={params.num_lights},"
+            f"ao_spp={params.ao_spp}")
+
+
+def tune_shadow(ctx, bvh, gbuf, params, reps=5):
+    """Time rq_render_shadow_ao in every launch shape (median of `reps` after
+    one warm-up run) and keep the fastest on the context.  Returns (shape,
+    trials)."""
+    import statistics
+    import torch
+    import rq
+    n = params.width * params.height
+    mask = torch.empty(n, dtype=torch.int32, device="cuda")
+    ao = torch.empty(n, dtype=torch.float32, device="cuda")
+    trials = []
+    for t, c, r in SHADE_SHAPES:
+        ctx.set_trace_tuning(t, c, r)
+        rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao)
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao)
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        ctx.sync_check()
+        trials.append({"threads": t, "chunk": c, "reg_cap": r, "ms": statistics.median(ms)})
+    best = min(trials, key=lambda x: x["ms"])
+    ctx.set_trace_tuning(best["threads"], best["chunk"], best["reg_cap"])
+    return {k: best[k] for k in ("threads", "chunk", "reg_cap")}, trials
+
+
+def lookup_shadow(key, path=TABLE):
+    e = load(path).get("shadow", {}).get(key)
+    return e["shape"] if e else None
+
+
 def tune_batched(ctx, descs, pos, idx, rays, mesh, flags, reps=5):
     import rq
     b = rq.Batch(ctx, descs)
@@ -55,6 +100,22 @@ def main():
     ap.add_argument("--reps", type=int, default=5)
     args = ap.parse_args()
     ctx = rq.Context(0)
+    table = load(args.out) if os.path.exists(args.out) else {}
+    table.setdefault("device", torch.cuda.get_device_name(0))
+    # the 1080p shadows + AO frame
+    pos, idx = W.shadow_mesh()
+    p = torch.from_numpy(pos).cuda()
+    i = torch.from_numpy(idx.view(np.int32)).cuda()
+    bvh = rq.Bvh.build(ctx, p, i)
+    params = W.shadow_params()
+    gbuf = rq.render_gbuffer(ctx, bvh, W.shadow_camera())
+    shape, trials = tune_shadow(ctx, bvh, gbuf, params, args.reps)
+    table.setdefault("shadow", {})[shadow_key(len(idx), params)] = {
+        "workload": "1080p shadows + AO frame (2.5M-triangle grid, seed 1, 16 lights, 1 AO ray)",
+        "shape": shape, "ms": min(t["ms"] for t in trials), "trials": trials}
+    print(json.dumps({"shadow_shape": shape, "ms": min(t["ms"] for t in trials)}))
+    bvh.destroy()
+    del p, i, gbuf
     sizes = W.batched_sizes(512, seed=2)
     pos, idx, descs = W.batched_meshes(sizes, seed=2)
     rays, mesh, flags = W.batched_rays(descs, 4096, 4096, seed=2)
@@ -64,8 +125,6 @@ def main():
     m = torch.from_numpy(mesh.view(np.int32)).cuda()
     f = torch.from_numpy(flags.view(np.int32)).cuda()
     shape, trials = tune_batched(ctx, descs, p, i, r, m, f, args.reps)
-    table = load(args.out) if os.path.exists(args.out) else {}
-    table.setdefault("device", torch.cuda.get_device_name(0))
     table.setdefault("entries", {})
     table["entries"][workload_key(descs, 8192)] = {
         "workload": "batched: 512 grids (seed 2), 4,096 any-hit + 4,096 closest-hit rays per mesh",

@@ -116,7 +116,7 @@ def test_every_launch_shape_gives_identical_results(ctx):
             assert all(x.tobytes() == y.tobytes() for x, y in zip(want_tree[m], b.download(m))), (bt, blocks, m)
     for tt in (64, 128, 256):
         for chunk in (32, 64):
-            for cap in (0, 1):
+            for cap in (0, 64, 80):
                 b.set_tuning({"trace_threads": tt, "trace_chunk": chunk, "trace_reg_cap": cap, "stack_entries": 128})
                 got = b.trace(rays_t, mesh_t, flags_t)[0].cpu().numpy()
                 ctx.sync_check()
@@ -136,7 +136,7 @@ def test_autotune_keeps_a_measured_shape(ctx):
     shape, trials = b.autotune(p, i, rays_t, mesh_t, flags_t, reps=2)
     builds = [t for t in trials if t["build_ms"] > 0]
     traces = [t for t in trials if t["trace_ms"] > 0]
-    assert len(traces) == 12 and len(builds) >= 3
+    assert len(traces) == 18 and len(builds) >= 3
     assert shape["build_ms"] == min(t["build_ms"] for t in builds)
     assert shape["trace_ms"] == min(t["trace_ms"] for t in traces)
     assert shape["stack_entries"] >= 3 * (max(b.info(m)["depth4"] for m in range(len(descs))) + 2) + 1

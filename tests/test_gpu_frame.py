@@ -85,3 +85,25 @@ def test_full_1080p_workload_sampled(ctx):
     # rough) and one AO ray per pixel
     assert 0.6 * 16 * 1920 * 1080 < rays <= 17 * 1920 * 1080
     b.destroy()
+
+
+def test_every_shadow_launch_shape_gives_identical_results(ctx):
+    from rq import tune as T
+    pos, idx = rq.scene_grid(96, 96, seed=4)
+    b = build(ctx, pos, idx)
+    w, h = 256, 144
+    cam = W.shadow_camera(w, h)
+    params = rq.shade_params(w, h, W.shadow_lights(16), ao_spp=2, ao_tmax=0.5)
+    gb = rq.render_gbuffer(ctx, b, cam)
+    base = ctx.trace_tuning()
+    assert base == {"threads": 128, "chunk": 32, "reg_cap": 80}
+    want_m, want_a = [x.cpu().numpy() for x in rq.render_shadow_ao(ctx, b, gb, params)]
+    for t, c, r in T.SHADE_SHAPES:
+        ctx.set_trace_tuning(t, c, r)
+        m, a = rq.render_shadow_ao(ctx, b, gb, params)
+        ctx.sync_check()
+        assert np.array_equal(m.cpu().numpy(), want_m) and a.cpu().numpy().tobytes() == want_a.tobytes(), (t, c, r)
+    with pytest.raises(rq.RqError):
+        ctx.set_trace_tuning(96, 32, 0)
+    ctx.set_trace_tuning(**base)
+    b.destroy()
