@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=6000, help="pixels in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the visibility / batched / serving workloads")
+    ap.add_argument("--extra", choices=["visibility", "batched", "serving"],
+                    help="run only this workload (--steps frames / steps / x50 ms of arrivals) and print its JSON")
     return ap.parse_args()
 
 
@@ -712,8 +714,26 @@ def run_visibility(ctx, dev, stream, frames=200):
     return out
 
 
+def run_extra(args):
+    """One secondary workload alone (for profiling): its JSON object."""
+    import torch
+    import rq
+    dev = torch.device("cuda", 0)
+    ctx = rq.Context(0)
+    if args.extra == "visibility":
+        out = run_visibility(ctx, dev, torch.cuda.current_stream(dev), frames=max(1, args.steps))
+    elif args.extra == "batched":
+        out = run_batched(ctx, dev, steps=max(1, args.steps), plain_steps=1)
+    else:
+        out = run_serving(dev, duration_s=max(0.05, args.steps * 0.05))
+    print(json.dumps({"extra": args.extra, **out}))
+
+
 def main():
     args = parse()
+    if args.extra:
+        run_extra(args)
+        return
     world, rank, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":
