@@ -131,11 +131,16 @@ def barrier(pg):
         pg.barrier()
 
 
+def _pg_device(pg):
+    """Tensor device of the process group's backend (gloo: CPU, nccl: GPU)."""
+    return "cpu" if pg.get_backend() == "gloo" else "cuda"
+
+
 def max_over_ranks(pg, x):
     import torch
     if pg is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_pg_device(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -144,9 +149,17 @@ def sum_over_ranks(pg, x):
     import torch
     if pg is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_pg_device(pg))
     pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
+
+
+def replica_line(pg, rank, world, ms_local, rays_local):
+    """Whole-job figures of N independent replicas: the step time is the
+    slowest rank's, the work is every rank's; rank 0 reports."""
+    ms = max_over_ranks(pg, ms_local)
+    rays = sum_over_ranks(pg, rays_local)
+    return {"ms_per_step": ms, "value": rays / (ms * 1e-3) / 1e6, "n_gpus": world} if rank == 0 else None
 
 
 def read_traffic(name):
@@ -325,8 +338,9 @@ def run_ours(args, world, rank, local, pg):
     build_ms = [ev[1 + 4 * s].elapsed_time(ev[2 + 4 * s]) for s in range(args.steps)]
     prim_ms = [ev[2 + 4 * s].elapsed_time(ev[3 + 4 * s]) for s in range(args.steps)]
     shade_ms = [ev[3 + 4 * s].elapsed_time(ev[4 + 4 * s]) for s in range(args.steps)]
-    ms_step = max_over_ranks(pg, total_ms / args.steps)
-    value = sum_over_ranks(pg, frame_rays) / (ms_step * 1e-3) / 1e6
+    agg = replica_line(pg, rank, world, total_ms / args.steps, frame_rays)
+    ms_step = agg["ms_per_step"] if agg else total_ms / args.steps
+    value = agg["value"] if agg else 0.0
 
     # end to end through the C ABI with host buffers: H2D of the mesh from
     # pinned memory, the frame, D2H of the light masks and AO values
