@@ -60,7 +60,7 @@ typedef struct rq_trace_tuning {
     uint32_t threads;  /* per block: 64, 128 or 256 (default 128) */
     uint32_t chunk;    /* ray ids a warp takes per refill: 32 or 64 (default 32) */
     uint32_t reg_cap;  /* registers per thread the launch bounds allow: 0 (no bound), 64 or 80 (default) */
-    uint32_t reserved;
+    uint32_t top_levels; /* 0, or 4: each block stages the tree's top 4 levels (<= 85 nodes) in shared memory */
 } rq_trace_tuning;
 int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out);
 /* RQ_ERR_INVALID_ARG for a shape that has no kernel. */

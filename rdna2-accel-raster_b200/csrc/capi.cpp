@@ -208,7 +208,6 @@ int rq_ctx_trace_tuning_set(rq_ctx* ctx, const rq_trace_tuning* t) {
     if (!ctx || !t) return RQ_ERR_INVALID_ARG;
     if (!rq_shade_shape_ok(*t)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
     ctx->shade_shape = *t;
-    ctx->shade_shape.reserved = 0;
     return RQ_OK;
 }
 

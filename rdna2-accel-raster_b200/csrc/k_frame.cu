@@ -208,12 +208,15 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
 
 // TT threads per block, CHUNK ray ids per refill, REGS: launch bounds that
 // hold registers to REGS (0: none) — the tuned shapes; `stack` rows per lane.
-template <bool MT, bool STATS, int TT, int CHUNK, int REGS>
+template <bool MT, bool STATS, int TT, int CHUNK, int REGS, int TOP>
 __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     k_shadow_ao(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
                 const rq_gbuffer_px* __restrict__ gbuf, const __grid_constant__ ShadeArgs sa,
                 unsigned long long* words, unsigned long long* counters, uint32_t* ctr, uint32_t* err, int stack) {
-    extern __shared__ int32_t s_stack[];
+    extern __shared__ __align__(16) int32_t s_stack[];
+    // shared memory: the stack (stack rows x TT), then the staged top levels
+    float4* s_top = reinterpret_cast<float4*>(s_stack + stack * TT);
+    if (TOP > 0) rq::stage_top<TOP>(nodes, s_top);
     ShadeSrc<STATS> src;
     src.kinds = sa.nl + sa.spp;
     src.tiles_x = (sa.w + kTileW - 1) / kTileW;
@@ -221,8 +224,9 @@ __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     src.s = &sa;
     src.gbuf = gbuf;
     src.words = words;
-    rq::trace_persistent<true, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK>(nodes, tris, src, ctr,
-                                                                         s_stack + threadIdx.x, err, stack);
+    rq::trace_persistent<true, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK, TOP>(nodes, tris, src, ctr,
+                                                                              s_stack + threadIdx.x, err, stack,
+                                                                              s_top);
     if (counters) {
         const uint32_t r = __reduce_add_sync(rq::kFull, src.rays);
         if ((threadIdx.x & 31u) == 0 && r) atomicAdd(counters, (unsigned long long)r);
@@ -260,14 +264,15 @@ cudaError_t with_stack(uint32_t bound, F&& f) {
 // counting and reference-arithmetic variants).
 template <bool MT, bool STATS>
 const void* shade_kernel(const rq_trace_tuning& t) {
-#define RQ_SHAPE(T, C, R) \
-    if (t.threads == T && t.chunk == C && t.reg_cap == R) return reinterpret_cast<const void*>(k_shadow_ao<MT, STATS, T, C, R>);
-#define RQ_SHAPES(T, C) RQ_SHAPE(T, C, 0) RQ_SHAPE(T, C, 64) RQ_SHAPE(T, C, 80)
+#define RQ_SHAPE(T, C, R, L)                                                               \
+    if (t.threads == T && t.chunk == C && t.reg_cap == R && t.top_levels == L) \
+        return reinterpret_cast<const void*>(k_shadow_ao<MT, STATS, T, C, R, L>);
+#define RQ_SHAPES(T, C) RQ_SHAPE(T, C, 0, 0) RQ_SHAPE(T, C, 64, 0) RQ_SHAPE(T, C, 80, 0) RQ_SHAPE(T, C, 80, 4)
     if constexpr (!MT && !STATS) {
         RQ_SHAPES(64, 32) RQ_SHAPES(64, 64) RQ_SHAPES(128, 64) RQ_SHAPES(256, 32) RQ_SHAPES(256, 64)
-        RQ_SHAPE(128, 32, 64) RQ_SHAPE(128, 32, 80)
+        RQ_SHAPE(128, 32, 64, 0) RQ_SHAPE(128, 32, 80, 0) RQ_SHAPE(128, 32, 80, 4)
     }
-    RQ_SHAPE(128, 32, 0)
+    RQ_SHAPE(128, 32, 0, 0)
 #undef RQ_SHAPES
 #undef RQ_SHAPE
     return nullptr;
@@ -344,12 +349,13 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
     if (e == cudaSuccess && p.num_lights + p.ao_spp > 0) {
         // the counting and reference-arithmetic variants run in the default shape
         const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0} : ctx->shade_shape;
+        const size_t top_bytes = shape.top_levels == 4 ? rq::TopLevels<4>::kBytes : 0;
         const void* k = mt ? (stats ? shade_kernel<true, true>(shape) : shade_kernel<true, false>(shape))
                            : (stats ? shade_kernel<false, true>(shape) : shade_kernel<false, false>(shape));
         if (!k) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
         // stack rows: the bound for the tree's depth, rounded up to 4
         const int stack = int((bound + 3u) & ~3u);
-        const size_t smem = size_t(stack) * shape.threads * sizeof(int32_t);
+        const size_t smem = size_t(stack) * shape.threads * sizeof(int32_t) + top_bytes;
         if (smem > 48 * 1024) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         int per_sm = 0;
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, int(shape.threads), smem);

@@ -73,13 +73,92 @@ struct Hit {
     uint32_t boxes, tris;
 };
 
+// ----------------------------------------------------------- top levels
+// The top TOP levels of a 4-wide tree (at most (4^TOP - 1) / 3 nodes, the
+// root first, breadth-first) staged in shared memory by every block.  A
+// staged node occupies kTopStride float4 (144 B: node k starts 4 banks
+// after node k-1, so 16-B reads of different nodes by one quarter-warp do
+// not collide); its inner children that are staged too have child index
+// kStaged | slot.  Stack entries with kStaged name a shared-memory slot.
+constexpr int32_t kStaged = 0x40000000;
+constexpr int kTopStride = 9;
+
+template <int TOP>
+struct TopLevels {
+    static constexpr int kMax = TOP <= 0 ? 0 : ((1 << (2 * TOP)) - 1) / 3;
+    // shared memory: the nodes, slot -> global index, slot x child -> slot, count
+    static constexpr size_t kBytes = TOP <= 0 ? 0 : size_t(kMax) * kTopStride * 16 + size_t(kMax) * 5 * 4 + 16;
+};
+
+// Stage the top levels (call with the whole block, before any traversal).
+// `s_top` points at TopLevels<TOP>::kBytes of 16-B aligned shared memory.
+template <int TOP>
+__device__ __forceinline__ void stage_top(const rq_bvh4_node* __restrict__ nodes, float4* s_top) {
+    constexpr int kMax = TopLevels<TOP>::kMax;
+    int32_t* s_g = reinterpret_cast<int32_t*>(s_top + kMax * kTopStride);
+    int32_t* s_c = s_g + kMax;
+    uint32_t* s_n = reinterpret_cast<uint32_t*>(s_c + 4 * kMax);
+    if (threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        for (int i = lane; i < 4 * kMax; i += 32) s_c[i] = -1;
+        if (lane == 0) s_g[0] = 0;
+        __syncwarp();
+        uint32_t n = 1, lo = 0, hi = 1;
+        for (int lvl = 1; lvl < TOP; ++lvl) {
+            for (uint32_t b = lo; b < hi; b += 32) {
+                const uint32_t s = b + lane;
+                int4 ci = make_int4(0, 0, 0, 0), cc = make_int4(0, 0, 0, 0);
+                if (s < hi) {
+                    const int4* np = reinterpret_cast<const int4*>(nodes + s_g[s]);
+                    ci = __ldg(np + 6);
+                    cc = __ldg(np + 7);
+                }
+                const int32_t x[4] = {ci.x, ci.y, ci.z, ci.w}, c[4] = {cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const bool inner = s < hi && c[k] < 0;
+                    const uint32_t m = __ballot_sync(kFull, inner);
+                    if (inner) {
+                        const uint32_t slot = n + __popc(m & ((1u << lane) - 1u));
+                        s_g[slot] = x[k];
+                        s_c[4 * s + k] = int32_t(slot);
+                    }
+                    n += __popc(m);
+                }
+                __syncwarp();
+            }
+            lo = hi;
+            hi = n;
+        }
+        if (lane == 0) *s_n = n;
+    }
+    __syncthreads();
+    const uint32_t n = *s_n;
+    for (uint32_t i = threadIdx.x; i < n * 8u; i += blockDim.x) {
+        const uint32_t s = i >> 3, j = i & 7u;
+        float4 v = __ldg(reinterpret_cast<const float4*>(nodes + s_g[s]) + j);
+        if (j == 6) {
+            int32_t ci[4] = {__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z), __float_as_int(v.w)};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (s_c[4 * s + k] >= 0) ci[k] = kStaged | s_c[4 * s + k];
+            v = make_float4(__int_as_float(ci[0]), __int_as_float(ci[1]), __int_as_float(ci[2]), __int_as_float(ci[3]));
+        }
+        s_top[s * kTopStride + j] = v;
+    }
+    __syncthreads();
+}
+
 // STACK bounds the entries per lane (stk has STACK rows of STRIDE words);
 // stack_cap, if smaller, is the bound actually allocated.  CHUNK: ray ids
-// taken per atomic.
-template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src, int CHUNK = int(kChunk)>
+// taken per atomic.  TOP > 0: the top levels were staged in s_top by
+// stage_top<TOP> (single-BVH sources only).
+template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src, int CHUNK = int(kChunk), int TOP = 0>
 __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict__ nodes,
                                                  const rq_triangle* __restrict__ tris, Src& src, uint32_t* ctr,
-                                                 int32_t* stk, uint32_t* err, int stack_cap = STACK) {
+                                                 int32_t* stk, uint32_t* err, int stack_cap = STACK,
+                                                 const float4* s_top = nullptr) {
+    static_assert(TOP == 0 || !IsMulti<Src>::value, "top-level staging needs one BVH per launch");
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     // warp-uniform chunk of ray ids
@@ -135,7 +214,7 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                     h.idx = kNoHit;
                     h.u = h.v = 0.0f;
                     h.boxes = h.tris = 0;
-                    stk[0] = 0;
+                    stk[0] = TOP > 0 ? kStaged : 0;  // the root (slot 0 when staged)
                     sp = 1;
                 }
             }
@@ -160,13 +239,31 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                 leaf = e;
                 continue;
             }
-            const rq_bvh4_node* nb = IsMulti<Src>::value ? ray.nodes : nodes;
-            const float4* np = reinterpret_cast<const float4*>(nb + e);
-            const float4 mnx = ldg4(np + 0), mxx = ldg4(np + 1);
-            const float4 mny = ldg4(np + 2), mxy = ldg4(np + 3);
-            const float4 mnz = ldg4(np + 4), mxz = ldg4(np + 5);
-            const int4 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
-            const int4 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
+            float4 mnx, mxx, mny, mxy, mnz, mxz;
+            int4 cix, cnt;
+            if (TOP > 0 && (e & kStaged)) {
+                const float4* sp4 = s_top + (e & ~kStaged) * kTopStride;
+                mnx = sp4[0];
+                mxx = sp4[1];
+                mny = sp4[2];
+                mxy = sp4[3];
+                mnz = sp4[4];
+                mxz = sp4[5];
+                const float4 a = sp4[6], b = sp4[7];
+                cix = make_int4(__float_as_int(a.x), __float_as_int(a.y), __float_as_int(a.z), __float_as_int(a.w));
+                cnt = make_int4(__float_as_int(b.x), __float_as_int(b.y), __float_as_int(b.z), __float_as_int(b.w));
+            } else {
+                const rq_bvh4_node* nb = IsMulti<Src>::value ? ray.nodes : nodes;
+                const float4* np = reinterpret_cast<const float4*>(nb + e);
+                mnx = ldg4(np + 0);
+                mxx = ldg4(np + 1);
+                mny = ldg4(np + 2);
+                mxy = ldg4(np + 3);
+                mnz = ldg4(np + 4);
+                mxz = ldg4(np + 5);
+                cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
+                cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
+            }
             if (STATS) h.boxes += 4;
             const float amnx[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, amxx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
             const float amny[4] = {mny.x, mny.y, mny.z, mny.w}, amxy[4] = {mxy.x, mxy.y, mxy.z, mxy.w};

@@ -92,7 +92,7 @@ class MeshDesc(C.Structure):
 
 
 class TraceTuning(C.Structure):
-    _fields_ = [("threads", C.c_uint32), ("chunk", C.c_uint32), ("reg_cap", C.c_uint32), ("reserved", C.c_uint32)]
+    _fields_ = [("threads", C.c_uint32), ("chunk", C.c_uint32), ("reg_cap", C.c_uint32), ("top_levels", C.c_uint32)]
 
 
 class BatchTuning(C.Structure):
@@ -280,10 +280,10 @@ class Context:
         """Launch shape of the shadow/AO traversal (rq_trace_tuning)."""
         t = TraceTuning()
         self.check(lib().rq_ctx_trace_tuning_get(self.h, C.byref(t)), "rq_ctx_trace_tuning_get")
-        return {"threads": t.threads, "chunk": t.chunk, "reg_cap": t.reg_cap}
+        return {"threads": t.threads, "chunk": t.chunk, "reg_cap": t.reg_cap, "top_levels": t.top_levels}
 
-    def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80):
-        t = TraceTuning(threads, chunk, reg_cap, 0)
+    def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80, top_levels=0):
+        t = TraceTuning(threads, chunk, reg_cap, top_levels)
         self.check(lib().rq_ctx_trace_tuning_set(self.h, C.byref(t)), "rq_ctx_trace_tuning_set")
 
 

@@ -39,7 +39,8 @@ def lookup(key, path=TABLE):
     return e["shape"] if e else None
 
 
-SHADE_SHAPES = [(t, c, r) for t in (64, 128, 256) for c in (32, 64) for r in (0, 64, 80)]
+SHADE_SHAPES = ([(t, c, r, 0) for t in (64, 128, 256) for c in (32, 64) for r in (0, 64, 80)]
+                + [(t, c, 80, 4) for t in (64, 128, 256) for c in (32, 64)])
 
 
 def shadow_key(ntri, params):
@@ -58,8 +59,8 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
     mask = torch.empty(n, dtype=torch.int32, device="cuda")
     ao = torch.empty(n, dtype=torch.float32, device="cuda")
     trials = []
-    for t, c, r in SHADE_SHAPES:
-        ctx.set_trace_tuning(t, c, r)
+    for t, c, r, top in SHADE_SHAPES:
+        ctx.set_trace_tuning(t, c, r, top)
         rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao)
         ms = []
         for _ in range(reps):
@@ -70,10 +71,10 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
             b.synchronize()
             ms.append(a.elapsed_time(b))
         ctx.sync_check()
-        trials.append({"threads": t, "chunk": c, "reg_cap": r, "ms": statistics.median(ms)})
+        trials.append({"threads": t, "chunk": c, "reg_cap": r, "top_levels": top, "ms": statistics.median(ms)})
     best = min(trials, key=lambda x: x["ms"])
-    ctx.set_trace_tuning(best["threads"], best["chunk"], best["reg_cap"])
-    return {k: best[k] for k in ("threads", "chunk", "reg_cap")}, trials
+    ctx.set_trace_tuning(best["threads"], best["chunk"], best["reg_cap"], best["top_levels"])
+    return {k: best[k] for k in ("threads", "chunk", "reg_cap", "top_levels")}, trials
 
 
 def lookup_shadow(key, path=TABLE):
