@@ -616,8 +616,9 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
         return [rq.Request(ids[int(mesh[i])], int(kind[i]), int(nrays[i]), int(seeds[i]), 0, 0, None,
                            base + 16 * offs[i], i) for i in range(n)]
 
-    def one(mode):
-        cfg = dict(mode=mode, budget_bytes=120 << 30, slots=4, max_wave_rays=1 << 24, max_wave_requests=1024)
+    def one(mode, rebuild=False):
+        cfg = dict(mode=mode, budget_bytes=120 << 30, slots=4, max_wave_rays=1 << 24, max_wave_requests=1024,
+                   rebuild=rebuild)
         srv = rq.Server(**cfg)
         ids = [srv.add_mesh(p, i) for p, i in meshes]
         # warm the resident cache: one 1,000-ray request per mesh
@@ -661,6 +662,7 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
 
     b = one(rq.RQ_SERVE_BATCHED)
     p = one(rq.RQ_SERVE_PLAIN)
+    pr = one(rq.RQ_SERVE_PLAIN, rebuild=True)
     torch.cuda.synchronize(dev)
     return {
         "workload": (f"serving: Poisson {W.SERVE_RATE:.0f} req/s for {duration_s:g} s (seed 4, {n} requests), "
@@ -668,9 +670,14 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
                      f"(mean {sizes.mean() / 1e3:.1f}k), rays log-uniform in [1k, 2M] (mean {nrays.mean() / 1e3:.1f}k), "
                      "50% shadow / 30% AO / 20% closest hit generated in the launch; 120 GB budget"),
         "requests": n, "rays": int(nrays.sum()), "catalogue_triangles": int(sizes.sum()),
-        "batched": b, "plain": p,
+        "batched": b, "plain": p, "plain_rebuild": pr,
+        "plain_modes": ("plain: one request per launch, one launch in flight, BVHs resident; plain_rebuild: the "
+                        "same with the request's BVH rebuilt before its trace (per-request build + trace)"),
         "stream_p99_ratio_plain_over_batched": round(p["stream"]["p99_ms"] / b["stream"]["p99_ms"], 2),
+        "stream_p99_ratio_plain_rebuild_over_batched": round(pr["stream"]["p99_ms"] / b["stream"]["p99_ms"], 2),
         "saturation_throughput_ratio": round(b["saturation"]["mrays_per_s"] / p["saturation"]["mrays_per_s"], 2),
+        "saturation_throughput_ratio_vs_plain_rebuild": round(
+            b["saturation"]["mrays_per_s"] / pr["saturation"]["mrays_per_s"], 2),
     }
 
 

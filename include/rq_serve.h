@@ -48,6 +48,8 @@ typedef struct rq_server_config {
     uint32_t max_wave_requests; /* requests coalesced into one launch, 1..1024 (plain: 1) */
     uint32_t max_leaf;          /* leaf size of the builds, 1..16 */
     uint32_t trace_flags;       /* 0 watertight, RQ_TRI_MT reference Moeller-Trumbore */
+    uint32_t rebuild;           /* plain mode only: rebuild the mesh's BVH (in place) before every request,
+                                   the per-request build + trace of the reference's hosts */
 } rq_server_config;
 
 typedef struct rq_request {

@@ -291,6 +291,17 @@ struct rq_server {
             bool built = false;
             int rc = m ? make_resident(m, built) : RQ_ERR_INVALID_ARG;
             if (rc == 1) break;  // wait for in-flight requests to unpin memory
+            if (rc == 0 && !built && cfg.rebuild) {
+                // plain per-request build: in place on the build stream (one
+                // launch in flight in plain mode, so nothing else reads it)
+                rc = rq_build(ctx, m->d_pos, 12, m->nv, m->d_idx, m->nt, cfg.max_leaf, RQ_BUILD_BVH4, &m->bvh,
+                              build_st);
+                built = rc == 0;
+                if (built) {
+                    std::lock_guard<std::mutex> g(stats_mu);
+                    ++st.builds;
+                }
+            }
             if (rc == 0 && 3u * (m->depth4 + 2u) + 1u > 128u) rc = RQ_ERR_UNSUPPORTED;
             if (rc != 0) {
                 complete(p, rc, now(), false);
@@ -453,7 +464,8 @@ uint64_t rq_server_mesh_bytes(uint32_t num_vertices, uint32_t num_triangles) {
 int rq_server_create(int device, const rq_server_config* cfg, rq_server** out) {
     if (!cfg || !out) return RQ_ERR_INVALID_ARG;
     rq_server_config c = *cfg;
-    if (c.mode > RQ_SERVE_PLAIN || c.max_leaf < 1 || c.max_leaf > 16 || (c.trace_flags & ~RQ_TRI_MT))
+    if (c.mode > RQ_SERVE_PLAIN || c.max_leaf < 1 || c.max_leaf > 16 || (c.trace_flags & ~RQ_TRI_MT) ||
+        c.rebuild > 1 || (c.rebuild && c.mode != RQ_SERVE_PLAIN))
         return RQ_ERR_INVALID_ARG;
     if (c.mode == RQ_SERVE_PLAIN) {
         c.slots = 1;

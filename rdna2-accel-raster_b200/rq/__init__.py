@@ -105,7 +105,7 @@ class BatchTuning(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("mode", C.c_uint32), ("slots", C.c_uint32),
                 ("max_wave_rays", C.c_uint32), ("max_wave_requests", C.c_uint32), ("max_leaf", C.c_uint32),
-                ("trace_flags", C.c_uint32)]
+                ("trace_flags", C.c_uint32), ("rebuild", C.c_uint32)]
 
 
 class Request(C.Structure):
@@ -650,8 +650,9 @@ class Server:
     a memory budget and coalesced traversal launches."""
 
     def __init__(self, device=0, budget_bytes=120 << 30, mode=RQ_SERVE_BATCHED, slots=4, max_wave_rays=1 << 24,
-                 max_wave_requests=1024, max_leaf=4, trace_flags=0):
-        cfg = ServerConfig(budget_bytes, mode, slots, max_wave_rays, max_wave_requests, max_leaf, trace_flags)
+                 max_wave_requests=1024, max_leaf=4, trace_flags=0, rebuild=False):
+        cfg = ServerConfig(budget_bytes, mode, slots, max_wave_rays, max_wave_requests, max_leaf, trace_flags,
+                           1 if rebuild else 0)
         h = _P()
         rc = lib().rq_server_create(device, C.byref(cfg), C.byref(h))
         if rc:

@@ -100,11 +100,16 @@ def test_served_equals_alone_plain_and_oracle(ctx):
     assert st["evictions"] > 0 and st["peak_resident_bytes"] <= budget
     plain, pcomp, ptickets, pst = serve(meshes, reqs, bufs, mode=rq.RQ_SERVE_PLAIN)
     assert pst["launches"] == len(reqs) and pst["max_requests_per_launch"] == 1
+    rebuilt, _, _, rst = serve(meshes, reqs, bufs, mode=rq.RQ_SERVE_PLAIN, rebuild=True)
+    assert rst["builds"] == len(reqs)  # first use builds, every later use rebuilds
+    with pytest.raises(rq.ServeError):
+        rq.Server(rebuild=True)  # batched mode keeps resident BVHs
     oracle_checked = 0
     for k, (m, kind, c, seed, flags) in enumerate(reqs):
         want, rays = alone(ctx, meshes[m], kind, c, seed, flags, bufs.get(k))
         assert got[k].tobytes() == want.tobytes(), f"request {k}: mix differs from alone"
         assert plain[k].tobytes() == want.tobytes(), f"request {k}: plain differs from alone"
+        assert rebuilt[k].tobytes() == want.tobytes(), f"request {k}: plain with rebuilds differs from alone"
         if c <= 2000 and SIZES[m] <= 9000 and oracle_checked < 8:
             pos, idx = meshes[m]
             o = O.lbvh_build(pos.reshape(-1), idx.reshape(-1))
