@@ -34,7 +34,8 @@ typedef enum rq_status {
     RQ_ERR_UNSUPPORTED = 6,     /* input outside what the kernels handle (e.g. > 2^27 triangles) */
     RQ_ERR_BUDGET = 7,          /* serving: request does not fit the memory budget */
     RQ_ERR_NO_DEVICE = 8,       /* no CUDA device, or the device is not sm_100 */
-    RQ_ERR_STATE = 9            /* handle used before it was built */
+    RQ_ERR_STATE = 9,           /* handle used before it was built */
+    RQ_ERR_CANCELLED = 10       /* serving: the request was cancelled before it was admitted */
 } rq_status;
 
 /* ------------------------------------------------------------------ */
@@ -53,6 +54,12 @@ const char* rq_ctx_last_error(const rq_ctx* ctx);
 int rq_ctx_check(rq_ctx* ctx, rq_stream stream);
 /* Bytes of device scratch the context currently holds. */
 uint64_t rq_ctx_scratch_bytes(const rq_ctx* ctx);
+/* Check of the failure path of bounded device waits: one thread waits for
+ * the device word *flag to leave 0, with the wait the grid barriers use,
+ * for at most `limit` polls (<= 2^20, 64 ns apart).  If nothing changes the
+ * word, the wait gives up and the next rq_ctx_check reports
+ * RQ_ERR_DEVICE_TIMEOUT; the context stays usable. */
+int rq_debug_wait_timeout(rq_ctx* ctx, const uint32_t* flag, uint32_t limit, rq_stream stream);
 
 /* Launch shape of the context's persistent shadow/AO traversal
  * (rq_render_shadow_ao).  Results do not depend on it. */

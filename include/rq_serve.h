@@ -107,6 +107,19 @@ int rq_server_drain(rq_server* s, uint32_t timeout_ms);
 double rq_server_now(const rq_server* s);
 int rq_server_stats_get(rq_server* s, rq_server_stats* out);
 const char* rq_server_last_error(const rq_server* s);
+/* Cancel a submitted request: if it has not been admitted to a launch yet, it
+ * completes with RQ_ERR_CANCELLED; otherwise it completes as it would have.
+ * RQ_ERR_INVALID_ARG for a ticket this server never issued. */
+int rq_server_cancel(rq_server* s, uint64_t ticket);
+
+/* Host-side fault injection (for failure-handling tests): the next `count`
+ * mesh uploads fail as if the device allocation had failed (their requests
+ * complete with RQ_ERR_OOM), or the next `count` launches fail as if the
+ * launch had returned an error (their requests complete with RQ_ERR_CUDA).
+ * The server keeps serving afterwards.  Nothing faults on the device. */
+#define RQ_FAULT_ALLOC 1u
+#define RQ_FAULT_LAUNCH 2u
+int rq_server_inject_fault(rq_server* s, uint32_t kind, uint32_t count);
 
 /* The rays a generated request of `kind` traces (mesh-local primitive ids):
  * writes num_rays rays and, per ray, its trace flag (RQ_TRACE_ANY /

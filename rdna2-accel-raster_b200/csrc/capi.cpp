@@ -94,7 +94,8 @@ const char* kStatusText[] = {"ok",
                              "unsupported input",
                              "memory budget exceeded",
                              "no sm_100 device",
-                             "handle not built"};
+                             "handle not built",
+                             "request cancelled"};
 
 bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
 
@@ -176,7 +177,7 @@ int rq_ctx_destroy(rq_ctx* ctx) {
 }
 
 const char* rq_status_string(int status) {
-    if (status < 0 || status > RQ_ERR_STATE) return "unknown status";
+    if (status < 0 || status > RQ_ERR_CANCELLED) return "unknown status";
     return kStatusText[status];
 }
 
@@ -197,6 +198,12 @@ int rq_ctx_check(rq_ctx* ctx, rq_stream stream) {
 }
 
 uint64_t rq_ctx_scratch_bytes(const rq_ctx* ctx) { return ctx ? ctx->scratch_bytes : 0; }
+
+int rq_debug_wait_timeout(rq_ctx* ctx, const uint32_t* flag, uint32_t limit, rq_stream stream) {
+    if (!ctx || !flag || limit > (1u << 20)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad wait check");
+    cudaSetDevice(ctx->device);
+    return rq_launch_wait_check(ctx, flag, limit, S(stream));
+}
 
 int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out) {
     if (!ctx || !out) return RQ_ERR_INVALID_ARG;

@@ -56,15 +56,7 @@ __device__ bool grid_sync(uint32_t* ctl, uint32_t* err) {
                 __threadfence();
                 rq::st_release(ctl + 2, g + 1u);
             } else {
-                uint32_t spins = 0;
-                while (rq::ld_acquire(ctl + 2) == g) {
-                    if (++spins > kBarrierSpin) {
-                        rq::set_err(err, RQ_DERR_GRID_BARRIER);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
+                ok = rq::wait_change(ctl + 2, g, kBarrierSpin, err, RQ_DERR_GRID_BARRIER) ? 1u : 0u;
             }
         }
         s_ok = ok;

@@ -114,3 +114,19 @@ int rq_launch_deform(rq_ctx* ctx, const float* base, float* out, uint32_t nv, fl
     k_deform_wave<<<(nv + kT - 1) / kT, kT, 0, st>>>(base, out, nv, t, amp, freq);
     return rq_cuda_status(ctx, cudaGetLastError(), "deform launch");
 }
+
+// ------------------------------------------------------------ wait check
+namespace {
+
+// One bounded wait on *flag changing from 0: the wait of the grid barriers
+// (rq::wait_change), for checking that a wait that runs out reports.
+__global__ void k_wait_check(const uint32_t* flag, uint32_t limit, uint32_t* err) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) rq::wait_change(flag, 0u, limit, err, RQ_DERR_WAIT_CHECK);
+}
+
+}  // namespace
+
+int rq_launch_wait_check(rq_ctx* ctx, const uint32_t* flag, uint32_t limit, cudaStream_t st) {
+    k_wait_check<<<1, 32, 0, st>>>(flag, limit, ctx->d_err);
+    return rq_cuda_status(ctx, cudaGetLastError(), "wait check launch");
+}

@@ -270,4 +270,18 @@ __device__ __forceinline__ F3 cosine_hemisphere(F3 N, float u1, float u2) {
 
 __device__ __forceinline__ void set_err(uint32_t* err, uint32_t bit) { atomicOr(err, bit); }
 
+// Wait until *p (read with acquire) differs from v: at most `limit` polls,
+// 64 ns apart.  On giving up, sets `bit` in the error word and returns false.
+__device__ __forceinline__ bool wait_change(const uint32_t* p, uint32_t v, uint32_t limit, uint32_t* err,
+                                            uint32_t bit) {
+    for (uint32_t spins = 0; ld_acquire(p) == v;) {
+        if (++spins > limit) {
+            set_err(err, bit);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
 }  // namespace rq

@@ -17,6 +17,7 @@
 #define RQ_DERR_REFIT 8u
 #define RQ_DERR_STACK 16u
 #define RQ_DERR_QUEUE 32u
+#define RQ_DERR_WAIT_CHECK 64u
 
 // Largest triangle count a leaf stack entry can address (27-bit first prim).
 #define RQ_MAX_TRIANGLES (1u << 27)
@@ -151,5 +152,6 @@ int rq_launch_gen_procedural(rq_ctx* ctx, const float cam[3], const float look[3
                              uint32_t coherent, rq_ray* rays, cudaStream_t st);
 int rq_launch_deform(rq_ctx* ctx, const float* base, float* out, uint32_t nv, float t, float amp, float freq,
                      cudaStream_t st);
+int rq_launch_wait_check(rq_ctx* ctx, const uint32_t* flag, uint32_t limit, cudaStream_t st);
 int rq_launch_deform_step(rq_ctx* ctx, const float* base, float* out, uint32_t nv, uint32_t* state, float dt,
                           float amp, float freq, cudaStream_t st);

@@ -32,6 +32,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <unordered_set>
 #include <vector>
 
 #include "rq_internal.h"
@@ -113,6 +114,10 @@ struct rq_server {
     std::deque<Pending> incoming;
     uint64_t next_ticket = 1;
     bool stop = false;
+    std::unordered_set<uint64_t> cancel_in;  // tickets to cancel, handed to the worker
+
+    // host-side fault injection (rq_server_inject_fault)
+    std::atomic<uint32_t> fault_alloc{0}, fault_launch{0};
 
     std::mutex out_mu;
     std::condition_variable out_cv;
@@ -120,6 +125,7 @@ struct rq_server {
 
     // worker-owned
     std::deque<Pending> pending;
+    std::unordered_set<uint64_t> cancelled;
     Slot slots[kMaxSlots];
     uint32_t seq = 0;
     uint64_t tick = 0;
@@ -192,6 +198,10 @@ struct rq_server {
             if (!lru) return 1;
             evict(lru);
         }
+        if (fault_alloc.load() > 0) {  // injected: as if the allocation failed
+            --fault_alloc;
+            return RQ_ERR_OOM;
+        }
         // scratch for the largest mesh registered so far, so it rarely regrows
         BuildScratch probe;
         int rc = rq_ensure_scratch(ctx, rq_build_scratch_carve(nullptr, max_mesh_tris.load(), probe), build_st);
@@ -257,6 +267,7 @@ struct rq_server {
                 // otherwise the launch ended without finishing it
                 const int status = flagged ? RQ_OK : (q == cudaSuccess ? RQ_ERR_DEVICE_TIMEOUT : RQ_ERR_CUDA);
                 complete(jb.p, status, jb.t_admit, jb.built);
+                cancelled.erase(jb.p.ticket);  // a cancel that came too late
                 changed = true;
             }
             if (ended && sl.remaining == 0) {
@@ -286,6 +297,12 @@ struct rq_server {
         bool any_built = false, failed = false;
         while (!pending.empty() && sel.size() < cfg.max_wave_requests) {
             Pending& p = pending.front();
+            if (cancelled.erase(p.ticket)) {
+                complete(p, RQ_ERR_CANCELLED, now(), false);
+                pending.pop_front();
+                failed = true;
+                continue;
+            }
             if (!sel.empty() && rays + p.req.num_rays > cfg.max_wave_rays) break;
             MeshRec* m = mesh(p.req.mesh);
             bool built = false;
@@ -359,6 +376,10 @@ struct rq_server {
             e = cudaMemcpyAsync(d + kBeginsOff, hb, sizeof(uint32_t) * (nj + 1), cudaMemcpyHostToDevice, sl->st);
         if (e == cudaSuccess) e = cudaMemsetAsync(d + kDoneOff, 0, kDoneBytes + 256, sl->st);
         int rc = e == cudaSuccess ? RQ_OK : rq_cuda_status(ctx, e, "serve table upload");
+        if (rc == RQ_OK && fault_launch.load() > 0) {  // injected: as if the launch had failed
+            --fault_launch;
+            rc = rq_set_error(ctx, RQ_ERR_CUDA, "injected launch failure");
+        }
         if (rc == RQ_OK)
             rc = rq_launch_serve(ctx, reinterpret_cast<const ServeJob*>(d), reinterpret_cast<const uint32_t*>(d + kBeginsOff),
                                  nj, begin, depth, cfg.trace_flags, seqno, reinterpret_cast<uint32_t*>(d + kDoneOff),
@@ -399,6 +420,8 @@ struct rq_server {
                     pending.push_back(incoming.front());
                     incoming.pop_front();
                 }
+                cancelled.insert(cancel_in.begin(), cancel_in.end());
+                cancel_in.clear();
                 stopping = stop;
             }
             bool changed = poll();
@@ -624,6 +647,28 @@ int rq_server_stats_get(rq_server* s, rq_server_stats* out) {
 }
 
 const char* rq_server_last_error(const rq_server* s) { return s ? s->last_error.c_str() : ""; }
+
+int rq_server_cancel(rq_server* s, uint64_t ticket) {
+    if (!s) return RQ_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> g(s->in_mu);
+        if (ticket == 0 || ticket >= s->next_ticket) return RQ_ERR_INVALID_ARG;
+        s->cancel_in.insert(ticket);
+    }
+    s->in_cv.notify_one();
+    return RQ_OK;
+}
+
+int rq_server_inject_fault(rq_server* s, uint32_t kind, uint32_t count) {
+    if (!s) return RQ_ERR_INVALID_ARG;
+    if (kind == RQ_FAULT_ALLOC)
+        s->fault_alloc += count;
+    else if (kind == RQ_FAULT_LAUNCH)
+        s->fault_launch += count;
+    else
+        return RQ_ERR_INVALID_ARG;
+    return RQ_OK;
+}
 
 int rq_gen_mesh_rays(rq_ctx* ctx, const float* pos, const uint32_t* idx, uint32_t num_triangles, uint32_t kind,
                      uint32_t seed, uint32_t num_rays, rq_ray* rays, uint32_t* any_flags, rq_stream stream) {

@@ -28,6 +28,9 @@ RQ_ERR_UNSUPPORTED = 6
 RQ_ERR_BUDGET = 7
 RQ_ERR_NO_DEVICE = 8
 RQ_ERR_STATE = 9
+RQ_ERR_CANCELLED = 10
+RQ_FAULT_ALLOC = 1
+RQ_FAULT_LAUNCH = 2
 
 RQ_BUILD_BVH4 = 1
 RQ_TRACE_CLOSEST = 0
@@ -137,6 +140,7 @@ SIGNATURES = [
     ("rq_ctx_scratch_bytes", C.c_uint64, [_P]),
     ("rq_ctx_trace_tuning_get", C.c_int, [_P, C.POINTER(TraceTuning)]),
     ("rq_ctx_trace_tuning_set", C.c_int, [_P, C.POINTER(TraceTuning)]),
+    ("rq_debug_wait_timeout", C.c_int, [_P, _P, _U32, _P]),
     ("rq_scene_grid", C.c_int, [_U32, _U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                 C.c_float, C.c_uint64, _P, _P]),
     ("rq_scene_rays_down", C.c_int, [_U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
@@ -187,6 +191,8 @@ SIGNATURES = [
     ("rq_server_stats_get", C.c_int, [_P, C.POINTER(ServerStats)]),
     ("rq_server_last_error", C.c_char_p, [_P]),
     ("rq_gen_mesh_rays", C.c_int, [_P, _P, _P, _U32, _U32, _U32, _U32, _P, _P, _P]),
+    ("rq_server_cancel", C.c_int, [_P, C.c_uint64]),
+    ("rq_server_inject_fault", C.c_int, [_P, _U32, _U32]),
 ]
 
 RQ_RAYS_BUFFER = 0
@@ -281,6 +287,10 @@ class Context:
         t = TraceTuning()
         self.check(lib().rq_ctx_trace_tuning_get(self.h, C.byref(t)), "rq_ctx_trace_tuning_get")
         return {"threads": t.threads, "chunk": t.chunk, "reg_cap": t.reg_cap, "top_levels": t.top_levels}
+
+    def debug_wait_timeout(self, flag, limit, stream=None):
+        """One bounded device wait on flag (int32 CUDA tensor) leaving 0."""
+        self.check(lib().rq_debug_wait_timeout(self.h, _ptr(flag), limit, _stream(stream)), "rq_debug_wait_timeout")
 
     def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80, top_levels=0):
         t = TraceTuning(threads, chunk, reg_cap, top_levels)
@@ -721,6 +731,12 @@ class Server:
 
     def now(self):
         return lib().rq_server_now(self.h)
+
+    def cancel(self, ticket):
+        self._check(lib().rq_server_cancel(self.h, int(ticket)), "rq_server_cancel")
+
+    def inject_fault(self, kind, count=1):
+        self._check(lib().rq_server_inject_fault(self.h, kind, count), "rq_server_inject_fault")
 
     def stats(self):
         s = ServerStats()

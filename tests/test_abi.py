@@ -82,3 +82,25 @@ def test_scene_rays_down():
     assert r.shape == (1000, 8)
     assert np.allclose(np.linalg.norm(r[:, 4:7], axis=1), 1.0, atol=1e-6)
     assert np.all(r[:, 2] == 2.0) and np.all(r[:, 6] < 0)
+
+
+def test_status_strings_cover_every_status():
+    names = {rq.RQ_OK: "ok", rq.RQ_ERR_BUDGET: "memory budget exceeded", rq.RQ_ERR_CANCELLED: "request cancelled"}
+    for code, text in names.items():
+        assert rq.lib().rq_status_string(code).decode() == text
+    assert rq.lib().rq_status_string(11).decode() == "unknown status"
+
+
+def test_server_refuses_bad_configs_without_a_device():
+    # configuration checks run before any device call
+    bad = [dict(mode=7), dict(max_leaf=0), dict(slots=0), dict(slots=9), dict(max_wave_requests=2000),
+           dict(rebuild=True)]
+    for kw in bad:
+        with pytest.raises(rq.ServeError) as e:
+            rq.Server(**kw)
+        assert e.value.status == rq.RQ_ERR_INVALID_ARG, kw
+
+
+def test_server_mesh_bytes_is_host_only():
+    b = rq.Server.mesh_bytes(1000, 2000)
+    assert b >= 12 * 1000 + 12 * 2000 + 2000 * (64 + 48 + 8 + 128)
