@@ -68,6 +68,8 @@ typedef struct rq_trace_tuning {
     uint32_t chunk;    /* ray ids a warp takes per refill: 32 or 64 (default 32) */
     uint32_t reg_cap;  /* registers per thread the launch bounds allow: 0 (no bound), 64 or 80 (default) */
     uint32_t top_levels; /* 0, or 4: each block stages the tree's top 4 levels (<= 85 nodes) in shared memory */
+    uint32_t speculative; /* 1: lanes holding a leaf keep taking inner nodes while the warp searches
+                             (the frame only reports hit or miss, so the order does not show) */
 } rq_trace_tuning;
 int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out);
 /* RQ_ERR_INVALID_ARG for a shape that has no kernel. */

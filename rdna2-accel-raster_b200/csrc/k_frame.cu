@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
 
 // TT threads per block, CHUNK ray ids per refill, REGS: launch bounds that
 // hold registers to REGS (0: none) — the tuned shapes; `stack` rows per lane.
-template <bool MT, bool STATS, int TT, int CHUNK, int REGS, int TOP>
+template <bool MT, bool STATS, int TT, int CHUNK, int REGS, int TOP, bool SPEC>
 __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     k_shadow_ao(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
                 const rq_gbuffer_px* __restrict__ gbuf, const __grid_constant__ ShadeArgs sa,
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     src.s = &sa;
     src.gbuf = gbuf;
     src.words = words;
-    rq::trace_persistent<true, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK, TOP>(nodes, tris, src, ctr,
+    rq::trace_persistent<1, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK, TOP, SPEC>(nodes, tris, src, ctr,
                                                                               s_stack + threadIdx.x, err, stack,
                                                                               s_top);
     if (counters) {
@@ -264,15 +264,18 @@ cudaError_t with_stack(uint32_t bound, F&& f) {
 // counting and reference-arithmetic variants).
 template <bool MT, bool STATS>
 const void* shade_kernel(const rq_trace_tuning& t) {
-#define RQ_SHAPE(T, C, R, L)                                                               \
-    if (t.threads == T && t.chunk == C && t.reg_cap == R && t.top_levels == L) \
-        return reinterpret_cast<const void*>(k_shadow_ao<MT, STATS, T, C, R, L>);
-#define RQ_SHAPES(T, C) RQ_SHAPE(T, C, 0, 0) RQ_SHAPE(T, C, 64, 0) RQ_SHAPE(T, C, 80, 0) RQ_SHAPE(T, C, 80, 4)
+#define RQ_SHAPE(T, C, R, L, S)                                                                             \
+    if (t.threads == T && t.chunk == C && t.reg_cap == R && t.top_levels == L && (t.speculative != 0) == S) \
+        return reinterpret_cast<const void*>(k_shadow_ao<MT, STATS, T, C, R, L, S>);
+#define RQ_SHAPES(T, C)                                                                              \
+    RQ_SHAPE(T, C, 0, 0, false) RQ_SHAPE(T, C, 64, 0, false) RQ_SHAPE(T, C, 80, 0, false) RQ_SHAPE(T, C, 80, 4, false) \
+    RQ_SHAPE(T, C, 80, 0, true)
     if constexpr (!MT && !STATS) {
         RQ_SHAPES(64, 32) RQ_SHAPES(64, 64) RQ_SHAPES(128, 64) RQ_SHAPES(256, 32) RQ_SHAPES(256, 64)
-        RQ_SHAPE(128, 32, 64, 0) RQ_SHAPE(128, 32, 80, 0) RQ_SHAPE(128, 32, 80, 4)
+        RQ_SHAPE(128, 32, 64, 0, false) RQ_SHAPE(128, 32, 80, 0, false) RQ_SHAPE(128, 32, 80, 4, false)
+        RQ_SHAPE(128, 32, 80, 0, true)
     }
-    RQ_SHAPE(128, 32, 0, 0)
+    RQ_SHAPE(128, 32, 0, 0, false)
 #undef RQ_SHAPES
 #undef RQ_SHAPE
     return nullptr;
@@ -348,7 +351,7 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
     if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
     if (e == cudaSuccess && p.num_lights + p.ao_spp > 0) {
         // the counting and reference-arithmetic variants run in the default shape
-        const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0} : ctx->shade_shape;
+        const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0, 0} : ctx->shade_shape;
         const size_t top_bytes = shape.top_levels == 4 ? rq::TopLevels<4>::kBytes : 0;
         const void* k = mt ? (stats ? shade_kernel<true, true>(shape) : shade_kernel<true, false>(shape))
                            : (stats ? shade_kernel<false, true>(shape) : shade_kernel<false, false>(shape));

@@ -152,13 +152,18 @@ __device__ __forceinline__ void stage_top(const rq_bvh4_node* __restrict__ nodes
 // STACK bounds the entries per lane (stk has STACK rows of STRIDE words);
 // stack_cap, if smaller, is the bound actually allocated.  CHUNK: ray ids
 // taken per atomic.  TOP > 0: the top levels were staged in s_top by
-// stage_top<TOP> (single-BVH sources only).
-template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src, int CHUNK = int(kChunk), int TOP = 0>
+// stage_top<TOP> (single-BVH sources only).  SPEC: speculative traversal
+// (Aila and Laine 2009) — it changes the order in which a ray meets its
+// nodes, so it is only for any-hit rays whose result is hit or miss alone
+// (which triangle was found first is not reported by such sources).
+template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src, int CHUNK = int(kChunk), int TOP = 0,
+          bool SPEC = false>
 __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict__ nodes,
                                                  const rq_triangle* __restrict__ tris, Src& src, uint32_t* ctr,
                                                  int32_t* stk, uint32_t* err, int stack_cap = STACK,
                                                  const float4* s_top = nullptr) {
     static_assert(TOP == 0 || !IsMulti<Src>::value, "top-level staging needs one BVH per launch");
+    static_assert(!SPEC || ANY == 1, "speculative traversal changes which hit an any-hit ray finds first");
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     // warp-uniform chunk of ray ids
@@ -228,15 +233,24 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
             continue;
         }
 
-        // ---- inner phase
+        // ---- inner phase (SPEC: lanes holding a leaf keep taking inner
+        // nodes while other lanes still search; a second leaf stays on the
+        // stack and stalls the lane until the leaf phase)
         int32_t leaf = kNoLeaf;
+        bool stalled = false;
         for (;;) {
-            const bool want = active && sp > 0 && leaf == kNoLeaf;
-            if (!__any_sync(kFull, want)) break;
+            const bool searching = active && sp > 0 && leaf == kNoLeaf;
+            if (!__any_sync(kFull, searching)) break;
+            const bool want = SPEC ? (active && sp > 0 && !stalled) : searching;
             if (!want) continue;
             const int32_t e = stk[(--sp) * STRIDE];
             if (e < 0) {
-                leaf = e;
+                if (!SPEC || leaf == kNoLeaf) {
+                    leaf = e;
+                } else {
+                    ++sp;
+                    stalled = true;
+                }
                 continue;
             }
             float4 mnx, mxx, mny, mxy, mnz, mxz;

@@ -2,7 +2,8 @@
 
 `python -m rq.tune --out FILE` times, on the device:
   - the 1080p shadows + AO frame's traversal (rq_render_shadow_ao) in every
-    block size x refill chunk x register budget (median of 5 runs each);
+    block size x refill chunk x register budget, with and without staged top
+    levels and speculative traversal (median of 5 runs each);
   - the batched workload (512 deforming grids, 4,096 any-hit + 4,096
     closest-hit rays per mesh) through rq_batch_autotune: every build block
     size x blocks per SM, every traversal block size x chunk x register budget;
@@ -39,8 +40,10 @@ def lookup(key, path=TABLE):
     return e["shape"] if e else None
 
 
-SHADE_SHAPES = ([(t, c, r, 0) for t in (64, 128, 256) for c in (32, 64) for r in (0, 64, 80)]
-                + [(t, c, 80, 4) for t in (64, 128, 256) for c in (32, 64)])
+# (threads, refill chunk, register budget, staged top levels, speculative)
+SHADE_SHAPES = ([(t, c, r, 0, 0) for t in (64, 128, 256) for c in (32, 64) for r in (0, 64, 80)]
+                + [(t, c, 80, 4, 0) for t in (64, 128, 256) for c in (32, 64)]
+                + [(t, c, 80, 0, 1) for t in (64, 128, 256) for c in (32, 64)])
 
 
 def shadow_key(ntri, params):
@@ -59,8 +62,8 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
     mask = torch.empty(n, dtype=torch.int32, device="cuda")
     ao = torch.empty(n, dtype=torch.float32, device="cuda")
     trials = []
-    for t, c, r, top in SHADE_SHAPES:
-        ctx.set_trace_tuning(t, c, r, top)
+    for t, c, r, top, spec in SHADE_SHAPES:
+        ctx.set_trace_tuning(t, c, r, top, spec)
         rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao)
         ms = []
         for _ in range(reps):
@@ -71,10 +74,12 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
             b.synchronize()
             ms.append(a.elapsed_time(b))
         ctx.sync_check()
-        trials.append({"threads": t, "chunk": c, "reg_cap": r, "top_levels": top, "ms": statistics.median(ms)})
+        trials.append({"threads": t, "chunk": c, "reg_cap": r, "top_levels": top, "speculative": spec,
+                       "ms": statistics.median(ms)})
     best = min(trials, key=lambda x: x["ms"])
-    ctx.set_trace_tuning(best["threads"], best["chunk"], best["reg_cap"], best["top_levels"])
-    return {k: best[k] for k in ("threads", "chunk", "reg_cap", "top_levels")}, trials
+    keys = ("threads", "chunk", "reg_cap", "top_levels", "speculative")
+    ctx.set_trace_tuning(**{k: best[k] for k in keys})
+    return {k: best[k] for k in keys}, trials
 
 
 def lookup_shadow(key, path=TABLE):
