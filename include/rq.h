@@ -373,6 +373,20 @@ int rq_render_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera* cam, rq_g
 int rq_render_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_shade_params* params,
                         uint32_t* light_mask, float* ao, unsigned long long* counters, rq_stream stream);
 
+/* Depth z/w of every G-buffer position under the view-projection `view_proj`
+ * (column-major, Vulkan [0,1] depth; 1.0 for pixels that saw no geometry),
+ * the depth the AO blur compares.  Device pointers, npix pixels. */
+int rq_gbuffer_depth(rq_ctx* ctx, const rq_gbuffer_px* gbuf, uint32_t npix, const float view_proj[16], float* depth,
+                     rq_stream stream);
+/* One pass of the depth-aware separable AO blur of shaders/bilateral_blur.comp:
+ * a 9-tap Gaussian along (dir_x, dir_y) = (1, 0) or (0, 1), taps whose depth
+ * differs from the centre's by depth_threshold or more dropped, pixels at
+ * depth >= 1 passed through; taps clamped to the image edge.  w x h floats,
+ * device pointers, out must not alias in.  Run twice (horizontal, vertical)
+ * for the full blur. */
+int rq_blur_ao(rq_ctx* ctx, const float* ao_in, const float* depth, float* ao_out, uint32_t width, uint32_t height,
+               int dir_x, int dir_y, float depth_threshold, rq_stream stream);
+
 /* ------------------------------------------------------------------ */
 /* RADV image (fast_bvh_builder.comp)                                  */
 /* ------------------------------------------------------------------ */
@@ -404,6 +418,35 @@ int rq_build_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* 
 #define RQ_RADV_NOALLOC_MAX_TRIANGLES (1u << 24)
 int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, void* as_image, uint64_t as_bytes,
                           rq_stream stream);
+
+/* Text description of a RADV image in host memory: the header, the root node's
+ * children and, if child 0 is a triangle, that node — the text of the
+ * reference's decoder dump_bvh_structure (include/radv_bvh.hpp:311-390).
+ * Writes at most `capacity` bytes (NUL-terminated) and the full length to
+ * *length; text may be NULL with capacity 0 to ask for the length.
+ * RQ_ERR_SIZE when the text was cut. */
+int rq_radv_describe(const void* host_image, uint64_t bytes, char* text, uint64_t capacity, uint64_t* length);
+
+/* Device-side decode of a whole RADV image (every Box32 node, every child
+ * reference, every triangle node) with its invariants counted: child ids
+ * that leave their region, child boxes that differ from the child's own
+ * bounds, nodes or triangle ids referenced other than exactly once.  Reads
+ * are range-checked, so a damaged image is reported, not dereferenced.
+ * Synchronous. */
+typedef struct rq_radv_check {
+    uint32_t header_ok;            /* header offsets and counts fit the image */
+    uint32_t reserved;
+    uint64_t box_nodes;            /* from the header */
+    uint64_t triangle_nodes;
+    uint64_t box_children;         /* valid Box32 child references found */
+    uint64_t triangle_children;    /* valid triangle child references found */
+    uint64_t bad_offsets;          /* child ids outside their region or stride, or of another type */
+    uint64_t bad_boxes;            /* child boxes unequal to the child's bounds */
+    uint64_t box_refs_wrong;       /* box nodes referenced other than once (the root: never) */
+    uint64_t triangle_refs_wrong;  /* triangle nodes referenced other than once */
+    uint64_t ids_wrong;            /* triangle ids 0..N-1 not present exactly once */
+} rq_radv_check;
+int rq_radv_validate(rq_ctx* ctx, const void* as_image, uint64_t as_bytes, rq_radv_check* out, rq_stream stream);
 
 /* Trace rays through a RADV image (the rayQueryEXT role of
  * shaders/verify_rayquery.comp:41-59): primitive IDs are the nodes'

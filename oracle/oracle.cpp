@@ -1062,6 +1062,53 @@ void orc_gen_rays_procedural(const float cam[3], const float look[3], uint32_t c
 
 void orc_sincos(float x, float* s, float* c) { sincos_taylor(x, s, c); }
 
+// Depth z/w of G-buffer positions under the column-major view-projection
+// `vp` (1.0 where the pixel saw no geometry).
+void orc_gbuffer_depth(const rq_gbuffer_px* g, uint32_t npix, const float* vp, float* depth) {
+    for (uint32_t p = 0; p < npix; ++p) {
+        if (g[p].vis == 0u) {
+            depth[p] = 1.0f;
+            continue;
+        }
+        const float x = g[p].pos[0], y = g[p].pos[1], z = g[p].pos[2];
+        const float zc = ((vp[2] * x + vp[6] * y) + vp[10] * z) + vp[14];
+        const float wc = ((vp[3] * x + vp[7] * y) + vp[11] * z) + vp[15];
+        depth[p] = zc / wc;
+    }
+}
+
+// One pass of shaders/bilateral_blur.comp:15-55 along (dx, dy): the 9-tap
+// Gaussian with depth rejection, taps at whole texels clamped to the edge.
+void orc_blur_ao(const float* in, const float* depth, float* out, uint32_t w, uint32_t h, int dx, int dy,
+                 float threshold) {
+    const float wt[4] = {0.1945946f, 0.1216216f, 0.054054f, 0.016216f};
+    auto clampi = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x) {
+            const uint32_t p = y * w + x;
+            const float cv = in[p], cd = depth[p];
+            if (cd >= 1.0f) {
+                out[p] = cv;
+                continue;
+            }
+            float total = 0.227027f;
+            float result = cv * total;
+            for (int i = 1; i <= 4; ++i) {
+                const uint32_t qp = uint32_t(clampi(int(y) + dy * i, 0, int(h) - 1)) * w +
+                                    uint32_t(clampi(int(x) + dx * i, 0, int(w) - 1));
+                const uint32_t qn = uint32_t(clampi(int(y) - dy * i, 0, int(h) - 1)) * w +
+                                    uint32_t(clampi(int(x) - dx * i, 0, int(w) - 1));
+                const float wp = wt[i - 1] * (std::fabs(depth[qp] - cd) < threshold ? 1.0f : 0.0f);
+                result = result + in[qp] * wp;
+                total = total + wp;
+                const float wn = wt[i - 1] * (std::fabs(depth[qn] - cd) < threshold ? 1.0f : 0.0f);
+                result = result + in[qn] * wn;
+                total = total + wn;
+            }
+            out[p] = result / fmax_(total, 0.001f);
+        }
+}
+
 // The generated rays of the serving requests (kind 1 shadow, 2 AO, 3
 // closest), ray i from draws pcg_hash(base + k) / 2^32 with
 // base = pcg_hash(seed ^ pcg_hash(i)).  Shadow and AO rays start on a point

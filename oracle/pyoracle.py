@@ -58,6 +58,8 @@ def lib():
         L.orc_gen_rays_procedural.argtypes = [_P, _P, C.c_uint32, C.c_uint32, _P]
         L.orc_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.orc_gen_mesh_rays.argtypes = [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]
+        L.orc_gbuffer_depth.argtypes = [_P, C.c_uint32, _P, _P]
+        L.orc_blur_ao.argtypes = [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_float]
         _lib = L
     return _lib
 
@@ -82,6 +84,8 @@ def ref():
         R.ref_terrain.argtypes = [C.c_uint32, C.c_float, _P, _P, _P, _P]
         R.ref_tree_layout.argtypes = [C.c_uint32, _P, _P, _P, _P, _P]
         R.ref_dynamic_grid.argtypes = [C.c_uint32, C.c_float, C.c_float, _P, _P]
+        R.ref_dump_bvh_structure.argtypes = [_P, C.c_size_t, _P, C.c_size_t]
+        R.ref_dump_bvh_structure.restype = C.c_size_t
         _ref = R
     return _ref
 
@@ -179,6 +183,22 @@ def trace_radv(img, rays, flags=0, want_bary=False):
     lib().orc_trace_radv(_ptr(np.ascontiguousarray(img)), _ptr(rays), len(rays), flags, _ptr(hits), _ptr(bary),
                          threads())
     return hits, bary
+
+
+def gbuffer_depth(gbuf, view_proj):
+    g = np.ascontiguousarray(gbuf)
+    vp = np.ascontiguousarray(view_proj, np.float32).reshape(-1)
+    d = np.empty(len(g), np.float32)
+    lib().orc_gbuffer_depth(_ptr(g), len(g), _ptr(vp), _ptr(d))
+    return d
+
+
+def blur_ao(ao, depth, w, h, dx, dy, threshold):
+    a = np.ascontiguousarray(ao, np.float32)
+    d = np.ascontiguousarray(depth, np.float32)
+    out = np.empty(w * h, np.float32)
+    lib().orc_blur_ao(_ptr(a), _ptr(d), _ptr(out), w, h, dx, dy, threshold)
+    return out
 
 
 def gen_mesh_rays(pos, idx, kind, seed, count):
@@ -301,6 +321,16 @@ def ref_dynamic_grid(n, time_val=0.0, extent=2.0):
     cen = np.empty(3 * n, np.float32)
     R.ref_dynamic_grid(n, time_val, extent, _ptr(tri9), _ptr(cen))
     return tri9, cen
+
+
+def ref_dump_bvh_structure(image):
+    """The reference's text dump of a RADV image (bytes / uint8 array)."""
+    R = ref()
+    img = np.ascontiguousarray(np.frombuffer(bytes(image), np.uint8))
+    n = R.ref_dump_bvh_structure(_ptr(img), len(img), None, 0)
+    buf = C.create_string_buffer(n + 1)
+    R.ref_dump_bvh_structure(_ptr(img), len(img), buf, n + 1)
+    return buf.value.decode()
 
 
 def recover_perm(tris_leaf_order, pos, idx):

@@ -10,6 +10,8 @@
 #include "radv_bvh.hpp"
 
 #include <cstring>
+#include <sstream>
+#include <string>
 #include <new>
 
 extern "C" {
@@ -102,6 +104,20 @@ void ref_dynamic_grid(uint32_t n, float time_val, float extent, float* tri9, flo
         centroids[3 * i + 1] = m.centroids[i].y;
         centroids[3 * i + 2] = m.centroids[i].z;
     }
+}
+
+// rdna2::dump_bvh_structure (include/radv_bvh.hpp:311-390) into `out`
+// (at most cap bytes, NUL-terminated); returns the full text length.
+size_t ref_dump_bvh_structure(const void* image, size_t bytes, char* out, size_t cap) {
+    std::ostringstream s;
+    rdna2::dump_bvh_structure(image, bytes, s);
+    const std::string t = s.str();
+    if (cap) {
+        const size_t n = t.size() < cap ? t.size() : cap - 1;
+        std::memcpy(out, t.data(), n);
+        out[n] = '\0';
+    }
+    return t.size();
 }
 
 } // extern "C"

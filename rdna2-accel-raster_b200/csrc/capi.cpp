@@ -603,4 +603,30 @@ int rq_trace_radv(rq_ctx* ctx, const void* as_image, uint64_t as_bytes, const rq
     return rq_launch_trace_radv(ctx, as_image, as_bytes, rays, n, flags, hits, bary, S(stream));
 }
 
+int rq_gbuffer_depth(rq_ctx* ctx, const rq_gbuffer_px* gbuf, uint32_t npix, const float view_proj[16], float* depth,
+                     rq_stream stream) {
+    if (!ctx || (npix && (!gbuf || !depth)) || !view_proj) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (!aligned(gbuf, 16)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "misaligned G-buffer");
+    cudaSetDevice(ctx->device);
+    return rq_launch_gbuffer_depth(ctx, gbuf, npix, view_proj, depth, S(stream));
+}
+
+int rq_blur_ao(rq_ctx* ctx, const float* ao_in, const float* depth, float* ao_out, uint32_t width, uint32_t height,
+               int dir_x, int dir_y, float depth_threshold, rq_stream stream) {
+    if (!ctx || ((width && height) && (!ao_in || !depth || !ao_out)))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (!((dir_x == 1 && dir_y == 0) || (dir_x == 0 && dir_y == 1)))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "blur direction must be (1,0) or (0,1)");
+    if (ao_in == ao_out) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "blur output aliases its input");
+    cudaSetDevice(ctx->device);
+    return rq_launch_blur_ao(ctx, ao_in, depth, ao_out, width, height, dir_x, dir_y, depth_threshold, S(stream));
+}
+
+int rq_radv_validate(rq_ctx* ctx, const void* as_image, uint64_t as_bytes, rq_radv_check* out, rq_stream stream) {
+    if (!ctx || !as_image || !out) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (!aligned(as_image, 16)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "misaligned image");
+    cudaSetDevice(ctx->device);
+    return rq_launch_radv_check(ctx, as_image, as_bytes, out, S(stream));
+}
+
 }  // extern "C"

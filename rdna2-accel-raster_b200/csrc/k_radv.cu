@@ -14,6 +14,7 @@
 // then reduces its subtree in shared memory for up to five levels.  The last
 // block to finish (atomic ticket) builds the remaining top levels and the
 // header from the per-block subtree boxes.
+#include <algorithm>
 #include <mutex>
 
 #include "rq_device.cuh"
@@ -383,4 +384,176 @@ int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const 
     cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st);
     k_radv<<<blocks, kT, 0, st>>>(a);
     return rq_cuda_status(ctx, cudaGetLastError(), "radv build launch");
+}
+
+// ------------------------------------------------------------ validation
+// Decode a whole RADV image on the device and check its invariants.  Box
+// nodes sit at 128-B strides from the root up to the leaf region, triangle
+// nodes at 64-B strides after it (the header says where).  One thread per
+// box node checks its four children:
+//  - the child id decodes to an offset inside the right region and stride
+//    (every read below is range-checked first, so a corrupt image is only
+//    counted, never dereferenced out of bounds);
+//  - a Box32 child's box equals the union of that node's child boxes, a
+//    triangle child's box equals its triangle's bounds;
+//  - references per node and per triangle id are counted.
+// A second pass counts nodes referenced other than exactly once (the root:
+// never) and triangle ids not seen exactly once.
+namespace {
+
+struct RadvCheckArgs {
+    const uint8_t* img;
+    uint64_t bytes;
+    uint32_t root;
+    uint64_t leaf_off;
+    uint32_t boxes;
+    uint32_t tris;
+    uint32_t* box_refs;  // boxes
+    uint32_t* tri_refs;  // tris
+    uint32_t* id_refs;   // tris
+    unsigned long long* out;  // rq_radv_check counters
+};
+
+__device__ __forceinline__ void box_of(const rq_radv_box32& b, float mn[3], float mx[3], uint32_t& valid) {
+    valid = 0;
+    for (int k = 0; k < 3; ++k) {
+        mn[k] = INFINITY;
+        mx[k] = -INFINITY;
+    }
+    for (int c = 0; c < 4; ++c) {
+        if (b.children[c] == RQ_RADV_INVALID_NODE) continue;
+        ++valid;
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fminf(mn[k], b.coords[c][k]);
+            mx[k] = fmaxf(mx[k], b.coords[c][3 + k]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_radv_check(RadvCheckArgs a) {
+    const uint32_t b = blockIdx.x * 256u + threadIdx.x;
+    if (b >= a.boxes) return;
+    unsigned long long bad_off = 0, bad_box = 0, tri_nodes = 0, box_children = 0;
+    rq_radv_box32 node;
+    memcpy(&node, a.img + a.root + 128ull * b, sizeof(node));
+    for (int c = 0; c < 4; ++c) {
+        const uint32_t id = node.children[c];
+        if (id == RQ_RADV_INVALID_NODE) continue;
+        const uint64_t at = uint64_t(a.root) + (uint64_t(id & ~7u) << 3);
+        const uint32_t type = id & 7u;
+        if (type == RQ_RADV_NODE_BOX32) {
+            const uint64_t rel = at - a.root;
+            if (at < a.root || rel % 128u || rel / 128u >= a.boxes || at + 128u > a.bytes) {
+                ++bad_off;
+                continue;
+            }
+            const uint32_t cb = uint32_t(rel / 128u);
+            atomicAdd(a.box_refs + cb, 1u);
+            ++box_children;
+            rq_radv_box32 child;
+            memcpy(&child, a.img + at, sizeof(child));
+            float mn[3], mx[3];
+            uint32_t valid;
+            box_of(child, mn, mx, valid);
+            bool same = valid > 0;
+            for (int k = 0; k < 3; ++k)
+                same = same && mn[k] == node.coords[c][k] && mx[k] == node.coords[c][3 + k];
+            if (!same) ++bad_box;
+        } else if (type == RQ_RADV_NODE_TRIANGLE) {
+            if (at < a.leaf_off || (at - a.leaf_off) % 64u || (at - a.leaf_off) / 64u >= a.tris || at + 64u > a.bytes) {
+                ++bad_off;
+                continue;
+            }
+            atomicAdd(a.tri_refs + uint32_t((at - a.leaf_off) / 64u), 1u);
+            ++tri_nodes;
+            rq_radv_tri t;
+            memcpy(&t, a.img + at, sizeof(t));
+            if (t.triangle_id < a.tris) atomicAdd(a.id_refs + t.triangle_id, 1u);
+            bool same = true;
+            for (int k = 0; k < 3; ++k) {
+                const float lo = fminf(fminf(t.coords[0][k], t.coords[1][k]), t.coords[2][k]);
+                const float hi = fmaxf(fmaxf(t.coords[0][k], t.coords[1][k]), t.coords[2][k]);
+                same = same && lo == node.coords[c][k] && hi == node.coords[c][3 + k];
+            }
+            if (!same) ++bad_box;
+        } else {
+            ++bad_off;
+        }
+    }
+    if (bad_off) atomicAdd(a.out + 2, bad_off);
+    if (bad_box) atomicAdd(a.out + 3, bad_box);
+    if (tri_nodes) atomicAdd(a.out + 1, tri_nodes);
+    if (box_children) atomicAdd(a.out + 0, box_children);
+}
+
+__global__ void __launch_bounds__(256) k_radv_check_refs(RadvCheckArgs a) {
+    const uint32_t i = blockIdx.x * 256u + threadIdx.x;
+    unsigned long long wrong_box = 0, wrong_tri = 0, wrong_id = 0;
+    if (i < a.boxes && a.box_refs[i] != (i == 0 ? 0u : 1u)) wrong_box = 1;
+    if (i < a.tris && a.tri_refs[i] != 1u) wrong_tri = 1;
+    if (i < a.tris && a.id_refs[i] != 1u) wrong_id = 1;
+    if (wrong_box) atomicAdd(a.out + 4, wrong_box);
+    if (wrong_tri) atomicAdd(a.out + 5, wrong_tri);
+    if (wrong_id) atomicAdd(a.out + 6, wrong_id);
+}
+
+}  // namespace
+
+int rq_launch_radv_check(rq_ctx* ctx, const void* img, uint64_t bytes, rq_radv_check* out, cudaStream_t st) {
+    rq_radv_check r{};
+    if (bytes < sizeof(rq_radv_header)) {
+        r.header_ok = 0;
+        *out = r;
+        return RQ_OK;
+    }
+    rq_radv_header h;
+    cudaError_t e = cudaMemcpyAsync(&h, img, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return rq_cuda_status(ctx, e, "radv header read");
+    const uint64_t n = h.primitive_count;
+    r.header_ok = h.bvh_offset >= sizeof(rq_radv_header) && h.leaf_nodes_offset >= h.bvh_offset &&
+                  (h.leaf_nodes_offset - h.bvh_offset) % 128u == 0 && n > 0 && n < (1ull << 30) &&
+                  h.leaf_nodes_offset + 64ull * n <= bytes && h.size <= bytes;
+    if (!r.header_ok) {
+        *out = r;
+        return RQ_OK;
+    }
+    const uint32_t boxes = uint32_t((h.leaf_nodes_offset - h.bvh_offset) / 128u);
+    r.box_nodes = boxes;
+    r.triangle_nodes = n;
+    const size_t need = sizeof(unsigned long long) * 8 + sizeof(uint32_t) * (size_t(boxes) + 2 * n) + 256;
+    int rc = rq_ensure_scratch(ctx, need, st);
+    if (rc) return rc;
+    Carve c{reinterpret_cast<uintptr_t>(ctx->scratch), 0};
+    RadvCheckArgs a;
+    a.img = static_cast<const uint8_t*>(img);
+    a.bytes = bytes;
+    a.root = h.bvh_offset;
+    a.leaf_off = h.leaf_nodes_offset;
+    a.boxes = boxes;
+    a.tris = uint32_t(n);
+    a.out = c.take<unsigned long long>(8);
+    a.box_refs = c.take<uint32_t>(boxes);
+    a.tri_refs = c.take<uint32_t>(n);
+    a.id_refs = c.take<uint32_t>(n);
+    e = cudaMemsetAsync(ctx->scratch, 0, c.off, st);
+    if (e == cudaSuccess) {
+        k_radv_check<<<(boxes + 255) / 256, 256, 0, st>>>(a);
+        const uint32_t m = std::max<uint32_t>(boxes, uint32_t(n));
+        k_radv_check_refs<<<(m + 255) / 256, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    unsigned long long cnt[8] = {0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, a.out, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return rq_cuda_status(ctx, e, "radv check");
+    r.box_children = cnt[0];
+    r.triangle_children = cnt[1];
+    r.bad_offsets = cnt[2];
+    r.bad_boxes = cnt[3];
+    r.box_refs_wrong = cnt[4];
+    r.triangle_refs_wrong = cnt[5];
+    r.ids_wrong = cnt[6];
+    *out = r;
+    return RQ_OK;
 }

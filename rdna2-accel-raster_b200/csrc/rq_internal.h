@@ -146,6 +146,13 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
 
 // ---------------------------------------------------------------- k_radv
 int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st);
+int rq_launch_radv_check(rq_ctx* ctx, const void* img, uint64_t bytes, rq_radv_check* out, cudaStream_t st);
+
+// ---------------------------------------------------------------- k_post
+int rq_launch_gbuffer_depth(rq_ctx* ctx, const rq_gbuffer_px* gbuf, uint32_t npix, const float vp[16], float* depth,
+                            cudaStream_t st);
+int rq_launch_blur_ao(rq_ctx* ctx, const float* in, const float* depth, float* out, uint32_t w, uint32_t h, int dx,
+                      int dy, float threshold, cudaStream_t st);
 
 // ---------------------------------------------------------------- k_raygen
 int rq_launch_gen_procedural(rq_ctx* ctx, const float cam[3], const float look[3], uint32_t count,

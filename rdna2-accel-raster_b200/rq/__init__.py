@@ -61,6 +61,12 @@ class BvhInfo(C.Structure):
                 ("device_bytes", C.c_uint64)]
 
 
+class RadvCheck(C.Structure):
+    _fields_ = [("header_ok", C.c_uint32), ("reserved", C.c_uint32)] + [
+        (k, C.c_uint64) for k in ("box_nodes", "triangle_nodes", "box_children", "triangle_children", "bad_offsets",
+                                  "bad_boxes", "box_refs_wrong", "triangle_refs_wrong", "ids_wrong")]
+
+
 class RadvLayout(C.Structure):
     _fields_ = [("num_triangles", C.c_uint32), ("total_boxes", C.c_uint32), ("num_levels", C.c_uint32),
                 ("total_as_size_lo", C.c_uint32), ("total_as_size", C.c_uint64),
@@ -164,10 +170,14 @@ SIGNATURES = [
     ("rq_camera_look_at", C.c_int, [_P, _P, _P, C.c_float, _U32, _U32, C.POINTER(Camera)]),
     ("rq_render_gbuffer", C.c_int, [_P, _P, C.POINTER(Camera), _P, _P]),
     ("rq_render_shadow_ao", C.c_int, [_P, _P, _P, C.POINTER(ShadeParams), _P, _P, _P, _P]),
+    ("rq_gbuffer_depth", C.c_int, [_P, _P, _U32, _P, _P, _P]),
+    ("rq_blur_ao", C.c_int, [_P, _P, _P, _P, _U32, _U32, C.c_int, C.c_int, C.c_float, _P]),
     ("rq_radv_layout_get", C.c_int, [_U32, C.POINTER(RadvLayout)]),
     ("rq_radv_size", C.c_uint64, [_U32]),
     ("rq_build_radv", C.c_int, [_P, _P, _U32, _P, C.c_uint64, _P]),
     ("rq_trace_radv", C.c_int, [_P, _P, C.c_uint64, _P, _U32, _U32, _P, _P, _P]),
+    ("rq_radv_describe", C.c_int, [_P, C.c_uint64, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("rq_radv_validate", C.c_int, [_P, _P, C.c_uint64, C.POINTER(RadvCheck), _P]),
     ("rq_build_radv_noalloc", C.c_int, [_P, _U32, _P, C.c_uint64, _P]),
     ("rq_batch_create", C.c_int, [_P, C.POINTER(MeshDesc), _U32, _U32, C.POINTER(_P)]),
     ("rq_batch_build", C.c_int, [_P, _P, _P, _U32, _P, _P]),
@@ -538,6 +548,29 @@ def build_radv(ctx, tri9, image=None, stream=None):
     return image
 
 
+def radv_describe(image):
+    """Text of a RADV image held on the host (bytes or a uint8 array), as the
+    reference's decoder prints it.  Host only: no device needed."""
+    img = np.ascontiguousarray(np.frombuffer(bytes(image), np.uint8))
+    n = C.c_uint64()
+    rc = lib().rq_radv_describe(_ptr(img), len(img), None, 0, C.byref(n))
+    if rc:
+        raise RqError(rc, "rq_radv_describe")
+    buf = C.create_string_buffer(n.value + 1)
+    rc = lib().rq_radv_describe(_ptr(img), len(img), buf, n.value + 1, C.byref(n))
+    if rc:
+        raise RqError(rc, "rq_radv_describe")
+    return buf.value.decode()
+
+
+def radv_validate(ctx, image, stream=None):
+    """Device-side decode and invariant counts of a RADV image (uint8 CUDA tensor)."""
+    out = RadvCheck()
+    ctx.check(lib().rq_radv_validate(ctx.h, _ptr(image), _count(image, 1), C.byref(out), _stream(stream)),
+              "rq_radv_validate")
+    return {k: getattr(out, k) for k, _ in RadvCheck._fields_ if k != "reserved"}
+
+
 def trace_radv(ctx, image, rays, flags=0, bary=False, stream=None):
     import torch
     n = _count(rays, 32)
@@ -605,6 +638,32 @@ def render_gbuffer(ctx, bvh, cam, gbuf=None, stream=None):
         gbuf = torch.empty((cam.width * cam.height, 8), dtype=torch.int32, device="cuda")
     ctx.check(lib().rq_render_gbuffer(ctx.h, bvh.h, C.byref(cam), _ptr(gbuf), _stream(stream)), "rq_render_gbuffer")
     return gbuf
+
+
+def view_proj_of(cam):
+    """Forward view-projection (column-major float32[16]) of a camera, the
+    inverse of its inv_view_proj computed in double precision."""
+    inv = np.array(cam.inv_view_proj, np.float64).reshape(4, 4).T
+    return np.ascontiguousarray(np.linalg.inv(inv).T.reshape(-1), np.float32)
+
+
+def gbuffer_depth(ctx, gbuf, view_proj, depth=None, stream=None):
+    """G-buffer (int32 [n,8] CUDA tensor) -> float32 [n] depth z/w (1.0 for misses)."""
+    import torch
+    n = _count(gbuf, 32)
+    depth = depth if depth is not None else torch.empty(n, dtype=torch.float32, device=gbuf.device)
+    vp = np.ascontiguousarray(view_proj, np.float32)
+    ctx.check(lib().rq_gbuffer_depth(ctx.h, _ptr(gbuf), n, _ptr(vp), _ptr(depth), _stream(stream)), "rq_gbuffer_depth")
+    return depth
+
+
+def blur_ao(ctx, ao, depth, width, height, dir_x, dir_y, threshold, out=None, stream=None):
+    """One pass of the depth-aware AO blur (float32 CUDA tensors of width*height)."""
+    import torch
+    out = out if out is not None else torch.empty_like(ao)
+    ctx.check(lib().rq_blur_ao(ctx.h, _ptr(ao), _ptr(depth), _ptr(out), width, height, dir_x, dir_y, threshold,
+                               _stream(stream)), "rq_blur_ao")
+    return out
 
 
 def render_shadow_ao(ctx, bvh, gbuf, params, mask=None, ao=None, counter=None, stream=None):

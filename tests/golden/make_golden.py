@@ -56,6 +56,16 @@ def main():
         grids[f"tri9_{n}"] = tri9
         grids[f"cen_{n}"] = cen
     np.savez_compressed(os.path.join(HERE, "ref_dynamic_grids.npz"), **grids)
+
+    # the reference decoder's text (dump_bvh_structure) of the RADV images of
+    # those grids (images from the fast-builder restatement, byte-equal to
+    # the device builder's)
+    dumps = {}
+    for n in (64, 256, 1024, 4096):
+        img = O.radv_build(grids[f"tri9_{n}"])
+        dumps[str(n)] = O.ref_dump_bvh_structure(img.tobytes())
+    with open(os.path.join(HERE, "radv_dumps.json"), "w") as f:
+        json.dump(dumps, f, indent=1)
     print("golden fixtures written to", HERE)
 
 

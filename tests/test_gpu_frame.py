@@ -107,3 +107,36 @@ def test_every_shadow_launch_shape_gives_identical_results(ctx):
         ctx.set_trace_tuning(96, 32, 0)
     ctx.set_trace_tuning(**base)
     b.destroy()
+
+
+def test_ao_blur_chain_bit_exact(ctx):
+    # frame -> AO -> depth -> horizontal blur -> vertical blur, against the
+    # oracle's statement of shaders/bilateral_blur.comp
+    pos, idx = rq.scene_grid(128, 128, seed=1)
+    b = build(ctx, pos, idx)
+    n2, tr, n4, perm = b.download()
+    w, h = 320, 180
+    cam = W.shadow_camera(w, h)
+    params = rq.shade_params(w, h, W.shadow_lights(16), ao_spp=4, ao_tmax=0.5)
+    gb, mask, ao, _ = frame(ctx, b, cam, params)
+    vp = rq.view_proj_of(cam)
+    depth = rq.gbuffer_depth(ctx, gb, vp)
+    d_want = O.gbuffer_depth(gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1), vp)
+    assert depth.cpu().numpy().tobytes() == d_want.tobytes()
+    dn = depth.cpu().numpy()
+    assert 0.0 < dn.min() and dn.max() < 1.0, "every pixel sees the mesh"
+    for thr in (1e-4, 5e-3, 1.0):
+        hpass = rq.blur_ao(ctx, ao, depth, w, h, 1, 0, thr)
+        vpass = rq.blur_ao(ctx, hpass, depth, w, h, 0, 1, thr)
+        ctx.sync_check()
+        oh = O.blur_ao(ao.cpu().numpy(), d_want, w, h, 1, 0, thr)
+        ov = O.blur_ao(oh, d_want, w, h, 0, 1, thr)
+        assert hpass.cpu().numpy().tobytes() == oh.tobytes(), thr
+        assert vpass.cpu().numpy().tobytes() == ov.tobytes(), thr
+    # background pixels (depth 1) pass through unchanged
+    d1 = torch.ones_like(depth)
+    same = rq.blur_ao(ctx, ao, d1, w, h, 1, 0, 0.01)
+    assert torch.equal(same, ao)
+    with pytest.raises(rq.RqError):
+        rq.blur_ao(ctx, ao, depth, w, h, 1, 1, 0.01)
+    b.destroy()

@@ -98,3 +98,50 @@ def test_radv_size_errors(ctx):
     with pytest.raises(rq.RqError) as e:
         rq.build_radv(ctx, t, image=small)
     assert e.value.status == rq.RQ_ERR_SIZE
+
+
+def test_device_images_describe_like_the_reference(ctx):
+    import json
+    grids = np.load(GRIDS)
+    dumps = json.load(open(GRIDS.replace("ref_dynamic_grids.npz", "radv_dumps.json")))
+    for n, text in dumps.items():
+        img = radv_gpu(ctx, grids[f"tri9_{n}"])
+        assert rq.radv_describe(img.cpu().numpy().tobytes()) == text, n
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 64, 4097, 100000])
+def test_validate_clean_images(ctx, n):
+    tri9 = np.random.default_rng(n).standard_normal(9 * n).astype(np.float32)
+    img = radv_gpu(ctx, tri9)
+    r = rq.radv_validate(ctx, img)
+    lay = rq.radv_layout(n)
+    assert r["header_ok"] == 1 and r["box_nodes"] == lay["total_boxes"] and r["triangle_nodes"] == n
+    assert r["box_children"] == lay["total_boxes"] - 1 and r["triangle_children"] == n
+    for k in ("bad_offsets", "bad_boxes", "box_refs_wrong", "triangle_refs_wrong", "ids_wrong"):
+        assert r[k] == 0, (k, r)
+
+
+def test_validate_reports_damage(ctx):
+    n = 1000
+    tri9 = np.random.default_rng(7).standard_normal(9 * n).astype(np.float32)
+    img = radv_gpu(ctx, tri9)
+    host = img.cpu().numpy()
+    leaf = int(host[96:104].view(np.uint64)[0])
+
+    def check(mutate):
+        h = host.copy()
+        mutate(h)
+        return rq.radv_validate(ctx, torch.from_numpy(h).cuda())
+
+    # a root child id that points past the image: counted, never read
+    r = check(lambda h: h.__setitem__(slice(196, 200), np.frombuffer((0x7ffffff8 | 5).to_bytes(4, "little"), np.uint8)))
+    assert r["bad_offsets"] >= 1 and r["box_refs_wrong"] >= 1
+    # a moved vertex in the first triangle node: its parent's box no longer fits
+    r = check(lambda h: h.__setitem__(slice(leaf, leaf + 4), np.frombuffer(np.float32(99.0).tobytes(), np.uint8)))
+    assert r["bad_boxes"] >= 1 and r["bad_offsets"] == 0
+    # two triangle nodes with the same id
+    r = check(lambda h: h.__setitem__(slice(leaf + 64 + 48, leaf + 64 + 52), h[leaf + 48:leaf + 52].copy()))
+    assert r["ids_wrong"] == 2
+    # a header whose leaf region runs past the image
+    r = check(lambda h: h.__setitem__(slice(96, 104), np.frombuffer(np.uint64(len(h)).tobytes(), np.uint8)))
+    assert r["header_ok"] == 0
