@@ -372,8 +372,34 @@ def run_ours(args, world, rank, local, pg):
     e2e_ms = max_over_ranks(pg, a.elapsed_time(b) / args.steps)
     e2e_value = sum_over_ranks(pg, frame_rays) / (e2e_ms * 1e-3) / 1e6
 
+    # the AO consumer after the frame: depth from the G-buffer, then the
+    # horizontal and vertical passes of the depth-aware blur (not part of the
+    # frame step above; timed on its own)
+    vp = rq.view_proj_of(cam)
+    depth = rq.gbuffer_depth(ctx, gbuf, vp)
+    tmp, blurred = torch.empty_like(ao), torch.empty_like(ao)
+
+    def blur_chain():
+        rq.gbuffer_depth(ctx, gbuf, vp, depth)
+        rq.blur_ao(ctx, ao, depth, WIDTH, HEIGHT, 1, 0, 0.005, tmp)
+        rq.blur_ao(ctx, tmp, depth, WIDTH, HEIGHT, 0, 1, 0.005, blurred)
+
+    for _ in range(3):
+        blur_chain()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(20):
+        blur_chain()
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    blur_ms = a.elapsed_time(b) / 20
+    # compulsory bytes per pixel: G-buffer 32 B in + depth 4 B out, then per
+    # pass AO and depth 4 + 4 B in and 4 B out (the other taps hit in cache)
+    blur = {"workload": "AO depth + 2-pass bilateral blur at 1920x1080", "ms": round(blur_ms, 4),
+            "gb_per_s_compulsory": round(npx * (36 + 2 * 12) / (blur_ms * 1e-3) / 1e9, 1)}
+
     bvh.destroy()
-    del p_d, i_d, gbuf, mask, ao
+    del p_d, i_d, gbuf, mask, ao, depth, tmp, blurred
     vis = run_visibility(ctx, dev, stream) if not args.no_extra else None
     batched = run_batched(ctx, dev) if not args.no_extra else None
     serving = run_serving(dev) if not args.no_extra else None
@@ -439,6 +465,7 @@ def run_ours(args, world, rank, local, pg):
         "clocks": clocks,
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "shadow_tuning": shade_tuning,
+        "ao_blur": blur,
         "visibility": vis,
         "batched": batched,
         "serving": serving,
