@@ -260,6 +260,34 @@ int rq_batch_download(rq_batch* batch, uint32_t mesh, int host, rq_bvh2_node* no
                       uint32_t* perm, uint32_t cap_perm);
 int rq_batch_destroy(rq_batch* batch);
 
+/* ------------------------------------------------------------------ */
+/* Two-level scenes: instances of BLAS handles under a top-level BVH   */
+/* ------------------------------------------------------------------ */
+
+typedef struct rq_tlas rq_tlas;
+
+/* One instance, as VkAccelerationStructureInstanceKHR describes it
+ * (benchmarks/exp1_visbuf/visbuf_main.cpp:762-771). */
+typedef struct rq_instance {
+    float transform[12];  /* object -> world, row-major 3x4 (VkTransformMatrixKHR) */
+    uint32_t instance_id; /* reported as rq_hit.instance_id (instanceCustomIndex) */
+    uint32_t mask;        /* seen by rays whose cull mask shares a bit with it */
+    const rq_bvh* blas;   /* built with RQ_BUILD_BVH4; many instances may share one */
+} rq_instance;
+
+/* Build the top level over `num_instances` instances (host array; copied).
+ * The handle refers to the BLAS arrays: keep them alive and unchanged (an
+ * in-place rebuild or refit of a BLAS needs a new rq_tlas_build).  Replaces
+ * the driver TLAS build of common/vk_bvh.cpp:237-336.  Synchronises once. */
+int rq_tlas_build(rq_ctx* ctx, const rq_instance* instances, uint32_t num_instances, rq_tlas** out,
+                  rq_stream stream);
+/* Trace rays through the scene: hits carry the instance id and the BLAS's
+ * mesh-local primitive id; t is world-space.  `cull_mask` as rayQueryEXT's
+ * cullMask (0xff: every instance).  Flags as rq_trace. */
+int rq_tlas_trace(rq_ctx* ctx, const rq_tlas* tlas, const rq_ray* rays, uint32_t n, uint32_t flags,
+                  uint32_t cull_mask, rq_hit* hits, rq_stream stream);
+int rq_tlas_destroy(rq_tlas* tlas);
+
 /* Launch shapes of a batch's two kernels.  Results do not depend on them. */
 typedef struct rq_batch_tuning {
     uint32_t build_threads;       /* threads per build block: 256, 512 or 1024 */

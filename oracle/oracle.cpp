@@ -1062,6 +1062,192 @@ void orc_gen_rays_procedural(const float cam[3], const float look[3], uint32_t c
 
 void orc_sincos(float x, float* s, float* c) { sincos_taylor(x, s, c); }
 
+// Two-level scenes (rq_tlas_build + rq_tlas_trace).  Instance i uses BLAS
+// blas_of[i] (arrays nodes4[b], tris[b], perm[b]) with the row-major 3x4
+// object-to-world transform xf + 12i.  The top level is rebuilt here the way
+// the engine builds it: inverse transforms in double (adjugate / det,
+// translation -A^-1 t, rounded once), each instance's BLAS root box
+// transformed corner by corner and widened by 2^-20 of the coordinate
+// magnitudes, stored as the degenerate triangle (min, max, min), then the
+// LBVH of those triangles with one per leaf.  Traversal: one stack; at an
+// instance leaf the ray moves to object space (direction not renormalised),
+// a marker entry and the BLAS root are pushed; popping the marker returns.
+void orc_tlas_trace(const uint64_t* blas_nodes4, const uint64_t* blas_tris, const uint64_t* blas_perm,
+                    const uint32_t* blas_of, const float* xf, const uint32_t* ids, const uint32_t* masks,
+                    uint32_t ninst, const rq_ray* rays, uint32_t n, uint32_t flags, uint32_t cull, rq_hit* hits,
+                    int threads) {
+    std::vector<float> inv(12ull * ninst), tri9(9ull * ninst);
+    for (uint32_t i = 0; i < ninst; ++i) {
+        const float* f = xf + 12ull * i;
+        const double a[3][3] = {{f[0], f[1], f[2]}, {f[4], f[5], f[6]}, {f[8], f[9], f[10]}};
+        const double t[3] = {f[3], f[7], f[11]};
+        const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+        const double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+        const double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+        const double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+        double m[3][3];
+        m[0][0] = c00 / det;
+        m[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+        m[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+        m[1][0] = c01 / det;
+        m[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+        m[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+        m[2][0] = c02 / det;
+        m[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+        m[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+        for (int r = 0; r < 3; ++r) {
+            const double tr = -((m[r][0] * t[0] + m[r][1] * t[1]) + m[r][2] * t[2]);
+            for (int c = 0; c < 3; ++c) inv[12ull * i + 4 * r + c] = float(m[r][c]);
+            inv[12ull * i + 4 * r + 3] = float(tr);
+        }
+        const rq_bvh4_node& root = reinterpret_cast<const rq_bvh4_node*>(blas_nodes4[blas_of[i]])[0];
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int k = 0; k < 4; ++k) {
+            if (root.child_count[k] == 0) continue;
+            lo[0] = fmin_(lo[0], root.min_x[k]);
+            lo[1] = fmin_(lo[1], root.min_y[k]);
+            lo[2] = fmin_(lo[2], root.min_z[k]);
+            hi[0] = fmax_(hi[0], root.max_x[k]);
+            hi[1] = fmax_(hi[1], root.max_y[k]);
+            hi[2] = fmax_(hi[2], root.max_z[k]);
+        }
+        float wlo[3] = {INFINITY, INFINITY, INFINITY}, whi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int c = 0; c < 8; ++c) {
+            const float x = (c & 1) ? hi[0] : lo[0], y = (c & 2) ? hi[1] : lo[1], z = (c & 4) ? hi[2] : lo[2];
+            for (int r = 0; r < 3; ++r) {
+                const float w = ((f[4 * r] * x + f[4 * r + 1] * y) + f[4 * r + 2] * z) + f[4 * r + 3];
+                wlo[r] = fmin_(wlo[r], w);
+                whi[r] = fmax_(whi[r], w);
+            }
+        }
+        for (int r = 0; r < 3; ++r) {
+            const float pad = (std::fabs(wlo[r]) + std::fabs(whi[r])) * 0x1p-20f;
+            tri9[9ull * i + r] = wlo[r] - pad;
+            tri9[9ull * i + 3 + r] = whi[r] + pad;
+            tri9[9ull * i + 6 + r] = wlo[r] - pad;
+        }
+    }
+    std::vector<uint32_t> top_perm(ninst);
+    std::vector<rq_bvh4_node> top4(ninst);
+    std::vector<rq_bvh2_node> top2(2ull * ninst);
+    uint32_t n2 = 0, n4 = 0, d4 = 0;
+    orc_lbvh_build(tri9.data(), 3, nullptr, ninst, 1, nullptr, top_perm.data(), top2.data(), &n2, nullptr,
+                   top4.data(), &n4, &d4);
+    const bool any = flags & 1u, mt = flags & 2u;
+    const int32_t kMarker = 0x40000000;
+    parallel_for(n, threads, [&](uint32_t id) {
+        const rq_ray& r = rays[id];
+        const V3 o{r.org[0], r.org[1], r.org[2]}, d{r.dir[0], r.dir[1], r.dir[2]};
+        const float tmin = r.tmin;
+        float best = r.tmax;
+        auto setup = [](V3 oo, V3 dd, float* iv, float* oi) {
+            iv[0] = safe_inv(dd.x);
+            iv[1] = safe_inv(dd.y);
+            iv[2] = safe_inv(dd.z);
+            oi[0] = oo.x * iv[0];
+            oi[1] = oo.y * iv[1];
+            oi[2] = oo.z * iv[2];
+        };
+        float wi[3], wo[3], ci[3], co[3];
+        setup(o, d, wi, wo);
+        std::memcpy(ci, wi, sizeof(ci));
+        std::memcpy(co, wo, sizeof(co));
+        V3 oo = o, od = d;
+        WtRay w = wt_setup(d);
+        bool inside = false, hit = false;
+        const rq_bvh4_node* nodes = top4.data();
+        const rq_triangle* tris = nullptr;
+        const uint32_t* perm = nullptr;
+        uint32_t cur_id = 0, hit_inst = 0xffffffffu, hit_prim = 0xffffffffu;
+        FixedStack<int32_t> st;
+        st.push_back(0);
+        bool done = false;
+        while (!st.empty() && !done) {
+            const int32_t e = st.back();
+            st.pop_back();
+            if (e == kMarker) {
+                inside = false;
+                nodes = top4.data();
+                std::memcpy(ci, wi, sizeof(ci));
+                std::memcpy(co, wo, sizeof(co));
+                continue;
+            }
+            if (e >= 0) {
+                const rq_bvh4_node& nd = nodes[e];
+                int32_t he[4];
+                float ht[4];
+                int nh = 0;
+                for (int k = 0; k < 4; ++k) {
+                    if (nd.child_count[k] == 0) continue;
+                    float tn;
+                    if (slab(ci, co, tmin, best, nd.min_x[k], nd.max_x[k], nd.min_y[k], nd.max_y[k], nd.min_z[k],
+                             nd.max_z[k], tn)) {
+                        const int32_t ent = nd.child_count[k] < 0
+                                                ? nd.child_index[k]
+                                                : int32_t(0x80000000u | (uint32_t(nd.child_count[k] - 1) << 27) |
+                                                          uint32_t(~nd.child_index[k]));
+                        int pos = nh;
+                        if (!any)
+                            while (pos > 0 && ht[pos - 1] > tn) {
+                                he[pos] = he[pos - 1];
+                                ht[pos] = ht[pos - 1];
+                                --pos;
+                            }
+                        he[pos] = ent;
+                        ht[pos] = tn;
+                        ++nh;
+                    }
+                }
+                for (int j = nh - 1; j >= 0; --j) st.push_back(he[j]);
+                continue;
+            }
+            const uint32_t first = uint32_t(e) & 0x07ffffffu, cnt = ((uint32_t(e) >> 27) & 15u) + 1u;
+            if (!inside) {
+                const uint32_t i = top_perm[first];
+                if ((masks[i] & cull) == 0u) continue;
+                const float* m = inv.data() + 12ull * i;
+                oo = V3{((m[0] * o.x + m[1] * o.y) + m[2] * o.z) + m[3], ((m[4] * o.x + m[5] * o.y) + m[6] * o.z) + m[7],
+                        ((m[8] * o.x + m[9] * o.y) + m[10] * o.z) + m[11]};
+                od = V3{(m[0] * d.x + m[1] * d.y) + m[2] * d.z, (m[4] * d.x + m[5] * d.y) + m[6] * d.z,
+                        (m[8] * d.x + m[9] * d.y) + m[10] * d.z};
+                setup(oo, od, ci, co);
+                w = wt_setup(od);
+                const uint32_t b = blas_of[i];
+                nodes = reinterpret_cast<const rq_bvh4_node*>(blas_nodes4[b]);
+                tris = reinterpret_cast<const rq_triangle*>(blas_tris[b]);
+                perm = reinterpret_cast<const uint32_t*>(blas_perm[b]);
+                cur_id = ids[i];
+                inside = true;
+                st.push_back(kMarker);
+                st.push_back(0);
+                continue;
+            }
+            for (uint32_t p = first; p < first + cnt; ++p) {
+                const rq_triangle& tr = tris[p];
+                V3 v0{tr.v0[0], tr.v0[1], tr.v0[2]}, v1{tr.v1[0], tr.v1[1], tr.v1[2]}, v2{tr.v2[0], tr.v2[1], tr.v2[2]};
+                float t, u, v;
+                const bool ok = mt ? mt_test(oo, od, v0, v1, v2, 1e-7f, t, u, v) : wt_test(w, oo, v0, v1, v2, t, u, v);
+                if (ok && t >= tmin && t < best) {
+                    best = t;
+                    hit = true;
+                    hit_inst = cur_id;
+                    hit_prim = perm[p];
+                    if (any) {
+                        done = true;
+                        break;
+                    }
+                }
+            }
+        }
+        rq_hit h;
+        h.hit = hit ? 1u : 0u;
+        h.t = hit ? best : -1.0f;
+        h.instance_id = hit ? hit_inst : 0xffffffffu;
+        h.primitive_id = hit ? hit_prim : 0xffffffffu;
+        hits[id] = h;
+    });
+}
+
 // Depth z/w of G-buffer positions under the column-major view-projection
 // `vp` (1.0 where the pixel saw no geometry).
 void orc_gbuffer_depth(const rq_gbuffer_px* g, uint32_t npix, const float* vp, float* depth) {

@@ -60,6 +60,8 @@ def lib():
         L.orc_gen_mesh_rays.argtypes = [_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]
         L.orc_gbuffer_depth.argtypes = [_P, C.c_uint32, _P, _P]
         L.orc_blur_ao.argtypes = [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_float]
+        L.orc_tlas_trace.argtypes = [_P, _P, _P, _P, _P, _P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, _P, C.c_int]
         _lib = L
     return _lib
 
@@ -183,6 +185,24 @@ def trace_radv(img, rays, flags=0, want_bary=False):
     lib().orc_trace_radv(_ptr(np.ascontiguousarray(img)), _ptr(rays), len(rays), flags, _ptr(hits), _ptr(bary),
                          threads())
     return hits, bary
+
+
+def tlas_trace(blas, blas_of, transforms, ids, masks, rays, flags=0, cull=0xFF):
+    """Two-level scene traversal.  blas: list of (nodes4, tris, perm) arrays;
+    instance i uses blas[blas_of[i]] with the row-major 3x4 transforms[i]."""
+    keep = [tuple(np.ascontiguousarray(x) for x in b) for b in blas]
+    nodes = np.array([k[0].ctypes.data for k in keep], np.uint64)
+    tris = np.array([k[1].ctypes.data for k in keep], np.uint64)
+    perm = np.array([k[2].ctypes.data for k in keep], np.uint64)
+    bo = np.ascontiguousarray(blas_of, np.uint32)
+    xf = np.ascontiguousarray(transforms, np.float32).reshape(-1)
+    ids = np.ascontiguousarray(ids, np.uint32)
+    masks = np.ascontiguousarray(masks, np.uint32)
+    rays = np.ascontiguousarray(rays)
+    hits = np.empty(len(rays), HIT)
+    lib().orc_tlas_trace(_ptr(nodes), _ptr(tris), _ptr(perm), _ptr(bo), _ptr(xf), _ptr(ids), _ptr(masks), len(bo),
+                         _ptr(rays), len(rays), flags, cull, _ptr(hits), threads())
+    return hits
 
 
 def gbuffer_depth(gbuf, view_proj):

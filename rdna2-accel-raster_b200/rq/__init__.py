@@ -100,6 +100,11 @@ class MeshDesc(C.Structure):
                 ("num_triangles", C.c_uint32)]
 
 
+class Instance(C.Structure):
+    _fields_ = [("transform", C.c_float * 12), ("instance_id", C.c_uint32), ("mask", C.c_uint32),
+                ("blas", C.c_void_p)]
+
+
 class TraceTuning(C.Structure):
     _fields_ = [("threads", C.c_uint32), ("chunk", C.c_uint32), ("reg_cap", C.c_uint32), ("top_levels", C.c_uint32),
                 ("speculative", C.c_uint32)]
@@ -185,6 +190,9 @@ SIGNATURES = [
     ("rq_batch_info_get", C.c_int, [_P, _U32, C.POINTER(BvhInfo)]),
     ("rq_batch_download", C.c_int, [_P, _U32, C.c_int, _P, _U32, _P, _U32, _P, _U32, _P, _U32]),
     ("rq_batch_destroy", C.c_int, [_P]),
+    ("rq_tlas_build", C.c_int, [_P, C.POINTER(Instance), _U32, C.POINTER(_P), _P]),
+    ("rq_tlas_trace", C.c_int, [_P, _P, _P, _U32, _U32, _U32, _P, _P]),
+    ("rq_tlas_destroy", C.c_int, [_P]),
     ("rq_batch_tuning_get", C.c_int, [_P, C.POINTER(BatchTuning)]),
     ("rq_batch_tuning_set", C.c_int, [_P, C.POINTER(BatchTuning)]),
     ("rq_batch_autotune", C.c_int, [_P, _P, _P, _U32, _P, _P, _P, _P, _U32, _P, _U32, C.POINTER(BatchTuning), _U32,
@@ -381,6 +389,40 @@ class Bvh:
     def destroy(self):
         if self.h:
             lib().rq_bvh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Tlas:
+    """An rq_tlas handle: instances of Bvh handles under a top-level BVH."""
+
+    def __init__(self, ctx, instances, stream=None):
+        """instances: sequence of (transform 3x4 row-major (12 floats), instance_id, mask, Bvh)."""
+        arr = (Instance * len(instances))()
+        for k, (xf, iid, mask, bvh) in enumerate(instances):
+            arr[k].transform = (C.c_float * 12)(*[float(x) for x in np.asarray(xf, np.float32).reshape(-1)])
+            arr[k].instance_id = iid
+            arr[k].mask = mask
+            arr[k].blas = bvh.h
+        h = _P()
+        ctx.check(lib().rq_tlas_build(ctx.h, arr, len(instances), C.byref(h), _stream(stream)), "rq_tlas_build")
+        self.ctx, self.h, self._blas = ctx, h, [x[3] for x in instances]
+
+    def trace(self, rays, flags=0, cull_mask=0xFF, hits=None, stream=None):
+        n = _count(rays, 32)
+        hits = hits if hits is not None else _empty_i32(n, 4, rays.device)
+        self.ctx.check(lib().rq_tlas_trace(self.ctx.h, self.h, _ptr(rays), n, flags, cull_mask, _ptr(hits),
+                                           _stream(stream)), "rq_tlas_trace")
+        return hits
+
+    def destroy(self):
+        if self.h:
+            lib().rq_tlas_destroy(self.h)
             self.h = None
 
     def __del__(self):
