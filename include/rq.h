@@ -113,6 +113,15 @@ int rq_deform_wave_step(rq_ctx* ctx, const float* base, float* out, uint32_t num
 /* ------------------------------------------------------------------ */
 
 #define RQ_BUILD_BVH4 1u /* also collapse to the 4-wide layout (needed by rq_trace) */
+/* Split like SoftwareBVH::recursiveBuild (common/software_bvh.hpp:90-175) instead
+ * of Morton order: median of the longest centroid axis, leaves of <= max_leaf
+ * primitives or of centroids spanning < 1e-6.  Where no centroid value
+ * repeats inside a node on its split axis, the binary nodes (boxes, child
+ * links, leaf offsets and counts) equal the reference's; the order of the
+ * triangles inside a leaf is the x-centroid order (the reference's is
+ * nth_element's).  Slower than the LBVH (one round per tree level); the
+ * sorted Morton keys of the handle are not written. */
+#define RQ_BUILD_MEDIAN 2u
 
 /* Build a binary BVH over `num_triangles` triangles.  Device pointers.
  * `positions`: float xyz per vertex with `stride_bytes` between vertices

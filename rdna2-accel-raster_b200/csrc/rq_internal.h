@@ -113,6 +113,9 @@ struct BuildScratch {
 size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s);
 int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
                     uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t s);
+// The reference's median-split topology (k_median.cu); synchronises once per tree level.
+int rq_launch_build_median(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
+                           uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t s);
 int rq_launch_refit(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
                     cudaStream_t s);
 

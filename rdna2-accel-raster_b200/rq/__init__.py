@@ -33,6 +33,7 @@ RQ_FAULT_ALLOC = 1
 RQ_FAULT_LAUNCH = 2
 
 RQ_BUILD_BVH4 = 1
+RQ_BUILD_MEDIAN = 2
 RQ_TRACE_CLOSEST = 0
 RQ_TRACE_ANY = 1
 RQ_TRI_WATERTIGHT = 0
@@ -325,14 +326,16 @@ class Bvh:
         self.h = handle
 
     @staticmethod
-    def build(ctx, pos, idx=None, max_leaf=4, bvh4=True, stride_bytes=12, stream=None, into=None):
+    def build(ctx, pos, idx=None, max_leaf=4, bvh4=True, stride_bytes=12, stream=None, into=None, median=False):
         """pos: float32 CUDA tensor of vertices; idx: int32/uint32 CUDA tensor
-        [T, 3] or None (non-indexed: 3 consecutive vertices per triangle)."""
+        [T, 3] or None (non-indexed: 3 consecutive vertices per triangle).
+        median: the reference's median-split topology (RQ_BUILD_MEDIAN)."""
         nverts = _count(pos, 4) * 4 // stride_bytes
         ntri = _count(idx, 12) if idx is not None else nverts // 3
         h = _P(into.h.value) if into is not None else _P()
-        rc = lib().rq_build(ctx.h, _ptr(pos), stride_bytes, nverts, _ptr(idx), ntri, max_leaf,
-                            RQ_BUILD_BVH4 if bvh4 else 0, C.byref(h), _stream(stream))
+        flags = (RQ_BUILD_BVH4 if bvh4 else 0) | (RQ_BUILD_MEDIAN if median else 0)
+        rc = lib().rq_build(ctx.h, _ptr(pos), stride_bytes, nverts, _ptr(idx), ntri, max_leaf, flags, C.byref(h),
+                            _stream(stream))
         ctx.check(rc, "rq_build")
         if into is not None:
             into.h = h

@@ -10,6 +10,9 @@ the tests read only the files this script writes.
                         SoftwareBVH / SoftwareBVH4 bytes for it
   ref_dynamic_grids.npz generate_dynamic_grid_mesh(N, 1.25) for the builder
                         verification sizes N = 64, 256, 1024, 4096
+  radv_dumps.json       dump_bvh_structure text of those grids' RADV images
+  ref_median_soups.npz  the reference's SoftwareBVH / SoftwareBVH4 bytes for
+                        random soups without repeated centroid values
 """
 import csv
 import json
@@ -66,6 +69,25 @@ def main():
         dumps[str(n)] = O.ref_dump_bvh_structure(img.tobytes())
     with open(os.path.join(HERE, "radv_dumps.json"), "w") as f:
         json.dump(dumps, f, indent=1)
+
+    # median-split trees of soups whose float32 centroids never repeat a
+    # value on an axis (the soup of tests/conftest.py, repeats removed)
+    med = {}
+    for tag, n, seed, leaf in (("a", 3000, 11, 4), ("b", 8000, 12, 2)):
+        rng = np.random.default_rng(seed)
+        c = rng.uniform(-1.0, 1.0, size=(n, 1, 3)).astype(np.float32)
+        e = rng.uniform(-0.05, 0.05, size=(n, 3, 3)).astype(np.float32)
+        v = (c + e).astype(np.float32)
+        cen = ((v[:, 0] + v[:, 1]) + v[:, 2]) / np.float32(3.0)
+        keep = np.ones(n, bool)
+        for a in range(3):
+            _, inv, cnt = np.unique(cen[:, a], return_inverse=True, return_counts=True)
+            keep &= cnt[inv] == 1
+        pos = np.ascontiguousarray(v[keep].reshape(-1, 3))
+        n2, tris, n4 = O.ref_build(pos, np.arange(len(pos), dtype=np.uint32), leaf)
+        med.update({f"pos_{tag}": pos, f"leaf_{tag}": np.uint32(leaf), f"nodes2_{tag}": n2.view(np.uint8),
+                    f"tris_{tag}": tris.view(np.uint8), f"nodes4_{tag}": n4.view(np.uint8)})
+    np.savez_compressed(os.path.join(HERE, "ref_median_soups.npz"), **med)
     print("golden fixtures written to", HERE)
 
 
