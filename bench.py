@@ -398,6 +398,23 @@ def run_ours(args, world, rank, local, pg):
     blur = {"workload": "AO depth + 2-pass bilateral blur at 1920x1080", "ms": round(blur_ms, 4),
             "gb_per_s_compulsory": round(npx * (36 + 2 * 12) / (blur_ms * 1e-3) / 1e9, 1)}
 
+    # the reference's median-split topology (RQ_BUILD_MEDIAN) on the same
+    # mesh: one round per tree level, each ending in a host read of the
+    # level's size, so it is timed on the host clock around a synchronised build
+    med = rq.Bvh.build(ctx, p_d, i_d, median=True)
+    torch.cuda.synchronize(dev)
+    med_ms = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        rq.Bvh.build(ctx, p_d, i_d, median=True, into=med)
+        torch.cuda.synchronize(dev)
+        med_ms.append((time.perf_counter() - t0) * 1e3)
+    med_info = med.info()
+    med.destroy()
+    median_build = {"workload": "median-split build of the frame mesh (2,499,848 triangles) + 4-wide collapse",
+                    "ms": round(min(med_ms), 2), "mtris_per_s": round(len(idx) / min(med_ms) / 1e3, 1),
+                    "nodes2": med_info["num_nodes2"], "depth4": med_info["depth4"]}
+
     bvh.destroy()
     del p_d, i_d, gbuf, mask, ao, depth, tmp, blurred
     vis = run_visibility(ctx, dev, stream) if not args.no_extra else None
@@ -466,6 +483,7 @@ def run_ours(args, world, rank, local, pg):
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "shadow_tuning": shade_tuning,
         "ao_blur": blur,
+        "median_build": median_build,
         "visibility": vis,
         "batched": batched,
         "serving": serving,

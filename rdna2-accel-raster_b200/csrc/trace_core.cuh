@@ -41,10 +41,19 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
     res.idx = kNoHit;
     res.u = res.v = 0.0f;
     res.boxes = res.tris = 0;
-    stk[0] = 0;
-    int sp = 1;
-    while (sp > 0) {
-        const int32_t e = stk[(--sp) * STRIDE];
+    // the stack's top entry lives in a register: the nearest child of a node
+    // is visited next without a round trip through shared memory
+    int32_t top = 0;
+    bool has_top = true;
+    int sp = 0;
+    while (has_top || sp > 0) {
+        int32_t e;
+        if (has_top) {
+            e = top;
+            has_top = false;
+        } else {
+            e = stk[(--sp) * STRIDE];
+        }
         if (e >= 0) {
             const float4* np = reinterpret_cast<const float4*>(nodes + e);
             const float4 mnx = ldg4(np + 0), mxx = ldg4(np + 1);
@@ -84,7 +93,11 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
                 set_err(err, RQ_DERR_STACK);
                 nh = STACK - sp;
             }
-            for (int j = nh - 1; j >= 0; --j) stk[(sp++) * STRIDE] = he[j];
+            for (int j = nh - 1; j >= 1; --j) stk[(sp++) * STRIDE] = he[j];
+            if (nh > 0) {
+                top = he[0];
+                has_top = true;
+            }
         } else {
             const uint32_t first = uint32_t(e) & 0x07ffffffu;
             const uint32_t cntl = ((uint32_t(e) >> 27) & 15u) + 1u;

@@ -14,7 +14,9 @@
 //      the result to the ray source and become idle.
 // Per ray this visits stack entries in exactly the order of a sequential
 // pop-process-push traversal, so results do not depend on which lane or
-// round a ray runs in and match the oracle's traversal bit for bit.
+// round a ray runs in and match the oracle's traversal bit for bit.  The
+// stack's top entry is held in a register (the first child to visit after a
+// node never goes through shared memory).
 //
 // A ray source provides:
 //   uint32_t total;                                 number of ray ids
@@ -177,7 +179,9 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
     SlabRay sr;
     WtRay w;
     float best = 0.0f;
-    int sp = 0;
+    int sp = 0;            // entries in the shared-memory stack
+    int32_t top = 0;       // the stack's top entry, kept in a register
+    bool has_top = false;
     Hit h;
     h.hit = false;
     h.t = 0.0f;
@@ -219,8 +223,9 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                     h.idx = kNoHit;
                     h.u = h.v = 0.0f;
                     h.boxes = h.tris = 0;
-                    stk[0] = TOP > 0 ? kStaged : 0;  // the root (slot 0 when staged)
-                    sp = 1;
+                    top = TOP > 0 ? kStaged : 0;  // the root (slot 0 when staged)
+                    has_top = true;
+                    sp = 0;
                 }
             }
             next += take;
@@ -239,16 +244,24 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
         int32_t leaf = kNoLeaf;
         bool stalled = false;
         for (;;) {
-            const bool searching = active && sp > 0 && leaf == kNoLeaf;
+            const bool left = has_top || sp > 0;
+            const bool searching = active && left && leaf == kNoLeaf;
             if (!__any_sync(kFull, searching)) break;
-            const bool want = SPEC ? (active && sp > 0 && !stalled) : searching;
+            const bool want = SPEC ? (active && left && !stalled) : searching;
             if (!want) continue;
-            const int32_t e = stk[(--sp) * STRIDE];
+            int32_t e;
+            if (has_top) {
+                e = top;
+                has_top = false;
+            } else {
+                e = stk[(--sp) * STRIDE];
+            }
             if (e < 0) {
                 if (!SPEC || leaf == kNoLeaf) {
                     leaf = e;
                 } else {
-                    ++sp;
+                    top = e;
+                    has_top = true;
                     stalled = true;
                 }
                 continue;
@@ -311,7 +324,12 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                 set_err(err, RQ_DERR_STACK);
                 nh = stack_cap - sp;
             }
-            for (int j = nh - 1; j >= 0; --j) stk[(sp++) * STRIDE] = he[j];
+            // the nearest (first to visit) child stays in the register
+            for (int j = nh - 1; j >= 1; --j) stk[(sp++) * STRIDE] = he[j];
+            if (nh > 0) {
+                top = he[0];
+                has_top = true;
+            }
         }
 
         // ---- leaf phase
@@ -343,7 +361,7 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
 
         // ---- report finished rays
         bool fin = false;
-        if (active && (done || sp == 0)) {
+        if (active && (done || (sp == 0 && !has_top))) {
             h.t = best;
             src.finish(rid, meta, ray, h);
             active = false;
