@@ -17,10 +17,15 @@
 // traversal shaders.  Unlike the reference, `perm` keeps the leaf-order ->
 // original triangle id map.  Errors throw rq::Error (C++ side only; the C ABI
 // itself never throws).
+//
+// The default tree is an LBVH (Morton order).  Split::Median builds the
+// reference's own median-split topology (RQ_BUILD_MEDIAN): where no centroid
+// value repeats on an axis its nodes equal SoftwareBVH::build's byte for byte.
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <cfloat>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -56,15 +61,32 @@ class Engine {
     rq_ctx* ctx_ = nullptr;
 };
 
+enum class Split { Morton, Median };
+
 struct SoftwareBVH {
     std::vector<rq_bvh2_node> nodes;
     std::vector<rq_triangle> triangles;
     std::vector<uint32_t> perm;  // leaf order -> original triangle id
 
     template <class Mesh>
-    static SoftwareBVH build(Engine& eng, const Mesh& mesh, uint32_t maxPrimsPerLeaf = 4) {
+    static SoftwareBVH build(Engine& eng, const Mesh& mesh, uint32_t maxPrimsPerLeaf = 4,
+                             Split split = Split::Morton) {
         const size_t nv = mesh.vertices.size();
         const uint32_t nt = uint32_t(mesh.indices.size() / 3);
+        if (nt == 0) {
+            // what the reference returns for an empty mesh: one leaf of no
+            // triangles over an empty box (common/software_bvh.hpp:101-124)
+            SoftwareBVH out;
+            rq_bvh2_node leaf{};
+            for (int c = 0; c < 3; ++c) {
+                leaf.aabb_min[c] = FLT_MAX;
+                leaf.aabb_max[c] = -FLT_MAX;
+            }
+            leaf.left_child = ~0;
+            leaf.right_child = 0;
+            out.nodes.push_back(leaf);
+            return out;
+        }
         std::vector<float> pos(3 * nv);
         for (size_t v = 0; v < nv; ++v)
             for (int c = 0; c < 3; ++c) pos[3 * v + c] = mesh.vertices[v].pos[c];
@@ -82,7 +104,8 @@ struct SoftwareBVH {
         fail(cudaMemcpy(d_pos, pos.data(), pos.size() * sizeof(float), cudaMemcpyHostToDevice));
         fail(cudaMemcpy(d_idx, mesh.indices.data(), mesh.indices.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
         rq_bvh* h = nullptr;
-        int st = rq_build(eng.get(), d_pos, 12, uint32_t(nv), d_idx, nt, maxPrimsPerLeaf, 0, &h, nullptr);
+        const uint32_t flags = split == Split::Median ? RQ_BUILD_MEDIAN : 0u;
+        int st = rq_build(eng.get(), d_pos, 12, uint32_t(nv), d_idx, nt, maxPrimsPerLeaf, flags, &h, nullptr);
         cudaFree(d_pos);
         cudaFree(d_idx);
         check(st, eng.get(), "rq_build");
@@ -110,6 +133,22 @@ struct SoftwareBVH4 {
         SoftwareBVH4 out;
         out.triangles = b2.triangles;
         if (b2.nodes.empty()) return out;
+        if (b2.triangles.empty()) {
+            // a single leaf of no triangles: slot 0 carries its box and
+            // encoded child as written (common/software_bvh.hpp:204-218)
+            const rq_bvh2_node& leaf = b2.nodes[0];
+            rq_bvh4_node n4{};
+            n4.min_x[0] = leaf.aabb_min[0];
+            n4.max_x[0] = leaf.aabb_max[0];
+            n4.min_y[0] = leaf.aabb_min[1];
+            n4.max_y[0] = leaf.aabb_max[1];
+            n4.min_z[0] = leaf.aabb_min[2];
+            n4.max_z[0] = leaf.aabb_max[2];
+            n4.child_index[0] = leaf.left_child;
+            n4.child_count[0] = leaf.right_child;
+            out.nodes.push_back(n4);
+            return out;
+        }
         rq_bvh2_node* d_n = nullptr;
         rq_triangle* d_t = nullptr;
         cudaError_t e = cudaMalloc(&d_n, b2.nodes.size() * sizeof(rq_bvh2_node));
