@@ -448,6 +448,27 @@ inline bool slab(const float inv[3], const float oinv[3], float tmin, float best
     return a <= b * kFarScale;
 }
 
+// The engine's 4-wide slab test (rq_device.cuh slab_nf): each axis's near
+// and far plane picked by the sign bit of inv (the max plane when inv is
+// negative), entry max(near_x, near_y, near_z, tmin), exit
+// min(far_x, far_y, far_z, best).  For boxes with min <= max this equals
+// slab() above; boxes with min > max on an axis are empty.
+inline bool slab4(const float inv[3], const float oinv[3], float tmin, float best, const rq_bvh4_node& n, int k,
+                  float& tn) {
+    const float* lo[3] = {n.min_x, n.min_y, n.min_z};
+    const float* hi[3] = {n.max_x, n.max_y, n.max_z};
+    float tnear[3], tfar[3];
+    for (int a = 0; a < 3; ++a) {
+        const bool neg = std::signbit(inv[a]);
+        tnear[a] = std::fmaf((neg ? hi[a] : lo[a])[k], inv[a], -oinv[a]);
+        tfar[a] = std::fmaf((neg ? lo[a] : hi[a])[k], inv[a], -oinv[a]);
+    }
+    const float a = fmax_(fmax_(fmax_(tnear[0], tnear[1]), tnear[2]), tmin);
+    const float b = fmin_(fmin_(fmin_(tfar[0], tfar[1]), tfar[2]), best);
+    tn = a;
+    return a <= b * kFarScale;
+}
+
 struct TraceOut {
     bool hit;
     float t;
@@ -488,8 +509,7 @@ TraceOut trace_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq
             for (int k = 0; k < 4; ++k) {
                 if (n.child_count[k] == 0) continue;
                 float tn;
-                if (slab(inv, oinv, tmin, best, n.min_x[k], n.max_x[k], n.min_y[k], n.max_y[k], n.min_z[k],
-                         n.max_z[k], tn)) {
+                if (slab4(inv, oinv, tmin, best, n, k, tn)) {
                     Entry c;
                     if (n.child_count[k] < 0) {
                         c = {n.child_index[k], -1};
@@ -1180,8 +1200,7 @@ void orc_tlas_trace(const uint64_t* blas_nodes4, const uint64_t* blas_tris, cons
                 for (int k = 0; k < 4; ++k) {
                     if (nd.child_count[k] == 0) continue;
                     float tn;
-                    if (slab(ci, co, tmin, best, nd.min_x[k], nd.max_x[k], nd.min_y[k], nd.max_y[k], nd.min_z[k],
-                             nd.max_z[k], tn)) {
+                    if (slab4(ci, co, tmin, best, nd, k, tn)) {
                         const int32_t ent = nd.child_count[k] < 0
                                                 ? nd.child_index[k]
                                                 : int32_t(0x80000000u | (uint32_t(nd.child_count[k] - 1) << 27) |

@@ -35,6 +35,7 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
     sr.ox = o.x * sr.ix;
     sr.oy = o.y * sr.iy;
     sr.oz = o.z * sr.iz;
+    slab_planes(sr);
     WtRay w;
     if (!MT) w = wt_setup(d);
     float best = tmax;
@@ -56,15 +57,16 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
         }
         if (e >= 0) {
             const float4* np = reinterpret_cast<const float4*>(nodes + e);
-            const float4 mnx = ldg4(np + 0), mxx = ldg4(np + 1);
-            const float4 mny = ldg4(np + 2), mxy = ldg4(np + 3);
-            const float4 mnz = ldg4(np + 4), mxz = ldg4(np + 5);
+            // each axis's near and far plane rows, chosen by the ray's signs
+            const float4 nx4 = ldg4(np + sr.nx), fx4 = ldg4(np + (sr.nx ^ 1));
+            const float4 ny4 = ldg4(np + sr.ny), fy4 = ldg4(np + (sr.ny ^ 1));
+            const float4 nz4 = ldg4(np + sr.nz), fz4 = ldg4(np + (sr.nz ^ 1));
             const int4 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
             const int4 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
             if (STATS) res.boxes += 4;
-            const float amnx[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, amxx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
-            const float amny[4] = {mny.x, mny.y, mny.z, mny.w}, amxy[4] = {mxy.x, mxy.y, mxy.z, mxy.w};
-            const float amnz[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, amxz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
+            const float anx[4] = {nx4.x, nx4.y, nx4.z, nx4.w}, afx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+            const float any_[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, afy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+            const float anz[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, afz[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
             const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
             int32_t he[4];
             float ht[4];
@@ -73,7 +75,7 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
             for (int k = 0; k < 4; ++k) {
                 if (acc[k] == 0) continue;
                 float tn;
-                if (slab(sr, tmin, best, amnx[k], amxx[k], amny[k], amxy[k], amnz[k], amxz[k], tn)) {
+                if (slab_nf(sr, tmin, best, anx[k], afx[k], any_[k], afy[k], anz[k], afz[k], tn)) {
                     const int32_t ent =
                         acc[k] < 0 ? aci[k] : int32_t(kLeafBit | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
                     int pos = nh;

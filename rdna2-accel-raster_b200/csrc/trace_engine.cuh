@@ -217,6 +217,7 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                     sr.ox = ray.o.x * sr.ix;
                     sr.oy = ray.o.y * sr.iy;
                     sr.oz = ray.o.z * sr.iz;
+                    slab_planes(sr);
                     if (!MT) w = wt_setup(ray.d);
                     best = ray.tmax;
                     h.hit = false;
@@ -266,35 +267,36 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                 }
                 continue;
             }
-            float4 mnx, mxx, mny, mxy, mnz, mxz;
+            // each axis's near and far plane rows, chosen by the ray's signs
+            float4 nx4, fx4, ny4, fy4, nz4, fz4;
             int4 cix, cnt;
             if (TOP > 0 && (e & kStaged)) {
                 const float4* sp4 = s_top + (e & ~kStaged) * kTopStride;
-                mnx = sp4[0];
-                mxx = sp4[1];
-                mny = sp4[2];
-                mxy = sp4[3];
-                mnz = sp4[4];
-                mxz = sp4[5];
+                nx4 = sp4[sr.nx];
+                fx4 = sp4[sr.nx ^ 1];
+                ny4 = sp4[sr.ny];
+                fy4 = sp4[sr.ny ^ 1];
+                nz4 = sp4[sr.nz];
+                fz4 = sp4[sr.nz ^ 1];
                 const float4 a = sp4[6], b = sp4[7];
                 cix = make_int4(__float_as_int(a.x), __float_as_int(a.y), __float_as_int(a.z), __float_as_int(a.w));
                 cnt = make_int4(__float_as_int(b.x), __float_as_int(b.y), __float_as_int(b.z), __float_as_int(b.w));
             } else {
                 const rq_bvh4_node* nb = IsMulti<Src>::value ? ray.nodes : nodes;
                 const float4* np = reinterpret_cast<const float4*>(nb + e);
-                mnx = ldg4(np + 0);
-                mxx = ldg4(np + 1);
-                mny = ldg4(np + 2);
-                mxy = ldg4(np + 3);
-                mnz = ldg4(np + 4);
-                mxz = ldg4(np + 5);
+                nx4 = ldg4(np + sr.nx);
+                fx4 = ldg4(np + (sr.nx ^ 1));
+                ny4 = ldg4(np + sr.ny);
+                fy4 = ldg4(np + (sr.ny ^ 1));
+                nz4 = ldg4(np + sr.nz);
+                fz4 = ldg4(np + (sr.nz ^ 1));
                 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
                 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
             }
             if (STATS) h.boxes += 4;
-            const float amnx[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, amxx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
-            const float amny[4] = {mny.x, mny.y, mny.z, mny.w}, amxy[4] = {mxy.x, mxy.y, mxy.z, mxy.w};
-            const float amnz[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, amxz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
+            const float anx[4] = {nx4.x, nx4.y, nx4.z, nx4.w}, afx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+            const float any_[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, afy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+            const float anz[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, afz[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
             const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
             int32_t he[4];
             float ht[4];
@@ -303,7 +305,7 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
             for (int k = 0; k < 4; ++k) {
                 if (acc[k] == 0) continue;
                 float tn;
-                if (slab(sr, ray.tmin, best, amnx[k], amxx[k], amny[k], amxy[k], amnz[k], amxz[k], tn)) {
+                if (slab_nf(sr, ray.tmin, best, anx[k], afx[k], any_[k], afy[k], anz[k], afz[k], tn)) {
                     const int32_t ent = acc[k] < 0
                                             ? aci[k]
                                             : int32_t(0x80000000u | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
