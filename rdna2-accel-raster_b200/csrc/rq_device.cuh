@@ -323,4 +323,82 @@ __device__ __forceinline__ bool wait_change(const uint32_t* p, uint32_t v, uint3
     return true;
 }
 
+// ------------------------------------------------------ 4-wide child push
+// Push the hit children of one 4-wide node (bit k of `hitm`: slot k hit, with
+// entry distance tk[k]; child_index ci[k] and child_count cc[k] as stored in
+// the node give its stack entry: the node index for an inner child, else
+// bit31 | (count-1) << 27 | first primitive) so that they pop in visit
+// order: ascending (tk, slot) when `sorted` (closest hit), ascending slot
+// otherwise.  The first child to visit goes to the register `top`, the rest
+// onto the shared-memory column `stk` (STRIDE words apart).  Each child's
+// place is its rank among the hits, so nothing is indexed by a run-time
+// value in registers.  With more hits than room (sp + hits > cap),
+// `overflow_bit` is set in the error word and only the first cap - sp
+// children in visit order are kept.
+template <int STRIDE>
+__device__ __forceinline__ void push_children(uint32_t hitm, const int32_t (&ci)[4], const int32_t (&cc)[4],
+                                              const float (&tk)[4],
+                                              bool sorted, int32_t* stk, int& sp, int cap, int32_t& top,
+                                              bool& has_top, uint32_t* err, uint32_t overflow_bit) {
+    int nh = __popc(hitm);
+    if (sp + nh > cap) {
+        set_err(err, overflow_bit);
+        nh = max(cap - sp, 0);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!((hitm >> k) & 1u)) continue;
+        int rank;
+        if (sorted) {
+            rank = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (j == k) continue;
+                const bool before = j < k ? tk[j] <= tk[k] : tk[j] < tk[k];
+                rank += int(((hitm >> j) & 1u) && before);
+            }
+        } else {
+            rank = __popc(hitm & ((1u << k) - 1u));
+        }
+        const int32_t ent = cc[k] < 0 ? ci[k] : int32_t(0x80000000u | (uint32_t(cc[k] - 1) << 27) | uint32_t(~ci[k]));
+        if (rank == 0) {
+            if (nh > 0) {
+                top = ent;
+                has_top = true;
+            }
+        } else if (rank < nh) {
+            stk[(sp + nh - 1 - rank) * STRIDE] = ent;
+        }
+    }
+    if (nh > 0) sp += nh - 1;
+}
+
+// Any-hit form of push_children (slot order, no distances): the hit slots
+// are walked from slot 3 down, each pushed when a lower hit slot follows, so
+// the lowest hit slot ends in `top`.
+template <int STRIDE>
+__device__ __forceinline__ void push_children_any(uint32_t hitm, const int32_t (&ci)[4], const int32_t (&cc)[4],
+                                                  int32_t* stk, int& sp, int cap, int32_t& top, bool& has_top,
+                                                  uint32_t* err, uint32_t overflow_bit) {
+    const int nh = __popc(hitm);
+    if (sp + nh > cap) {
+        set_err(err, overflow_bit);
+        const int keep = max(cap - sp, 0);
+        while (__popc(hitm) > keep) hitm &= ~(0x80000000u >> __clz(hitm));  // drop the highest slot
+    }
+    bool pending = false;
+    int32_t pend = 0;
+#pragma unroll
+    for (int k = 3; k >= 0; --k) {
+        if (!((hitm >> k) & 1u)) continue;
+        if (pending) stk[(sp++) * STRIDE] = pend;
+        pend = cc[k] < 0 ? ci[k] : int32_t(0x80000000u | (uint32_t(cc[k] - 1) << 27) | uint32_t(~ci[k]));
+        pending = true;
+    }
+    if (pending) {
+        top = pend;
+        has_top = true;
+    }
+}
+
 }  // namespace rq

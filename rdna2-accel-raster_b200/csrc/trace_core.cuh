@@ -68,38 +68,16 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
             const float any_[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, afy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
             const float anz[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, afz[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
             const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
-            int32_t he[4];
-            float ht[4];
-            int nh = 0;
+            float tk[4];
+            uint32_t hitm = 0;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (acc[k] == 0) continue;
-                float tn;
-                if (slab_nf(sr, tmin, best, anx[k], afx[k], any_[k], afy[k], anz[k], afz[k], tn)) {
-                    const int32_t ent =
-                        acc[k] < 0 ? aci[k] : int32_t(kLeafBit | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
-                    int pos = nh;
-                    if (!ANY) {
-                        while (pos > 0 && ht[pos - 1] > tn) {
-                            he[pos] = he[pos - 1];
-                            ht[pos] = ht[pos - 1];
-                            --pos;
-                        }
-                    }
-                    he[pos] = ent;
-                    ht[pos] = tn;
-                    ++nh;
-                }
-            }
-            if (sp + nh > STACK) {
-                set_err(err, RQ_DERR_STACK);
-                nh = STACK - sp;
-            }
-            for (int j = nh - 1; j >= 1; --j) stk[(sp++) * STRIDE] = he[j];
-            if (nh > 0) {
-                top = he[0];
-                has_top = true;
-            }
+            for (int k = 0; k < 4; ++k)
+                if (acc[k] != 0 && slab_nf(sr, tmin, best, anx[k], afx[k], any_[k], afy[k], anz[k], afz[k], tk[k]))
+                    hitm |= 1u << k;
+            if (ANY)
+                push_children_any<STRIDE>(hitm, aci, acc, stk, sp, STACK, top, has_top, err, RQ_DERR_STACK);
+            else
+                push_children<STRIDE>(hitm, aci, acc, tk, true, stk, sp, STACK, top, has_top, err, RQ_DERR_STACK);
         } else {
             const uint32_t first = uint32_t(e) & 0x07ffffffu;
             const uint32_t cntl = ((uint32_t(e) >> 27) & 15u) + 1u;
