@@ -66,7 +66,8 @@ int rq_debug_wait_timeout(rq_ctx* ctx, const uint32_t* flag, uint32_t limit, rq_
 typedef struct rq_trace_tuning {
     uint32_t threads;  /* per block: 64, 128 or 256 (default 128) */
     uint32_t chunk;    /* ray ids a warp takes per refill: 32 or 64 (default 32) */
-    uint32_t reg_cap;  /* registers per thread the launch bounds allow: 0 (no bound), 64 or 80 (default) */
+    uint32_t reg_cap;  /* registers per thread the launch bounds allow: 0 (no bound), 64, 72 (threads
+                          64 or 128 only) or 80 (default) */
     uint32_t top_levels; /* 0, or 4: each block stages the tree's top 4 levels (<= 85 nodes) in shared memory */
     uint32_t speculative; /* 1: lanes holding a leaf keep taking inner nodes while the warp searches
                              (the frame only reports hit or miss, so the order does not show) */
@@ -303,7 +304,8 @@ typedef struct rq_batch_tuning {
     uint32_t build_blocks;        /* persistent build blocks (clamped to max_build_blocks) */
     uint32_t trace_threads;       /* threads per traversal block: 64, 128 or 256 */
     uint32_t trace_chunk;         /* ray ids a warp takes per refill: 32 or 64 */
-    uint32_t trace_reg_cap;       /* registers per thread the launch bounds allow: 0 (none), 64 or 80 */
+    uint32_t trace_reg_cap;       /* registers per thread the launch bounds allow: 0 (none), 64, 72
+                                     (threads 64 or 128 only) or 80 */
     uint32_t trace_blocks_per_sm; /* 0: as many as fit */
     uint32_t stack_entries;       /* stack entries per lane; 0 or anything below
                                      3 * (depth + 2) + 1 means that bound */

@@ -154,7 +154,8 @@ int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint
     if (rc == RQ_OK && n) {
         for (uint32_t tt : {64u, 128u, 256u})
             for (uint32_t chunk : {32u, 64u})
-                for (uint32_t regs : {0u, 64u, 80u}) {
+                for (uint32_t regs : {0u, 64u, 72u, 80u}) {
+                    if (regs == 72u && tt == 256u) continue;  // same occupancy as 80 at 256 threads
                     rq_batch_tuning t = best_b;
                     t.trace_threads = tt;
                     t.trace_chunk = chunk;

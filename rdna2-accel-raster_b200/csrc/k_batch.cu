@@ -433,6 +433,8 @@ const void* trace_kernel(uint32_t tt, uint32_t chunk, uint32_t regs) {
     if constexpr (!MT && !STATS) {
         RQ_SHAPES(64, 32) RQ_SHAPES(64, 64) RQ_SHAPES(128, 64) RQ_SHAPES(256, 32) RQ_SHAPES(256, 64)
         RQ_SHAPE(128, 32, 64) RQ_SHAPE(128, 32, 80)
+        // a budget of 72 registers: 7 blocks of 128 (14 of 64) threads per SM
+        RQ_SHAPE(64, 32, 72) RQ_SHAPE(64, 64, 72) RQ_SHAPE(128, 32, 72) RQ_SHAPE(128, 64, 72)
     }
     RQ_SHAPE(128, 32, 0)
 #undef RQ_SHAPES

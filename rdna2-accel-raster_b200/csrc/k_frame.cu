@@ -274,6 +274,10 @@ const void* shade_kernel(const rq_trace_tuning& t) {
         RQ_SHAPES(64, 32) RQ_SHAPES(64, 64) RQ_SHAPES(128, 64) RQ_SHAPES(256, 32) RQ_SHAPES(256, 64)
         RQ_SHAPE(128, 32, 64, 0, false) RQ_SHAPE(128, 32, 80, 0, false) RQ_SHAPE(128, 32, 80, 4, false)
         RQ_SHAPE(128, 32, 80, 0, true)
+        // a budget of 72 registers: 7 blocks of 128 (14 of 64) threads per SM
+        RQ_SHAPE(64, 32, 72, 0, false) RQ_SHAPE(64, 32, 72, 0, true) RQ_SHAPE(64, 64, 72, 0, false)
+        RQ_SHAPE(64, 64, 72, 0, true) RQ_SHAPE(128, 32, 72, 0, false) RQ_SHAPE(128, 32, 72, 0, true)
+        RQ_SHAPE(128, 64, 72, 0, false) RQ_SHAPE(128, 64, 72, 0, true)
     }
     RQ_SHAPE(128, 32, 0, 0, false)
 #undef RQ_SHAPES

@@ -145,6 +145,51 @@ __device__ __forceinline__ bool slab_nf(const SlabRay& r, float tmin, float best
     return a <= b * RQ_FAR_SCALE;
 }
 
+// slab_nf for the 4 children of one 4-wide node, one axis at a time, so that
+// only one axis's two plane rows are held at once.  `row(i)` returns row i of
+// the node (16 B: min_x, max_x, min_y, max_y, min_z, max_z, child_index,
+// child_count).  Entry and exit are the same values as slab_nf's (max and
+// min are associative); returns the hit mask (bit k: slot k non-empty and
+// hit), entry distances in tk.
+template <class Row>
+__device__ __forceinline__ uint32_t box4_nf(Row row, const SlabRay& r, float tmin, float best, float (&tk)[4]) {
+    float tf[4];
+    {
+        const float4 n = row(r.nx), f = row(r.nx ^ 1);
+        const float an[4] = {n.x, n.y, n.z, n.w}, af[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            tk[k] = __fmaf_rn(an[k], r.ix, -r.ox);
+            tf[k] = __fmaf_rn(af[k], r.ix, -r.ox);
+        }
+    }
+    {
+        const float4 n = row(r.ny), f = row(r.ny ^ 1);
+        const float an[4] = {n.x, n.y, n.z, n.w}, af[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            tk[k] = fmaxf(tk[k], __fmaf_rn(an[k], r.iy, -r.oy));
+            tf[k] = fminf(tf[k], __fmaf_rn(af[k], r.iy, -r.oy));
+        }
+    }
+    {
+        const float4 n = row(r.nz), f = row(r.nz ^ 1);
+        const float an[4] = {n.x, n.y, n.z, n.w}, af[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            tk[k] = fmax3(tk[k], __fmaf_rn(an[k], r.iz, -r.oz), tmin);
+            tf[k] = fmin3(tf[k], __fmaf_rn(af[k], r.iz, -r.oz), best);
+        }
+    }
+    const float4 c = row(7);
+    const int32_t cc[4] = {__float_as_int(c.x), __float_as_int(c.y), __float_as_int(c.z), __float_as_int(c.w)};
+    uint32_t hitm = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (cc[k] != 0 && tk[k] <= tf[k] * RQ_FAR_SCALE) hitm |= 1u << k;
+    return hitm;
+}
+
 // ------------------------------------------------------- triangle tests
 struct F3 {
     float x, y, z;

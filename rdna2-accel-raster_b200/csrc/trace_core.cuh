@@ -57,23 +57,14 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
         }
         if (e >= 0) {
             const float4* np = reinterpret_cast<const float4*>(nodes + e);
-            // each axis's near and far plane rows, chosen by the ray's signs
-            const float4 nx4 = ldg4(np + sr.nx), fx4 = ldg4(np + (sr.nx ^ 1));
-            const float4 ny4 = ldg4(np + sr.ny), fy4 = ldg4(np + (sr.ny ^ 1));
-            const float4 nz4 = ldg4(np + sr.nz), fz4 = ldg4(np + (sr.nz ^ 1));
+            // box tests, each axis's near and far plane rows chosen by the
+            // ray's signs
+            float tk[4];
+            const uint32_t hitm = box4_nf([&](int i) { return ldg4(np + i); }, sr, tmin, best, tk);
             const int4 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
             const int4 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
             if (STATS) res.boxes += 4;
-            const float anx[4] = {nx4.x, nx4.y, nx4.z, nx4.w}, afx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
-            const float any_[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, afy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
-            const float anz[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, afz[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
             const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
-            float tk[4];
-            uint32_t hitm = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (acc[k] != 0 && slab_nf(sr, tmin, best, anx[k], afx[k], any_[k], afy[k], anz[k], afz[k], tk[k]))
-                    hitm |= 1u << k;
             if (ANY)
                 push_children_any<STRIDE>(hitm, aci, acc, stk, sp, STACK, top, has_top, err, RQ_DERR_STACK);
             else

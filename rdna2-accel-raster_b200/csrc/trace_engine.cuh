@@ -267,43 +267,26 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                 }
                 continue;
             }
-            // each axis's near and far plane rows, chosen by the ray's signs
-            float4 nx4, fx4, ny4, fy4, nz4, fz4;
+            // box tests, each axis's near and far plane rows chosen by the
+            // ray's signs
+            float tk[4];
+            uint32_t hitm;
             int4 cix, cnt;
             if (TOP > 0 && (e & kStaged)) {
                 const float4* sp4 = s_top + (e & ~kStaged) * kTopStride;
-                nx4 = sp4[sr.nx];
-                fx4 = sp4[sr.nx ^ 1];
-                ny4 = sp4[sr.ny];
-                fy4 = sp4[sr.ny ^ 1];
-                nz4 = sp4[sr.nz];
-                fz4 = sp4[sr.nz ^ 1];
+                hitm = box4_nf([&](int i) { return sp4[i]; }, sr, ray.tmin, best, tk);
                 const float4 a = sp4[6], b = sp4[7];
                 cix = make_int4(__float_as_int(a.x), __float_as_int(a.y), __float_as_int(a.z), __float_as_int(a.w));
                 cnt = make_int4(__float_as_int(b.x), __float_as_int(b.y), __float_as_int(b.z), __float_as_int(b.w));
             } else {
                 const rq_bvh4_node* nb = IsMulti<Src>::value ? ray.nodes : nodes;
                 const float4* np = reinterpret_cast<const float4*>(nb + e);
-                nx4 = ldg4(np + sr.nx);
-                fx4 = ldg4(np + (sr.nx ^ 1));
-                ny4 = ldg4(np + sr.ny);
-                fy4 = ldg4(np + (sr.ny ^ 1));
-                nz4 = ldg4(np + sr.nz);
-                fz4 = ldg4(np + (sr.nz ^ 1));
+                hitm = box4_nf([&](int i) { return ldg4(np + i); }, sr, ray.tmin, best, tk);
                 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
                 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
             }
             if (STATS) h.boxes += 4;
-            const float anx[4] = {nx4.x, nx4.y, nx4.z, nx4.w}, afx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
-            const float any_[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, afy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
-            const float anz[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, afz[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
             const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
-            float tk[4];
-            uint32_t hitm = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (acc[k] != 0 && slab_nf(sr, ray.tmin, best, anx[k], afx[k], any_[k], afy[k], anz[k], afz[k], tk[k]))
-                    hitm |= 1u << k;
             // closest hit: near to far; any hit: slot order.  The first child
             // to visit stays in the register.
             if (ANY == 1 || (ANY == kAnyPerRay && ray.any))

@@ -43,7 +43,8 @@ def lookup(key, path=TABLE):
 # (threads, refill chunk, register budget, staged top levels, speculative)
 SHADE_SHAPES = ([(t, c, r, 0, 0) for t in (64, 128, 256) for c in (32, 64) for r in (0, 64, 80)]
                 + [(t, c, 80, 4, 0) for t in (64, 128, 256) for c in (32, 64)]
-                + [(t, c, 80, 0, 1) for t in (64, 128, 256) for c in (32, 64)])
+                + [(t, c, 80, 0, 1) for t in (64, 128, 256) for c in (32, 64)]
+                + [(t, c, 72, 0, s) for t in (64, 128) for c in (32, 64) for s in (0, 1)])
 
 
 def shadow_key(ntri, params):
