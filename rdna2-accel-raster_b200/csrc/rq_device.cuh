@@ -145,40 +145,82 @@ __device__ __forceinline__ bool slab_nf(const SlabRay& r, float tmin, float best
     return a <= b * RQ_FAR_SCALE;
 }
 
+// Two IEEE single-precision operations per instruction (the packed f32x2
+// forms of sm_100); each lane is one rounding, as the scalar form.
+__device__ __forceinline__ unsigned long long pack2(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long fmul2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// Plane distances b*inv - o*inv of the 4 children on one axis, two children
+// per packed fused multiply-add.
+__device__ __forceinline__ void planes4(float4 b, float inv, float oinv, float (&t)[4]) {
+    const unsigned long long i2 = pack2(inv, inv), o2 = pack2(-oinv, -oinv);
+    const float2 lo = unpack2(ffma2(pack2(b.x, b.y), i2, o2)), hi = unpack2(ffma2(pack2(b.z, b.w), i2, o2));
+    t[0] = lo.x;
+    t[1] = lo.y;
+    t[2] = hi.x;
+    t[3] = hi.y;
+}
+
 // slab_nf for the 4 children of one 4-wide node, one axis at a time, so that
 // only one axis's two plane rows are held at once.  `row(i)` returns row i of
 // the node (16 B: min_x, max_x, min_y, max_y, min_z, max_z, child_index,
 // child_count).  Entry and exit are the same values as slab_nf's (max and
 // min are associative); returns the hit mask (bit k: slot k non-empty and
 // hit), entry distances in tk.
-template <class Row>
+// PACKED: plane distances two per packed instruction (measured faster for
+// the one-ray-per-thread camera traversal, slower in the persistent engine).
+template <bool PACKED, class Row>
 __device__ __forceinline__ uint32_t box4_nf(Row row, const SlabRay& r, float tmin, float best, float (&tk)[4]) {
+    auto planes = [](float4 b, float inv, float oinv, float (&t)[4]) {
+        if (PACKED) {
+            planes4(b, inv, oinv, t);
+        } else {
+            t[0] = __fmaf_rn(b.x, inv, -oinv);
+            t[1] = __fmaf_rn(b.y, inv, -oinv);
+            t[2] = __fmaf_rn(b.z, inv, -oinv);
+            t[3] = __fmaf_rn(b.w, inv, -oinv);
+        }
+    };
     float tf[4];
+    planes(row(r.nx), r.ix, r.ox, tk);
+    planes(row(r.nx ^ 1), r.ix, r.ox, tf);
     {
-        const float4 n = row(r.nx), f = row(r.nx ^ 1);
-        const float an[4] = {n.x, n.y, n.z, n.w}, af[4] = {f.x, f.y, f.z, f.w};
+        float an[4], af[4];
+        planes(row(r.ny), r.iy, r.oy, an);
+        planes(row(r.ny ^ 1), r.iy, r.oy, af);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            tk[k] = __fmaf_rn(an[k], r.ix, -r.ox);
-            tf[k] = __fmaf_rn(af[k], r.ix, -r.ox);
+            tk[k] = fmaxf(tk[k], an[k]);
+            tf[k] = fminf(tf[k], af[k]);
         }
     }
     {
-        const float4 n = row(r.ny), f = row(r.ny ^ 1);
-        const float an[4] = {n.x, n.y, n.z, n.w}, af[4] = {f.x, f.y, f.z, f.w};
+        float an[4], af[4];
+        planes(row(r.nz), r.iz, r.oz, an);
+        planes(row(r.nz ^ 1), r.iz, r.oz, af);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            tk[k] = fmaxf(tk[k], __fmaf_rn(an[k], r.iy, -r.oy));
-            tf[k] = fminf(tf[k], __fmaf_rn(af[k], r.iy, -r.oy));
-        }
-    }
-    {
-        const float4 n = row(r.nz), f = row(r.nz ^ 1);
-        const float an[4] = {n.x, n.y, n.z, n.w}, af[4] = {f.x, f.y, f.z, f.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            tk[k] = fmax3(tk[k], __fmaf_rn(an[k], r.iz, -r.oz), tmin);
-            tf[k] = fmin3(tf[k], __fmaf_rn(af[k], r.iz, -r.oz), best);
+            tk[k] = fmax3(tk[k], an[k], tmin);
+            tf[k] = fmin3(tf[k], af[k], best);
         }
     }
     const float4 c = row(7);

@@ -60,7 +60,7 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
             // box tests, each axis's near and far plane rows chosen by the
             // ray's signs
             float tk[4];
-            const uint32_t hitm = box4_nf([&](int i) { return ldg4(np + i); }, sr, tmin, best, tk);
+            const uint32_t hitm = box4_nf<true>([&](int i) { return ldg4(np + i); }, sr, tmin, best, tk);
             const int4 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
             const int4 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
             if (STATS) res.boxes += 4;

@@ -274,14 +274,14 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
             int4 cix, cnt;
             if (TOP > 0 && (e & kStaged)) {
                 const float4* sp4 = s_top + (e & ~kStaged) * kTopStride;
-                hitm = box4_nf([&](int i) { return sp4[i]; }, sr, ray.tmin, best, tk);
+                hitm = box4_nf<false>([&](int i) { return sp4[i]; }, sr, ray.tmin, best, tk);
                 const float4 a = sp4[6], b = sp4[7];
                 cix = make_int4(__float_as_int(a.x), __float_as_int(a.y), __float_as_int(a.z), __float_as_int(a.w));
                 cnt = make_int4(__float_as_int(b.x), __float_as_int(b.y), __float_as_int(b.z), __float_as_int(b.w));
             } else {
                 const rq_bvh4_node* nb = IsMulti<Src>::value ? ray.nodes : nodes;
                 const float4* np = reinterpret_cast<const float4*>(nb + e);
-                hitm = box4_nf([&](int i) { return ldg4(np + i); }, sr, ray.tmin, best, tk);
+                hitm = box4_nf<false>([&](int i) { return ldg4(np + i); }, sr, ray.tmin, best, tk);
                 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
                 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
             }
