@@ -200,13 +200,16 @@ __device__ __forceinline__ uint32_t box4_nf(Row row, const SlabRay& r, float tmi
             t[3] = __fmaf_rn(b.w, inv, -oinv);
         }
     };
+    // near-plane rows from the signs (recomputed per node: fewer live registers)
+    const int nx = int(__float_as_uint(r.ix) >> 31), ny = 2 + int(__float_as_uint(r.iy) >> 31),
+              nz = 4 + int(__float_as_uint(r.iz) >> 31);
     float tf[4];
-    planes(row(r.nx), r.ix, r.ox, tk);
-    planes(row(r.nx ^ 1), r.ix, r.ox, tf);
+    planes(row(nx), r.ix, r.ox, tk);
+    planes(row(nx ^ 1), r.ix, r.ox, tf);
     {
         float an[4], af[4];
-        planes(row(r.ny), r.iy, r.oy, an);
-        planes(row(r.ny ^ 1), r.iy, r.oy, af);
+        planes(row(ny), r.iy, r.oy, an);
+        planes(row(ny ^ 1), r.iy, r.oy, af);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             tk[k] = fmaxf(tk[k], an[k]);
@@ -215,8 +218,8 @@ __device__ __forceinline__ uint32_t box4_nf(Row row, const SlabRay& r, float tmi
     }
     {
         float an[4], af[4];
-        planes(row(r.nz), r.iz, r.oz, an);
-        planes(row(r.nz ^ 1), r.iz, r.oz, af);
+        planes(row(nz), r.iz, r.oz, an);
+        planes(row(nz ^ 1), r.iz, r.oz, af);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             tk[k] = fmax3(tk[k], an[k], tmin);

@@ -44,7 +44,8 @@ def lookup(key, path=TABLE):
 SHADE_SHAPES = ([(t, c, r, 0, 0) for t in (64, 128, 256) for c in (32, 64) for r in (0, 64, 80)]
                 + [(t, c, 80, 4, 0) for t in (64, 128, 256) for c in (32, 64)]
                 + [(t, c, 80, 0, 1) for t in (64, 128, 256) for c in (32, 64)]
-                + [(t, c, 72, 0, s) for t in (64, 128) for c in (32, 64) for s in (0, 1)])
+                + [(t, c, 72, 0, s) for t in (64, 128) for c in (32, 64) for s in (0, 1)]
+                + [(t, 64, 64, 0, 1) for t in (64, 128)])
 
 
 def shadow_key(ntri, params):
