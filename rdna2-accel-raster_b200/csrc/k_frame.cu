@@ -179,11 +179,12 @@ struct ShadeSrc {
 };
 
 // One camera ray per thread, 16x8 pixels per block: primary rays are
-// coherent, so lanes stay together without refilling.
+// coherent, so lanes stay together without refilling.  `stack` rows of
+// shared memory per thread (the tree's bound, at most STACK).
 template <bool MT, int STACK>
 __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restrict__ nodes,
                                                     const rq_triangle* __restrict__ tris,
-                                                    const __grid_constant__ GbufSrc src, uint32_t* err) {
+                                                    const __grid_constant__ GbufSrc src, uint32_t* err, int stack) {
     extern __shared__ int32_t s_stack[];
     const uint32_t px = blockIdx.x * 16 + threadIdx.x % 16;
     const uint32_t py = blockIdx.y * 8 + threadIdx.x / 16;
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
     src.make(id, r, m);
     rq::TraceResult res;
     rq::trace_ray<false, MT, false, STACK, kT>(nodes, tris, s_stack + threadIdx.x, r.o, r.d, r.tmin, r.tmax, res,
-                                               err);
+                                               err, stack);
     rq::Hit h;
     h.hit = res.idx != rq::kNoHit;
     h.t = res.t;
@@ -314,12 +315,12 @@ int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_g
     cudaError_t e = with_stack(bound, [&](auto S) {
         constexpr int STACK = decltype(S)::value;
         auto k = mt ? k_gbuffer_seq<true, STACK> : k_gbuffer_seq<false, STACK>;
-        const size_t smem = size_t(STACK) * kT * 4;
+        const size_t smem = size_t(bound) * kT * 4;  // bound <= STACK
         if (smem > 48 * 1024) {
             cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             if (r != cudaSuccess) return r;
         }
-        k<<<grid, kT, smem, st>>>(bvh->nodes4, bvh->tris, src, ctx->d_err);
+        k<<<grid, kT, smem, st>>>(bvh->nodes4, bvh->tris, src, ctx->d_err, int(bound));
         return cudaGetLastError();
     });
     return rq_cuda_status(ctx, e, "gbuffer launch");

@@ -24,10 +24,12 @@ struct TraceResult {
     uint32_t tris;  // triangles tested
 };
 
+// stack_cap: rows of the stack column actually allocated (at most STACK).
 template <bool ANY, bool MT, bool STATS, int STACK, int STRIDE>
 __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes,
                                           const rq_triangle* __restrict__ tris, int32_t* stk, F3 o, F3 d,
-                                          float tmin, float tmax, TraceResult& res, uint32_t* err) {
+                                          float tmin, float tmax, TraceResult& res, uint32_t* err,
+                                          int stack_cap = STACK) {
     SlabRay sr;
     sr.ix = safe_inv(d.x);
     sr.iy = safe_inv(d.y);
@@ -66,9 +68,9 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
             if (STATS) res.boxes += 4;
             const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
             if (ANY)
-                push_children_any<STRIDE>(hitm, aci, acc, stk, sp, STACK, top, has_top, err, RQ_DERR_STACK);
+                push_children_any<STRIDE>(hitm, aci, acc, stk, sp, stack_cap, top, has_top, err, RQ_DERR_STACK);
             else
-                push_children<STRIDE>(hitm, aci, acc, tk, true, stk, sp, STACK, top, has_top, err, RQ_DERR_STACK);
+                push_children<STRIDE>(hitm, aci, acc, tk, true, stk, sp, stack_cap, top, has_top, err, RQ_DERR_STACK);
         } else {
             const uint32_t first = uint32_t(e) & 0x07ffffffu;
             const uint32_t cntl = ((uint32_t(e) >> 27) & 15u) + 1u;
