@@ -162,11 +162,12 @@ struct ServeSrc {
 };
 
 // At most 72 registers per thread (7 blocks of 128 threads per SM), the
-// budget that measured fastest for the frame's any-hit traversal.
+// budget that measured fastest for the frame's any-hit traversal.  `stack`
+// rows of shared memory per thread (the deepest tree's bound, at most STACK).
 template <bool MT, int STACK>
 __global__ void __launch_bounds__(kST, 7) k_serve(const ServeJob* __restrict__ jobs, const uint32_t* __restrict__ begins,
                                                uint32_t njobs, uint32_t total, uint32_t seq, uint32_t* done,
-                                               uint32_t* ctr, uint32_t* err) {
+                                               uint32_t* ctr, uint32_t* err, int stack) {
     extern __shared__ int32_t smem[];
     uint32_t* s_begin = reinterpret_cast<uint32_t*>(smem);
     for (uint32_t k = threadIdx.x; k <= njobs; k += kST) s_begin[k] = __ldg(begins + k);
@@ -179,7 +180,8 @@ __global__ void __launch_bounds__(kST, 7) k_serve(const ServeJob* __restrict__ j
     src.jobs = jobs;
     src.s_begin = s_begin;
     src.done = done;
-    rq::trace_persistent<rq::kAnyPerRay, MT, false, STACK, kST>(nullptr, nullptr, src, ctr, stk + threadIdx.x, err);
+    rq::trace_persistent<rq::kAnyPerRay, MT, false, STACK, kST>(nullptr, nullptr, src, ctr, stk + threadIdx.x, err,
+                                                                 stack);
 }
 
 __global__ void __launch_bounds__(256) k_gen_mesh_rays(const float* __restrict__ pos,
@@ -216,7 +218,7 @@ int rq_launch_serve(rq_ctx* ctx, const ServeJob* jobs, const uint32_t* begins, u
     cudaError_t e = with_stack(bound, [&](auto S) {
         constexpr int STACK = decltype(S)::value;
         auto kern = mt ? k_serve<true, STACK> : k_serve<false, STACK>;
-        const size_t smem = size_t((njobs + 1 + 3) & ~3u) * 4u + size_t(STACK) * kST * 4u;
+        const size_t smem = size_t((njobs + 1 + 3) & ~3u) * 4u + size_t(bound) * kST * 4u;  // bound <= STACK
         const size_t smem_max = size_t((RQ_SERVE_MAX_JOBS + 1 + 3) & ~3u) * 4u + size_t(STACK) * kST * 4u;
         cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max));
         int per_sm = 0;
@@ -224,7 +226,7 @@ int rq_launch_serve(rq_ctx* ctx, const ServeJob* jobs, const uint32_t* begins, u
         if (r != cudaSuccess) return r;
         uint32_t blocks = uint32_t(ctx->num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
         blocks = std::min(blocks, (total + kST - 1) / kST);
-        kern<<<blocks, kST, smem, st>>>(jobs, begins, njobs, total, seq, done, ctr, ctx->d_err);
+        kern<<<blocks, kST, smem, st>>>(jobs, begins, njobs, total, seq, done, ctr, ctx->d_err, int(bound));
         return cudaGetLastError();
     });
     return rq_cuda_status(ctx, e, "serve launch");
