@@ -71,6 +71,8 @@ typedef struct rq_trace_tuning {
     uint32_t top_levels; /* 0, or 4: each block stages the tree's top 4 levels (<= 85 nodes) in shared memory */
     uint32_t speculative; /* 1: lanes holding a leaf keep taking inner nodes while the warp searches
                              (the frame only reports hit or miss, so the order does not show) */
+    uint32_t refill_min;  /* a warp hands new rays to its idle lanes only once at least this many of
+                             its 32 lanes are idle (or all are): 1..32; 0 means 1 */
 } rq_trace_tuning;
 int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out);
 /* RQ_ERR_INVALID_ARG for a shape that has no kernel. */

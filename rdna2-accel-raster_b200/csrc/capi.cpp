@@ -214,7 +214,9 @@ int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out) {
 int rq_ctx_trace_tuning_set(rq_ctx* ctx, const rq_trace_tuning* t) {
     if (!ctx || !t) return RQ_ERR_INVALID_ARG;
     if (!rq_shade_shape_ok(*t)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
+    if (t->refill_min > 32) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "refill_min above 32");
     ctx->shade_shape = *t;
+    if (ctx->shade_shape.refill_min == 0) ctx->shade_shape.refill_min = 1;
     return RQ_OK;
 }
 

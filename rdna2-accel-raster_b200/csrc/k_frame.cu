@@ -208,12 +208,14 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
 }
 
 // TT threads per block, CHUNK ray ids per refill, REGS: launch bounds that
-// hold registers to REGS (0: none) — the tuned shapes; `stack` rows per lane.
+// hold registers to REGS (0: none) — the tuned shapes; `stack` rows per lane;
+// idle lanes are refilled once `refill_min` of a warp's lanes are idle.
 template <bool MT, bool STATS, int TT, int CHUNK, int REGS, int TOP, bool SPEC>
 __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     k_shadow_ao(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
                 const rq_gbuffer_px* __restrict__ gbuf, const __grid_constant__ ShadeArgs sa,
-                unsigned long long* words, unsigned long long* counters, uint32_t* ctr, uint32_t* err, int stack) {
+                unsigned long long* words, unsigned long long* counters, uint32_t* ctr, uint32_t* err, int stack,
+                int refill_min) {
     extern __shared__ __align__(16) int32_t s_stack[];
     // shared memory: the stack (stack rows x TT), then the staged top levels
     float4* s_top = reinterpret_cast<float4*>(s_stack + stack * TT);
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     src.words = words;
     rq::trace_persistent<1, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK, TOP, SPEC>(nodes, tris, src, ctr,
                                                                               s_stack + threadIdx.x, err, stack,
-                                                                              s_top);
+                                                                              s_top, refill_min);
     if (counters) {
         const uint32_t r = __reduce_add_sync(rq::kFull, src.rays);
         if ((threadIdx.x & 31u) == 0 && r) atomicAdd(counters, (unsigned long long)r);
@@ -357,7 +359,7 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
     if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
     if (e == cudaSuccess && p.num_lights + p.ao_spp > 0) {
         // the counting and reference-arithmetic variants run in the default shape
-        const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0, 0} : ctx->shade_shape;
+        const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0, 0, 1} : ctx->shade_shape;
         const size_t top_bytes = shape.top_levels == 4 ? rq::TopLevels<4>::kBytes : 0;
         const void* k = mt ? (stats ? shade_kernel<true, true>(shape) : shade_kernel<true, false>(shape))
                            : (stats ? shade_kernel<false, true>(shape) : shade_kernel<false, false>(shape));
@@ -373,7 +375,9 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
             const rq_bvh4_node* nodes = bvh->nodes4;
             const rq_triangle* tris = bvh->tris;
             uint32_t* err = ctx->d_err;
-            void* args[] = {&nodes, &tris, &gbuf, &s, &words, &counter, &ctr, &err, const_cast<int*>(&stack)};
+            int refill_min = int(shape.refill_min ? shape.refill_min : 1u);
+            void* args[] = {&nodes, &tris, &gbuf, &s, &words, &counter, &ctr, &err, const_cast<int*>(&stack),
+                            &refill_min};
             e = cudaLaunchKernel(k, dim3(blocks), dim3(shape.threads), args, smem, st);
         }
     }

@@ -32,7 +32,7 @@ struct rq_ctx {
     uint32_t* d_ctr = nullptr;      // work counters of persistent launches (zeroed per launch)
     std::string last_error;
     int collapse_blocks = 0;        // co-resident blocks of the collapse kernel
-    rq_trace_tuning shade_shape{128, 32, 80, 0, 0};  // shadow/AO traversal launch shape
+    rq_trace_tuning shade_shape{128, 32, 80, 0, 0, 1};  // shadow/AO traversal launch shape
 };
 
 struct rq_bvh {

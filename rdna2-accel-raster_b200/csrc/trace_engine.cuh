@@ -153,7 +153,9 @@ __device__ __forceinline__ void stage_top(const rq_bvh4_node* __restrict__ nodes
 
 // STACK bounds the entries per lane (stk has STACK rows of STRIDE words);
 // stack_cap, if smaller, is the bound actually allocated.  CHUNK: ray ids
-// taken per atomic.  TOP > 0: the top levels were staged in s_top by
+// taken per atomic.  refill_min: idle lanes get new rays only once at least
+// this many lanes of the warp are idle (or all are), so that lanes join in
+// groups and a warp's rays stay closer in position and direction.  TOP > 0: the top levels were staged in s_top by
 // stage_top<TOP> (single-BVH sources only).  SPEC: speculative traversal
 // (Aila and Laine 2009) — it changes the order in which a ray meets its
 // nodes, so it is only for any-hit rays whose result is hit or miss alone
@@ -163,7 +165,7 @@ template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src, int CH
 __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict__ nodes,
                                                  const rq_triangle* __restrict__ tris, Src& src, uint32_t* ctr,
                                                  int32_t* stk, uint32_t* err, int stack_cap = STACK,
-                                                 const float4* s_top = nullptr) {
+                                                 const float4* s_top = nullptr, int refill_min = 1) {
     static_assert(TOP == 0 || !IsMulti<Src>::value, "top-level staging needs one BVH per launch");
     static_assert(!SPEC || ANY == 1, "speculative traversal changes which hit an any-hit ray finds first");
     const uint32_t lane = threadIdx.x & 31u;
@@ -192,7 +194,8 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
     for (;;) {
         // ---- refill idle lanes
         uint32_t idle = __ballot_sync(kFull, !active);
-        while (idle && !exhausted) {
+        const bool refill = __popc(idle) >= refill_min || idle == kFull;
+        while (refill && idle && !exhausted) {
             if (next == end) {
                 uint32_t base = 0;
                 if (lane == 0) base = atomicAdd(ctr, uint32_t(CHUNK));

@@ -108,7 +108,7 @@ class Instance(C.Structure):
 
 class TraceTuning(C.Structure):
     _fields_ = [("threads", C.c_uint32), ("chunk", C.c_uint32), ("reg_cap", C.c_uint32), ("top_levels", C.c_uint32),
-                ("speculative", C.c_uint32)]
+                ("speculative", C.c_uint32), ("refill_min", C.c_uint32)]
 
 
 class BatchTuning(C.Structure):
@@ -307,14 +307,14 @@ class Context:
         t = TraceTuning()
         self.check(lib().rq_ctx_trace_tuning_get(self.h, C.byref(t)), "rq_ctx_trace_tuning_get")
         return {"threads": t.threads, "chunk": t.chunk, "reg_cap": t.reg_cap, "top_levels": t.top_levels,
-                "speculative": t.speculative}
+                "speculative": t.speculative, "refill_min": t.refill_min}
 
     def debug_wait_timeout(self, flag, limit, stream=None):
         """One bounded device wait on flag (int32 CUDA tensor) leaving 0."""
         self.check(lib().rq_debug_wait_timeout(self.h, _ptr(flag), limit, _stream(stream)), "rq_debug_wait_timeout")
 
-    def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80, top_levels=0, speculative=0):
-        t = TraceTuning(threads, chunk, reg_cap, top_levels, speculative)
+    def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80, top_levels=0, speculative=0, refill_min=1):
+        t = TraceTuning(threads, chunk, reg_cap, top_levels, speculative, refill_min)
         self.check(lib().rq_ctx_trace_tuning_set(self.h, C.byref(t)), "rq_ctx_trace_tuning_set")
 
 

@@ -46,6 +46,9 @@ SHADE_SHAPES = ([(t, c, r, 0, 0) for t in (64, 128, 256) for c in (32, 64) for r
                 + [(t, c, 80, 0, 1) for t in (64, 128, 256) for c in (32, 64)]
                 + [(t, c, 72, 0, s) for t in (64, 128) for c in (32, 64) for s in (0, 1)]
                 + [(t, 64, 64, 0, 1) for t in (64, 128)])
+# second stage: the refill threshold (idle lanes out of 32) for the fastest shapes
+REFILL_MINS = (4, 8, 12, 16, 20, 24)
+REFILL_TOP = 4
 
 
 def shadow_key(ntri, params):
@@ -64,8 +67,9 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
     mask = torch.empty(n, dtype=torch.int32, device="cuda")
     ao = torch.empty(n, dtype=torch.float32, device="cuda")
     trials = []
-    for t, c, r, top, spec in SHADE_SHAPES:
-        ctx.set_trace_tuning(t, c, r, top, spec)
+
+    def timed(t, c, r, top, spec, refill):
+        ctx.set_trace_tuning(t, c, r, top, spec, refill)
         rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao)
         ms = []
         for _ in range(reps):
@@ -77,9 +81,15 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
             ms.append(a.elapsed_time(b))
         ctx.sync_check()
         trials.append({"threads": t, "chunk": c, "reg_cap": r, "top_levels": top, "speculative": spec,
-                       "ms": statistics.median(ms)})
+                       "refill_min": refill, "ms": statistics.median(ms)})
+
+    for t, c, r, top, spec in SHADE_SHAPES:
+        timed(t, c, r, top, spec, 1)
+    for s in sorted(trials, key=lambda x: x["ms"])[:REFILL_TOP]:
+        for refill in REFILL_MINS:
+            timed(s["threads"], s["chunk"], s["reg_cap"], s["top_levels"], s["speculative"], refill)
     best = min(trials, key=lambda x: x["ms"])
-    keys = ("threads", "chunk", "reg_cap", "top_levels", "speculative")
+    keys = ("threads", "chunk", "reg_cap", "top_levels", "speculative", "refill_min")
     ctx.set_trace_tuning(**{k: best[k] for k in keys})
     return {k: best[k] for k in keys}, trials
 

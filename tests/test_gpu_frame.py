@@ -96,15 +96,22 @@ def test_every_shadow_launch_shape_gives_identical_results(ctx):
     params = rq.shade_params(w, h, W.shadow_lights(16), ao_spp=2, ao_tmax=0.5)
     gb = rq.render_gbuffer(ctx, b, cam)
     base = ctx.trace_tuning()
-    assert base == {"threads": 128, "chunk": 32, "reg_cap": 80, "top_levels": 0, "speculative": 0}
+    assert base == {"threads": 128, "chunk": 32, "reg_cap": 80, "top_levels": 0, "speculative": 0, "refill_min": 1}
     want_m, want_a = [x.cpu().numpy() for x in rq.render_shadow_ao(ctx, b, gb, params)]
     for t, c, r, top, spec in T.SHADE_SHAPES:
         ctx.set_trace_tuning(t, c, r, top, spec)
         m, a = rq.render_shadow_ao(ctx, b, gb, params)
         ctx.sync_check()
         assert np.array_equal(m.cpu().numpy(), want_m) and a.cpu().numpy().tobytes() == want_a.tobytes(), (t, c, r, top, spec)
+    for refill in (0, 8, 16, 32):
+        ctx.set_trace_tuning(64, 64, 64, 0, 0, refill)
+        m, a = rq.render_shadow_ao(ctx, b, gb, params)
+        ctx.sync_check()
+        assert np.array_equal(m.cpu().numpy(), want_m) and a.cpu().numpy().tobytes() == want_a.tobytes(), refill
     with pytest.raises(rq.RqError):
         ctx.set_trace_tuning(96, 32, 0)
+    with pytest.raises(rq.RqError):
+        ctx.set_trace_tuning(64, 64, 64, 0, 0, 33)
     ctx.set_trace_tuning(**base)
     b.destroy()
 
