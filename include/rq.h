@@ -314,6 +314,8 @@ typedef struct rq_batch_tuning {
     uint32_t max_build_blocks;    /* read only: build scratch slices the batch holds */
     float build_ms;               /* rq_batch_autotune: measured time of this shape */
     float trace_ms;
+    uint32_t trace_refill_min;    /* idle lanes of a traversal warp get new rays once at least this
+                                     many of 32 are idle (or all are): 1..32; 0 means 1 */
 } rq_batch_tuning;
 
 int rq_batch_tuning_get(const rq_batch* batch, rq_batch_tuning* out);
@@ -321,8 +323,9 @@ int rq_batch_tuning_get(const rq_batch* batch, rq_batch_tuning* out);
 int rq_batch_tuning_set(rq_batch* batch, const rq_batch_tuning* t);
 /* Autotuner: builds the batch and traces the given rays once per candidate
  * shape — every build block size with 1..occupancy blocks per SM, every
- * traversal block size x refill chunk x register cap — timing each with CUDA
- * events (median of `reps`), and keeps the fastest build and traversal shape.
+ * traversal block size x refill chunk x register cap, then refill thresholds
+ * for the fastest traversal shape — timing each with CUDA events (median of
+ * `reps`), and keeps the fastest build and traversal shape.
  * The stack depth is the smallest safe one for the batch's deepest tree.
  * Writes up to `cap` measured candidates to `trials` (build_ms set for build
  * shapes, trace_ms for traversal shapes) and their number to *count.

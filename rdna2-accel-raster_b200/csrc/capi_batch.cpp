@@ -47,6 +47,7 @@ rq_batch_tuning default_tuning(rq_ctx* ctx, uint32_t slices) {
     t.trace_blocks_per_sm = 0;
     t.stack_entries = 0;
     t.max_build_blocks = slices;
+    t.trace_refill_min = 1;
     return t;
 }
 
@@ -92,7 +93,8 @@ int rq_batch_tuning_get(const rq_batch* batch, rq_batch_tuning* out) {
 int rq_batch_tuning_set(rq_batch* batch, const rq_batch_tuning* t) {
     if (!batch || !t) return RQ_ERR_INVALID_ARG;
     if ((t->build_threads != 256 && t->build_threads != 512 && t->build_threads != 1024) || t->build_blocks == 0 ||
-        !rq_batch_trace_shape_ok(t->trace_threads, t->trace_chunk, t->trace_reg_cap) || t->stack_entries > 128)
+        !rq_batch_trace_shape_ok(t->trace_threads, t->trace_chunk, t->trace_reg_cap) || t->stack_entries > 128 ||
+        t->trace_refill_min > 32)
         return rq_set_error(batch->ctx, RQ_ERR_INVALID_ARG, "no kernel for this batch shape");
     const float bm = batch->tune.build_ms, tm = batch->tune.trace_ms;
     batch->tune = *t;
@@ -162,6 +164,7 @@ int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint
                     t.trace_reg_cap = regs;
                     t.trace_blocks_per_sm = 0;
                     t.stack_entries = 0;
+                    t.trace_refill_min = 1;
                     batch->tune = t;
                     float ms = 0.0f;
                     rc = time_median(ctx, st, reps,
@@ -179,12 +182,36 @@ int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint
                         best_t = t;
                     }
                 }
+        // refill thresholds for the fastest traversal shape
+        const rq_batch_tuning shape = best_t;
+        for (uint32_t refill : {8u, 12u, 16u, 20u}) {
+            if (rc) break;
+            rq_batch_tuning t = shape;
+            t.trace_refill_min = refill;
+            batch->tune = t;
+            float ms = 0.0f;
+            rc = time_median(ctx, st, reps,
+                             [&] {
+                                 return rq_launch_batch_trace(ctx, batch, rays, ray_mesh, ray_flags, n, 0u, hits,
+                                                              nullptr, ctx->d_ctr, st);
+                             },
+                             &ms);
+            if (rc) break;
+            t.build_ms = 0.0f;
+            t.trace_ms = ms;
+            record(t);
+            if (ms < best_tms) {
+                best_tms = ms;
+                best_t = t;
+            }
+        }
     }
     rq_batch_tuning fin = best_b;
     fin.trace_threads = best_t.trace_threads;
     fin.trace_chunk = best_t.trace_chunk;
     fin.trace_reg_cap = best_t.trace_reg_cap;
     fin.trace_blocks_per_sm = best_t.trace_blocks_per_sm;
+    fin.trace_refill_min = best_t.trace_refill_min;
     fin.stack_entries = (3u * (batch->max_depth + 2u) + 1u + 3u) & ~3u;
     fin.build_ms = std::max(0.0f, best_bms);
     fin.trace_ms = std::max(0.0f, best_tms);

@@ -397,13 +397,15 @@ struct BatchSrc {
 
 // Traversal blocks of TT threads, ray ids taken CHUNK at a time, and (REGS)
 // launch bounds that hold registers to REGS per thread: the tuned shapes.
-// The stack has `stack` rows (runtime, from the batch's deepest tree).
+// The stack has `stack` rows (runtime, from the batch's deepest tree); idle
+// lanes are refilled once `refill_min` of a warp's lanes are idle.
 template <bool MT, bool STATS, int TT, int CHUNK, int REGS>
 __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
-    k_batch_trace(const __grid_constant__ BatchSrc<STATS> src, uint32_t* ctr, uint32_t* err, int stack) {
+    k_batch_trace(const __grid_constant__ BatchSrc<STATS> src, uint32_t* ctr, uint32_t* err, int stack,
+                  int refill_min) {
     extern __shared__ int32_t s_stack[];
     rq::trace_persistent<rq::kAnyPerRay, MT, STATS, 128, TT, const BatchSrc<STATS>, CHUNK>(
-        nullptr, nullptr, src, ctr, s_stack + threadIdx.x, err, stack);
+        nullptr, nullptr, src, ctr, s_stack + threadIdx.x, err, stack, nullptr, refill_min);
 }
 
 template <int BT>
@@ -504,6 +506,7 @@ int rq_launch_batch_trace(rq_ctx* ctx, const rq_batch* b, const rq_ray* rays, co
     const uint32_t tt = tuned ? b->tune.trace_threads : 128u;
     const uint32_t chunk = tuned ? b->tune.trace_chunk : 32u;
     const uint32_t regs = tuned ? b->tune.trace_reg_cap : 0u;
+    int refill_min = int(tuned && b->tune.trace_refill_min ? b->tune.trace_refill_min : 1u);
     // stack rows: the bound, rounded up to a multiple of 4 (16-B rows)
     const int stack = int((std::max(bound, b->tune.stack_entries) + 3u) & ~3u);
     const void* kern = mt ? (stats ? trace_kernel<true, true>(tt, chunk, regs) : trace_kernel<true, false>(tt, chunk, regs))
@@ -524,12 +527,12 @@ int rq_launch_batch_trace(rq_ctx* ctx, const rq_batch* b, const rq_ray* rays, co
         if (stats) {
             BatchSrc<true> src{n, rays, ray_mesh, ray_flags, flags, b->d_meshes, b->nodes4, b->tris, b->perm, hits,
                                stats};
-            void* args[] = {&src, &ctr, &err, const_cast<int*>(&stack)};
+            void* args[] = {&src, &ctr, &err, const_cast<int*>(&stack), &refill_min};
             e = cudaLaunchKernel(kern, dim3(blocks), dim3(tt), args, smem, st);
         } else {
             BatchSrc<false> src{n, rays, ray_mesh, ray_flags, flags, b->d_meshes, b->nodes4, b->tris, b->perm, hits,
                                 nullptr};
-            void* args[] = {&src, &ctr, &err, const_cast<int*>(&stack)};
+            void* args[] = {&src, &ctr, &err, const_cast<int*>(&stack), &refill_min};
             e = cudaLaunchKernel(kern, dim3(blocks), dim3(tt), args, smem, st);
         }
     }

@@ -24,6 +24,12 @@
 namespace {
 
 constexpr int kST = 128;
+// idle lanes of a warp get new rays once this many of 32 are idle (16: the
+// frame's tuned threshold; equal or faster than 1 on the serving stream)
+#ifndef RQ_SERVE_REFILL
+#define RQ_SERVE_REFILL 16
+#endif
+constexpr int kServeRefill = RQ_SERVE_REFILL;
 
 // Ray i of a generated request: up to eight draws pcg_hash(base + k) / 2^32
 // with base = pcg_hash(seed ^ pcg_hash(i)).
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(kST, 7) k_serve(const ServeJob* __restrict__ j
     src.s_begin = s_begin;
     src.done = done;
     rq::trace_persistent<rq::kAnyPerRay, MT, false, STACK, kST>(nullptr, nullptr, src, ctr, stk + threadIdx.x, err,
-                                                                 stack);
+                                                                 stack, nullptr, kServeRefill);
 }
 
 __global__ void __launch_bounds__(256) k_gen_mesh_rays(const float* __restrict__ pos,

@@ -136,8 +136,9 @@ def test_autotune_keeps_a_measured_shape(ctx):
     shape, trials = b.autotune(p, i, rays_t, mesh_t, flags_t, reps=2)
     builds = [t for t in trials if t["build_ms"] > 0]
     traces = [t for t in trials if t["trace_ms"] > 0]
-    # 3 block sizes x 2 chunks x budgets {none, 64, 80}, plus 72 at 64 and 128 threads
-    assert len(traces) == 22 and len(builds) >= 3
+    # 3 block sizes x 2 chunks x budgets {none, 64, 80}, plus 72 at 64 and 128 threads, then 4 refill
+    # thresholds for the fastest of those
+    assert len(traces) == 26 and len(builds) >= 3
     assert shape["build_ms"] == min(t["build_ms"] for t in builds)
     assert shape["trace_ms"] == min(t["trace_ms"] for t in traces)
     assert shape["stack_entries"] >= 3 * (max(b.info(m)["depth4"] for m in range(len(descs))) + 2) + 1
