@@ -281,7 +281,7 @@ const void* shade_kernel(const rq_trace_tuning& t) {
         RQ_SHAPE(64, 32, 72, 0, false) RQ_SHAPE(64, 32, 72, 0, true) RQ_SHAPE(64, 64, 72, 0, false)
         RQ_SHAPE(64, 64, 72, 0, true) RQ_SHAPE(128, 32, 72, 0, false) RQ_SHAPE(128, 32, 72, 0, true)
         RQ_SHAPE(128, 64, 72, 0, false) RQ_SHAPE(128, 64, 72, 0, true)
-        RQ_SHAPE(64, 64, 64, 0, true) RQ_SHAPE(128, 64, 64, 0, true)
+        RQ_SHAPE(64, 64, 64, 0, true) RQ_SHAPE(128, 64, 64, 0, true) RQ_SHAPE(256, 64, 64, 0, true)
     }
     RQ_SHAPE(128, 32, 0, 0, false)
 #undef RQ_SHAPES

@@ -45,8 +45,9 @@ SHADE_SHAPES = ([(t, c, r, 0, 0) for t in (64, 128, 256) for c in (32, 64) for r
                 + [(t, c, 80, 4, 0) for t in (64, 128, 256) for c in (32, 64)]
                 + [(t, c, 80, 0, 1) for t in (64, 128, 256) for c in (32, 64)]
                 + [(t, c, 72, 0, s) for t in (64, 128) for c in (32, 64) for s in (0, 1)]
-                + [(t, 64, 64, 0, 1) for t in (64, 128)])
-# second stage: the refill threshold (idle lanes out of 32) for the fastest shapes
+                + [(t, 64, 64, 0, 1) for t in (64, 128, 256)])
+# second stage: the refill threshold (idle lanes out of 32), with and without
+# speculation, for the fastest block size / chunk / register budgets
 REFILL_MINS = (4, 8, 12, 16, 20, 24)
 REFILL_TOP = 4
 
@@ -85,9 +86,17 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
 
     for t, c, r, top, spec in SHADE_SHAPES:
         timed(t, c, r, top, spec, 1)
-    for s in sorted(trials, key=lambda x: x["ms"])[:REFILL_TOP]:
-        for refill in REFILL_MINS:
-            timed(s["threads"], s["chunk"], s["reg_cap"], s["top_levels"], s["speculative"], refill)
+    bases = []
+    for s in sorted(trials, key=lambda x: x["ms"]):
+        b = (s["threads"], s["chunk"], s["reg_cap"], s["top_levels"])
+        if b not in bases:
+            bases.append(b)
+    for t, c, r, top in bases[:REFILL_TOP]:
+        for spec in (0, 1):
+            if (t, c, r, top, spec) not in SHADE_SHAPES:
+                continue
+            for refill in REFILL_MINS:
+                timed(t, c, r, top, spec, refill)
     best = min(trials, key=lambda x: x["ms"])
     keys = ("threads", "chunk", "reg_cap", "top_levels", "speculative", "refill_min")
     ctx.set_trace_tuning(**{k: best[k] for k in keys})
