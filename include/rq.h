@@ -449,6 +449,18 @@ uint64_t rq_radv_size(uint32_t num_triangles);
 int rq_build_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* as_image,
                   uint64_t as_bytes, rq_stream stream);
 
+/* Refit an image built by rq_build_radv (or a refit) after the vertices moved,
+ * with the triangle count unchanged — the driver's refit of the same
+ * acceleration structure (common/vk_bvh.cpp:558-611).  The fast builder's
+ * topology depends only on the triangle count (four consecutive triangles
+ * per leaf box, four consecutive children per parent), so the refit keeps
+ * it and rewrites the triangle nodes, every box and the header's total box:
+ * the bytes equal rq_build_radv's on the new vertices.  The image's header
+ * must describe num_triangles; if not, the image is rebuilt all the same and
+ * the next rq_ctx_check reports RQ_ERR_STATE. */
+int rq_refit_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* as_image, uint64_t as_bytes,
+                  rq_stream stream);
+
 /* Allocation-free variant of rq_build_radv, with no counterpart in the
  * reference.  For callers that own all of their device memory and cannot let
  * a library call cudaMalloc/cudaFree (which synchronise the device and can

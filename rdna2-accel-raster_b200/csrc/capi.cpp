@@ -194,6 +194,8 @@ int rq_ctx_check(rq_ctx* ctx, rq_stream stream) {
     cudaMemset(ctx->d_err, 0, sizeof(uint32_t));
     if (w == RQ_DERR_STACK)
         return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "traversal stack too small for the tree's live depth");
+    if (w == RQ_DERR_RADV_IMAGE)
+        return rq_set_error(ctx, RQ_ERR_STATE, "rq_refit_radv: the image was not built for this triangle count");
     return rq_set_error(ctx, RQ_ERR_DEVICE_TIMEOUT, "device error word 0x" + std::to_string(w));
 }
 
@@ -596,6 +598,20 @@ int rq_build_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* 
     if (as_bytes < L.total_as_size) return rq_set_error(ctx, RQ_ERR_SIZE, "image buffer smaller than rq_radv_size");
     cudaSetDevice(ctx->device);
     return rq_launch_radv(ctx, tri9, num_triangles, as_image, L, S(stream));
+}
+
+int rq_refit_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* as_image, uint64_t as_bytes,
+                  rq_stream stream) {
+    if (!ctx || !tri9 || !as_image) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (num_triangles == 0) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no triangles");
+    if (num_triangles > (1u << 25))
+        return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "RADV node offsets are 32-bit: at most 2^25 triangles");
+    if (!aligned(as_image, 16)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "image must be 16-byte aligned");
+    rq_radv_layout L;
+    if (rq_radv_layout_get(num_triangles, &L)) return RQ_ERR_UNSUPPORTED;
+    if (as_bytes < L.total_as_size) return rq_set_error(ctx, RQ_ERR_SIZE, "image buffer smaller than rq_radv_size");
+    cudaSetDevice(ctx->device);
+    return rq_launch_radv(ctx, tri9, num_triangles, as_image, L, S(stream), true);
 }
 
 int rq_trace_radv(rq_ctx* ctx, const void* as_image, uint64_t as_bytes, const rq_ray* rays, uint32_t n,

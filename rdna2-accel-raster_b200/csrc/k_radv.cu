@@ -37,6 +37,8 @@ struct RadvArgs {
     float4* top;        // 2 per block: subtree box lo, hi (then reused for the top levels)
     uint32_t* ticket;
     uint64_t size;
+    uint32_t check_header = 0;  // refit: the image's header must already describe n triangles
+    uint32_t* err = nullptr;
 };
 
 __device__ __forceinline__ void write_box(uint8_t* boxes, uint32_t node, const uint32_t ch[4], const float mn[4][3],
@@ -128,6 +130,15 @@ __global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
     float* cmx_src = s_mx0;
     float* cmn_dst = s_mn1;
     float* cmx_dst = s_mx1;
+    if (A.check_header && blockIdx.x == 0 && threadIdx.x == 0) {
+        // read before this block takes its ticket, so before the last block
+        // rewrites the header
+        const uint32_t* h = reinterpret_cast<const uint32_t*>(A.img);
+        const uint64_t* h64 = reinterpret_cast<const uint64_t*>(A.img);
+        if (h[0] != 192u || h64[0x60 / 8] != 192ull + 128ull * A.total_boxes || h64[0x68 / 8] != A.n ||
+            h64[0x50 / 8] != A.size)
+            rq::set_err(A.err, RQ_DERR_RADV_IMAGE);
+    }
     const uint32_t L = A.levels;
     const uint32_t leaf_lvl = L - 1;
     const uint32_t leaf_cnt = A.counts[leaf_lvl];
@@ -362,7 +373,8 @@ extern "C" int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, 
     return RQ_OK;
 }
 
-int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st) {
+int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st,
+                   bool refit) {
     const uint32_t leaf_cnt = L.level_counts[L.num_levels - 1];
     const uint32_t blocks = (leaf_cnt + kLeafBoxes - 1) / kLeafBoxes;
     size_t need = sizeof(float4) * 4ull * blocks + 256;
@@ -381,6 +393,8 @@ int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const 
     a.ticket = static_cast<uint32_t*>(ctx->scratch);
     a.top = reinterpret_cast<float4*>(static_cast<char*>(ctx->scratch) + 256);
     a.size = L.total_as_size;
+    a.check_header = refit ? 1u : 0u;
+    a.err = ctx->d_err;
     cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st);
     k_radv<<<blocks, kT, 0, st>>>(a);
     return rq_cuda_status(ctx, cudaGetLastError(), "radv build launch");

@@ -29,7 +29,6 @@ using namespace rq;
 
 constexpr int kTT = 128;
 constexpr int32_t kMarker = 0x40000000;  // "leave the instance" (inner entries are < 2^27)
-constexpr uint32_t kLeaf = 0x80000000u;
 
 __global__ void __launch_bounds__(128) k_instance_boxes(const TlasInst* __restrict__ inst,
                                                         const float* __restrict__ fwd, uint32_t n,
@@ -124,43 +123,21 @@ __global__ void __launch_bounds__(kTT) k_trace_tlas(const rq_bvh4_node* __restri
         }
         if (e >= 0) {
             const float4* np = reinterpret_cast<const float4*>(nodes + e);
-            const float4 nx4 = ldg4(np + sr.nx), fx4 = ldg4(np + (sr.nx ^ 1));
-            const float4 ny4 = ldg4(np + sr.ny), fy4 = ldg4(np + (sr.ny ^ 1));
-            const float4 nz4 = ldg4(np + sr.nz), fz4 = ldg4(np + (sr.nz ^ 1));
+            float tk[4];
+            const uint32_t hitm = box4_nf<false>(GlobalRows{np}, sr, tmin, best, tk);
             const int4 cix = ldg4i(reinterpret_cast<const int4*>(np + 6));
             const int4 cnt = ldg4i(reinterpret_cast<const int4*>(np + 7));
-            const float anx[4] = {nx4.x, nx4.y, nx4.z, nx4.w}, afx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
-            const float any_[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, afy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
-            const float anz[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, afz[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
             const int32_t aci[4] = {cix.x, cix.y, cix.z, cix.w}, acc[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
-            int32_t he[4];
-            float ht[4];
-            int nh = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (acc[k] == 0) continue;
-                float tn;
-                if (slab_nf(sr, tmin, best, anx[k], afx[k], any_[k], afy[k], anz[k], afz[k], tn)) {
-                    const int32_t ent =
-                        acc[k] < 0 ? aci[k] : int32_t(kLeaf | (uint32_t(acc[k] - 1) << 27) | uint32_t(~aci[k]));
-                    int pos = nh;
-                    if (!ANY) {
-                        while (pos > 0 && ht[pos - 1] > tn) {
-                            he[pos] = he[pos - 1];
-                            ht[pos] = ht[pos - 1];
-                            --pos;
-                        }
-                    }
-                    he[pos] = ent;
-                    ht[pos] = tn;
-                    ++nh;
-                }
-            }
-            if (sp + nh > stack_cap) {
-                set_err(err, RQ_DERR_STACK);
-                nh = stack_cap - sp;
-            }
-            for (int j = nh - 1; j >= 0; --j) stk[(sp++) * kTT] = he[j];
+            // the first child to visit comes back as `first`; here it goes on
+            // top of the shared-memory stack with the others
+            int32_t first = 0;
+            bool has_first = false;
+            if (ANY)
+                push_children_any<kTT>(hitm, aci, acc, stk, sp, stack_cap, first, has_first, err, RQ_DERR_STACK);
+            else
+                push_children<kTT>(hitm, aci, acc, tk, true, stk, sp, stack_cap, first, has_first, err,
+                                   RQ_DERR_STACK);
+            if (has_first) stk[(sp++) * kTT] = first;
             continue;
         }
         const uint32_t first = uint32_t(e) & 0x07ffffffu;

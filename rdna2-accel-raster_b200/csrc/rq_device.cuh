@@ -186,6 +186,12 @@ __device__ __forceinline__ void planes4(float4 b, float inv, float oinv, float (
 // child_count).  Entry and exit are the same values as slab_nf's (max and
 // min are associative); returns the hit mask (bit k: slot k non-empty and
 // hit), entry distances in tk.
+// Rows of a node in global memory, for box4_nf.
+struct GlobalRows {
+    const float4* np;
+    __device__ __forceinline__ float4 operator()(int i) const { return __ldg(np + i); }
+};
+
 // PACKED: plane distances two per packed instruction (measured faster for
 // the one-ray-per-thread camera traversal, slower in the persistent engine).
 template <bool PACKED, class Row>

@@ -18,6 +18,7 @@
 #define RQ_DERR_STACK 16u
 #define RQ_DERR_QUEUE 32u
 #define RQ_DERR_WAIT_CHECK 64u
+#define RQ_DERR_RADV_IMAGE 128u  // rq_refit_radv: the image's header is not for this triangle count
 
 // Largest triangle count a leaf stack entry can address (27-bit first prim).
 #define RQ_MAX_TRIANGLES (1u << 27)
@@ -148,7 +149,8 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
                         uint32_t* mask, float* ao, unsigned long long* counter, cudaStream_t st);
 
 // ---------------------------------------------------------------- k_radv
-int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st);
+int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st,
+                   bool refit = false);
 int rq_launch_radv_check(rq_ctx* ctx, const void* img, uint64_t bytes, rq_radv_check* out, cudaStream_t st);
 
 // ---------------------------------------------------------------- k_post

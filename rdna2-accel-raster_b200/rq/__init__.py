@@ -181,6 +181,7 @@ SIGNATURES = [
     ("rq_radv_layout_get", C.c_int, [_U32, C.POINTER(RadvLayout)]),
     ("rq_radv_size", C.c_uint64, [_U32]),
     ("rq_build_radv", C.c_int, [_P, _P, _U32, _P, C.c_uint64, _P]),
+    ("rq_refit_radv", C.c_int, [_P, _P, _U32, _P, C.c_uint64, _P]),
     ("rq_trace_radv", C.c_int, [_P, _P, C.c_uint64, _P, _U32, _U32, _P, _P, _P]),
     ("rq_radv_describe", C.c_int, [_P, C.c_uint64, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("rq_radv_validate", C.c_int, [_P, _P, C.c_uint64, C.POINTER(RadvCheck), _P]),
@@ -590,6 +591,13 @@ def build_radv(ctx, tri9, image=None, stream=None):
         image = torch.empty(size, dtype=torch.uint8, device=tri9.device)
     rc = lib().rq_build_radv(ctx.h, _ptr(tri9), n, _ptr(image), _count(image, 1), _stream(stream))
     ctx.check(rc, "rq_build_radv")
+    return image
+
+
+def refit_radv(ctx, tri9, image, stream=None):
+    """Refit an image in place after its vertices moved (same triangle count)."""
+    rc = lib().rq_refit_radv(ctx.h, _ptr(tri9), _count(tri9, 36), _ptr(image), _count(image, 1), _stream(stream))
+    ctx.check(rc, "rq_refit_radv")
     return image
 
 

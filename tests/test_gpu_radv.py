@@ -145,3 +145,28 @@ def test_validate_reports_damage(ctx):
     # a header whose leaf region runs past the image
     r = check(lambda h: h.__setitem__(slice(96, 104), np.frombuffer(np.uint64(len(h)).tobytes(), np.uint8)))
     assert r["header_ok"] == 0
+
+
+@pytest.mark.parametrize("n", [5, 4097, 100000])
+def test_radv_refit_equals_rebuild(ctx, n):
+    # rq_refit_radv after the vertices move: the bytes of a fresh build on the
+    # new vertices (and of the oracle's image of them)
+    a = soup(n, 300 + n).reshape(-1)
+    moved = (a + np.float32(0.25) * np.sin(np.arange(a.size, dtype=np.float32))).astype(np.float32)
+    img = radv_gpu(ctx, a)
+    rq.refit_radv(ctx, torch.from_numpy(moved).cuda(), img)
+    ctx.sync_check()
+    assert np.array_equal(img.cpu().numpy(), O.radv_build(moved))
+
+
+def test_radv_refit_of_another_count_is_reported(ctx):
+    # an image built for 100 triangles refitted as 64: the header check
+    # reports it on the next rq_ctx_check; the context stays usable
+    img = radv_gpu(ctx, soup(100, 5).reshape(-1))
+    tri64 = torch.from_numpy(soup(64, 6).reshape(-1)).cuda()
+    rq.refit_radv(ctx, tri64, img)
+    with pytest.raises(rq.RqError) as ei:
+        ctx.sync_check()
+    assert ei.value.status == rq.RQ_ERR_STATE
+    out = radv_gpu(ctx, soup(64, 6).reshape(-1))  # later calls work
+    assert np.array_equal(out.cpu().numpy(), O.radv_build(soup(64, 6).reshape(-1)))
