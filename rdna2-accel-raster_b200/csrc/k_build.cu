@@ -81,20 +81,81 @@ __global__ void __launch_bounds__(kT) k_karras(const uint32_t* __restrict__ keys
     if (n == 1 && blockIdx.x == 0 && threadIdx.x == 0) par_lf[0] = rq::kNoParent;
 }
 
-__global__ void __launch_bounds__(kT) k_leaves(const float* __restrict__ pos, uint32_t sf,
-                                               const uint32_t* __restrict__ idx, uint32_t n, uint32_t max_leaf,
-                                               const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
-                                               const int32_t* __restrict__ kl, const int32_t* __restrict__ kr,
-                                               const uint32_t* __restrict__ klo, const uint32_t* __restrict__ khi,
-                                               const uint32_t* __restrict__ par_in, const uint32_t* __restrict__ par_lf,
-                                               float4* box_in, float4* __restrict__ box_lf, uint32_t* refit_flag,
-                                               uint32_t* __restrict__ c_out, rq_triangle* __restrict__ tris,
-                                               uint32_t* __restrict__ perm, uint32_t* __restrict__ keys_out,
-                                               uint32_t* err) {
-    for (uint32_t k = blockIdx.x * kT + threadIdx.x; k < n; k += gridDim.x * kT) {
+// Leaves and refit with the bottom of the tree refitted in shared memory.
+// Block b owns the sorted leaves [kLocal*b, kLocal*(b+1)).  A Karras node's
+// index is one end of its leaf range, so a node whose range lies inside the
+// block's has its index inside it too: such nodes take their arrival count
+// and box in shared memory (CTA-scope ordering), and write the box to global
+// memory once for the emission.  Only nodes whose range crosses a block
+// boundary (a few per block and level) use the device-scope acquire-release
+// count of refit_walk.  Unions are exact, so the boxes equal refit_walk's.
+constexpr uint32_t kLocal = 512;  // 34 KB of shared memory per block
+
+__global__ void __launch_bounds__(kT) k_leaves_local(
+    const float* __restrict__ pos, uint32_t sf, const uint32_t* __restrict__ idx, uint32_t n, uint32_t max_leaf,
+    const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids, const int32_t* __restrict__ kl,
+    const int32_t* __restrict__ kr, const uint32_t* __restrict__ klo, const uint32_t* __restrict__ khi,
+    const uint32_t* __restrict__ par_in, const uint32_t* __restrict__ par_lf, float4* box_in,
+    float4* __restrict__ box_lf, uint32_t* refit_flag, uint32_t* __restrict__ c_out, rq_triangle* __restrict__ tris,
+    uint32_t* __restrict__ perm, uint32_t* __restrict__ keys_out, uint32_t* err) {
+    __shared__ uint32_t s_flag[kLocal];
+    __shared__ float4 s_lf[2 * kLocal];  // leaf boxes (lo, hi) of the block's leaves
+    __shared__ float4 s_in[2 * kLocal];  // boxes of the block's inner nodes
+    const uint32_t L0 = blockIdx.x * kLocal;
+    const uint32_t L1 = min(L0 + kLocal, n);
+    for (uint32_t i = threadIdx.x; i < kLocal; i += kT) s_flag[i] = 0u;
+    for (uint32_t k = L0 + threadIdx.x; k < L1; k += kT) {
         rq::leaf_step(k, pos, sf, idx, max_leaf, skeys, sids, klo, khi, par_in, par_lf, box_lf, c_out, tris, perm,
                       keys_out);
-        rq::refit_walk(k, kl, kr, par_in, par_lf, box_in, box_lf, refit_flag, err);
+        s_lf[2 * (k - L0)] = box_lf[2 * size_t(k)];
+        s_lf[2 * (k - L0) + 1] = box_lf[2 * size_t(k) + 1];
+    }
+    __syncthreads();
+    for (uint32_t k = L0 + threadIdx.x; k < L1; k += kT) {
+        uint32_t par = par_lf[k];
+        uint32_t guard = 0;
+        bool local = true;
+        while (par != rq::kNoParent) {
+            const uint32_t p = par >> 1;
+            const int32_t a = kl[p], b = kr[p];
+            float4 alo, ahi, blo, bhi;
+            if (local && __ldg(klo + p) >= L0 && __ldg(khi + p) < L1) {
+                __threadfence_block();  // release this thread's shared-memory box
+                if (atomicAdd(&s_flag[p - L0], 1u) == 0u) break;
+                __threadfence_block();  // acquire the sibling's
+                const float4* pa = a < 0 ? s_lf + 2 * ((uint32_t(a) & 0x7fffffffu) - L0) : s_in + 2 * (a - L0);
+                const float4* pb = b < 0 ? s_lf + 2 * ((uint32_t(b) & 0x7fffffffu) - L0) : s_in + 2 * (b - L0);
+                alo = pa[0];
+                ahi = pa[1];
+                blo = pb[0];
+                bhi = pb[1];
+                const float4 lo = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f);
+                const float4 hi = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f);
+                s_in[2 * (p - L0)] = lo;
+                s_in[2 * (p - L0) + 1] = hi;
+                __stcg(box_in + 2 * size_t(p), lo);
+                __stcg(box_in + 2 * size_t(p) + 1, hi);
+            } else {
+                // from here up every range crosses a block boundary
+                local = false;
+                if (rq::atom_add_acq_rel(&refit_flag[p], 1u) == 0u) break;
+                const float4* ba = a < 0 ? box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : box_in + 2 * size_t(a);
+                const float4* bb = b < 0 ? box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : box_in + 2 * size_t(b);
+                alo = rq::ld_cg4(ba);
+                ahi = rq::ld_cg4(ba + 1);
+                blo = rq::ld_cg4(bb);
+                bhi = rq::ld_cg4(bb + 1);
+                __stcg(box_in + 2 * size_t(p),
+                       make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f));
+                __stcg(box_in + 2 * size_t(p) + 1,
+                       make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f));
+            }
+            par = par_in[p];
+            if (++guard > 128u) {
+                rq::set_err(err, RQ_DERR_REFIT);
+                break;
+            }
+        }
     }
 }
 
@@ -269,9 +330,10 @@ int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_
     const uint32_t* skeys = s.keys[rb];
     const uint32_t* sids = s.vals[rb];
     k_karras<<<grid_for(n, sms), kT, 0, st>>>(skeys, n, s.kl, s.kr, s.klo, s.khi, s.par_in, s.par_lf);
-    k_leaves<<<grid_for(n, sms), kT, 0, st>>>(pos, sf, idx, n, max_leaf, skeys, sids, s.kl, s.kr, s.klo, s.khi,
-                                              s.par_in, s.par_lf, s.box_in, s.box_lf, s.refit_flag, s.c, bvh->tris,
-                                              bvh->perm, bvh->skeys, ctx->d_err);
+    k_leaves_local<<<(n + kLocal - 1) / kLocal, kT, 0, st>>>(pos, sf, idx, n, max_leaf, skeys, sids, s.kl, s.kr,
+                                                             s.klo, s.khi, s.par_in, s.par_lf, s.box_in, s.box_lf,
+                                                             s.refit_flag, s.c, bvh->tris, bvh->perm, bvh->skeys,
+                                                             ctx->d_err);
     rq_launch_scan(ctx, s.c, s.a, n, s.scan_status, s.tile_ctr + 8, st);
     k_emit2<<<grid_for(n, sms), kT, 0, st>>>(n, max_leaf, s.kr, s.klo, s.khi, s.par_in, s.par_lf, s.box_in, s.box_lf,
                                              s.c, s.a, bvh->nodes2, bvh->d_counts);
