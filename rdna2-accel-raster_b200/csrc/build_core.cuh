@@ -325,28 +325,46 @@ struct CollapseIO {
     int32_t* cand;      // 4 per queue entry
     int32_t* child_q;   // 4 per queue entry: queue index of inner children, -1
     uint32_t* sz;       // subtree sizes
-    uint32_t* pre;      // pre-order positions
+    uint32_t* par;      // per queue entry: (parent entry << 2) | slot, kNoParent for the root
+    unsigned long long* acc;  // per queue entry: (arrived inner children << 32) | their summed sizes
     uint32_t* tail;     // queue length (atomic)
     rq_bvh4_node* out4;
     int32_t* map4;
 };
 
+// Inner children (queue entries) of entry e.
+__device__ __forceinline__ uint32_t inner_children(const CollapseIO& io, uint32_t e) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c += __ldcg(io.child_q + 4 * size_t(e) + k) >= 0 ? 1u : 0u;
+    return c;
+}
+
 // The three phases of the collapse, run by `nthreads` cooperating threads
 // (index tid) that meet at `sync()` (false = a barrier gave up; abort):
-//   1. top-down per level: candidates, inner candidates appended to q;
-//   2. bottom-up over the recorded levels: subtree sizes;
-//   3. top-down: pre-order position of every child (parent + 1 + sizes of
-//      the earlier inner siblings) and the node writes.
+//   1. top-down per level: candidates, inner candidates appended to q with
+//      their parent link;
+//   2. subtree sizes bottom-up without level barriers: each entry with no
+//      inner children starts a walk; at each parent one 64-bit atomic adds
+//      (one arrival, the child's size) and returns the earlier arrivals and
+//      sizes, so the arrival that completes the parent carries its size on;
+//   3. every entry's pre-order position is the sum over its ancestors of
+//      1 + the sizes of the earlier inner siblings (a walk to the root), then
+//      the node write.
+// LEVELS: phases 2 and 3 level by level instead (bottom-up sizes, then
+// top-down positions, one sync per level; `acc` holds the positions) — the
+// faster form when sync() is a block barrier.
 // s_lvl (shared, max_levels + 2 entries) records the level boundaries.
 // Data written inside the collapse is read with ld.cg: other blocks wrote it.
-template <bool NC, class Sync>
+template <bool NC, bool LEVELS, class Sync>
 __device__ __forceinline__ bool collapse_levels(const CollapseIO& io, uint32_t tid, uint32_t nthreads,
                                                 uint32_t* s_lvl, uint32_t max_levels, Sync sync, uint32_t* err,
                                                 uint32_t* total_out, uint32_t* depth_out) {
     const bool root_leaf = load_n2<NC>(io.n2, 0).l < 0;
     if (tid == 0) {
         __stcg(io.q, 0u);
-        __stcg(io.pre, 0u);
+        __stcg(io.par, kNoParent);
+        __stcg(io.acc, 0ull);
         atomicExch(io.tail, 1u);
     }
     if (!sync()) return false;
@@ -366,6 +384,8 @@ __device__ __forceinline__ bool collapse_levels(const CollapseIO& io, uint32_t t
                 if (c[k] >= 0 && !root_leaf && load_n2<NC>(io.n2, c[k]).l >= 0) {
                     const uint32_t pos = atomicAdd(io.tail, 1u);
                     __stcg(io.q + pos, uint32_t(c[k]));
+                    __stcg(io.par + pos, (e << 2) | uint32_t(k));
+                    __stcg(io.acc + pos, 0ull);
                     cq = int32_t(pos);
                 }
                 __stcg(io.cand + 4 * size_t(e) + k, c[k]);
@@ -382,42 +402,93 @@ __device__ __forceinline__ bool collapse_levels(const CollapseIO& io, uint32_t t
         }
     }
     if (threadIdx.x == 0) s_lvl[depth] = end;
-    __syncthreads();
-    for (int lv = int(depth) - 1; lv >= 0; --lv) {
-        for (uint32_t e = s_lvl[lv] + tid; e < s_lvl[lv + 1]; e += nthreads) {
-            uint32_t s = 1;
+    struct SizeOf {
+        const uint32_t* sz;
+        __device__ uint32_t operator()(int32_t i) const { return __ldcg(sz + i); }
+    };
+    if constexpr (LEVELS) {
+        __syncthreads();
+        uint32_t* pre = reinterpret_cast<uint32_t*>(io.acc);  // acc[0] = 0: the root at 0
+        for (int lv = int(depth) - 1; lv >= 0; --lv) {
+            for (uint32_t e = s_lvl[lv] + tid; e < s_lvl[lv + 1]; e += nthreads) {
+                uint32_t s = 1;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int32_t cq = __ldcg(io.child_q + 4 * size_t(e) + k);
-                if (cq >= 0) s += __ldcg(io.sz + cq);
+                for (int k = 0; k < 4; ++k) {
+                    const int32_t cq = __ldcg(io.child_q + 4 * size_t(e) + k);
+                    if (cq >= 0) s += __ldcg(io.sz + cq);
+                }
+                __stcg(io.sz + e, s);
             }
-            __stcg(io.sz + e, s);
+            if (!sync()) return false;
+        }
+        struct PreOut {
+            uint32_t* pre;
+            __device__ void operator()(int32_t i, uint32_t v) const { __stcg(pre + i, v); }
+        };
+        for (uint32_t lv = 0; lv < depth; ++lv) {
+            for (uint32_t e = s_lvl[lv] + tid; e < s_lvl[lv + 1]; e += nthreads) {
+                int32_t cand[4], cq[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    cand[k] = __ldcg(io.cand + 4 * size_t(e) + k);
+                    cq[k] = __ldcg(io.child_q + 4 * size_t(e) + k);
+                }
+                write_node4<NC>(io.n2, cand, cq, __ldcg(pre + e), SizeOf{io.sz}, PreOut{pre}, io.out4, io.map4);
+            }
+            if (!sync()) return false;
+        }
+        *total_out = end;
+        *depth_out = depth;
+        return true;
+    } else {
+        for (uint32_t e = tid; e < end; e += nthreads) {
+            if (inner_children(io, e) != 0u) continue;
+            uint32_t cur = e, s = 1u;
+            __stcg(io.sz + cur, s);
+            for (uint32_t guard = 0;; ++guard) {
+                const uint32_t pk = __ldcg(io.par + cur);
+                if (pk == kNoParent) break;
+                if (guard >= max_levels) {
+                    set_err(err, RQ_DERR_QUEUE);
+                    break;
+                }
+                const uint32_t p = pk >> 2;
+                const unsigned long long old = atomicAdd(io.acc + p, (1ull << 32) | s);
+                if (uint32_t(old >> 32) + 1u < inner_children(io, p)) break;
+                s = 1u + uint32_t(old) + s;
+                __stcg(io.sz + p, s);
+                cur = p;
+            }
         }
         if (!sync()) return false;
-    }
-    for (uint32_t lv = 0; lv < depth; ++lv) {
-        for (uint32_t e = s_lvl[lv] + tid; e < s_lvl[lv + 1]; e += nthreads) {
+        struct NoPre {
+            __device__ void operator()(int32_t, uint32_t) const {}
+        };
+        for (uint32_t e = tid; e < end; e += nthreads) {
+            uint32_t pre = 0, cur = e;
+            for (uint32_t pk = __ldcg(io.par + cur); pk != kNoParent; pk = __ldcg(io.par + cur)) {
+                const uint32_t p = pk >> 2, slot = pk & 3u;
+                uint32_t off = 1u;
+                for (uint32_t j = 0; j < slot; ++j) {
+                    const int32_t cq = __ldcg(io.child_q + 4 * size_t(p) + j);
+                    if (cq >= 0) off += __ldcg(io.sz + cq);
+                }
+                pre += off;
+                cur = p;
+            }
             int32_t cand[4], cq[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 cand[k] = __ldcg(io.cand + 4 * size_t(e) + k);
                 cq[k] = __ldcg(io.child_q + 4 * size_t(e) + k);
             }
-            struct SizeOf {
-                const uint32_t* sz;
-                __device__ uint32_t operator()(int32_t i) const { return __ldcg(sz + i); }
-            };
-            struct PreOut {
-                uint32_t* pre;
-                __device__ void operator()(int32_t i, uint32_t v) const { __stcg(pre + i, v); }
-            };
-            write_node4<NC>(io.n2, cand, cq, __ldcg(io.pre + e), SizeOf{io.sz}, PreOut{io.pre}, io.out4, io.map4);
+            write_node4<NC>(io.n2, cand, cq, pre, SizeOf{io.sz}, NoPre{}, io.out4, io.map4);
         }
         if (!sync()) return false;
+        *total_out = end;
+        *depth_out = depth;
+        return true;
     }
-    *total_out = end;
-    *depth_out = depth;
-    return true;
 }
 
 }  // namespace rq

@@ -38,7 +38,8 @@ struct BlockScratch {
     uint32_t *refit_flag, *c, *a;
     uint32_t* q;
     int32_t *cand, *child_q;
-    uint32_t *sz, *pre, *tail;
+    uint32_t *sz, *par, *tail;
+    unsigned long long* acc;
 };
 
 __host__ __device__ size_t carve_block(uintptr_t base, uint32_t n, BlockScratch& s) {
@@ -64,7 +65,8 @@ __host__ __device__ size_t carve_block(uintptr_t base, uint32_t n, BlockScratch&
     s.cand = c.take<int32_t>(4 * N);
     s.child_q = c.take<int32_t>(4 * N);
     s.sz = c.take<uint32_t>(N);
-    s.pre = c.take<uint32_t>(N);
+    s.par = c.take<uint32_t>(N);
+    s.acc = c.take<unsigned long long>(N);
     s.tail = c.take<uint32_t>(64);
     return (c.off + 255) & ~size_t(255);
 }
@@ -335,7 +337,8 @@ __global__ void __launch_bounds__(BT) k_batch_build(BuildArgs A) {
         io.cand = S.cand;
         io.child_q = S.child_q;
         io.sz = S.sz;
-        io.pre = S.pre;
+        io.par = S.par;
+        io.acc = S.acc;
         io.tail = S.tail;
         io.out4 = out4;
         io.map4 = map4;
@@ -344,7 +347,7 @@ __global__ void __launch_bounds__(BT) k_batch_build(BuildArgs A) {
             __syncthreads();
             return true;
         };
-        if (rq::collapse_levels<false>(io, threadIdx.x, kBT, s_lvl, kMaxLevels, sync, A.err, &total, &depth) &&
+        if (rq::collapse_levels<false, true>(io, threadIdx.x, kBT, s_lvl, kMaxLevels, sync, A.err, &total, &depth) &&
             threadIdx.x == 0) {
             counts[1] = total;
             counts[2] = depth;

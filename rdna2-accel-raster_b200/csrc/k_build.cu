@@ -301,7 +301,8 @@ size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s) {
     s.cand = c.take<int32_t>(4 * N);
     s.child_q = c.take<int32_t>(4 * N);
     s.sz = c.take<uint32_t>(N);
-    s.pre = c.take<uint32_t>(N);
+    s.cpar = c.take<uint32_t>(N);
+    s.cacc = c.take<unsigned long long>(N);
     s.coll_ctl = c.take<uint32_t>(256);
     return c.off + 256;
 }

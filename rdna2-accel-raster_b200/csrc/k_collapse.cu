@@ -10,9 +10,10 @@
 // One persistent cooperative launch, all blocks co-resident:
 //   phase 1  top-down, one grid barrier per 4-wide level: candidates of each
 //            frontier node, inner candidates appended to a queue;
-//   phase 2  bottom-up over the recorded levels: subtree sizes;
-//   phase 3  top-down: pre-order index of each child = parent + 1 + sizes of
-//            the earlier inner siblings; node and slot-map writes.
+//   phase 2  subtree sizes bottom-up by atomic arrival counts (no barrier per
+//            level);
+//   phase 3  each node's pre-order index from its ancestors' sibling sizes
+//            (no barrier per level); node and slot-map writes.
 // Grid barriers spin with an iteration cap; on timeout they set
 // RQ_DERR_GRID_BARRIER and every block leaves the kernel.
 #include <algorithm>
@@ -36,7 +37,8 @@ struct CollapseArgs {
     int32_t* cand;
     int32_t* child_q;
     uint32_t* sz;
-    uint32_t* pre;
+    uint32_t* par;
+    unsigned long long* acc;
     uint32_t* ctl;  // [0] queue tail [1] barrier arrivals [2] barrier generation
     uint32_t* err;
 };
@@ -73,13 +75,14 @@ __global__ void __launch_bounds__(kT) k_collapse(CollapseArgs A) {
     io.cand = A.cand;
     io.child_q = A.child_q;
     io.sz = A.sz;
-    io.pre = A.pre;
+    io.par = A.par;
+    io.acc = A.acc;
     io.tail = A.ctl;
     io.out4 = A.out4;
     io.map4 = A.map4;
     uint32_t total = 0, depth = 0;
     auto sync = [&]() { return grid_sync(A.ctl, A.err); };
-    if (!rq::collapse_levels<true>(io, blockIdx.x * kT + threadIdx.x, gridDim.x * kT, s_lvl, kMaxLevels, sync, A.err,
+    if (!rq::collapse_levels<true, false>(io, blockIdx.x * kT + threadIdx.x, gridDim.x * kT, s_lvl, kMaxLevels, sync, A.err,
                                    &total, &depth))
         return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -110,7 +113,8 @@ int rq_launch_collapse(rq_ctx* ctx, rq_bvh* bvh, BuildScratch& s, cudaStream_t s
     a.cand = s.cand;
     a.child_q = s.child_q;
     a.sz = s.sz;
-    a.pre = s.pre;
+    a.par = s.cpar;
+    a.acc = s.cacc;
     a.ctl = s.coll_ctl;
     a.err = ctx->d_err;
     void* args[] = {&a};

@@ -105,7 +105,8 @@ struct BuildScratch {
     int32_t* cand;         // 4N candidates (BVH2 ids)
     int32_t* child_q;      // 4N queue index of inner children (-1 none)
     uint32_t* sz;          // N subtree sizes
-    uint32_t* pre;         // N pre-order index
+    uint32_t* cpar;        // N parent link of each queue entry
+    unsigned long long* cacc;  // N arrival counts and size sums
     uint32_t* coll_ctl;    // 96 words: [0] tail [1] barrier count [2] barrier gen [8..] level starts
 };
 
