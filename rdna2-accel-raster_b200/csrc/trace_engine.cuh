@@ -155,8 +155,9 @@ __device__ __forceinline__ void stage_top(const rq_bvh4_node* __restrict__ nodes
 // stack_cap, if smaller, is the bound actually allocated.  CHUNK: ray ids
 // taken per atomic.  refill_min: idle lanes get new rays only once at least
 // this many lanes of the warp are idle (or all are), so that lanes join in
-// groups and a warp's rays stay closer in position and direction.  TOP > 0: the top levels were staged in s_top by
-// stage_top<TOP> (single-BVH sources only).  SPEC: speculative traversal
+// groups and a warp's rays stay closer in position and direction.  TOP > 0:
+// the top levels were staged in s_top by stage_top<TOP> (single-BVH sources
+// only).  SPEC: speculative traversal
 // (Aila and Laine 2009) — it changes the order in which a ray meets its
 // nodes, so it is only for any-hit rays whose result is hit or miss alone
 // (which triangle was found first is not reported by such sources).
