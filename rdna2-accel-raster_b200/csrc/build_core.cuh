@@ -327,7 +327,7 @@ struct CollapseIO {
     uint32_t* sz;       // subtree sizes
     uint32_t* par;      // per queue entry: (parent entry << 2) | slot, kNoParent for the root
     unsigned long long* acc;  // per queue entry: (arrived inner children << 32) | their summed sizes
-    uint32_t* tail;     // queue length (atomic)
+    uint32_t* tail;     // control words: [4..6] per-level append counts, [8..10] hand-over
     rq_bvh4_node* out4;
     int32_t* map4;
 };
@@ -353,49 +353,83 @@ __device__ __forceinline__ uint32_t inner_children(const CollapseIO& io, uint32_
 //      the node write.
 // LEVELS: phases 2 and 3 level by level instead (bottom-up sizes, then
 // top-down positions, one sync per level; `acc` holds the positions) — the
-// faster form when sync() is a block barrier.
+// faster form when sync() is a block barrier.  NARROW > 0 (grid-wide use):
+// block 0 alone expands the top levels while they hold at most NARROW
+// entries.  io.tail holds 16 control words.
 // s_lvl (shared, max_levels + 2 entries) records the level boundaries.
 // Data written inside the collapse is read with ld.cg: other blocks wrote it.
-template <bool NC, bool LEVELS, class Sync>
+template <bool NC, bool LEVELS, uint32_t NARROW, class Sync>
 __device__ __forceinline__ bool collapse_levels(const CollapseIO& io, uint32_t tid, uint32_t nthreads,
                                                 uint32_t* s_lvl, uint32_t max_levels, Sync sync, uint32_t* err,
                                                 uint32_t* total_out, uint32_t* depth_out) {
     const bool root_leaf = load_n2<NC>(io.n2, 0).l < 0;
+    // Entries of level L+1 are appended at end(L) + an atomic count of their
+    // own, io.tail[4 + L % 3]: after the level's sync every thread reads that
+    // count while the next level appends to another one, and the one after
+    // that is cleared during level L, two syncs after its last reader.
+    uint32_t* lvl_cnt = io.tail + 4;
+    auto expand = [&](uint32_t e, uint32_t end, uint32_t depth) {
+        const int32_t u = int32_t(__ldcg(io.q + e));
+        int32_t c[4] = {-1, -1, -1, -1};
+        if (root_leaf)
+            c[0] = 0;
+        else
+            greedy_candidates<NC>(io.n2, u, c);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int32_t cq = -1;
+            if (c[k] >= 0 && !root_leaf && load_n2<NC>(io.n2, c[k]).l >= 0) {
+                const uint32_t pos = end + atomicAdd(lvl_cnt + depth % 3u, 1u);
+                __stcg(io.q + pos, uint32_t(c[k]));
+                __stcg(io.par + pos, (e << 2) | uint32_t(k));
+                __stcg(io.acc + pos, 0ull);
+                cq = int32_t(pos);
+            }
+            __stcg(io.cand + 4 * size_t(e) + k, c[k]);
+            __stcg(io.child_q + 4 * size_t(e) + k, cq);
+        }
+    };
     if (tid == 0) {
         __stcg(io.q, 0u);
         __stcg(io.par, kNoParent);
         __stcg(io.acc, 0ull);
-        atomicExch(io.tail, 1u);
+        atomicExch(lvl_cnt, 0u);
     }
     if (!sync()) return false;
     uint32_t start = 0, end = 1, depth = 0;
-    while (start < end) {
-        if (threadIdx.x == 0) s_lvl[depth] = start;
-        for (uint32_t e = start + tid; e < end; e += nthreads) {
-            const int32_t u = int32_t(__ldcg(io.q + e));
-            int32_t c[4] = {-1, -1, -1, -1};
-            if (root_leaf)
-                c[0] = 0;
-            else
-                greedy_candidates<NC>(io.n2, u, c);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                int32_t cq = -1;
-                if (c[k] >= 0 && !root_leaf && load_n2<NC>(io.n2, c[k]).l >= 0) {
-                    const uint32_t pos = atomicAdd(io.tail, 1u);
-                    __stcg(io.q + pos, uint32_t(c[k]));
-                    __stcg(io.par + pos, (e << 2) | uint32_t(k));
-                    __stcg(io.acc + pos, 0ull);
-                    cq = int32_t(pos);
-                }
-                __stcg(io.cand + 4 * size_t(e) + k, c[k]);
-                __stcg(io.child_q + 4 * size_t(e) + k, cq);
+    if (NARROW > 0) {
+        // the narrow top levels (at most NARROW entries each) by block 0
+        // alone, with block barriers; then one sync hands the frontier over
+        if (blockIdx.x == 0) {
+            while (start < end && end - start <= NARROW && depth + 1 < max_levels) {
+                if (threadIdx.x == 0) atomicExch(lvl_cnt + (depth + 1) % 3u, 0u);
+                for (uint32_t e = start + threadIdx.x; e < end; e += blockDim.x) expand(e, end, depth);
+                __syncthreads();
+                const uint32_t n = __ldcg(lvl_cnt + depth % 3u);
+                ++depth;
+                start = end;
+                end += n;
+            }
+            if (threadIdx.x == 0) {
+                __stcg(io.tail + 8, start);
+                __stcg(io.tail + 9, end);
+                __stcg(io.tail + 10, depth);
             }
         }
         if (!sync()) return false;
+        start = __ldcg(io.tail + 8);
+        end = __ldcg(io.tail + 9);
+        depth = __ldcg(io.tail + 10);
+    }
+    while (start < end) {
+        if (threadIdx.x == 0) s_lvl[depth] = start;
+        if (tid == 0) atomicExch(lvl_cnt + (depth + 1) % 3u, 0u);
+        for (uint32_t e = start + tid; e < end; e += nthreads) expand(e, end, depth);
+        if (!sync()) return false;
+        const uint32_t n = __ldcg(lvl_cnt + depth % 3u);
         ++depth;
         start = end;
-        end = __ldcg(io.tail);
+        end += n;
         if (depth >= max_levels) {
             if (tid == 0) set_err(err, RQ_DERR_QUEUE);
             return false;

@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(BT) k_batch_build(BuildArgs A) {
             __syncthreads();
             return true;
         };
-        if (rq::collapse_levels<false, true>(io, threadIdx.x, kBT, s_lvl, kMaxLevels, sync, A.err, &total, &depth) &&
+        if (rq::collapse_levels<false, true, 0>(io, threadIdx.x, kBT, s_lvl, kMaxLevels, sync, A.err, &total, &depth) &&
             threadIdx.x == 0) {
             counts[1] = total;
             counts[2] = depth;

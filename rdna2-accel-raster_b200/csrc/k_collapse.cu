@@ -8,8 +8,9 @@
 // the bytes equal fromBVH2's for the same binary BVH.
 //
 // One persistent cooperative launch, all blocks co-resident:
-//   phase 1  top-down, one grid barrier per 4-wide level: candidates of each
-//            frontier node, inner candidates appended to a queue;
+//   phase 1  top-down, one grid barrier per 4-wide level (the narrow top
+//            levels by one block): candidates of each frontier node, inner
+//            candidates appended to a queue;
 //   phase 2  subtree sizes bottom-up by atomic arrival counts (no barrier per
 //            level);
 //   phase 3  each node's pre-order index from its ancestors' sibling sizes
@@ -39,7 +40,7 @@ struct CollapseArgs {
     uint32_t* sz;
     uint32_t* par;
     unsigned long long* acc;
-    uint32_t* ctl;  // [0] queue tail [1] barrier arrivals [2] barrier generation
+    uint32_t* ctl;  // [1] barrier arrivals [2] barrier generation, [4..10] collapse_levels control
     uint32_t* err;
 };
 
@@ -82,8 +83,9 @@ __global__ void __launch_bounds__(kT) k_collapse(CollapseArgs A) {
     io.map4 = A.map4;
     uint32_t total = 0, depth = 0;
     auto sync = [&]() { return grid_sync(A.ctl, A.err); };
-    if (!rq::collapse_levels<true, false>(io, blockIdx.x * kT + threadIdx.x, gridDim.x * kT, s_lvl, kMaxLevels, sync, A.err,
-                                   &total, &depth))
+    // levels of at most 256 entries by block 0 alone (measured: a little faster than a grid barrier each)
+    if (!rq::collapse_levels<true, false, 256>(io, blockIdx.x * kT + threadIdx.x, gridDim.x * kT, s_lvl, kMaxLevels,
+                                               sync, A.err, &total, &depth))
         return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.counts[1] = total;

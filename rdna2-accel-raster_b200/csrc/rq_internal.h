@@ -107,7 +107,7 @@ struct BuildScratch {
     uint32_t* sz;          // N subtree sizes
     uint32_t* cpar;        // N parent link of each queue entry
     unsigned long long* cacc;  // N arrival counts and size sums
-    uint32_t* coll_ctl;    // 96 words: [0] tail [1] barrier count [2] barrier gen [8..] level starts
+    uint32_t* coll_ctl;    // 256 words: [1] barrier count [2] barrier gen, [4..10] collapse control
 };
 
 // Carve the build scratch for n triangles out of `base`; returns its size
