@@ -219,30 +219,42 @@ __global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ 
     }
     uint32_t total;
     uint32_t ex = block_exclusive_scan(sum, s_warp, &total);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        // warp-wide decoupled look-back: 32 predecessors per step; the
+        // nearest one with its inclusive prefix ends the walk
+        const uint32_t lane = threadIdx.x;
         if (tile == 0) {
-            rq::st_release(&status[0], kFlagPrefix | total);
-            s_prefix = 0;
-        } else {
-            rq::st_release(&status[tile], kFlagAgg | total);
-            uint32_t acc = 0, spins = 0;
-            int t = int(tile) - 1;
-            while (t >= 0) {
-                uint32_t s = rq::ld_acquire(&status[t]);
-                uint32_t flag = s & ~kValueMask;
-                if (flag == 0u) {
-                    if (++spins > kSpinLimit) {
-                        rq::set_err(err, RQ_DERR_SCAN_LOOKBACK);
-                        break;
-                    }
-                    continue;
-                }
-                acc += s & kValueMask;
-                if (flag == kFlagPrefix) break;
-                --t;
+            if (lane == 0) {
+                rq::st_release(&status[0], kFlagPrefix | total);
+                s_prefix = 0;
             }
-            rq::st_release(&status[tile], kFlagPrefix | (acc + total));
-            s_prefix = acc;
+        } else {
+            if (lane == 0) rq::st_release(&status[tile], kFlagAgg | total);
+            uint32_t acc = 0, spins = 0;
+            for (int t0 = int(tile) - 1;; t0 -= 32) {
+                const int t = t0 - int(lane);
+                uint32_t st = kFlagPrefix;  // before tile 0: an inclusive prefix of 0
+                if (t >= 0) {
+                    for (;;) {
+                        st = rq::ld_acquire(&status[t]);
+                        if (st & ~kValueMask) break;
+                        if (++spins > kSpinLimit) {
+                            rq::set_err(err, RQ_DERR_SCAN_LOOKBACK);
+                            st = kFlagPrefix;
+                            break;
+                        }
+                    }
+                }
+                const uint32_t pm = __ballot_sync(0xffffffffu, (st & ~kValueMask) == kFlagPrefix);
+                uint32_t val = st & kValueMask;
+                if (pm && int(lane) > __ffs(pm) - 1) val = 0u;
+                acc += __reduce_add_sync(0xffffffffu, val);
+                if (pm) break;
+            }
+            if (lane == 0) {
+                rq::st_release(&status[tile], kFlagPrefix | (acc + total));
+                s_prefix = acc;
+            }
         }
     }
     __syncthreads();
