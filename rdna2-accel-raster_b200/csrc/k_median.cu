@@ -40,8 +40,7 @@ struct MedScratch {
     uint32_t* order[3];
     uint32_t* alt[3];
     uint32_t* flag;     // per primitive: 1 left (or staying), 0 right
-    uint32_t* gath;     // flags gathered in one axis order
-    uint32_t* scan;     // exclusive scan of gath
+    uint32_t* scan;     // exclusive scan of the flags in one axis order
     int32_t* pos_seg;   // per position: frontier index, -1 once in a leaf
     Seg* front[2];
     uint32_t* seg_axis;
@@ -65,7 +64,6 @@ size_t carve_med(uintptr_t base, uint32_t n, MedScratch& m) {
     for (int a = 0; a < 3; ++a) m.order[a] = c.take<uint32_t>(N);
     for (int a = 0; a < 3; ++a) m.alt[a] = c.take<uint32_t>(N);
     m.flag = c.take<uint32_t>(N);
-    m.gath = c.take<uint32_t>(N);
     m.scan = c.take<uint32_t>(N);
     m.pos_seg = c.take<int32_t>(N);
     m.front[0] = c.take<Seg>(N);
@@ -185,11 +183,6 @@ __global__ void __launch_bounds__(kT) k_med_flags(uint32_t n, MedScratch m) {
             m.flag[m.order[m.seg_axis[j]][i]] = i < m.seg_mid[j] ? 1u : 0u;
         }
     }
-}
-
-__global__ void __launch_bounds__(kT) k_med_gather(uint32_t n, const uint32_t* __restrict__ order,
-                                                   const uint32_t* __restrict__ flag, uint32_t* __restrict__ g) {
-    for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) g[i] = flag[order[i]];
 }
 
 // Stable partition of one axis order inside every splitting node.
@@ -322,9 +315,9 @@ int rq_launch_build_median(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t 
         k_med_decide<<<(nf + kT - 1) / kT, kT, 0, st>>>(m.front[cur], nf, max_leaf, s.cent, m, m.front[cur ^ 1]);
         k_med_flags<<<g, kT, 0, st>>>(n, m);
         for (int a = 0; a < 3; ++a) {
-            k_med_gather<<<g, kT, 0, st>>>(n, m.order[a], m.flag, m.gath);
+            // exclusive scan of the membership flags in this axis's order
             cudaMemsetAsync(s.tile_ctr + 8, 0, sizeof(uint32_t), st);
-            rq_launch_scan(ctx, m.gath, m.scan, n, s.scan_status, s.tile_ctr + 8, st);
+            rq_launch_scan(ctx, m.flag, m.scan, n, s.scan_status, s.tile_ctr + 8, st, m.order[a]);
             k_med_scatter<<<g, kT, 0, st>>>(n, m.order[a], m.alt[a], m.front[cur], m);
             std::swap(m.order[a], m.alt[a]);
         }

@@ -201,9 +201,11 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kThreads * kScanItems;
 
-__global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                   uint32_t n, uint32_t* status, uint32_t* tile_ctr,
-                                                   uint32_t* err) {
+// GATHER: the i-th input is in[order[i]].
+template <bool GATHER>
+__global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ in, const uint32_t* __restrict__ order,
+                                                   uint32_t* __restrict__ out, uint32_t n, uint32_t* status,
+                                                   uint32_t* tile_ctr, uint32_t* err) {
     __shared__ uint32_t s_warp[kWarps];
     __shared__ uint32_t s_tile, s_prefix;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ 
     uint32_t sum = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
-        v[i] = base + i < n ? in[base + i] : 0u;
+        v[i] = base + i < n ? in[GATHER ? order[base + i] : base + i] : 0u;
         sum += v[i];
     }
     uint32_t total;
@@ -290,8 +292,11 @@ int rq_launch_sort(rq_ctx* ctx, BuildScratch& s, uint32_t n, uint32_t bits, cuda
 }
 
 void rq_launch_scan(rq_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* status,
-                    uint32_t* tile_ctr, cudaStream_t st) {
+                    uint32_t* tile_ctr, cudaStream_t st, const uint32_t* order) {
     const uint32_t tiles = rq_scan_tiles(n);
     cudaMemsetAsync(status, 0, sizeof(uint32_t) * tiles, st);
-    k_scan<<<tiles, kThreads, 0, st>>>(in, out, n, status, tile_ctr, ctx->d_err);
+    if (order)
+        k_scan<true><<<tiles, kThreads, 0, st>>>(in, order, out, n, status, tile_ctr, ctx->d_err);
+    else
+        k_scan<false><<<tiles, kThreads, 0, st>>>(in, nullptr, out, n, status, tile_ctr, ctx->d_err);
 }

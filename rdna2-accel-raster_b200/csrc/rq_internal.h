@@ -127,8 +127,9 @@ uint32_t rq_sort_tiles(uint32_t n);
 // in buffer index returned (0 or 1).
 int rq_launch_sort(rq_ctx* ctx, BuildScratch& s, uint32_t n, uint32_t bits, cudaStream_t st, int* result_buf);
 uint32_t rq_scan_tiles(uint32_t n);
+// Exclusive scan of in[0..n) (of in[order[i]] when order is given).
 void rq_launch_scan(rq_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* status,
-                    uint32_t* tile_ctr, cudaStream_t st);
+                    uint32_t* tile_ctr, cudaStream_t st, const uint32_t* order = nullptr);
 
 // ---------------------------------------------------------------- k_collapse
 int rq_launch_collapse(rq_ctx* ctx, rq_bvh* bvh, BuildScratch& s, cudaStream_t st);
