@@ -68,6 +68,30 @@ def test_large_soup_parity(ctx):
     assert_same_as_oracle(ctx, soup(300000, 11), None)
 
 
+@pytest.mark.parametrize("n", [511, 512, 513, 1023, 1025, 2049, 65537])
+def test_block_boundary_sizes_parity(ctx, n):
+    # sizes around the refit kernel's 512-leaf blocks and the collapse's
+    # one-block top levels
+    assert_same_as_oracle(ctx, soup(n, 700 + n), None)
+
+
+def test_repeated_in_place_rebuilds_parity(ctx):
+    # one handle rebuilt in place over changing inputs (larger, smaller, larger
+    # again): every build equals the oracle's, so no scratch state of an
+    # earlier build leaks into a later one
+    b = None
+    for k, n in enumerate((20000, 513, 70000, 4097, 70000)):
+        pos = soup(n, 900 + k)
+        p = torch.from_numpy(pos).cuda()
+        b = rq.Bvh.build(ctx, p, None, into=b) if b is not None else rq.Bvh.build(ctx, p, None)
+        ctx.sync_check()
+        n2, tr, n4, perm = b.download()
+        o = O.lbvh_build(pos.reshape(-1), None, 4)
+        assert n2.tobytes() == o["nodes2"].tobytes() and n4.tobytes() == o["nodes4"].tobytes(), n
+        assert tr.tobytes() == o["tris"].tobytes() and np.array_equal(perm, o["sorted"]), n
+    b.destroy()
+
+
 def test_reference_terrain_parity(ctx):
     d = np.load(__file__.replace("test_gpu_build.py", "golden/ref_terrain1000.npz"))
     assert_same_as_oracle(ctx, d["pos"], d["idx"])
