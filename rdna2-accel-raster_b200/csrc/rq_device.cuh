@@ -310,15 +310,19 @@ __device__ __forceinline__ WtRay wt_setup(F3 d) {
 
 // Shared-edge edge functions are exact negations of each other (plain float
 // products), exact zeros are re-evaluated in double, t = T / det rounded once.
-__device__ __forceinline__ bool wt_test(const WtRay& w, F3 o, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v) {
+// KX, KY, KZ: the ray's permuted axes fixed at compile time (no per-vertex
+// component selection); -1: taken from w at run time.
+template <int KX, int KY, int KZ>
+__device__ __forceinline__ bool wt_test_k(const WtRay& w, F3 o, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v) {
+    const int kx = KX < 0 ? w.kx : KX, ky = KY < 0 ? w.ky : KY, kz = KZ < 0 ? w.kz : KZ;
     F3 A = f3sub(v0, o), B = f3sub(v1, o), C = f3sub(v2, o);
-    float Az0 = f3c(A, w.kz), Bz0 = f3c(B, w.kz), Cz0 = f3c(C, w.kz);
-    float Ax = __fmaf_rn(-w.sx, Az0, f3c(A, w.kx));
-    float Ay = __fmaf_rn(-w.sy, Az0, f3c(A, w.ky));
-    float Bx = __fmaf_rn(-w.sx, Bz0, f3c(B, w.kx));
-    float By = __fmaf_rn(-w.sy, Bz0, f3c(B, w.ky));
-    float Cx = __fmaf_rn(-w.sx, Cz0, f3c(C, w.kx));
-    float Cy = __fmaf_rn(-w.sy, Cz0, f3c(C, w.ky));
+    float Az0 = f3c(A, kz), Bz0 = f3c(B, kz), Cz0 = f3c(C, kz);
+    float Ax = __fmaf_rn(-w.sx, Az0, f3c(A, kx));
+    float Ay = __fmaf_rn(-w.sy, Az0, f3c(A, ky));
+    float Bx = __fmaf_rn(-w.sx, Bz0, f3c(B, kx));
+    float By = __fmaf_rn(-w.sy, Bz0, f3c(B, ky));
+    float Cx = __fmaf_rn(-w.sx, Cz0, f3c(C, kx));
+    float Cy = __fmaf_rn(-w.sy, Cz0, f3c(C, ky));
     float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
     float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
     float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
@@ -336,6 +340,25 @@ __device__ __forceinline__ bool wt_test(const WtRay& w, F3 o, F3 v0, F3 v1, F3 v
     u = V / det;
     v = W / det;
     return true;
+}
+
+__device__ __forceinline__ bool wt_test(const WtRay& w, F3 o, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v) {
+    return wt_test_k<-1, -1, -1>(w, o, v0, v1, v2, t, u, v);
+}
+
+// The same test through one of the six fixed-axis forms, chosen per ray (the
+// rays of a warp mostly share one): fewer instructions per triangle, more
+// code.  Faster for the one-ray-per-thread camera traversal, not in the
+// persistent engine.
+__device__ __forceinline__ bool wt_test_fixed(const WtRay& w, F3 o, F3 v0, F3 v1, F3 v2, float& t, float& u,
+                                              float& v) {
+    if (w.kz == 2)
+        return w.kx == 0 ? wt_test_k<0, 1, 2>(w, o, v0, v1, v2, t, u, v)
+                         : wt_test_k<1, 0, 2>(w, o, v0, v1, v2, t, u, v);
+    if (w.kz == 1)
+        return w.kx == 2 ? wt_test_k<2, 0, 1>(w, o, v0, v1, v2, t, u, v)
+                         : wt_test_k<0, 2, 1>(w, o, v0, v1, v2, t, u, v);
+    return w.kx == 1 ? wt_test_k<1, 2, 0>(w, o, v0, v1, v2, t, u, v) : wt_test_k<2, 1, 0>(w, o, v0, v1, v2, t, u, v);
 }
 
 // ------------------------------------------------------------------ hashes

@@ -81,7 +81,7 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
                 const F3 v0{a.x, a.y, a.z}, v1{b.x, b.y, b.z}, v2{c.x, c.y, c.z};
                 if (STATS) ++res.tris;
                 float t, u, v;
-                const bool ok = MT ? mt_test(o, d, v0, v1, v2, 1e-7f, t, u, v) : wt_test(w, o, v0, v1, v2, t, u, v);
+                const bool ok = MT ? mt_test(o, d, v0, v1, v2, 1e-7f, t, u, v) : wt_test_fixed(w, o, v0, v1, v2, t, u, v);
                 if (ok && t >= tmin && t < best) {
                     best = t;
                     res.idx = p;
