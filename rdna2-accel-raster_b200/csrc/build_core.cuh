@@ -349,8 +349,9 @@ __device__ __forceinline__ uint32_t inner_children(const CollapseIO& io, uint32_
 //      (one arrival, the child's size) and returns the earlier arrivals and
 //      sizes, so the arrival that completes the parent carries its size on;
 //   3. every entry's pre-order position is the sum over its ancestors of
-//      1 + the sizes of the earlier inner siblings (a walk to the root), then
-//      the node write.
+//      1 + the sizes of the earlier inner siblings (a walk up that stops at
+//      the first ancestor whose position a written parent already
+//      published), then the node write.
 // LEVELS: phases 2 and 3 level by level instead (bottom-up sizes, then
 // top-down positions, one sync per level; `acc` holds the positions) — the
 // faster form when sync() is a block barrier.  NARROW > 0 (grid-wide use):
@@ -495,12 +496,22 @@ __device__ __forceinline__ bool collapse_levels(const CollapseIO& io, uint32_t t
             }
         }
         if (!sync()) return false;
-        struct NoPre {
-            __device__ void operator()(int32_t, uint32_t) const {}
+        // a written node publishes its inner children's positions in `acc`
+        // (bit 63 set; phase 2 never sets it), so most walks stop at once
+        struct PrePublish {
+            unsigned long long* acc;
+            __device__ void operator()(int32_t i, uint32_t v) const { __stcg(acc + i, (1ull << 63) | v); }
         };
         for (uint32_t e = tid; e < end; e += nthreads) {
             uint32_t pre = 0, cur = e;
-            for (uint32_t pk = __ldcg(io.par + cur); pk != kNoParent; pk = __ldcg(io.par + cur)) {
+            for (;;) {
+                const unsigned long long a = __ldcg(io.acc + cur);
+                if (a >> 63) {
+                    pre += uint32_t(a);
+                    break;
+                }
+                const uint32_t pk = __ldcg(io.par + cur);
+                if (pk == kNoParent) break;  // the root, at 0
                 const uint32_t p = pk >> 2, slot = pk & 3u;
                 uint32_t off = 1u;
                 for (uint32_t j = 0; j < slot; ++j) {
@@ -516,7 +527,7 @@ __device__ __forceinline__ bool collapse_levels(const CollapseIO& io, uint32_t t
                 cand[k] = __ldcg(io.cand + 4 * size_t(e) + k);
                 cq[k] = __ldcg(io.child_q + 4 * size_t(e) + k);
             }
-            write_node4<NC>(io.n2, cand, cq, pre, SizeOf{io.sz}, NoPre{}, io.out4, io.map4);
+            write_node4<NC>(io.n2, cand, cq, pre, SizeOf{io.sz}, PrePublish{io.acc}, io.out4, io.map4);
         }
         if (!sync()) return false;
         *total_out = end;
