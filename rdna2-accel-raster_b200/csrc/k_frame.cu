@@ -186,8 +186,11 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
                                                     const rq_triangle* __restrict__ tris,
                                                     const __grid_constant__ GbufSrc src, uint32_t* err, int stack) {
     extern __shared__ int32_t s_stack[];
-    const uint32_t px = blockIdx.x * 16 + threadIdx.x % 16;
-    const uint32_t py = blockIdx.y * 8 + threadIdx.x / 16;
+    // each warp takes an 8x4 pixel tile of the block's 16x8 (the most compact
+    // footprint, so its rays stay close)
+    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u;
+    const uint32_t px = blockIdx.x * 16 + (w & 1u) * 8 + (l & 7u);
+    const uint32_t py = blockIdx.y * 8 + (w >> 1) * 4 + (l >> 3);
     if (px >= src.c.w || py >= src.c.h) return;
     const uint32_t id = ((py / kTileH) * src.tiles_x + px / kTileW) * 32u + (py % kTileH) * kTileW + px % kTileW;
     rq::Ray r;
