@@ -448,7 +448,7 @@ inline bool slab(const float inv[3], const float oinv[3], float tmin, float best
     return a <= b * kFarScale;
 }
 
-// The engine's 4-wide slab test (rq_device.cuh slab_nf): each axis's near
+// The engine's 4-wide slab test (rq_device.cuh box4_nf): each axis's near
 // and far plane picked by the sign bit of inv (the max plane when inv is
 // negative), entry max(near_x, near_y, near_z, tmin), exit
 // min(far_x, far_y, far_z, best).  For boxes with min <= max this equals

@@ -80,7 +80,6 @@ __device__ __forceinline__ SlabRay slab_setup(F3 o, F3 d) {
     sr.ox = o.x * sr.ix;
     sr.oy = o.y * sr.iy;
     sr.oz = o.z * sr.iz;
-    slab_planes(sr);
     return sr;
 }
 

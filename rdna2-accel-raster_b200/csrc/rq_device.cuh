@@ -90,18 +90,7 @@ __device__ __forceinline__ float safe_inv(float d) {
 struct SlabRay {
     float ix, iy, iz;  // inverse direction
     float ox, oy, oz;  // origin * inverse direction
-    // near-plane rows of a 4-wide node (min_x = row 0, max_x = 1, min_y = 2,
-    // ...): the max plane on an axis whose inverse direction is negative;
-    // the far plane is the other row of the pair (row ^ 1)
-    int nx, ny, nz;
 };
-
-// Fill the near-plane rows from the signs of ix, iy, iz (set those first).
-__device__ __forceinline__ void slab_planes(SlabRay& r) {
-    r.nx = int(__float_as_uint(r.ix) >> 31);
-    r.ny = 2 + int(__float_as_uint(r.iy) >> 31);
-    r.nz = 4 + int(__float_as_uint(r.iz) >> 31);
-}
 
 __device__ __forceinline__ float fmax3(float a, float b, float c) {
     float r;
@@ -124,23 +113,6 @@ __device__ __forceinline__ bool slab(const SlabRay& r, float tmin, float best, f
     float tz0 = __fmaf_rn(mnz, r.iz, -r.oz), tz1 = __fmaf_rn(mxz, r.iz, -r.oz);
     float a = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
     float b = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), best));
-    tn = a;
-    return a <= b * RQ_FAR_SCALE;
-}
-
-// The same test with each axis's near and far plane already chosen by the
-// ray's direction signs (slab_planes).  b*inv - o*inv, one rounding, is
-// monotonic in b, so for every box with min <= max the near plane's distance
-// is the smaller of the pair: entry and exit equal slab()'s (up to the sign
-// of a zero entry, which no comparison sees).  Boxes with min > max on an axis
-// are empty here.
-__device__ __forceinline__ bool slab_nf(const SlabRay& r, float tmin, float best, float nx, float fx, float ny,
-                                        float fy, float nz, float fz, float& tn) {
-    const float tnx = __fmaf_rn(nx, r.ix, -r.ox), tfx = __fmaf_rn(fx, r.ix, -r.ox);
-    const float tny = __fmaf_rn(ny, r.iy, -r.oy), tfy = __fmaf_rn(fy, r.iy, -r.oy);
-    const float tnz = __fmaf_rn(nz, r.iz, -r.oz), tfz = __fmaf_rn(fz, r.iz, -r.oz);
-    const float a = fmaxf(fmax3(tnx, tny, tnz), tmin);
-    const float b = fminf(fmin3(tfx, tfy, tfz), best);
     tn = a;
     return a <= b * RQ_FAR_SCALE;
 }
@@ -180,20 +152,26 @@ __device__ __forceinline__ void planes4(float4 b, float inv, float oinv, float (
     t[3] = hi.y;
 }
 
-// slab_nf for the 4 children of one 4-wide node, one axis at a time, so that
-// only one axis's two plane rows are held at once.  `row(i)` returns row i of
-// the node (16 B: min_x, max_x, min_y, max_y, min_z, max_z, child_index,
-// child_count).  Entry and exit are the same values as slab_nf's (max and
-// min are associative); returns the hit mask (bit k: slot k non-empty and
-// hit), entry distances in tk.
 // Rows of a node in global memory, for box4_nf.
 struct GlobalRows {
     const float4* np;
     __device__ __forceinline__ float4 operator()(int i) const { return __ldg(np + i); }
 };
 
-// PACKED: plane distances two per packed instruction (measured faster for
-// the one-ray-per-thread camera traversal, slower in the persistent engine).
+// The slab test of the 4 children of one 4-wide node, one axis at a time, so
+// that only one axis's two plane rows are held at once.  `row(i)` returns row
+// i of the node (16 B: min_x, max_x, min_y, max_y, min_z, max_z, child_index,
+// child_count).  Each axis's near plane is picked by the sign of the inverse
+// direction (the max row when it is negative): b*inv - o*inv, one rounding, is
+// monotonic in b, so for every box with min <= max the near plane's distance
+// is the smaller of the pair, and entry and exit equal slab()'s (up to the
+// sign of a zero entry, which no comparison sees); boxes with min > max on an
+// axis are empty here.  Entry max(near_x, near_y, near_z, tmin), exit
+// min(far_x, far_y, far_z, best) widened by 2^-20 relative, with sm_100's
+// three-input min/max.  Returns the hit mask (bit k: slot k non-empty and
+// hit) and the entry distances in tk.  PACKED: plane distances two per packed
+// instruction (measured faster for the one-ray-per-thread camera traversal,
+// slower in the persistent engine).
 template <bool PACKED, class Row>
 __device__ __forceinline__ uint32_t box4_nf(Row row, const SlabRay& r, float tmin, float best, float (&tk)[4]) {
     auto planes = [](float4 b, float inv, float oinv, float (&t)[4]) {

@@ -37,7 +37,6 @@ __device__ __forceinline__ void trace_ray(const rq_bvh4_node* __restrict__ nodes
     sr.ox = o.x * sr.ix;
     sr.oy = o.y * sr.iy;
     sr.oz = o.z * sr.iz;
-    slab_planes(sr);
     WtRay w;
     if (!MT) w = wt_setup(d);
     float best = tmax;

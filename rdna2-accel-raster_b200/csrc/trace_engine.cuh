@@ -221,7 +221,6 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                     sr.ox = ray.o.x * sr.ix;
                     sr.oy = ray.o.y * sr.iy;
                     sr.oz = ray.o.z * sr.iz;
-                    slab_planes(sr);
                     if (!MT) w = wt_setup(ray.d);
                     best = ray.tmax;
                     h.hit = false;
