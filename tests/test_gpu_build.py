@@ -68,9 +68,9 @@ def test_large_soup_parity(ctx):
     assert_same_as_oracle(ctx, soup(300000, 11), None)
 
 
-@pytest.mark.parametrize("n", [511, 512, 513, 1023, 1025, 2049, 65537])
+@pytest.mark.parametrize("n", [255, 256, 257, 511, 512, 513, 1023, 1025, 2049, 65537])
 def test_block_boundary_sizes_parity(ctx, n):
-    # sizes around the refit kernel's 512-leaf blocks and the collapse's
+    # sizes around the refit kernel's 256-leaf blocks and the collapse's
     # one-block top levels
     assert_same_as_oracle(ctx, soup(n, 700 + n), None)
 
