@@ -480,6 +480,7 @@ def run_ours(args, world, rank, local, pg):
 
     bvh.destroy()
     del p_d, i_d, gbuf, mask, ao, depth, tmp, blurred
+    refbench = run_reference_benchmarks(ctx, dev) if not args.no_extra else None
     vis = run_visibility(ctx, dev, stream) if not args.no_extra else None
     batched = run_batched(ctx, dev) if not args.no_extra else None
     serving = run_serving(dev) if not args.no_extra else None
@@ -560,6 +561,7 @@ def run_ours(args, world, rank, local, pg):
         "shadow_tuning": shade_tuning,
         "ao_blur": blur,
         "median_build": median_build,
+        "reference_benchmarks": refbench,
         "visibility": vis,
         "batched": batched,
         "serving": serving,
@@ -800,6 +802,81 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
         "saturation_throughput_ratio_vs_plain_rebuild": round(
             b["saturation"]["mrays_per_s"] / pr["saturation"]["mrays_per_s"], 2),
     }
+
+
+def run_reference_benchmarks(ctx, dev):
+    """The reference's own micro-benchmarks of this path, on the B200, beside the figures the
+    reference published for an RX 6700 XT (Vulkan): the fast RADV builder at N = 64 ... 4,096
+    (README.md:48-51) and the SW BVH4 traversal of 1,048,576 procedural rays, coherent and
+    incoherent, at 968 / 99,458 / 999,698 triangles (results/exp0_throughput.csv).  The terrain
+    is a height field of this repository with the reference's triangle counts and extent (Y up,
+    100 units wide), not the reference's own terrain; the rays come from the reference's
+    generators (camera (0, 50, -45) looking at (0, 0, 5)).  CUDA-event medians."""
+    import numpy as np
+    import torch
+    import rq
+
+    def timed(fn, reps):
+        fn()
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.median(ms)
+
+    # the builder's device time: 50 builds captured in a CUDA graph and replayed, so that the
+    # host's per-call launch cost (larger than these kernels) does not count, as the
+    # reference's GPU timestamps do not count its host
+    radv = {}
+    published_radv = {64: 9.41, 256: 5.14, 1024: 15.59, 4096: 80.35}
+    side = torch.cuda.Stream(dev)
+    for n in (64, 256, 1024, 4096):
+        rng = np.random.default_rng(n)
+        tri9 = torch.from_numpy(rng.uniform(-1, 1, size=9 * n).astype(np.float32)).to(dev)
+        img = torch.empty(rq.radv_size(n), dtype=torch.uint8, device=dev)
+        with torch.cuda.stream(side):
+            rq.build_radv(ctx, tri9, img)  # scratch allocated before the capture
+            side.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=side):
+                for _ in range(50):
+                    rq.build_radv(ctx, tri9, img)
+        ctx.sync_check()
+        us = 1e3 * timed(g.replay, 20) / 50
+        del g
+        radv[str(n)] = {"us": round(us, 2), "reference_rx6700xt_us": published_radv[n]}
+    published_sw = {968: (1839.7, 1197.7), 99458: (883.5, 67.5), 999698: (447.4, 27.7)}
+    sw = {}
+    for q, n in ((22, 968), (223, 99458), (707, 999698)):
+        pos, idx = rq.scene_grid(q, q, amp=0.05, seed=7)
+        pos = np.ascontiguousarray(np.stack([50.0 * pos[:, 0], 50.0 * pos[:, 2], 50.0 * pos[:, 1]], 1),
+                                   dtype=np.float32)
+        p = torch.from_numpy(pos).to(dev)
+        i = torch.from_numpy(idx.view(np.int32)).to(dev)
+        b = rq.Bvh.build(ctx, p, i)
+        n2, tr, n4, _ = b.download()
+        t_n4 = torch.from_numpy(n4.view(np.uint8).copy()).to(dev)
+        t_tr = torch.from_numpy(tr.view(np.uint8).copy()).to(dev)
+        row = {}
+        for name, coh in (("coherent", 1), ("incoherent", 0)):
+            rays = rq.gen_rays_procedural(ctx, [0, 50, -45], [0, 0, 5], 1 << 20, coh)
+            hits = torch.empty((1 << 20, 4), dtype=torch.int32, device=dev)
+            ms_ref = timed(lambda: rq.trace_ref_bvh4(ctx, t_n4, t_tr, rays), 20)
+            ms_eng = timed(lambda: rq.trace(ctx, b, rays, rq.RQ_TRI_MT, hits=hits), 20)
+            row[name] = {"published_arithmetic_mrays_per_s": round((1 << 20) / ms_ref / 1e3, 1),
+                         "engine_mrays_per_s": round((1 << 20) / ms_eng / 1e3, 1),
+                         "reference_rx6700xt_mrays_per_s": published_sw[n][0 if coh else 1]}
+        sw[str(n)] = row
+        b.destroy()
+    torch.cuda.synchronize(dev)
+    return {"fast_bvh_builder": radv, "sw_bvh4_traversal": sw,
+            "note": ("reference figures: RX 6700 XT through Vulkan, as published; ours: this B200. "
+                     "published_arithmetic = k_ref4 (software_bvh_bvh4.comp restated, closest hit, "
+                     "Moller-Trumbore); engine = rq_trace closest hit with the same triangle test")}
 
 
 def run_visibility(ctx, dev, stream, frames=200):

@@ -150,7 +150,10 @@ __global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
     // ---- leaf boxes and triangle nodes
     const uint32_t lb0 = blockIdx.x * kLeafBoxes;
     const uint32_t nlb = min(uint32_t(kLeafBoxes), leaf_cnt - lb0);
-    for (uint32_t r = 0; r < 16; ++r) {
+    // rounds of kT triangles that hold any of this block's (fewer than 16
+    // for a small image; the same for every thread)
+    const uint32_t rounds = (nlb * 4u + kT - 1) / kT;
+    for (uint32_t r = 0; r < rounds; ++r) {
         const uint32_t local = r * kT + threadIdx.x;  // triangle within block
         const uint32_t ti = lb0 * 4u + local;
         const bool valid = local < nlb * 4u && ti < A.n;
@@ -395,7 +398,7 @@ int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const 
     a.size = L.total_as_size;
     a.check_header = refit ? 1u : 0u;
     a.err = ctx->d_err;
-    cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st);
+    if (blocks > 1) cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st);  // one block never takes a ticket
     k_radv<<<blocks, kT, 0, st>>>(a);
     return rq_cuda_status(ctx, cudaGetLastError(), "radv build launch");
 }
