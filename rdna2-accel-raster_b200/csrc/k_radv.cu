@@ -8,12 +8,17 @@
 // and the pre-root dwords at bytes 180 (= 5) and 188 (= 0xFFFFFFFF).  Bytes
 // the shader never writes (136..191 apart from those two dwords) are zeroed.
 //
-// Block b owns leaf boxes [1024b, 1024b+1024): 4096 triangles, one per
-// thread per round, so the four triangles of a leaf box sit in four
-// consecutive lanes and their boxes meet through warp shuffles.  The block
-// then reduces its subtree in shared memory for up to five levels.  The last
-// block to finish (atomic ticket) builds the remaining top levels and the
-// header from the per-block subtree boxes.
+// Block b owns leaf boxes [LB*b, LB*b+LB) (LB = 64 or 256, a power of four):
+// 4*LB triangles in rounds of one per thread.  In a multi-block image each
+// warp stages its 32 triangles in shared memory so that the triangle and
+// leaf box nodes go out as coalesced 16-B stores; a one-block image (up to
+// 256 triangles) has each lane read and write its own triangle instead.
+// The block then reduces its subtree in shared memory for log4(LB) levels.
+// The last block to finish (atomic ticket) builds the remaining top levels
+// and the header from the per-block subtree boxes, then puts the ticket back
+// to 0 for the next launch on the stream.  Up to 131,072 triangles the
+// subtrees are 64 leaf boxes (a 4,096-triangle image is 16 blocks of one
+// round), above that 256.
 #include <algorithm>
 #include <mutex>
 
@@ -23,7 +28,14 @@
 namespace {
 
 constexpr int kT = 256;
-constexpr int kLeafBoxes = 1024;  // per block
+// 64-leaf-box subtrees up to this many blocks, 256-leaf-box ones above
+constexpr uint32_t kSmallBlocksMax = 512;
+
+// leaf boxes per block: 64 while that gives at most kSmallBlocksMax blocks,
+// then 256 (measured on B200)
+uint32_t radv_leaf_boxes(uint32_t leaf_cnt) { return leaf_cnt <= 64u * kSmallBlocksMax ? 64u : 256u; }
+// blocks for a given subtree size
+uint32_t radv_blocks(uint32_t leaf_cnt, uint32_t lb) { return (leaf_cnt + lb - 1) / lb; }
 constexpr uint32_t kQNaN = 0x7fc00000u;
 
 struct RadvArgs {
@@ -35,58 +47,105 @@ struct RadvArgs {
     uint32_t counts[16];
     uint32_t offs[16];
     float4* top;        // 2 per block: subtree box lo, hi (then reused for the top levels)
-    uint32_t* ticket;
+    uint32_t* ticket;   // 0 at launch; the last block puts it back to 0
     uint64_t size;
     uint32_t check_header = 0;  // refit: the image's header must already describe n triangles
     uint32_t* err = nullptr;
 };
 
-__device__ __forceinline__ void write_box(uint8_t* boxes, uint32_t node, const uint32_t ch[4], const float mn[4][3],
-                                          const float mx[4][3]) {
-    float4* o = reinterpret_cast<float4*>(boxes + 128ull * node);
-    float c[24];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        c[6 * k + 0] = mn[k][0];
-        c[6 * k + 1] = mn[k][1];
-        c[6 * k + 2] = mn[k][2];
-        c[6 * k + 3] = mx[k][0];
-        c[6 * k + 4] = mx[k][1];
-        c[6 * k + 5] = mx[k][2];
-    }
-    reinterpret_cast<uint4*>(o)[0] = make_uint4(ch[0], ch[1], ch[2], ch[3]);
-#pragma unroll
-    for (int q = 0; q < 6; ++q) o[1 + q] = make_float4(c[4 * q], c[4 * q + 1], c[4 * q + 2], c[4 * q + 3]);
-    reinterpret_cast<uint4*>(o)[7] = make_uint4(0u, 0u, 0u, 0u);
-}
-
-// Parent box over up to four children held in (cmn, cmx); writes the Box32
-// node and returns the union through (umn, umx).
+// Box32 node over up to four children, child c's bounds fetched by
+// get(c, mn, mx); writes the node and returns the union through (umn, umx).
+// The union runs over the children in order 0..3, as the shader's min/max
+// chain does.
+template <class Get>
 __device__ __forceinline__ void make_parent(uint8_t* boxes, uint32_t node, uint32_t child_global0, uint32_t nvalid,
-                                            const float* cmn, const float* cmx, float umn[3], float umx[3]) {
-    uint32_t ch[4];
-    float mn[4][3], mx[4][3];
+                                            Get get, float umn[3], float umx[3]) {
     const float qn = __uint_as_float(kQNaN);
+    uint8_t* nd = boxes + 128ull * node;
+    uint32_t ch[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        ch[c] = uint32_t(c) < nvalid ? (((child_global0 + c) * 128u) >> 3) | RQ_RADV_NODE_BOX32 : RQ_RADV_INVALID_NODE;
+    reinterpret_cast<uint4*>(nd)[0] = make_uint4(ch[0], ch[1], ch[2], ch[3]);
     umn[0] = umn[1] = umn[2] = 1e30f;
     umx[0] = umx[1] = umx[2] = -1e30f;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
+        float mn[3] = {qn, qn, qn}, mx[3] = {qn, qn, qn};
         if (uint32_t(c) < nvalid) {
-            ch[c] = (((child_global0 + c) * 128u) >> 3) | RQ_RADV_NODE_BOX32;
+            get(c, mn, mx);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                mn[c][k] = cmn[3 * c + k];
-                mx[c][k] = cmx[3 * c + k];
-                umn[k] = fminf(umn[k], mn[c][k]);
-                umx[k] = fmaxf(umx[k], mx[c][k]);
+                umn[k] = fminf(umn[k], mn[k]);
+                umx[k] = fmaxf(umx[k], mx[k]);
             }
-        } else {
-            ch[c] = RQ_RADV_INVALID_NODE;
+        }
+        float2* b = reinterpret_cast<float2*>(nd + 16 + 24 * c);
+        b[0] = make_float2(mn[0], mn[1]);
+        b[1] = make_float2(mn[2], mx[0]);
+        b[2] = make_float2(mx[1], mx[2]);
+    }
+    reinterpret_cast<uint4*>(nd)[7] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// children held as 3 floats each in shared memory
+struct SmemChildren {
+    const float* mn;
+    const float* mx;
+    __device__ __forceinline__ void operator()(int c, float m[3], float x[3]) const {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) mn[c][k] = mx[c][k] = qn;
+        for (int k = 0; k < 3; ++k) {
+            m[k] = mn[3 * c + k];
+            x[k] = mx[3 * c + k];
         }
     }
-    write_box(boxes, node, ch, mn, mx);
+};
+
+// children held as (lo, hi) float4 pairs in global memory (L2)
+struct GlobalChildren {
+    const float4* p;
+    __device__ __forceinline__ void operator()(int c, float m[3], float x[3]) const {
+        const float4 a = __ldcg(p + 2 * c), b = __ldcg(p + 2 * c + 1);
+        m[0] = a.x;
+        m[1] = a.y;
+        m[2] = a.z;
+        x[0] = b.x;
+        x[1] = b.y;
+        x[2] = b.z;
+    }
+};
+
+// Parent levels over `nchild` children whose boxes sit in shared memory
+// (src), for at most max_levels levels or up to the root; ping-pongs src and
+// dst and leaves the last level's boxes in src.
+__device__ __forceinline__ void smem_levels(const RadvArgs& A, uint8_t* boxes, float*& mn_src, float*& mx_src,
+                                            float*& mn_dst, float*& mx_dst, uint32_t& nchild, uint32_t& child_base,
+                                            uint32_t& lvl, uint32_t max_levels) {
+    for (uint32_t j = 1; j <= max_levels && lvl > 0; ++j) {
+        const uint32_t plvl = lvl - 1;
+        const uint32_t np = (nchild + 3) / 4;
+        const uint32_t pbase = child_base >> 2;
+        for (uint32_t t = threadIdx.x; t < np; t += kT) {
+            float umn[3], umx[3];
+            make_parent(boxes, A.offs[plvl] + pbase + t, A.offs[lvl] + child_base + 4 * t, min(4u, nchild - 4 * t),
+                        SmemChildren{mn_src + 12 * t, mx_src + 12 * t}, umn, umx);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                mn_dst[3 * t + k] = umn[k];
+                mx_dst[3 * t + k] = umx[k];
+            }
+        }
+        __syncthreads();
+        float* tn = mn_src;
+        mn_src = mn_dst;
+        mn_dst = tn;
+        float* tx = mx_src;
+        mx_src = mx_dst;
+        mx_dst = tx;
+        nchild = np;
+        child_base = pbase;
+        lvl = plvl;
+    }
 }
 
 __device__ void write_header(const RadvArgs& A, const float mn[3], const float mx[3]) {
@@ -121,10 +180,19 @@ __device__ void write_header(const RadvArgs& A, const float mn[3], const float m
     h[188 / 4] = 0xffffffffu;
 }
 
-__global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
-    // leaf-level boxes (1024) and the first parent level (256) ping-pong
-    __shared__ float s_mn0[kLeafBoxes * 3], s_mx0[kLeafBoxes * 3];
-    __shared__ float s_mn1[kLeafBoxes / 4 * 3], s_mx1[kLeafBoxes / 4 * 3];
+// STAGE: the warp-staged leaf round (coalesced); without it each lane reads
+// its own triangle and writes its own node parts, which has fewer dependent
+// steps and is faster for a one-block image.
+template <int LB, bool STAGE>
+__global__ void __launch_bounds__(kT, LB == 64 ? 4 : 6) k_radv(RadvArgs A) {
+    static_assert(LB == 64 || LB == 256, "a block's subtree is a complete 4-ary tree");
+    constexpr uint32_t kInLevels = LB == 256 ? 4u : 3u;  // log4(LB)
+    // leaf-level boxes (LB) and the first parent level (LB/4) ping-pong
+    __shared__ float s_mn0[LB * 3], s_mx0[LB * 3];
+    __shared__ float s_mn1[LB / 4 * 3], s_mx1[LB / 4 * 3];
+    // per warp: its 32 triangles' vertices as read, and their bounds
+    __shared__ float s_raw[STAGE ? kT / 32 : 1][32 * 9];
+    __shared__ float s_tbox[STAGE ? kT / 32 : 1][32 * 6];
     __shared__ uint32_t s_last;
     float* cmn_src = s_mn0;
     float* cmx_src = s_mx0;
@@ -148,104 +216,183 @@ __global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
     const float qn = __uint_as_float(kQNaN);
 
     // ---- leaf boxes and triangle nodes
-    const uint32_t lb0 = blockIdx.x * kLeafBoxes;
-    const uint32_t nlb = min(uint32_t(kLeafBoxes), leaf_cnt - lb0);
-    // rounds of kT triangles that hold any of this block's (fewer than 16
-    // for a small image; the same for every thread)
+    // A round is kT consecutive triangles, 32 per warp.  Each warp reads its
+    // triangles' 1,152 B with coalesced loads into shared memory, then
+    // writes their 64-B triangle nodes (2 KB) and the 8 leaf box nodes over
+    // them (1 KB) as runs of 16 B per lane, consecutive lanes on consecutive
+    // addresses.
+    const uint32_t w = threadIdx.x >> 5;
+    float* raw = s_raw[STAGE ? w : 0];
+    float* tbox = s_tbox[STAGE ? w : 0];
+    const uint32_t lb0 = blockIdx.x * LB;
+    const uint32_t nlb = min(uint32_t(LB), leaf_cnt - lb0);
+    const uint32_t tend = min(A.n, (lb0 + nlb) * 4u);  // end of this block's triangles
+    // rounds that hold any of this block's triangles (at most 4*LB/kT; the
+    // same for every thread)
     const uint32_t rounds = (nlb * 4u + kT - 1) / kT;
     for (uint32_t r = 0; r < rounds; ++r) {
-        const uint32_t local = r * kT + threadIdx.x;  // triangle within block
-        const uint32_t ti = lb0 * 4u + local;
-        const bool valid = local < nlb * 4u && ti < A.n;
-        float tmn[3] = {qn, qn, qn}, tmx[3] = {qn, qn, qn};
-        if (valid) {
-            const float* v = A.tri9 + 9ull * ti;
-            float f[9];
+        const uint32_t wl = r * kT + w * 32;  // first triangle of this warp, within the block
+        const uint32_t tb = lb0 * 4u + wl;    // the same, in the mesh
+        if (tb >= tend) continue;             // the warp holds no triangle and no leaf box
+        const uint32_t nt = min(32u, tend - tb);
+        if constexpr (!STAGE) {
+            float tmn[3] = {qn, qn, qn}, tmx[3] = {qn, qn, qn};
+            const uint32_t ti = tb + lane;
+            const bool valid = lane < nt;
+            if (valid) {
+                const float* v = A.tri9 + 9ull * ti;
+                float f[9];
 #pragma unroll
-            for (int q = 0; q < 9; ++q) f[q] = __ldg(v + q);
-            float4* o = reinterpret_cast<float4*>(trin + 64ull * ti);
-            o[0] = make_float4(f[0], f[1], f[2], f[3]);
-            o[1] = make_float4(f[4], f[5], f[6], f[7]);
-            o[2] = make_float4(f[8], 0.0f, 0.0f, 0.0f);
-            reinterpret_cast<uint4*>(o)[3] =
-                make_uint4(ti, RQ_RADV_GEOMETRY_OPAQUE, 0u, RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
+                for (int q = 0; q < 9; ++q) f[q] = __ldg(v + q);
+                uint4* o = reinterpret_cast<uint4*>(trin + 64ull * ti);
+                o[0] = make_uint4(__float_as_uint(f[0]), __float_as_uint(f[1]), __float_as_uint(f[2]),
+                                  __float_as_uint(f[3]));
+                o[1] = make_uint4(__float_as_uint(f[4]), __float_as_uint(f[5]), __float_as_uint(f[6]),
+                                  __float_as_uint(f[7]));
+                o[2] = make_uint4(__float_as_uint(f[8]), 0u, 0u, 0u);
+                o[3] = make_uint4(ti, RQ_RADV_GEOMETRY_OPAQUE, 0u, RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                tmn[k] = fminf(f[k], fminf(f[3 + k], f[6 + k]));
-                tmx[k] = fmaxf(f[k], fmaxf(f[3 + k], f[6 + k]));
-            }
-        }
-        // gather the four triangles of this lane's leaf box (lanes 4j..4j+3)
-        const uint32_t g0 = lane & ~3u;
-        uint32_t okm = __ballot_sync(0xffffffffu, valid);
-        float cmn[4][3], cmx[4][3];
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                cmn[c][k] = __shfl_sync(0xffffffffu, tmn[k], g0 + c);
-                cmx[c][k] = __shfl_sync(0xffffffffu, tmx[k], g0 + c);
-            }
-        const uint32_t lbl = local >> 2;  // leaf box within block
-        if ((lane & 3u) == 0u && lbl < nlb) {
-            uint32_t ch[4];
-            float umn[3] = {1e30f, 1e30f, 1e30f}, umx[3] = {-1e30f, -1e30f, -1e30f};
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                if ((okm >> (g0 + c)) & 1u) {
-                    uint32_t tic = (lb0 + lbl) * 4u + c;
-                    ch[c] = ((A.total_boxes * 128u + tic * 64u) >> 3) | RQ_RADV_NODE_TRIANGLE;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        umn[k] = fminf(umn[k], cmn[c][k]);
-                        umx[k] = fmaxf(umx[k], cmx[c][k]);
-                    }
-                } else {
-                    ch[c] = RQ_RADV_INVALID_NODE;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) cmn[c][k] = cmx[c][k] = qn;
+                for (int k = 0; k < 3; ++k) {
+                    tmn[k] = fminf(f[k], fminf(f[3 + k], f[6 + k]));
+                    tmx[k] = fmaxf(f[k], fmaxf(f[3 + k], f[6 + k]));
                 }
             }
-            write_box(boxes, A.offs[leaf_lvl] + lb0 + lbl, ch, cmn, cmx);
+            // this lane's quarter of its leaf box node: child id, child box
+            // and one dword of the zero tail
+            const uint32_t lbl = (wl + lane) >> 2;
+            const uint32_t c = lane & 3u;
+            if (lbl < nlb) {
+                uint8_t* nd = boxes + 128ull * (A.offs[leaf_lvl] + lb0 + lbl);
+                reinterpret_cast<uint32_t*>(nd)[c] =
+                    valid ? ((A.total_boxes * 128u + ti * 64u) >> 3) | RQ_RADV_NODE_TRIANGLE : RQ_RADV_INVALID_NODE;
+                float2* b = reinterpret_cast<float2*>(nd + 16 + 24 * c);
+                b[0] = make_float2(tmn[0], tmn[1]);
+                b[1] = make_float2(tmn[2], tmx[0]);
+                b[2] = make_float2(tmx[1], tmx[2]);
+                reinterpret_cast<uint32_t*>(nd + 112)[c] = 0u;
+            }
+            // the leaf box's bounds, children in order 0..3
+            const uint32_t g0 = lane & ~3u;
+            float umn[3] = {1e30f, 1e30f, 1e30f}, umx[3] = {-1e30f, -1e30f, -1e30f};
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    umn[k] = fminf(umn[k], __shfl_sync(0xffffffffu, tmn[k], g0 + cc));
+                    umx[k] = fmaxf(umx[k], __shfl_sync(0xffffffffu, tmx[k], g0 + cc));
+                }
+            if (c == 0u && lbl < nlb) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    s_mn0[3 * lbl + k] = umn[k];
+                    s_mx0[3 * lbl + k] = umx[k];
+                }
+            }
+            continue;
+        }
+        const float* src = A.tri9 + 9ull * tb;
+#pragma unroll
+        for (uint32_t j = 0; j < 9; ++j) {
+            const uint32_t q = j * 32 + lane;
+            if (q < 9 * nt) raw[q] = __ldg(src + q);
+        }
+        __syncwarp();
+        // this lane's triangle bounds (qNaN for a slot past the mesh's end)
+        float tmn[3] = {qn, qn, qn}, tmx[3] = {qn, qn, qn};
+        if (lane < nt) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float a = raw[9 * lane + k], b = raw[9 * lane + 3 + k], c = raw[9 * lane + 6 + k];
+                tmn[k] = fminf(a, fminf(b, c));
+                tmx[k] = fmaxf(a, fmaxf(b, c));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            tbox[6 * lane + k] = tmn[k];
+            tbox[6 * lane + 3 + k] = tmx[k];
+        }
+        __syncwarp();
+        // triangle nodes: 16-B part p of triangle t, four triangles per 4 lanes
+        {
+            const uint32_t p = lane & 3u;
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) {
+                const uint32_t t = 8 * q + (lane >> 2);
+                if (t < nt) {
+                    const float* f = raw + 9 * t;
+                    uint4 v;
+                    if (p == 0u)
+                        v = make_uint4(__float_as_uint(f[0]), __float_as_uint(f[1]), __float_as_uint(f[2]),
+                                       __float_as_uint(f[3]));
+                    else if (p == 1u)
+                        v = make_uint4(__float_as_uint(f[4]), __float_as_uint(f[5]), __float_as_uint(f[6]),
+                                       __float_as_uint(f[7]));
+                    else if (p == 2u)
+                        v = make_uint4(__float_as_uint(f[8]), 0u, 0u, 0u);
+                    else
+                        v = make_uint4(tb + t, RQ_RADV_GEOMETRY_OPAQUE, 0u, RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
+                    reinterpret_cast<uint4*>(trin + 64ull * (tb + t))[p] = v;
+                }
+            }
+        }
+        // leaf box nodes: 16-B part F of node d (ids, six runs of the four
+        // child boxes, zero tail), eight lanes per node
+        {
+            const uint32_t F = lane & 7u;
+#pragma unroll
+            for (uint32_t q = 0; q < 2; ++q) {
+                const uint32_t d = 4 * q + (lane >> 3);
+                const uint32_t lbl = wl / 4 + d;  // leaf box within block
+                if (lbl < nlb) {
+                    uint4 v;
+                    if (F == 0u) {
+                        uint32_t id[4];
+#pragma unroll
+                        for (uint32_t c = 0; c < 4; ++c) {
+                            const uint32_t t = 4 * d + c;
+                            id[c] = t < nt ? ((A.total_boxes * 128u + (tb + t) * 64u) >> 3) | RQ_RADV_NODE_TRIANGLE
+                                           : RQ_RADV_INVALID_NODE;
+                        }
+                        v = make_uint4(id[0], id[1], id[2], id[3]);
+                    } else if (F == 7u) {
+                        v = make_uint4(0u, 0u, 0u, 0u);
+                    } else {
+                        const float* b = tbox + 24 * d + 4 * (F - 1);
+                        v = make_uint4(__float_as_uint(b[0]), __float_as_uint(b[1]), __float_as_uint(b[2]),
+                                       __float_as_uint(b[3]));
+                    }
+                    reinterpret_cast<uint4*>(boxes + 128ull * (A.offs[leaf_lvl] + lb0 + lbl))[F] = v;
+                }
+            }
+        }
+        // leaf box bounds for the parent levels: children in order 0..3 (a
+        // missing child's qNaN is skipped by fminf/fmaxf)
+        if (lane < 8u && wl / 4 + lane < nlb) {
+            float umn[3] = {1e30f, 1e30f, 1e30f}, umx[3] = {-1e30f, -1e30f, -1e30f};
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    umn[k] = fminf(umn[k], tbox[24 * lane + 6 * c + k]);
+                    umx[k] = fmaxf(umx[k], tbox[24 * lane + 6 * c + 3 + k]);
+                }
+            const uint32_t lbl = wl / 4 + lane;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 s_mn0[3 * lbl + k] = umn[k];
                 s_mx0[3 * lbl + k] = umx[k];
             }
         }
+        __syncwarp();  // the next round rewrites raw and tbox
     }
     __syncthreads();
 
-    // ---- in-block levels (up to five)
-    uint32_t nchild = nlb;                // children at the current level in this block
-    uint32_t child_base = lb0;            // first child index within its level
-    uint32_t lvl = leaf_lvl;              // level of the children
-    for (uint32_t j = 1; j <= 5 && lvl > 0; ++j) {
-        const uint32_t plvl = lvl - 1;
-        const uint32_t np = (nchild + 3) / 4;
-        const uint32_t pbase = child_base >> 2;
-        for (uint32_t t = threadIdx.x; t < np; t += kT) {
-            uint32_t nv = min(4u, nchild - 4 * t);
-            float umn[3], umx[3];
-            make_parent(boxes, A.offs[plvl] + pbase + t, A.offs[lvl] + child_base + 4 * t, nv, cmn_src + 12 * t,
-                        cmx_src + 12 * t, umn, umx);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                cmn_dst[3 * t + k] = umn[k];
-                cmx_dst[3 * t + k] = umx[k];
-            }
-        }
-        __syncthreads();
-        float* tn = cmn_src;
-        cmn_src = cmn_dst;
-        cmn_dst = tn;
-        float* tx = cmx_src;
-        cmx_src = cmx_dst;
-        cmx_dst = tx;
-        nchild = np;
-        child_base = pbase;
-        lvl = plvl;
-    }
+    // ---- in-block levels (log4(LB))
+    uint32_t nchild = nlb;      // children at the current level in this block
+    uint32_t child_base = lb0;  // first child index within its level
+    uint32_t lvl = leaf_lvl;    // level of the children
+    smem_levels(A, boxes, cmn_src, cmx_src, cmn_dst, cmx_dst, nchild, child_base, lvl, kInLevels);
 
     if (lvl == 0) {
         // this block built the root (single-block image)
@@ -266,44 +413,64 @@ __global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
     }
     __syncthreads();
     if (!s_last) return;
+    // every other block has taken its ticket: ready it for the next launch
+    if (threadIdx.x == 0) *A.ticket = 0u;
     __threadfence();
-    // level `lvl` holds gridDim.x nodes whose boxes are in A.top[2b], A.top[2b+1]
+    // level `lvl` holds gridDim.x nodes whose boxes are in A.top[2b], A.top[2b+1];
+    // parents through global memory while there are more than LB of them,
+    // then the rest of the way in shared memory
     float4* src = A.top;
     float4* dst = A.top + 2 * gridDim.x;
-    uint32_t ncnt = A.counts[lvl];
-    while (lvl > 0) {
+    nchild = A.counts[lvl];
+    while (nchild > uint32_t(LB)) {
         const uint32_t plvl = lvl - 1;
         const uint32_t np = A.counts[plvl];
         for (uint32_t t = threadIdx.x; t < np; t += kT) {
-            uint32_t nv = min(4u, ncnt - 4 * t);
-            float cmn[12], cmx[12];
-            for (uint32_t c = 0; c < nv; ++c) {
-                float4 a = __ldcg(src + 2 * (4 * t + c)), b = __ldcg(src + 2 * (4 * t + c) + 1);
-                cmn[3 * c] = a.x;
-                cmn[3 * c + 1] = a.y;
-                cmn[3 * c + 2] = a.z;
-                cmx[3 * c] = b.x;
-                cmx[3 * c + 1] = b.y;
-                cmx[3 * c + 2] = b.z;
-            }
             float umn[3], umx[3];
-            make_parent(boxes, A.offs[plvl] + t, A.offs[lvl] + 4 * t, nv, cmn, cmx, umn, umx);
+            make_parent(boxes, A.offs[plvl] + t, A.offs[lvl] + 4 * t, min(4u, nchild - 4 * t),
+                        GlobalChildren{src + 8 * t}, umn, umx);
             __stcg(dst + 2 * t, make_float4(umn[0], umn[1], umn[2], 0.0f));
             __stcg(dst + 2 * t + 1, make_float4(umx[0], umx[1], umx[2], 0.0f));
         }
-        __threadfence();
-        __syncthreads();
+        __syncthreads();  // the block's own global writes are visible to it after the barrier
         float4* tmp = src;
         src = dst;
         dst = tmp;
-        ncnt = np;
+        nchild = np;
         lvl = plvl;
     }
+    for (uint32_t t = threadIdx.x; t < nchild; t += kT) {
+        const float4 a = __ldcg(src + 2 * t), b = __ldcg(src + 2 * t + 1);
+        s_mn0[3 * t] = a.x;
+        s_mn0[3 * t + 1] = a.y;
+        s_mn0[3 * t + 2] = a.z;
+        s_mx0[3 * t] = b.x;
+        s_mx0[3 * t + 1] = b.y;
+        s_mx0[3 * t + 2] = b.z;
+    }
+    __syncthreads();
+    cmn_src = s_mn0;
+    cmx_src = s_mx0;
+    cmn_dst = s_mn1;
+    cmx_dst = s_mx1;
+    child_base = 0;
+    smem_levels(A, boxes, cmn_src, cmx_src, cmn_dst, cmx_dst, nchild, child_base, lvl, 32u);
     if (threadIdx.x == 0) {
-        float4 a = __ldcg(src), b = __ldcg(src + 1);
-        float mn[3] = {a.x, a.y, a.z}, mx[3] = {b.x, b.y, b.z};
+        float mn[3] = {cmn_src[0], cmn_src[1], cmn_src[2]};
+        float mx[3] = {cmx_src[0], cmx_src[1], cmx_src[2]};
         write_header(A, mn, mx);
     }
+}
+
+void launch_radv(const RadvArgs& a, uint32_t leaf_cnt, cudaStream_t st) {
+    const uint32_t lb = radv_leaf_boxes(leaf_cnt);
+    const uint32_t blocks = radv_blocks(leaf_cnt, lb);
+    if (lb == 256u)
+        k_radv<256, true><<<blocks, kT, 0, st>>>(a);
+    else if (blocks > 1)
+        k_radv<64, true><<<blocks, kT, 0, st>>>(a);
+    else
+        k_radv<64, false><<<1, kT, 0, st>>>(a);
 }
 
 }  // namespace
@@ -314,12 +481,17 @@ __global__ void __launch_bounds__(kT) k_radv(RadvArgs A) {
 // and cannot let a library call cudaMalloc / cudaFree, which synchronise the
 // whole device and can fail mid-frame.  This variant takes only the vertex
 // buffer and the image buffer from the caller; its scratch (the finishing
-// ticket and two boxes per block for the top levels) lives in the static
+// ticket and two boxes per block, twice, for the top levels) lives in the static
 // device array below, sized for at most RQ_RADV_NOALLOC_MAX_TRIANGLES
-// triangles.  Every GPU that loads librq.so holds the array until the
-// process exits.
-static __device__ __align__(256) unsigned char rq_radv_noalloc_scratch
-    [256 + 4 * sizeof(float4) * ((RQ_RADV_NOALLOC_MAX_TRIANGLES / 4 + kLeafBoxes - 1) / kLeafBoxes)];
+// triangles (1 MiB).  Every GPU that loads librq.so holds the array until
+// the process exits.  The array starts at zero and every build leaves the
+// ticket at zero.
+// The most blocks a build of at most RQ_RADV_NOALLOC_MAX_TRIANGLES takes:
+// 256-leaf-box subtrees at the largest size, or at most kSmallBlocksMax
+// blocks of 64-leaf-box ones.
+constexpr uint32_t kNoallocBlocks =
+    std::max<uint32_t>((RQ_RADV_NOALLOC_MAX_TRIANGLES / 4 + 255u) / 256u, kSmallBlocksMax);
+static __device__ __align__(256) unsigned char rq_radv_noalloc_scratch[256 + 4 * sizeof(float4) * kNoallocBlocks];
 
 namespace {
 std::mutex g_noalloc_mu;
@@ -365,13 +537,8 @@ extern "C" int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, 
     a.ticket = static_cast<uint32_t*>(base);
     a.top = reinterpret_cast<float4*>(static_cast<char*>(base) + 256);
     a.size = L.total_as_size;
-    // the array keeps the previous call's contents: the ticket must start at 0
-    if (cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st) != cudaSuccess) {
-        cudaGetLastError();
-        return RQ_ERR_CUDA;
-    }
     const uint32_t leaf_cnt = L.level_counts[L.num_levels - 1];
-    k_radv<<<(leaf_cnt + kLeafBoxes - 1) / kLeafBoxes, kT, 0, st>>>(a);
+    launch_radv(a, leaf_cnt, st);
     if (cudaGetLastError() != cudaSuccess) return RQ_ERR_CUDA;
     return RQ_OK;
 }
@@ -379,7 +546,7 @@ extern "C" int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, 
 int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st,
                    bool refit) {
     const uint32_t leaf_cnt = L.level_counts[L.num_levels - 1];
-    const uint32_t blocks = (leaf_cnt + kLeafBoxes - 1) / kLeafBoxes;
+    const uint32_t blocks = radv_blocks(leaf_cnt, radv_leaf_boxes(leaf_cnt));
     size_t need = sizeof(float4) * 4ull * blocks + 256;
     int rc = rq_ensure_scratch(ctx, need, st);
     if (rc) return rc;
@@ -393,13 +560,12 @@ int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const 
         a.counts[i] = L.level_counts[i];
         a.offs[i] = L.level_offsets[i];
     }
-    a.ticket = static_cast<uint32_t*>(ctx->scratch);
+    a.ticket = ctx->d_err + RQ_CTX_RADV_TICKET;
     a.top = reinterpret_cast<float4*>(static_cast<char*>(ctx->scratch) + 256);
     a.size = L.total_as_size;
     a.check_header = refit ? 1u : 0u;
     a.err = ctx->d_err;
-    if (blocks > 1) cudaMemsetAsync(a.ticket, 0, sizeof(uint32_t), st);  // one block never takes a ticket
-    k_radv<<<blocks, kT, 0, st>>>(a);
+    launch_radv(a, leaf_cnt, st);
     return rq_cuda_status(ctx, cudaGetLastError(), "radv build launch");
 }
 

@@ -20,6 +20,10 @@
 #define RQ_DERR_WAIT_CHECK 64u
 #define RQ_DERR_RADV_IMAGE 128u  // rq_refit_radv: the image's header is not for this triangle count
 
+// Word of rq_ctx::d_err that holds the RADV build's finishing ticket: 0
+// between launches, since the build's last block resets it.
+#define RQ_CTX_RADV_TICKET 32
+
 // Largest triangle count a leaf stack entry can address (27-bit first prim).
 #define RQ_MAX_TRIANGLES (1u << 27)
 
@@ -28,7 +32,7 @@ struct rq_ctx {
     int num_sms = 0;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
-    uint32_t* d_err = nullptr;      // device error word
+    uint32_t* d_err = nullptr;      // device error word ([0]); 256 B, zeroed at creation
     uint32_t* h_err = nullptr;      // pinned mirror
     uint32_t* d_ctr = nullptr;      // work counters of persistent launches (zeroed per launch)
     std::string last_error;

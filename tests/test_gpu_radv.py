@@ -25,8 +25,11 @@ def radv_gpu(ctx, tri9):
     return img
 
 
+# 302,080 / 302,081 and 1,208,320 / 1,208,321 triangles sit on either side of
+# the sizes where a block's subtree grows from 64 to 256 and from 256 to 1,024
+# leaf boxes (fewer than 296 blocks of the larger subtree)
 @pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 63, 64, 65, 256, 1023, 1024, 1025, 4096, 4097, 4100, 16385,
-                               100000, 1 << 20])
+                               100000, 1 << 20, 302080, 302081, 1208320, 1208321])
 def test_radv_bytes_match_oracle(ctx, n):
     tri9 = soup(n, 40 + n).reshape(-1)
     img = radv_gpu(ctx, tri9).cpu().numpy()
@@ -147,7 +150,7 @@ def test_validate_reports_damage(ctx):
     assert r["header_ok"] == 0
 
 
-@pytest.mark.parametrize("n", [5, 4097, 100000])
+@pytest.mark.parametrize("n", [5, 4097, 100000, 400000, 1300000])
 def test_radv_refit_equals_rebuild(ctx, n):
     # rq_refit_radv after the vertices move: the bytes of a fresh build on the
     # new vertices (and of the oracle's image of them)
@@ -170,3 +173,28 @@ def test_radv_refit_of_another_count_is_reported(ctx):
     assert ei.value.status == rq.RQ_ERR_STATE
     out = radv_gpu(ctx, soup(64, 6).reshape(-1))  # later calls work
     assert np.array_equal(out.cpu().numpy(), O.radv_build(soup(64, 6).reshape(-1)))
+
+
+@pytest.mark.parametrize("n", [1000, 20000, 600000])
+def test_radv_builds_replayed_from_a_graph(ctx, n):
+    # multi-block builds leave their finishing ticket ready for the next
+    # launch: builds replayed back to back from a CUDA graph all finish
+    tri9 = soup(n, 500 + n).reshape(-1)
+    t = torch.from_numpy(np.ascontiguousarray(tri9)).cuda()
+    img = torch.empty(rq.radv_size(n), dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        rq.build_radv(ctx, t, img)  # scratch allocated before the capture
+        side.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            for _ in range(3):
+                rq.build_radv(ctx, t, img)
+    ref = O.radv_build(tri9)
+    for _ in range(2):
+        img.fill_(0xAB)
+        g.replay()
+        torch.cuda.synchronize()
+        ctx.sync_check()
+        assert np.array_equal(img.cpu().numpy(), ref)
+    del g
