@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=6000, help="pixels in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the visibility / batched / serving workloads")
-    ap.add_argument("--extra", choices=["visibility", "batched", "serving"],
+    ap.add_argument("--extra", choices=["visibility", "batched", "serving", "radv"],
                     help="run only this workload (--steps frames / steps / x50 ms of arrivals) and print its JSON")
     return ap.parse_args()
 
@@ -481,16 +481,14 @@ def run_ours(args, world, rank, local, pg):
     bvh.destroy()
     del p_d, i_d, gbuf, mask, ao, depth, tmp, blurred
     refbench = run_reference_benchmarks(ctx, dev) if not args.no_extra else None
+    radv_build = run_radv_build(ctx, dev, load_peaks()) if not args.no_extra else None
     vis = run_visibility(ctx, dev, stream) if not args.no_extra else None
     batched = run_batched(ctx, dev) if not args.no_extra else None
     serving = run_serving(dev) if not args.no_extra else None
 
     if rank != 0:
         return
-    peaks = {}
-    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(pk):
-        peaks = json.load(open(pk))
+    peaks = load_peaks()
     hbm = peaks.get("hbm_gbs", 6650.0)
     shade_med = statistics.median(shade_ms)
     # algorithmic bytes of the shadow/AO launch: G-buffer read (32 B/pixel),
@@ -562,12 +560,19 @@ def run_ours(args, world, rank, local, pg):
         "ao_blur": blur,
         "median_build": median_build,
         "reference_benchmarks": refbench,
+        "radv_build": radv_build,
         "visibility": vis,
         "batched": batched,
         "serving": serving,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def load_peaks():
+    """The measured HBM copy bandwidth and GEMM peaks of this GPU model, if present."""
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    return json.load(open(pk)) if os.path.exists(pk) else {}
 
 
 def percentile(xs, q):
@@ -879,6 +884,45 @@ def run_reference_benchmarks(ctx, dev):
                      "Moller-Trumbore); engine = rq_trace closest hit with the same triangle test")}
 
 
+def run_radv_build(ctx, dev, peaks, reps=50, meshes=None):
+    """The fast builder (fast_bvh_builder.comp, rq_build_radv) at the frame's and the visibility
+    workload's triangle counts: the meshes' triangles as a vertex soup (9 floats each), one image
+    rebuilt per launch.  Algorithmic bytes per launch = 36 B per triangle read + the whole image
+    written (64 B triangle nodes, 128 B box nodes, 192 B header); both exceed L2 (126 MB).
+    CUDA-event median over `reps` back-to-back builds."""
+    import numpy as np
+    import torch
+    import rq
+    from rq import workloads as W
+
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    out = {}
+    for name, mesh in (meshes or (("frame_2.5M", W.shadow_mesh), ("visibility_8.3M", W.visibility_mesh))):
+        pos, idx = mesh()
+        n = len(idx)
+        tri9 = torch.from_numpy(pos).to(dev)[torch.from_numpy(idx.astype(np.int64)).to(dev)].reshape(-1)
+        tri9 = tri9.contiguous()
+        img = torch.empty(rq.radv_size(n), dtype=torch.uint8, device=dev)
+        for _ in range(3):
+            rq.build_radv(ctx, tri9, img)
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            rq.build_radv(ctx, tri9, img)
+            b.record()
+            ms.append((a, b))
+        torch.cuda.synchronize(dev)
+        ctx.sync_check()
+        med = statistics.median(a.elapsed_time(b) for a, b in ms)
+        alg = 36 * n + rq.radv_size(n)
+        gbs = alg / med / 1e6
+        out[name] = {"triangles": n, "us": round(1e3 * med, 2), "mtris_per_s": round(n / med / 1e3, 1),
+                     "algorithmic_bytes": alg, "achieved_gbs": round(gbs, 1), "frac_of_hbm": round(gbs / hbm, 4)}
+        del tri9, img
+    return out
+
+
 def run_visibility(ctx, dev, stream, frames=200):
     """Subpixel visibility: 8,323,200 triangles (2040x2040 quads, seed 3) deforming
     every frame (z = z0 + 0.05 sin(0.1 f + x)); 1920x1080 jittered primary rays
@@ -943,6 +987,10 @@ def run_extra(args):
         out = run_visibility(ctx, dev, torch.cuda.current_stream(dev), frames=max(1, args.steps))
     elif args.extra == "batched":
         out = run_batched(ctx, dev, steps=max(1, args.steps), plain_steps=1)
+    elif args.extra == "radv":
+        from rq import workloads as W
+        out = run_radv_build(ctx, dev, load_peaks(), reps=max(1, args.steps),
+                             meshes=(("frame_2.5M", W.shadow_mesh),))
     else:
         out = run_serving(dev, duration_s=max(0.05, args.steps * 0.05))
     print(json.dumps({"extra": args.extra, **out}))

@@ -8,7 +8,7 @@
 // and the pre-root dwords at bytes 180 (= 5) and 188 (= 0xFFFFFFFF).  Bytes
 // the shader never writes (136..191 apart from those two dwords) are zeroed.
 //
-// Block b owns leaf boxes [LB*b, LB*b+LB) (LB = 64 or 256, a power of four):
+// Block b owns leaf boxes [LB*b, LB*b+LB) (LB = 64, 256 or 1024, a power of four):
 // 4*LB triangles in rounds of one per thread.  In a multi-block image each
 // warp stages its 32 triangles in shared memory so that the triangle and
 // leaf box nodes go out as coalesced 16-B stores; a one-block image (up to
@@ -18,7 +18,7 @@
 // and the header from the per-block subtree boxes, then puts the ticket back
 // to 0 for the next launch on the stream.  Up to 131,072 triangles the
 // subtrees are 64 leaf boxes (a 4,096-triangle image is 16 blocks of one
-// round), above that 256.
+// round), from 4,194,304 on 1024, 256 between.
 #include <algorithm>
 #include <mutex>
 
@@ -30,10 +30,16 @@ namespace {
 constexpr int kT = 256;
 // 64-leaf-box subtrees up to this many blocks, 256-leaf-box ones above
 constexpr uint32_t kSmallBlocksMax = 512;
+// 1024-leaf-box subtrees (16 rounds, so the read-ahead of the next round
+// covers more of the block's life) from this many blocks on
+constexpr uint32_t kLargeBlocksMin = 1024;
 
-// leaf boxes per block: 64 while that gives at most kSmallBlocksMax blocks,
-// then 256 (measured on B200)
-uint32_t radv_leaf_boxes(uint32_t leaf_cnt) { return leaf_cnt <= 64u * kSmallBlocksMax ? 64u : 256u; }
+// leaf boxes per block (measured on B200): 64 while that gives at most
+// kSmallBlocksMax blocks, 1024 from kLargeBlocksMin blocks, 256 between
+uint32_t radv_leaf_boxes(uint32_t leaf_cnt) {
+    if (leaf_cnt <= 64u * kSmallBlocksMax) return 64u;
+    return leaf_cnt >= 1024u * kLargeBlocksMin ? 1024u : 256u;
+}
 // blocks for a given subtree size
 uint32_t radv_blocks(uint32_t leaf_cnt, uint32_t lb) { return (leaf_cnt + lb - 1) / lb; }
 constexpr uint32_t kQNaN = 0x7fc00000u;
@@ -184,9 +190,9 @@ __device__ void write_header(const RadvArgs& A, const float mn[3], const float m
 // its own triangle and writes its own node parts, which has fewer dependent
 // steps and is faster for a one-block image.
 template <int LB, bool STAGE>
-__global__ void __launch_bounds__(kT, LB == 64 ? 4 : 6) k_radv(RadvArgs A) {
-    static_assert(LB == 64 || LB == 256, "a block's subtree is a complete 4-ary tree");
-    constexpr uint32_t kInLevels = LB == 256 ? 4u : 3u;  // log4(LB)
+__global__ void __launch_bounds__(kT, LB == 256 ? 6 : 4) k_radv(RadvArgs A) {
+    static_assert(LB == 64 || LB == 256 || LB == 1024, "a block's subtree is a complete 4-ary tree");
+    constexpr uint32_t kInLevels = LB == 1024 ? 5u : LB == 256 ? 4u : 3u;  // log4(LB)
     // leaf-level boxes (LB) and the first parent level (LB/4) ping-pong
     __shared__ float s_mn0[LB * 3], s_mx0[LB * 3];
     __shared__ float s_mn1[LB / 4 * 3], s_mx1[LB / 4 * 3];
@@ -230,6 +236,21 @@ __global__ void __launch_bounds__(kT, LB == 64 ? 4 : 6) k_radv(RadvArgs A) {
     // rounds that hold any of this block's triangles (at most 4*LB/kT; the
     // same for every thread)
     const uint32_t rounds = (nlb * 4u + kT - 1) / kT;
+    // staged rounds read the next round's triangles into registers while the
+    // current round is written out
+    float pf[9];
+    if constexpr (STAGE) {
+        const uint32_t tb0 = lb0 * 4u + w * 32;
+        if (tb0 < tend) {
+            const uint32_t nt0 = min(32u, tend - tb0);
+            const float* src = A.tri9 + 9ull * tb0;
+#pragma unroll
+            for (uint32_t j = 0; j < 9; ++j) {
+                const uint32_t q = j * 32 + lane;
+                pf[j] = q < 9 * nt0 ? __ldg(src + q) : 0.0f;
+            }
+        }
+    }
     for (uint32_t r = 0; r < rounds; ++r) {
         const uint32_t wl = r * kT + w * 32;  // first triangle of this warp, within the block
         const uint32_t tb = lb0 * 4u + wl;    // the same, in the mesh
@@ -288,103 +309,111 @@ __global__ void __launch_bounds__(kT, LB == 64 ? 4 : 6) k_radv(RadvArgs A) {
                     s_mx0[3 * lbl + k] = umx[k];
                 }
             }
-            continue;
-        }
-        const float* src = A.tri9 + 9ull * tb;
+        } else {
 #pragma unroll
-        for (uint32_t j = 0; j < 9; ++j) {
-            const uint32_t q = j * 32 + lane;
-            if (q < 9 * nt) raw[q] = __ldg(src + q);
-        }
-        __syncwarp();
-        // this lane's triangle bounds (qNaN for a slot past the mesh's end)
-        float tmn[3] = {qn, qn, qn}, tmx[3] = {qn, qn, qn};
-        if (lane < nt) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float a = raw[9 * lane + k], b = raw[9 * lane + 3 + k], c = raw[9 * lane + 6 + k];
-                tmn[k] = fminf(a, fminf(b, c));
-                tmx[k] = fmaxf(a, fmaxf(b, c));
+            for (uint32_t j = 0; j < 9; ++j) {
+                const uint32_t q = j * 32 + lane;
+                if (q < 9 * nt) raw[q] = pf[j];
             }
-        }
+            __syncwarp();
+            if (r + 1 < rounds && tb + kT < tend) {
+                const uint32_t ntn = min(32u, tend - (tb + kT));
+                const float* src = A.tri9 + 9ull * (tb + kT);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            tbox[6 * lane + k] = tmn[k];
-            tbox[6 * lane + 3 + k] = tmx[k];
-        }
-        __syncwarp();
-        // triangle nodes: 16-B part p of triangle t, four triangles per 4 lanes
-        {
-            const uint32_t p = lane & 3u;
-#pragma unroll
-            for (uint32_t q = 0; q < 4; ++q) {
-                const uint32_t t = 8 * q + (lane >> 2);
-                if (t < nt) {
-                    const float* f = raw + 9 * t;
-                    uint4 v;
-                    if (p == 0u)
-                        v = make_uint4(__float_as_uint(f[0]), __float_as_uint(f[1]), __float_as_uint(f[2]),
-                                       __float_as_uint(f[3]));
-                    else if (p == 1u)
-                        v = make_uint4(__float_as_uint(f[4]), __float_as_uint(f[5]), __float_as_uint(f[6]),
-                                       __float_as_uint(f[7]));
-                    else if (p == 2u)
-                        v = make_uint4(__float_as_uint(f[8]), 0u, 0u, 0u);
-                    else
-                        v = make_uint4(tb + t, RQ_RADV_GEOMETRY_OPAQUE, 0u, RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
-                    reinterpret_cast<uint4*>(trin + 64ull * (tb + t))[p] = v;
+                for (uint32_t j = 0; j < 9; ++j) {
+                    const uint32_t q = j * 32 + lane;
+                    pf[j] = q < 9 * ntn ? __ldg(src + q) : 0.0f;
                 }
             }
-        }
-        // leaf box nodes: 16-B part F of node d (ids, six runs of the four
-        // child boxes, zero tail), eight lanes per node
-        {
-            const uint32_t F = lane & 7u;
-#pragma unroll
-            for (uint32_t q = 0; q < 2; ++q) {
-                const uint32_t d = 4 * q + (lane >> 3);
-                const uint32_t lbl = wl / 4 + d;  // leaf box within block
-                if (lbl < nlb) {
-                    uint4 v;
-                    if (F == 0u) {
-                        uint32_t id[4];
-#pragma unroll
-                        for (uint32_t c = 0; c < 4; ++c) {
-                            const uint32_t t = 4 * d + c;
-                            id[c] = t < nt ? ((A.total_boxes * 128u + (tb + t) * 64u) >> 3) | RQ_RADV_NODE_TRIANGLE
-                                           : RQ_RADV_INVALID_NODE;
-                        }
-                        v = make_uint4(id[0], id[1], id[2], id[3]);
-                    } else if (F == 7u) {
-                        v = make_uint4(0u, 0u, 0u, 0u);
-                    } else {
-                        const float* b = tbox + 24 * d + 4 * (F - 1);
-                        v = make_uint4(__float_as_uint(b[0]), __float_as_uint(b[1]), __float_as_uint(b[2]),
-                                       __float_as_uint(b[3]));
-                    }
-                    reinterpret_cast<uint4*>(boxes + 128ull * (A.offs[leaf_lvl] + lb0 + lbl))[F] = v;
-                }
-            }
-        }
-        // leaf box bounds for the parent levels: children in order 0..3 (a
-        // missing child's qNaN is skipped by fminf/fmaxf)
-        if (lane < 8u && wl / 4 + lane < nlb) {
-            float umn[3] = {1e30f, 1e30f, 1e30f}, umx[3] = {-1e30f, -1e30f, -1e30f};
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
+            // this lane's triangle bounds (qNaN for a slot past the mesh's end)
+            float tmn[3] = {qn, qn, qn}, tmx[3] = {qn, qn, qn};
+            if (lane < nt) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    umn[k] = fminf(umn[k], tbox[24 * lane + 6 * c + k]);
-                    umx[k] = fmaxf(umx[k], tbox[24 * lane + 6 * c + 3 + k]);
+                    const float a = raw[9 * lane + k], b = raw[9 * lane + 3 + k], c = raw[9 * lane + 6 + k];
+                    tmn[k] = fminf(a, fminf(b, c));
+                    tmx[k] = fmaxf(a, fmaxf(b, c));
                 }
-            const uint32_t lbl = wl / 4 + lane;
+            }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                s_mn0[3 * lbl + k] = umn[k];
-                s_mx0[3 * lbl + k] = umx[k];
+                tbox[6 * lane + k] = tmn[k];
+                tbox[6 * lane + 3 + k] = tmx[k];
             }
+            __syncwarp();
+            // triangle nodes: 16-B part p of triangle t, four triangles per 4 lanes
+            {
+                const uint32_t p = lane & 3u;
+#pragma unroll
+                for (uint32_t q = 0; q < 4; ++q) {
+                    const uint32_t t = 8 * q + (lane >> 2);
+                    if (t < nt) {
+                        const float* f = raw + 9 * t;
+                        uint4 v;
+                        if (p == 0u)
+                            v = make_uint4(__float_as_uint(f[0]), __float_as_uint(f[1]), __float_as_uint(f[2]),
+                                           __float_as_uint(f[3]));
+                        else if (p == 1u)
+                            v = make_uint4(__float_as_uint(f[4]), __float_as_uint(f[5]), __float_as_uint(f[6]),
+                                           __float_as_uint(f[7]));
+                        else if (p == 2u)
+                            v = make_uint4(__float_as_uint(f[8]), 0u, 0u, 0u);
+                        else
+                            v = make_uint4(tb + t, RQ_RADV_GEOMETRY_OPAQUE, 0u, RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
+                        reinterpret_cast<uint4*>(trin + 64ull * (tb + t))[p] = v;
+                    }
+                }
+            }
+            // leaf box nodes: 16-B part F of node d (ids, six runs of the four
+            // child boxes, zero tail), eight lanes per node
+            {
+                const uint32_t F = lane & 7u;
+#pragma unroll
+                for (uint32_t q = 0; q < 2; ++q) {
+                    const uint32_t d = 4 * q + (lane >> 3);
+                    const uint32_t lbl = wl / 4 + d;  // leaf box within block
+                    if (lbl < nlb) {
+                        uint4 v;
+                        if (F == 0u) {
+                            uint32_t id[4];
+#pragma unroll
+                            for (uint32_t c = 0; c < 4; ++c) {
+                                const uint32_t t = 4 * d + c;
+                                id[c] = t < nt ? ((A.total_boxes * 128u + (tb + t) * 64u) >> 3) | RQ_RADV_NODE_TRIANGLE
+                                               : RQ_RADV_INVALID_NODE;
+                            }
+                            v = make_uint4(id[0], id[1], id[2], id[3]);
+                        } else if (F == 7u) {
+                            v = make_uint4(0u, 0u, 0u, 0u);
+                        } else {
+                            const float* b = tbox + 24 * d + 4 * (F - 1);
+                            v = make_uint4(__float_as_uint(b[0]), __float_as_uint(b[1]), __float_as_uint(b[2]),
+                                           __float_as_uint(b[3]));
+                        }
+                        reinterpret_cast<uint4*>(boxes + 128ull * (A.offs[leaf_lvl] + lb0 + lbl))[F] = v;
+                    }
+                }
+            }
+            // leaf box bounds for the parent levels: children in order 0..3 (a
+            // missing child's qNaN is skipped by fminf/fmaxf)
+            if (lane < 8u && wl / 4 + lane < nlb) {
+                float umn[3] = {1e30f, 1e30f, 1e30f}, umx[3] = {-1e30f, -1e30f, -1e30f};
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        umn[k] = fminf(umn[k], tbox[24 * lane + 6 * c + k]);
+                        umx[k] = fmaxf(umx[k], tbox[24 * lane + 6 * c + 3 + k]);
+                    }
+                const uint32_t lbl = wl / 4 + lane;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    s_mn0[3 * lbl + k] = umn[k];
+                    s_mx0[3 * lbl + k] = umx[k];
+                }
+            }
+            __syncwarp();  // the next round rewrites raw and tbox
         }
-        __syncwarp();  // the next round rewrites raw and tbox
     }
     __syncthreads();
 
@@ -465,7 +494,9 @@ __global__ void __launch_bounds__(kT, LB == 64 ? 4 : 6) k_radv(RadvArgs A) {
 void launch_radv(const RadvArgs& a, uint32_t leaf_cnt, cudaStream_t st) {
     const uint32_t lb = radv_leaf_boxes(leaf_cnt);
     const uint32_t blocks = radv_blocks(leaf_cnt, lb);
-    if (lb == 256u)
+    if (lb == 1024u)
+        k_radv<1024, true><<<blocks, kT, 0, st>>>(a);
+    else if (lb == 256u)
         k_radv<256, true><<<blocks, kT, 0, st>>>(a);
     else if (blocks > 1)
         k_radv<64, true><<<blocks, kT, 0, st>>>(a);
@@ -483,14 +514,14 @@ void launch_radv(const RadvArgs& a, uint32_t leaf_cnt, cudaStream_t st) {
 // buffer and the image buffer from the caller; its scratch (the finishing
 // ticket and two boxes per block, twice, for the top levels) lives in the static
 // device array below, sized for at most RQ_RADV_NOALLOC_MAX_TRIANGLES
-// triangles (1 MiB).  Every GPU that loads librq.so holds the array until
+// triangles (256 KiB).  Every GPU that loads librq.so holds the array until
 // the process exits.  The array starts at zero and every build leaves the
 // ticket at zero.
 // The most blocks a build of at most RQ_RADV_NOALLOC_MAX_TRIANGLES takes:
-// 256-leaf-box subtrees at the largest size, or at most kSmallBlocksMax
-// blocks of 64-leaf-box ones.
-constexpr uint32_t kNoallocBlocks =
-    std::max<uint32_t>((RQ_RADV_NOALLOC_MAX_TRIANGLES / 4 + 255u) / 256u, kSmallBlocksMax);
+// 1024-leaf-box subtrees at the largest size, fewer than 4 * kLargeBlocksMin
+// of 256 leaf boxes, or at most kSmallBlocksMax of 64.
+constexpr uint32_t kNoallocBlocks = std::max<uint32_t>(
+    {(RQ_RADV_NOALLOC_MAX_TRIANGLES / 4 + 1023u) / 1024u, 4 * kLargeBlocksMin, kSmallBlocksMax});
 static __device__ __align__(256) unsigned char rq_radv_noalloc_scratch[256 + 4 * sizeof(float4) * kNoallocBlocks];
 
 namespace {

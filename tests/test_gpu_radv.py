@@ -25,11 +25,11 @@ def radv_gpu(ctx, tri9):
     return img
 
 
-# 302,080 / 302,081 and 1,208,320 / 1,208,321 triangles sit on either side of
-# the sizes where a block's subtree grows from 64 to 256 and from 256 to 1,024
-# leaf boxes (fewer than 296 blocks of the larger subtree)
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 63, 64, 65, 256, 1023, 1024, 1025, 4096, 4097, 4100, 16385,
-                               100000, 1 << 20, 302080, 302081, 1208320, 1208321])
+# 256 / 257 triangles: one block (each lane its own triangle) or two staged
+# blocks; 131,072 / 131,073 and 4,194,300 / 4,194,304: the subtree per block
+# grows from 64 to 256 and from 256 to 1,024 leaf boxes
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 63, 64, 65, 255, 256, 257, 1023, 1024, 1025, 4096, 4097, 4100,
+                               16385, 100000, 131072, 131073, 1 << 20, 1208321, 4194300, 4194304])
 def test_radv_bytes_match_oracle(ctx, n):
     tri9 = soup(n, 40 + n).reshape(-1)
     img = radv_gpu(ctx, tri9).cpu().numpy()
@@ -150,7 +150,7 @@ def test_validate_reports_damage(ctx):
     assert r["header_ok"] == 0
 
 
-@pytest.mark.parametrize("n", [5, 4097, 100000, 400000, 1300000])
+@pytest.mark.parametrize("n", [5, 4097, 100000, 400000, 4500000])
 def test_radv_refit_equals_rebuild(ctx, n):
     # rq_refit_radv after the vertices move: the bytes of a fresh build on the
     # new vertices (and of the oracle's image of them)
