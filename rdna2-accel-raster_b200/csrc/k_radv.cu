@@ -197,8 +197,10 @@ __global__ void __launch_bounds__(kT, LB == 256 ? 6 : 4) k_radv(RadvArgs A) {
     __shared__ float s_mn0[LB * 3], s_mx0[LB * 3];
     __shared__ float s_mn1[LB / 4 * 3], s_mx1[LB / 4 * 3];
     // per warp: its 32 triangles' vertices as read, and their bounds
-    __shared__ float s_raw[STAGE ? kT / 32 : 1][32 * 9];
-    __shared__ float s_tbox[STAGE ? kT / 32 : 1][32 * 6];
+    // (rows padded: a lane may read 3 floats past its warp's last triangle;
+    // box rows at a stride of 7 floats, which keeps the lanes on distinct banks)
+    __shared__ float s_raw[STAGE ? kT / 32 : 1][32 * 9 + 4];
+    __shared__ float s_tbox[STAGE ? kT / 32 : 1][32 * 7];
     __shared__ uint32_t s_last;
     float* cmn_src = s_mn0;
     float* cmx_src = s_mx0;
@@ -337,29 +339,28 @@ __global__ void __launch_bounds__(kT, LB == 256 ? 6 : 4) k_radv(RadvArgs A) {
             }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                tbox[6 * lane + k] = tmn[k];
-                tbox[6 * lane + 3 + k] = tmx[k];
+                tbox[7 * lane + k] = tmn[k];
+                tbox[7 * lane + 3 + k] = tmx[k];
             }
             __syncwarp();
             // triangle nodes: 16-B part p of triangle t, four triangles per 4 lanes
             {
+                // every lane reads four floats (from vertex float 0, 4 or 8)
+                // and keeps what its part needs, so the lanes do not diverge
                 const uint32_t p = lane & 3u;
+                const uint32_t pk = p < 2u ? 4u * p : 8u;
 #pragma unroll
                 for (uint32_t q = 0; q < 4; ++q) {
                     const uint32_t t = 8 * q + (lane >> 2);
                     if (t < nt) {
-                        const float* f = raw + 9 * t;
-                        uint4 v;
-                        if (p == 0u)
-                            v = make_uint4(__float_as_uint(f[0]), __float_as_uint(f[1]), __float_as_uint(f[2]),
-                                           __float_as_uint(f[3]));
-                        else if (p == 1u)
-                            v = make_uint4(__float_as_uint(f[4]), __float_as_uint(f[5]), __float_as_uint(f[6]),
-                                           __float_as_uint(f[7]));
-                        else if (p == 2u)
-                            v = make_uint4(__float_as_uint(f[8]), 0u, 0u, 0u);
-                        else
-                            v = make_uint4(tb + t, RQ_RADV_GEOMETRY_OPAQUE, 0u, RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
+                        const float* f = raw + 9 * t + pk;
+                        const uint32_t a0 = __float_as_uint(f[0]), a1 = __float_as_uint(f[1]),
+                                       a2 = __float_as_uint(f[2]), a3 = __float_as_uint(f[3]);
+                        const uint4 v =
+                            p < 2u ? make_uint4(a0, a1, a2, a3)
+                                   : p == 2u ? make_uint4(a0, 0u, 0u, 0u)
+                                             : make_uint4(tb + t, RQ_RADV_GEOMETRY_OPAQUE, 0u,
+                                                          RQ_RADV_BARYCENTRICS_CONTROL_DEFAULT);
                         reinterpret_cast<uint4*>(trin + 64ull * (tb + t))[p] = v;
                     }
                 }
@@ -386,9 +387,14 @@ __global__ void __launch_bounds__(kT, LB == 256 ? 6 : 4) k_radv(RadvArgs A) {
                         } else if (F == 7u) {
                             v = make_uint4(0u, 0u, 0u, 0u);
                         } else {
-                            const float* b = tbox + 24 * d + 4 * (F - 1);
-                            v = make_uint4(__float_as_uint(b[0]), __float_as_uint(b[1]), __float_as_uint(b[2]),
-                                           __float_as_uint(b[3]));
+                            // floats e..e+3 of the four child boxes (6 floats each)
+                            uint32_t x[4];
+#pragma unroll
+                            for (uint32_t i = 0; i < 4; ++i) {
+                                const uint32_t e = 4 * (F - 1) + i;
+                                x[i] = __float_as_uint(tbox[7 * (4 * d + e / 6) + e % 6]);
+                            }
+                            v = make_uint4(x[0], x[1], x[2], x[3]);
                         }
                         reinterpret_cast<uint4*>(boxes + 128ull * (A.offs[leaf_lvl] + lb0 + lbl))[F] = v;
                     }
@@ -402,8 +408,8 @@ __global__ void __launch_bounds__(kT, LB == 256 ? 6 : 4) k_radv(RadvArgs A) {
                 for (int c = 0; c < 4; ++c)
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        umn[k] = fminf(umn[k], tbox[24 * lane + 6 * c + k]);
-                        umx[k] = fmaxf(umx[k], tbox[24 * lane + 6 * c + 3 + k]);
+                        umn[k] = fminf(umn[k], tbox[7 * (4 * lane + c) + k]);
+                        umx[k] = fmaxf(umx[k], tbox[7 * (4 * lane + c) + 3 + k]);
                     }
                 const uint32_t lbl = wl / 4 + lane;
 #pragma unroll
