@@ -80,7 +80,9 @@ __global__ void __launch_bounds__(kThreads) k_hist_scan(uint32_t* hist) {
     h[threadIdx.x] = ex;
 }
 
-__global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in,
+// 4 blocks per SM (64 registers): the 2.5M-triangle build 1.047 -> 1.038 ms
+// against 3 blocks at 80 registers; 5 blocks spill more and are slower
+__global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __restrict__ keys_in,
                                                        const uint32_t* __restrict__ vals_in,
                                                        uint32_t* __restrict__ keys_out,
                                                        uint32_t* __restrict__ vals_out, uint32_t n,
