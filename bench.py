@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-sample", type=int, default=6000, help="pixels in the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=200000, help="pixels in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the visibility / batched / serving workloads")
     ap.add_argument("--extra", choices=["visibility", "batched", "serving", "radv"],
@@ -176,17 +176,27 @@ def read_traffic(name):
     return None
 
 
-def cpu_frame_baseline(pos, idx, sample, threads):
-    """CPU time of one frame: the reference's SoftwareBVH build (+ fromBVH2,
-    single-threaded as written) on the full mesh and the CPU statement of the
-    frame's rays over `sample` pixels on `threads` threads, projected to all
-    pixels.  Returns dict(value Mrays/s, build_s, trace_s, rays, ...)."""
-    import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as O
-    from rq import workloads as W
+def frame_config(world):
+    """The workload description both arms print (the measured counts of a
+    frame go to the line's `frame` key)."""
+    return {
+        "workload": ("1080p shadows + AO: 2,499,848-triangle grid (1118x1118 quads, seed 1), per-frame BVH "
+                     "rebuild, 1920x1080 primary rays, 16 any-hit shadow rays + 1 SPP AO (tmax 0.5) per pixel"),
+        "triangles": 2499848, "width": WIDTH, "height": HEIGHT, "lights": 16, "ao_spp": 1,
+        "l2": "inputs larger than L2: the per-step rebuild writes ~0.2 GB of nodes and triangles",
+        "parallelism": "replicas" if world > 1 else "single",
+    }
 
-    ntri = len(idx)
+
+def cpu_frame_sample(O, pos, idx, cam, params, sample, threads, seed, gfull):
+    """One step of the CPU path of the frame: the reference's own
+    SoftwareBVH::build + SoftwareBVH4::fromBVH2 on the full mesh
+    (oracle/_ref, single-threaded as written; Oracle B where the reference
+    library is absent), then the frame's primary, shadow and AO rays at
+    `sample` random pixels traced on `threads` host threads by the CPU
+    statement of the traversal (the reference has no CPU traversal).
+    Returns the measured times and the frame throughput they project to."""
+    import numpy as np
     t0 = time.perf_counter()
     if O.have_ref():
         n2, tr, n4 = O.ref_build(pos.reshape(-1), idx.reshape(-1))
@@ -196,58 +206,74 @@ def cpu_frame_baseline(pos, idx, sample, threads):
         n2, tr, n4 = b["nodes2"], b["tris"], b["nodes4"]
         kind = "port"
     build_s = time.perf_counter() - t0
-    cam = W.shadow_camera()
-    params = W.shadow_params()
-    rng = np.random.default_rng(123)
+    rng = np.random.default_rng(seed)
     pixels = np.sort(rng.choice(WIDTH * HEIGHT, sample, replace=False)).astype(np.uint32)
     t0 = time.perf_counter()
     g = O.render_gbuffer(n4, tr, None, cam, pixels)
-    gfull = np.zeros(WIDTH * HEIGHT, O.GBUFFER_PX)
     gfull[pixels] = g
     _, _, sec_rays = O.render_shadow_ao(n4, tr, gfull, params, pixels)
     trace_s = time.perf_counter() - t0
     rays_sample = sample + sec_rays
-    frame_rays = rays_sample * (WIDTH * HEIGHT) / sample
-    frame_s = build_s + trace_s * (WIDTH * HEIGHT) / sample
+    npix = WIDTH * HEIGHT
+    frame_rays = rays_sample * npix / sample
+    frame_s = build_s + trace_s * npix / sample
     return dict(value=frame_rays / frame_s / 1e6, build_s=build_s, trace_s=trace_s, rays_sample=rays_sample,
-                frame_s=frame_s, kind=kind, cores=threads, triangles=ntri,
-                build_mtris=ntri / build_s / 1e6, trace_mrays=rays_sample / trace_s / 1e6)
+                frame_s=frame_s, frame_rays=frame_rays, kind=kind, cores=threads, triangles=len(idx),
+                build_mtris=len(idx) / build_s / 1e6, trace_mrays=rays_sample / trace_s / 1e6)
+
+
+def cpu_inputs():
+    """The frame's inputs made by the oracle's generators alone (no engine
+    library is loaded): positions, indices, camera, shading parameters."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    return (O,) + O.shadow_frame_inputs(WIDTH, HEIGHT)
+
+
+def cpu_sample_text(r, sample):
+    return (f"per step: reference SoftwareBVH::build + fromBVH2 on the full mesh ({r['build_s']:.2f} s, 1 thread "
+            f"as written, {r['build_mtris']:.2f} Mtris/s) + the frame's primary, shadow and AO rays at {sample} "
+            f"random pixels ({r['rays_sample']} rays, {r['trace_mrays']:.2f} Mrays/s on {r['cores']} threads); "
+            f"value = the frame's rays / (build time + the sample's trace time scaled to {WIDTH}x{HEIGHT})")
 
 
 def run_reference(args, world, rank, pg):
-    """The reference arm: CPU implementation of the path, rank 0 only."""
+    """The reference arm: the CPU implementation of the path on the host
+    cores, rank 0 only.  Each step is measured whole (reference build + the
+    sampled rays); the frame throughput is projected from the step's two
+    measured parts, and the projection is stated in its own key."""
     if rank != 0:
         return
     import numpy as np
-    from rq import workloads as W
-
-    pos, idx = W.shadow_mesh()
+    O, pos, idx, cam, params = cpu_inputs()
     threads = os.cpu_count() or 1
-    steps_done, vals, frame_s = 0, [], []
-    budget_s = 150.0
-    t_start = time.perf_counter()
+    gfull = np.zeros(WIDTH * HEIGHT, O.GBUFFER_PX)
+    step_ms, vals, frame_ms, last = [], [], [], None
     for s in range(args.warmup + args.steps):
-        r = cpu_frame_baseline(pos, idx, args.cpu_sample, threads)
+        t0 = time.perf_counter()
+        r = cpu_frame_sample(O, pos, idx, cam, params, args.cpu_sample, threads, 123 + s, gfull)
+        dt = time.perf_counter() - t0
         if s >= args.warmup:
+            step_ms.append(dt * 1e3)
             vals.append(r["value"])
-            frame_s.append(r["frame_s"])
-            steps_done += 1
-        if time.perf_counter() - t_start > budget_s and steps_done >= 1:
-            break
+            frame_ms.append(r["frame_s"] * 1e3)
+            last = r
     v = statistics.median(vals)
-    pct = (lambda q: float(np.percentile(vals, q))) if vals else (lambda q: v)
+    pct = (lambda q: float(np.percentile(vals, q)))
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Mrays/s", "n_gpus": world,
-        "steps": steps_done, "warmup": args.warmup, "ms_per_step": round(1000 * statistics.median(frame_s), 1),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": "1080p shadows + AO (2,499,848 triangles, 1920x1080, 16 lights, 1 SPP AO)",
-                   "parallelism": "cpu"},
-        "cpu_baseline": {"value": round(v, 3), "unit": "Mrays/s", "cores": threads, "kind": r["kind"],
-                         "sample": (f"per step: reference SoftwareBVH::build+fromBVH2 on the full mesh "
-                                    f"({r['build_s']:.2f}s, 1 thread) + {args.cpu_sample} random pixels' primary, "
-                                    f"shadow and AO rays ({r['rays_sample']} rays, {threads} threads), projected to "
-                                    f"{WIDTH}x{HEIGHT}"),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(statistics.median(step_ms), 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": frame_config(world),
+        "projection": {"frame_ms": round(statistics.median(frame_ms), 1),
+                       "build_ms": round(1e3 * last["build_s"], 1),
+                       "sample_trace_ms": round(1e3 * last["trace_s"], 1),
+                       "sample_pixels": args.cpu_sample, "frame_pixels": WIDTH * HEIGHT,
+                       "frame_rays": round(last["frame_rays"]),
+                       "method": ("ms_per_step is the measured step (full build + sampled rays); value = frame "
+                                  "rays / (measured build + measured sample trace x frame pixels / sample pixels)")},
+        "cpu_baseline": {"value": round(v, 3), "unit": "Mrays/s", "cores": threads, "kind": last["kind"],
+                         "sample": cpu_sample_text(last, args.cpu_sample),
                          "p5": round(pct(5), 3), "p50": round(pct(50), 3), "p95": round(pct(95), 3)},
         "e2e": {"value": round(v, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -462,16 +488,19 @@ def run_ours(args, world, rank, local, pg):
             "gb_per_s_compulsory": round(npx * (36 + 2 * 12) / (blur_ms * 1e-3) / 1e9, 1)}
 
     # the reference's median-split topology (RQ_BUILD_MEDIAN) on the same
-    # mesh: one round per tree level, each ending in a host read of the
-    # level's size, so it is timed on the host clock around a synchronised build
+    # mesh: stream-ordered (one round of launches per possible tree level, no
+    # host synchronisation), timed with CUDA events
     med = rq.Bvh.build(ctx, p_d, i_d, median=True)
     torch.cuda.synchronize(dev)
     med_ms = []
-    for _ in range(3):
-        t0 = time.perf_counter()
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
         rq.Bvh.build(ctx, p_d, i_d, median=True, into=med)
-        torch.cuda.synchronize(dev)
-        med_ms.append((time.perf_counter() - t0) * 1e3)
+        b.record(stream)
+        b.synchronize()
+        med_ms.append(a.elapsed_time(b))
+    ctx.sync_check()
     med_info = med.info()
     med.destroy()
     median_build = {"workload": "median-split build of the frame mesh (2,499,848 triangles) + 4-wide collapse",
@@ -503,12 +532,12 @@ def run_ours(args, world, rank, local, pg):
     clocks = clk.summary()
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        r = cpu_frame_baseline(pos, idx, args.cpu_sample, os.cpu_count() or 1)
+        import numpy as np
+        O, cpos, cidx, ccam, cparams = cpu_inputs()
+        r = cpu_frame_sample(O, cpos, cidx, ccam, cparams, args.cpu_sample, os.cpu_count() or 1, 123,
+                             np.zeros(WIDTH * HEIGHT, O.GBUFFER_PX))
         cpu = {"value": round(r["value"], 3), "unit": "Mrays/s", "cores": r["cores"], "kind": r["kind"],
-               "sample": (f"reference SoftwareBVH::build+fromBVH2 on the full mesh ({r['build_s']:.2f}s, 1 thread, "
-                          f"{r['build_mtris']:.2f} Mtris/s) + {args.cpu_sample} random pixels' primary, shadow and AO "
-                          f"rays ({r['rays_sample']} rays, {r['trace_mrays']:.2f} Mrays/s on {r['cores']} threads), "
-                          f"projected to {WIDTH}x{HEIGHT}")}
+               "sample": cpu_sample_text(r, args.cpu_sample)}
     line = {
         "metric": METRIC,
         "value": round(value, 2),
@@ -522,14 +551,9 @@ def run_ours(args, world, rank, local, pg):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {
-            "workload": ("1080p shadows + AO: 2,499,848-triangle grid (1118x1118 quads, seed 1), per-frame LBVH "
-                         "rebuild, 1920x1080 primary rays, 16 any-hit shadow rays + 1 SPP AO (tmax 0.5) per pixel"),
-            "triangles": ntri, "width": WIDTH, "height": HEIGHT, "lights": 16, "ao_spp": 1,
-            "rays_per_step": frame_rays, "primary_rays": npx, "secondary_rays": sec_rays, "primary_hits": hits,
-            "l2": "inputs larger than L2: the per-step rebuild writes ~0.2 GB of nodes and triangles",
-            "parallelism": "replicas" if world > 1 else "single",
-        },
+        "config": frame_config(world),
+        "frame": {"triangles": ntri, "rays_per_step": frame_rays, "primary_rays": npx, "secondary_rays": sec_rays,
+                  "primary_hits": hits},
         "build_mtris_per_s": round(ntri / statistics.median(build_ms) / 1e3, 1),
         "build_ms": round(statistics.median(build_ms), 4),
         "primary_mrays_per_s": round(npx / statistics.median(prim_ms) / 1e3, 1),
@@ -720,7 +744,9 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
     the timed stream.  Batched: up to 1,024 requests / 16M rays per launch,
     4 launches in flight.  Plain: one request per launch, one in flight.
     Latency = completion seen by the host - submission at the arrival time.
-    Also a saturation run (every request at t=0) for throughput."""
+    Also a saturation run (every request at t=0) for throughput, and a sweep
+    of arrival rates (the same requests, arrival times scaled) giving p50 /
+    p99 per rate and the highest rate each mode sustains under a p99 bound."""
     import numpy as np
     import torch
     import rq
@@ -743,6 +769,17 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
     def make_reqs(srv, ids):
         return [rq.Request(ids[int(mesh[i])], int(kind[i]), int(nrays[i]), int(seeds[i]), 0, 0, None,
                            base + 16 * offs[i], i) for i in range(n)]
+
+    rates = (1000, 2000, 4000, 6000, 8000, 12000, 16000, 24000)
+
+    def run_stream(srv, reqs, arrivals):
+        tickets = srv.replay(reqs, arrivals)
+        comp = srv.completions()
+        lat = np.array([comp[t]["t_done"] - comp[t]["t_submit"] for t in tickets])
+        t_first = min(comp[t]["t_submit"] for t in tickets)
+        t_last = max(comp[t]["t_done"] for t in tickets)
+        ok = all(comp[t]["status"] == 0 for t in tickets)
+        return lat, t_first, t_last, ok
 
     def one(mode, rebuild=False):
         cfg = dict(mode=mode, budget_bytes=120 << 30, slots=4, max_wave_rays=1 << 24, max_wave_requests=1024,
@@ -783,15 +820,40 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
                "requests_per_s": round(n / (t_last - t_first), 1),
                "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
                "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3)}
+        # arrival-rate sweep: the same requests, arrivals scaled to each rate
+        sweep = []
+        for r in rates:
+            s0 = srv.stats()
+            lat, t_first, t_last, ok_r = run_stream(srv, reqs, t_arr * (W.SERVE_RATE / r))
+            s1 = srv.stats()
+            sweep.append({"rate": r, "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                          "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                          "mrays_per_s": round(float(nrays.sum()) / (t_last - t_first) / 1e6, 1),
+                          "requests_per_s": round(n / (t_last - t_first), 1),
+                          "requests_per_launch": round(n / max(1, s1["launches"] - s0["launches"]), 2),
+                          "all_ok": bool(ok_r)})
         st = srv.stats()
         srv.close()
-        return {"stream": stream, "saturation": sat, "warm_build_s": round(t_warm, 3),
+        return {"stream": stream, "saturation": sat, "sweep": sweep, "warm_build_s": round(t_warm, 3),
                 "resident_gb": round(st["peak_resident_bytes"] / 1e9, 2), "builds": int(st["builds"])}
 
     b = one(rq.RQ_SERVE_BATCHED)
     p = one(rq.RQ_SERVE_PLAIN)
     pr = one(rq.RQ_SERVE_PLAIN, rebuild=True)
     torch.cuda.synchronize(dev)
+
+    def sustained(m, bound_ms):
+        """Highest swept rate whose p99 stays within the bound and whose
+        achieved request rate keeps up with the offered one (within 10 %)."""
+        ok = [x for x in m["sweep"] if x["p99_ms"] <= bound_ms and x["requests_per_s"] >= 0.9 * x["rate"]]
+        return max((x["rate"] for x in ok), default=None)
+
+    at_p99 = []
+    for bound in (1.0, 2.0, 5.0, 10.0, 20.0):
+        rb, rp, rr = sustained(b, bound), sustained(p, bound), sustained(pr, bound)
+        at_p99.append({"p99_bound_ms": bound, "batched_rate": rb, "plain_rate": rp, "plain_rebuild_rate": rr,
+                       "batched_over_plain": round(rb / rp, 2) if rb and rp else None,
+                       "batched_over_plain_rebuild": round(rb / rr, 2) if rb and rr else None})
     return {
         "workload": (f"serving: Poisson {W.SERVE_RATE:.0f} req/s for {duration_s:g} s (seed 4, {n} requests), "
                      f"{catalogue} resident height-field meshes with triangle counts log-uniform in [64, 1M] "
@@ -806,6 +868,11 @@ def run_serving(dev, duration_s=2.0, catalogue=256):
         "saturation_throughput_ratio": round(b["saturation"]["mrays_per_s"] / p["saturation"]["mrays_per_s"], 2),
         "saturation_throughput_ratio_vs_plain_rebuild": round(
             b["saturation"]["mrays_per_s"] / pr["saturation"]["mrays_per_s"], 2),
+        "sweep_rates": list(rates),
+        "sustained_at_p99": at_p99,
+        "sustained_how": ("for each p99 bound, the highest swept arrival rate (same requests, arrivals scaled) at "
+                          "which the mode's p99 stays within the bound and its achieved request rate is at least "
+                          "90 % of the offered rate; ratios are served (batched) over plain at the same bound"),
     }
 
 

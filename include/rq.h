@@ -73,6 +73,10 @@ typedef struct rq_trace_tuning {
                              (the frame only reports hit or miss, so the order does not show) */
     uint32_t refill_min;  /* a warp hands new rays to its idle lanes only once at least this many of
                              its 32 lanes are idle (or all are): 1..32; 0 means 1 */
+    uint32_t leaf_batch;  /* 0: rays finish and lanes refill between rounds only.  1..32: a lane whose
+                             ray runs out of nodes reports at once and idle lanes refill inside the
+                             node loop, which hands over to the leaf tests once this many lanes hold a
+                             leaf (speculative shapes only) */
 } rq_trace_tuning;
 int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out);
 /* RQ_ERR_INVALID_ARG for a shape that has no kernel. */
@@ -417,6 +421,57 @@ int rq_render_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera* cam, rq_g
 int rq_render_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_shade_params* params,
                         uint32_t* light_mask, float* ao, unsigned long long* counters, rq_stream stream);
 
+/* Reflection rays of shaders/tiled_lighting_ra.comp:91-113: per G-buffer
+ * pixel with a hit, R = reflect(normalize(P - cam_pos), N) (GLSL reflect,
+ * I - 2 dot(N, I) N, not renormalised) from P + bias*N over [tmin, tmax],
+ * closest hit with gl_RayFlagsOpaqueEXT semantics. */
+typedef struct rq_reflect_params {
+    uint32_t width;
+    uint32_t height;
+    float cam_pos[3];
+    float tmin;     /* 0.02 */
+    float tmax;     /* 100 */
+    float bias;     /* 0.04 */
+    uint32_t flags; /* RQ_TRI_* */
+} rq_reflect_params;
+
+/* Closest-hit reflection ray of every G-buffer pixel into hits[p] (rq_hit:
+ * hit, t, instance id 0, original primitive id; t = -1 and ids 0xFFFFFFFF
+ * for a miss and for pixels that saw no geometry, whose reflection the
+ * shader skips).  The lighting pass reads only hit / miss (:111-113); the
+ * full record is kept for callers that shade the reflected surface.
+ * `params` is a host pointer; gbuf and hits are device pointers. */
+int rq_render_reflect(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_reflect_params* params,
+                      rq_hit* hits, rq_stream stream);
+
+/* Ambient occlusion from a depth buffer, as shaders/rq_ao.comp:47-97 computes
+ * it: per pixel (x, y), uv = ((x, y) + 0.5) / (W, H); depth >= 1 gives
+ * AO = 1; otherwise the world position is inv_view_proj * (uv*2-1, depth, 1)
+ * divided by w, and the normal is the normalised cross product of the right
+ * and upper neighbours' reconstructed positions minus it (uv + one texel,
+ * depth read at the neighbouring pixel, clamped to the image edge as a
+ * clamp-to-edge sampler at texel centres reads it), turned toward cam_pos.
+ * max(1, spp) cosine-hemisphere any-hit rays (seed y*W + x + 5544) leave
+ * P + bias*N over [tmin, max_distance]; AO = the unoccluded fraction. */
+typedef struct rq_ao_depth_params {
+    float inv_view_proj[16]; /* column-major, Vulkan [0,1] depth */
+    float cam_pos[3];
+    uint32_t width;
+    uint32_t height;
+    uint32_t spp;        /* samplesPerPixel */
+    float max_distance;  /* maxAoDistance */
+    float tmin;          /* 0.01 */
+    float bias;          /* 0.03 */
+    uint32_t flags;      /* RQ_TRI_* */
+} rq_ao_depth_params;
+
+/* rq_ao.comp's AO pass over a width x height depth buffer (device, e.g. the
+ * output of rq_gbuffer_depth) into ao (device, width*height floats).
+ * `counters` (device, may be NULL) accumulates [0] rays cast.  `params` is a
+ * host pointer.  At most 32 samples per pixel. */
+int rq_render_ao_depth(rq_ctx* ctx, const rq_bvh* bvh, const float* depth, const rq_ao_depth_params* params, float* ao,
+                       unsigned long long* counters, rq_stream stream);
+
 /* Depth z/w of every G-buffer position under the view-projection `view_proj`
  * (column-major, Vulkan [0,1] depth; 1.0 for pixels that saw no geometry),
  * the depth the AO blur compares.  Device pointers, npix pixels. */
@@ -467,10 +522,13 @@ int rq_refit_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* 
  * fail under a fixed budget): it takes no context, allocates nothing, and
  * keeps its scratch in a static device array inside librq.so, so it accepts
  * at most RQ_RADV_NOALLOC_MAX_TRIANGLES triangles (RQ_ERR_UNSUPPORTED
- * beyond).  Runs on the current device.  Its first call on a device looks up
- * the array's device address; make that first call before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU
- * race, so order them on one stream.  Output bytes equal rq_build_radv's. */
+ * beyond).  Runs on the current device.  Every call looks up the array's
+ * device address there (cudaGetSymbolAddress, which allocates nothing); the
+ * first call on a device, and the first after a device reset, also loads the
+ * library's device code, so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU race, so
+ * order them on one stream.  tri9 must be 4-byte and as_image 16-byte
+ * aligned (RQ_ERR_INVALID_ARG).  Output bytes equal rq_build_radv's. */
 #define RQ_RADV_NOALLOC_MAX_TRIANGLES (1u << 24)
 int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, void* as_image, uint64_t as_bytes,
                           rq_stream stream);

@@ -4,7 +4,10 @@
 //   SoftwareBVH  bvh  = SoftwareBVH::build(mesh, maxPrimsPerLeaf);   // common/software_bvh.hpp:35
 //   SoftwareBVH4 bvh4 = SoftwareBVH4::fromBVH2(bvh);                // common/software_bvh.hpp:193
 //
-// becomes
+// compiles unchanged against this header with `rq::` in front (or a
+// `using namespace rq;`): those two calls run on the calling thread's default
+// engine, created on the current CUDA device at its first use.  A caller that
+// wants to choose the device or hold the context passes an engine:
 //
 //   rq::Engine eng;                                   // one context per device / thread
 //   rq::SoftwareBVH  bvh  = rq::SoftwareBVH::build(eng, mesh, maxPrimsPerLeaf);
@@ -61,12 +64,33 @@ class Engine {
     rq_ctx* ctx_ = nullptr;
 };
 
+// The engine of the reference-shaped calls (no Engine argument): one per
+// thread, on the CUDA device current at its first use.  It lives until the
+// process exits (it is not destroyed at thread exit, when the CUDA runtime
+// may already be shutting down); its device memory goes with the process.
+inline Engine& default_engine() {
+    thread_local Engine* eng = nullptr;
+    if (!eng) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+        eng = new Engine(dev);
+    }
+    return *eng;
+}
+
 enum class Split { Morton, Median };
 
 struct SoftwareBVH {
     std::vector<rq_bvh2_node> nodes;
     std::vector<rq_triangle> triangles;
     std::vector<uint32_t> perm;  // leaf order -> original triangle id
+
+    // SoftwareBVH::build(mesh, maxPrimsPerLeaf) (common/software_bvh.hpp:35),
+    // on the calling thread's default engine.
+    template <class Mesh>
+    static SoftwareBVH build(const Mesh& mesh, uint32_t maxPrimsPerLeaf = 4) {
+        return build(default_engine(), mesh, maxPrimsPerLeaf, Split::Morton);
+    }
 
     template <class Mesh>
     static SoftwareBVH build(Engine& eng, const Mesh& mesh, uint32_t maxPrimsPerLeaf = 4,
@@ -128,6 +152,10 @@ struct SoftwareBVH {
 struct SoftwareBVH4 {
     std::vector<rq_bvh4_node> nodes;
     std::vector<rq_triangle> triangles;
+
+    // SoftwareBVH4::fromBVH2(bvh) (common/software_bvh.hpp:193), on the
+    // calling thread's default engine.
+    static SoftwareBVH4 fromBVH2(const SoftwareBVH& b2) { return fromBVH2(default_engine(), b2); }
 
     static SoftwareBVH4 fromBVH2(Engine& eng, const SoftwareBVH& b2) {
         SoftwareBVH4 out;

@@ -60,18 +60,22 @@ inline V3 normalize(V3 v) {
 }
 inline float comp(V3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
 
+// Items handed out in chunks of 16..1024, at least 16 chunks per thread
+// when n allows, so small batches of heavy items (a pixel's 17 rays) still
+// keep every thread busy.
 template <class F>
 void parallel_for(uint32_t n, int threads, F&& f) {
-    if (threads <= 1 || n < 4096) {
+    if (threads <= 1 || n < 64) {
         for (uint32_t i = 0; i < n; ++i) f(i);
         return;
     }
+    const uint32_t chunk = std::max(16u, std::min(1024u, n / (16u * uint32_t(threads))));
     std::atomic<uint32_t> next{0};
     auto worker = [&]() {
         for (;;) {
-            uint32_t b = next.fetch_add(1024);
+            uint32_t b = next.fetch_add(chunk);
             if (b >= n) break;
-            uint32_t e = std::min(n, b + 1024);
+            uint32_t e = std::min(n, b + chunk);
             for (uint32_t i = b; i < e; ++i) f(i);
         }
     };
@@ -872,9 +876,11 @@ int orc_radv_build(const float* tri9, uint32_t n, uint8_t* img) {
 
 // Reference semantics of software_bvh_bvh4.comp:96-195 on explicit rays
 // (ray tmin/tmax replace the shader's constants 0.01 / 1000).  Hit IDs are
-// leaf-order indices (:181).
+// leaf-order indices (:181).  The shader's 24-entry stack drops a push that
+// does not fit (:185); dropped[i] (may be NULL) counts them per ray, so a
+// miss caused by a dropped subtree can be told from a geometric one.
 void orc_trace_ref_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq_ray* rays, uint32_t n,
-                        rq_ray_stats* stats, rq_hit* hits, int threads) {
+                        rq_ray_stats* stats, rq_hit* hits, uint32_t* dropped, int threads) {
     parallel_for(n, threads, [&](uint32_t idx) {
         const rq_ray& r = rays[idx];
         V3 o{r.org[0], r.org[1], r.org[2]}, d{r.dir[0], r.dir[1], r.dir[2]};
@@ -886,6 +892,7 @@ void orc_trace_ref_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, cons
         int32_t stack[24];
         stack[0] = 0;
         int ptr = 1;
+        uint32_t drops = 0;
         while (ptr > 0) {
             const rq_bvh4_node& nd = nodes[stack[--ptr]];
             boxTests += 4;
@@ -934,10 +941,14 @@ void orc_trace_ref_bvh4(const rq_bvh4_node* nodes, const rq_triangle* tris, cons
                         }
                     }
                 } else if (nd.child_count[k] < 0) {
-                    if (ptr < 24) stack[ptr++] = nd.child_index[k];
+                    if (ptr < 24)
+                        stack[ptr++] = nd.child_index[k];
+                    else
+                        ++drops;
                 }
             }
         }
+        if (dropped) dropped[idx] = drops;
         if (stats) stats[idx] = {hitPrim >= 0 ? 1u : 0u, boxTests, triTests, 0u};
         if (hits) {
             if (hitPrim >= 0)
@@ -1374,6 +1385,206 @@ void orc_gen_mesh_rays(const float* pos, const uint32_t* idx, uint32_t ntri, uin
     }
 }
 
+}  // extern "C"
+
+namespace {
+
+// Primary ray of visbuf_raycast.comp:15-51 for one pixel (optional per-pixel
+// jitter from the camera's seed).
+rq_ray camera_ray(const rq_camera& c, uint32_t pixel) {
+    const uint32_t px = pixel % c.width, py = pixel / c.width;
+    float jx = 0.5f, jy = 0.5f;
+    if (c.jitter) {
+        uint32_t h = pcg_hash(c.seed ^ pcg_hash(pixel));
+        jx = float(h) * kInv2Pow32;
+        jy = float(pcg_hash(h)) * kInv2Pow32;
+    }
+    const float u = (float(px) + jx) / float(c.width);
+    const float v = (float(py) + jy) / float(c.height);
+    const float cl[4] = {u * 2.0f - 1.0f, v * 2.0f - 1.0f, 1.0f, 1.0f};
+    float wt[4];
+    mat4_mul(c.inv_view_proj, cl, wt);
+    const V3 o{c.cam_pos[0], c.cam_pos[1], c.cam_pos[2]};
+    const V3 target{wt[0] / wt[3], wt[1] / wt[3], wt[2] / wt[3]};
+    const V3 d = normalize(sub(target, o));
+    return rq_ray{{o.x, o.y, o.z}, c.tmin, {d.x, d.y, d.z}, c.tmax};
+}
+
+// hemisphereSample of rq_ao.comp:32-45: two draws of the one-at-a-time hash
+// advance `seed`; sin/cos through sincos_taylor.
+V3 hemisphere_dir(V3 N, uint32_t& seed) {
+    seed = ao_hash(seed);
+    const float u1 = float(seed) * kInv2Pow32;
+    seed = ao_hash(seed);
+    const float u2 = float(seed) * kInv2Pow32;
+    const float rr = std::sqrt(u1);
+    const float theta = 6.2831853f * u2;
+    float sn, cs;
+    sincos_taylor(theta, &sn, &cs);
+    const float x = rr * cs, y = rr * sn, z = std::sqrt(fmax_(0.0f, 1.0f - u1));
+    const V3 up = std::fabs(N.z) < 0.999f ? V3{0.0f, 0.0f, 1.0f} : V3{1.0f, 0.0f, 0.0f};
+    const V3 tg = normalize(cross(up, N));
+    const V3 bt = cross(N, tg);
+    return normalize(V3{(tg.x * x + bt.x * y) + N.x * z, (tg.y * x + bt.y * y) + N.y * z,
+                        (tg.z * x + bt.z * y) + N.z * z});
+}
+
+// The secondary rays of one G-buffer pixel, in the order the frame casts
+// them: emit(slot, ray) for every light k that casts a shadow ray
+// (shaders/tiled_lighting_ra.comp:118-148; slot k) and every AO sample s
+// (shaders/rq_ao.comp:70-94 with the G-buffer's position and normal; slot
+// 32 + s).  Pixels without geometry cast nothing.
+template <class F>
+void shade_pixel_rays(const rq_gbuffer_px& g, const rq_shade_params& p, uint32_t pixel, F&& emit) {
+    if (g.vis == 0u) return;
+    const V3 P{g.pos[0], g.pos[1], g.pos[2]}, N{g.nrm[0], g.nrm[1], g.nrm[2]};
+    const V3 os{P.x + N.x * p.shadow_bias, P.y + N.y * p.shadow_bias, P.z + N.z * p.shadow_bias};
+    for (uint32_t k = 0; k < p.num_lights; ++k) {
+        const rq_light& L0 = p.lights[k];
+        const V3 tl{L0.pos[0] - P.x, L0.pos[1] - P.y, L0.pos[2] - P.z};
+        const float dist = std::sqrt(dot(tl, tl));
+        if (dist > L0.radius || dist < 0.001f) continue;
+        const V3 L{tl.x / dist, tl.y / dist, tl.z / dist};
+        if (fmax_(0.0f, dot(N, L)) <= 0.0f) continue;
+        emit(k, rq_ray{{os.x, os.y, os.z}, p.shadow_tmin, {L.x, L.y, L.z}, dist - p.shadow_bias});
+    }
+    if (p.ao_spp) {
+        uint32_t seed = pixel + 5544u;
+        const V3 oa{P.x + N.x * p.ao_bias, P.y + N.y * p.ao_bias, P.z + N.z * p.ao_bias};
+        for (uint32_t s = 0; s < p.ao_spp; ++s) {
+            const V3 dir = hemisphere_dir(N, seed);
+            emit(32u + s, rq_ray{{oa.x, oa.y, oa.z}, p.ao_tmin, {dir.x, dir.y, dir.z}, p.ao_tmax});
+        }
+    }
+}
+
+// The reflection ray of shaders/tiled_lighting_ra.comp:91-113 for one
+// G-buffer pixel: R = reflect(normalize(P - cam), N) (GLSL reflect:
+// I - 2 dot(N, I) N), from P + bias N over [tmin, tmax].
+rq_ray reflect_ray(const rq_gbuffer_px& g, const rq_reflect_params& p) {
+    const V3 P{g.pos[0], g.pos[1], g.pos[2]}, N{g.nrm[0], g.nrm[1], g.nrm[2]};
+    const V3 V = normalize(sub(P, V3{p.cam_pos[0], p.cam_pos[1], p.cam_pos[2]}));
+    const float k = 2.0f * dot(N, V);
+    const V3 R{V.x - k * N.x, V.y - k * N.y, V.z - k * N.z};
+    return rq_ray{{P.x + N.x * p.bias, P.y + N.y * p.bias, P.z + N.z * p.bias}, p.tmin, {R.x, R.y, R.z}, p.tmax};
+}
+
+// rq_ao.comp:47-69 for one pixel: the world position reconstructed from the
+// depth at the pixel centre through inv_view_proj, the normal from the
+// cross product of the right and upper neighbours' reconstructed positions
+// (depth read clamped at the image edge, as a clamp-to-edge sampler at texel
+// centres reads it), turned toward the camera.  Returns false where
+// depth >= 1 (no geometry).
+bool ao_depth_surface(const float* depth, const rq_ao_depth_params& p, uint32_t px, uint32_t py, V3& P, V3& N) {
+    const uint32_t w = p.width, h = p.height;
+    const float d = depth[size_t(py) * w + px];
+    if (d >= 1.0f) return false;
+    const float fw = float(w), fh = float(h);
+    const float u = (float(px) + 0.5f) / fw, v = (float(py) + 0.5f) / fh;
+    const float tx = 1.0f / fw, ty = 1.0f / fh;
+    const float dr = depth[size_t(py) * w + (px + 1 < w ? px + 1 : w - 1)];
+    const float du = depth[size_t(py + 1 < h ? py + 1 : h - 1) * w + px];
+    auto unproject = [&](float uu, float vv, float dd) {
+        const float ndc[4] = {uu * 2.0f - 1.0f, vv * 2.0f - 1.0f, dd, 1.0f};
+        float o[4];
+        mat4_mul(p.inv_view_proj, ndc, o);
+        return V3{o[0] / o[3], o[1] / o[3], o[2] / o[3]};
+    };
+    P = unproject(u, v, d);
+    const V3 pr = unproject(u + tx, v, dr);
+    const V3 pu = unproject(u, v + ty, du);
+    N = normalize(cross(sub(pr, P), sub(pu, P)));
+    if (dot(N, sub(V3{p.cam_pos[0], p.cam_pos[1], p.cam_pos[2]}, P)) < 0.0f) N = {-N.x, -N.y, -N.z};
+    return true;
+}
+
+// The AO rays of one pixel of rq_ao.comp:70-94 from a reconstructed surface:
+// max(1, spp) samples seeded y*W + x + 5544, from P + bias N.
+template <class F>
+void ao_depth_rays(const rq_ao_depth_params& p, uint32_t pixel, V3 P, V3 N, F&& emit) {
+    uint32_t seed = pixel + 5544u;
+    const uint32_t spp = p.spp > 1u ? p.spp : 1u;
+    const V3 o{P.x + N.x * p.bias, P.y + N.y * p.bias, P.z + N.z * p.bias};
+    for (uint32_t s = 0; s < spp; ++s) {
+        const V3 dir = hemisphere_dir(N, seed);
+        emit(s, rq_ray{{o.x, o.y, o.z}, p.tmin, {dir.x, dir.y, dir.z}, p.max_distance});
+    }
+}
+
+// Box of one triangle (as the builds compute it) and unions.
+struct Box {
+    float mn[3], mx[3];
+};
+inline Box tri_box(const rq_triangle& t) {
+    Box b;
+    for (int a = 0; a < 3; ++a) {
+        b.mn[a] = fmin_(fmin_(t.v0[a], t.v1[a]), t.v2[a]);
+        b.mx[a] = fmax_(fmax_(t.v0[a], t.v1[a]), t.v2[a]);
+    }
+    return b;
+}
+inline Box box_union(const Box& a, const Box& b) {
+    Box r;
+    for (int k = 0; k < 3; ++k) {
+        r.mn[k] = fmin_(a.mn[k], b.mn[k]);
+        r.mx[k] = fmax_(a.mx[k], b.mx[k]);
+    }
+    return r;
+}
+Box range_box(const rq_triangle* tris, uint32_t first, uint32_t count) {
+    Box b = tri_box(tris[first]);
+    for (uint32_t i = 1; i < count; ++i) b = box_union(b, tri_box(tris[first + i]));
+    return b;
+}
+
+Box refit2(rq_bvh2_node* n, const rq_triangle* tris, int32_t i) {
+    rq_bvh2_node& nd = n[i];
+    Box b;
+    if (nd.left_child < 0)
+        b = range_box(tris, uint32_t(~nd.left_child), uint32_t(nd.right_child));
+    else
+        b = box_union(refit2(n, tris, nd.left_child), refit2(n, tris, nd.right_child));
+    for (int a = 0; a < 3; ++a) {
+        nd.aabb_min[a] = b.mn[a];
+        nd.aabb_max[a] = b.mx[a];
+    }
+    return b;
+}
+
+Box refit4(rq_bvh4_node* n, const rq_triangle* tris, int32_t i) {
+    rq_bvh4_node& nd = n[i];
+    Box all{{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}};
+    for (int k = 0; k < 4; ++k) {
+        if (nd.child_count[k] == 0) continue;
+        const Box b = nd.child_count[k] < 0 ? refit4(n, tris, nd.child_index[k])
+                                            : range_box(tris, uint32_t(~nd.child_index[k]), uint32_t(nd.child_count[k]));
+        nd.min_x[k] = b.mn[0];
+        nd.min_y[k] = b.mn[1];
+        nd.min_z[k] = b.mn[2];
+        nd.max_x[k] = b.mx[0];
+        nd.max_y[k] = b.mx[1];
+        nd.max_z[k] = b.mx[2];
+        all = box_union(all, b);
+    }
+    return all;
+}
+
+// SplitMix64 with a (0, 1] double draw: the workload generator's PRNG.
+struct SplitMix64 {
+    uint64_t s;
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return double((next() >> 11) + 1) * (1.0 / 9007199254740992.0); }
+};
+
+}  // namespace
+
+extern "C" {
+
 // Primary rays of visbuf_raycast.comp:15-51 (optional per-pixel jitter),
 // closest hit with the engine traversal, G-buffer pixel as rq_render_gbuffer
 // writes it.  `pixels` lists the pixel indices to evaluate (NULL = all);
@@ -1382,23 +1593,9 @@ void orc_render_gbuffer(const rq_bvh4_node* nodes, const rq_triangle* tris, cons
                         const uint32_t* pixels, uint32_t npix, rq_gbuffer_px* out, int threads) {
     const rq_camera c = *cam;
     parallel_for(npix, threads, [&](uint32_t i) {
-        uint32_t pixel = pixels ? pixels[i] : i;
-        uint32_t px = pixel % c.width, py = pixel / c.width;
-        float jx = 0.5f, jy = 0.5f;
-        if (c.jitter) {
-            uint32_t h = pcg_hash(c.seed ^ pcg_hash(pixel));
-            jx = float(h) * kInv2Pow32;
-            jy = float(pcg_hash(h)) * kInv2Pow32;
-        }
-        float u = (float(px) + jx) / float(c.width);
-        float v = (float(py) + jy) / float(c.height);
-        float cl[4] = {u * 2.0f - 1.0f, v * 2.0f - 1.0f, 1.0f, 1.0f};
-        float wt[4];
-        mat4_mul(c.inv_view_proj, cl, wt);
-        V3 o{c.cam_pos[0], c.cam_pos[1], c.cam_pos[2]};
-        V3 target{wt[0] / wt[3], wt[1] / wt[3], wt[2] / wt[3]};
-        V3 d = normalize(sub(target, o));
-        rq_ray r{{o.x, o.y, o.z}, c.tmin, {d.x, d.y, d.z}, c.tmax};
+        const uint32_t pixel = pixels ? pixels[i] : i;
+        const rq_ray r = camera_ray(c, pixel);
+        const V3 o{r.org[0], r.org[1], r.org[2]}, d{r.dir[0], r.dir[1], r.dir[2]};
         TraceOut t = trace_bvh4(nodes, tris, r, c.flags & 2u);
         rq_gbuffer_px g;
         if (!t.hit) {
@@ -1417,6 +1614,11 @@ void orc_render_gbuffer(const rq_bvh4_node* nodes, const rq_triangle* tris, cons
     });
 }
 
+// The primary rays themselves (rays[i] for pixel pixels[i], NULL = all).
+void orc_camera_rays(const rq_camera* cam, const uint32_t* pixels, uint32_t npix, rq_ray* rays) {
+    for (uint32_t i = 0; i < npix; ++i) rays[i] = camera_ray(*cam, pixels ? pixels[i] : i);
+}
+
 // Shadow rays of shaders/tiled_lighting_ra.comp:118-148 and AO rays of
 // rq_ao.comp:18-94 for the listed pixels of a full-size G-buffer.
 void orc_render_shadow_ao(const rq_bvh4_node* nodes, const rq_triangle* tris, const rq_gbuffer_px* gbuf,
@@ -1425,55 +1627,294 @@ void orc_render_shadow_ao(const rq_bvh4_node* nodes, const rq_triangle* tris, co
     const rq_shade_params p = *prm;
     std::atomic<uint64_t> total{0};
     parallel_for(npix, threads, [&](uint32_t i) {
-        uint32_t pixel = pixels ? pixels[i] : i;
+        const uint32_t pixel = pixels ? pixels[i] : i;
         const rq_gbuffer_px& g = gbuf[pixel];
         uint32_t m = 0, rays = 0;
-        float occl = 1.0f;
-        if (g.vis != 0u) {
-            V3 P{g.pos[0], g.pos[1], g.pos[2]}, N{g.nrm[0], g.nrm[1], g.nrm[2]};
-            V3 os{P.x + N.x * p.shadow_bias, P.y + N.y * p.shadow_bias, P.z + N.z * p.shadow_bias};
-            for (uint32_t k = 0; k < p.num_lights; ++k) {
-                const rq_light& L0 = p.lights[k];
-                V3 tl{L0.pos[0] - P.x, L0.pos[1] - P.y, L0.pos[2] - P.z};
-                float dist = std::sqrt(dot(tl, tl));
-                if (dist > L0.radius || dist < 0.001f) continue;
-                V3 L{tl.x / dist, tl.y / dist, tl.z / dist};
-                if (fmax_(0.0f, dot(N, L)) <= 0.0f) continue;
-                ++rays;
-                rq_ray r{{os.x, os.y, os.z}, p.shadow_tmin, {L.x, L.y, L.z}, dist - p.shadow_bias};
-                if (!trace_bvh4(nodes, tris, r, 1u | (p.flags & 2u)).hit) m |= 1u << k;
-            }
-            if (p.ao_spp) {
-                uint32_t seed = pixel + 5544u;
-                V3 oa{P.x + N.x * p.ao_bias, P.y + N.y * p.ao_bias, P.z + N.z * p.ao_bias};
-                float unocc = 0.0f;
-                for (uint32_t s = 0; s < p.ao_spp; ++s) {
-                    seed = ao_hash(seed);
-                    float u1 = float(seed) * kInv2Pow32;
-                    seed = ao_hash(seed);
-                    float u2 = float(seed) * kInv2Pow32;
-                    float rr = std::sqrt(u1);
-                    float theta = 6.2831853f * u2;
-                    float sn, cs;
-                    sincos_taylor(theta, &sn, &cs);
-                    float x = rr * cs, y = rr * sn, z = std::sqrt(fmax_(0.0f, 1.0f - u1));
-                    V3 up = std::fabs(N.z) < 0.999f ? V3{0.0f, 0.0f, 1.0f} : V3{1.0f, 0.0f, 0.0f};
-                    V3 tg = normalize(cross(up, N));
-                    V3 bt = cross(N, tg);
-                    V3 dir = normalize(V3{(tg.x * x + bt.x * y) + N.x * z, (tg.y * x + bt.y * y) + N.y * z,
-                                          (tg.z * x + bt.z * y) + N.z * z});
-                    ++rays;
-                    rq_ray r{{oa.x, oa.y, oa.z}, p.ao_tmin, {dir.x, dir.y, dir.z}, p.ao_tmax};
-                    if (!trace_bvh4(nodes, tris, r, 1u | (p.flags & 2u)).hit) unocc += 1.0f;
-                }
-                occl = unocc / float(p.ao_spp);
-            }
-        }
+        float unocc = 0.0f;
+        shade_pixel_rays(g, p, pixel, [&](uint32_t slot, const rq_ray& r) {
+            ++rays;
+            const bool hit = trace_bvh4(nodes, tris, r, 1u | (p.flags & 2u)).hit;
+            if (hit) return;
+            if (slot < 32u)
+                m |= 1u << slot;
+            else
+                unocc += 1.0f;
+        });
         mask[i] = m;
-        ao[i] = occl;
+        ao[i] = (g.vis != 0u && p.ao_spp) ? unocc / float(p.ao_spp) : 1.0f;
         total += rays;
     });
     if (rays_out) *rays_out = total;
+}
+
+// The secondary rays of the listed pixels, in casting order: rays[j] with
+// ray_pixel[j] = its index into `pixels` and ray_slot[j] = light k (< 32) or
+// 32 + AO sample.  At most `cap` rays are written; *count gets the total.
+void orc_shade_rays(const rq_gbuffer_px* gbuf, const rq_shade_params* prm, const uint32_t* pixels, uint32_t npix,
+                    rq_ray* rays, uint32_t* ray_pixel, uint32_t* ray_slot, uint64_t cap, uint64_t* count) {
+    const rq_shade_params p = *prm;
+    uint64_t n = 0;
+    for (uint32_t i = 0; i < npix; ++i) {
+        const uint32_t pixel = pixels ? pixels[i] : i;
+        shade_pixel_rays(gbuf[pixel], p, pixel, [&](uint32_t slot, const rq_ray& r) {
+            if (n < cap) {
+                rays[n] = r;
+                ray_pixel[n] = i;
+                ray_slot[n] = slot;
+            }
+            ++n;
+        });
+    }
+    *count = n;
+}
+
+// Reflection closest-hit rays (shaders/tiled_lighting_ra.comp:91-113) for
+// the listed pixels: hits[i] is rq_render_reflect's record of pixel
+// pixels[i] (original primitive id; a miss record where the G-buffer pixel
+// saw nothing).  rays (may be NULL) receives the rays themselves.
+void orc_render_reflect(const rq_bvh4_node* nodes, const rq_triangle* tris, const uint32_t* perm,
+                        const rq_gbuffer_px* gbuf, const rq_reflect_params* prm, const uint32_t* pixels,
+                        uint32_t npix, rq_hit* hits, rq_ray* rays, int threads) {
+    const rq_reflect_params p = *prm;
+    parallel_for(npix, threads, [&](uint32_t i) {
+        const uint32_t pixel = pixels ? pixels[i] : i;
+        const rq_gbuffer_px& g = gbuf[pixel];
+        if (g.vis == 0u) {
+            hits[i] = {0u, -1.0f, 0xffffffffu, 0xffffffffu};
+            if (rays) rays[i] = rq_ray{{0.0f, 0.0f, 0.0f}, 0.0f, {0.0f, 0.0f, 0.0f}, -1.0f};
+            return;
+        }
+        const rq_ray r = reflect_ray(g, p);
+        if (rays) rays[i] = r;
+        const TraceOut t = trace_bvh4(nodes, tris, r, p.flags & 2u);
+        hits[i] = t.hit ? rq_hit{1u, t.t, 0u, perm ? perm[t.prim] : t.prim}
+                        : rq_hit{0u, -1.0f, 0xffffffffu, 0xffffffffu};
+    });
+}
+
+// rq_ao.comp:47-97 from a depth buffer: ao[i] for pixel pixels[i] (NULL =
+// all): 1.0 where depth >= 1, else the unoccluded fraction of max(1, spp)
+// any-hit rays.  rays_out (may be NULL) accumulates the rays cast.
+void orc_render_ao_depth(const rq_bvh4_node* nodes, const rq_triangle* tris, const float* depth,
+                         const rq_ao_depth_params* prm, const uint32_t* pixels, uint32_t npix, float* ao,
+                         uint64_t* rays_out, int threads) {
+    const rq_ao_depth_params p = *prm;
+    std::atomic<uint64_t> total{0};
+    parallel_for(npix, threads, [&](uint32_t i) {
+        const uint32_t pixel = pixels ? pixels[i] : i;
+        V3 P, N;
+        if (!ao_depth_surface(depth, p, pixel % p.width, pixel / p.width, P, N)) {
+            ao[i] = 1.0f;
+            return;
+        }
+        float unocc = 0.0f;
+        uint32_t rays = 0;
+        ao_depth_rays(p, pixel, P, N, [&](uint32_t, const rq_ray& r) {
+            ++rays;
+            if (!trace_bvh4(nodes, tris, r, 1u | (p.flags & 2u)).hit) unocc += 1.0f;
+        });
+        ao[i] = unocc / float(p.spp > 1u ? p.spp : 1u);
+        total += rays;
+    });
+    if (rays_out) *rays_out = total;
+}
+
+// The AO rays of rq_ao.comp for the listed pixels, in order (ray_pixel[j]:
+// index into `pixels`); pixels at depth >= 1 cast none.
+void orc_ao_depth_rays(const float* depth, const rq_ao_depth_params* prm, const uint32_t* pixels, uint32_t npix,
+                       rq_ray* rays, uint32_t* ray_pixel, uint64_t cap, uint64_t* count) {
+    const rq_ao_depth_params p = *prm;
+    uint64_t n = 0;
+    for (uint32_t i = 0; i < npix; ++i) {
+        const uint32_t pixel = pixels ? pixels[i] : i;
+        V3 P, N;
+        if (!ao_depth_surface(depth, p, pixel % p.width, pixel / p.width, P, N)) continue;
+        ao_depth_rays(p, pixel, P, N, [&](uint32_t, const rq_ray& r) {
+            if (n < cap) {
+                rays[n] = r;
+                ray_pixel[n] = i;
+            }
+            ++n;
+        });
+    }
+    *count = n;
+}
+
+// Refit of a built tree to moved geometry: tris (leaf order, written) from
+// pos/idx through perm, then every binary and 4-wide box as the union of
+// the triangle boxes below it.  The topology (child links, counts) is kept.
+void orc_refit(const float* pos, const uint32_t* idx, const uint32_t* perm, uint32_t n, rq_triangle* tris,
+               rq_bvh2_node* nodes2, uint32_t n2, rq_bvh4_node* nodes4, uint32_t n4) {
+    for (uint32_t i = 0; i < n; ++i) {
+        V3 p0, p1, p2;
+        tri_vertices(pos, 3, idx, perm[i], p0, p1, p2);
+        tris[i] = rq_triangle{{p0.x, p0.y, p0.z, 0.0f}, {p1.x, p1.y, p1.z, 0.0f}, {p2.x, p2.y, p2.z, 0.0f}};
+    }
+    if (nodes2 && n2) refit2(nodes2, tris, 0);
+    if (nodes4 && n4) refit4(nodes4, tris, 0);
+}
+
+// Leaf-order -> input triangle ids by the 9 float bit patterns of every
+// triangle (the reference's SoftwareBVH drops its permutation,
+// common/software_bvh.hpp:60-63).  Returns 0, or 1 when the input
+// triangles are not unique by their bits or a leaf triangle is not found.
+int orc_recover_perm(const rq_triangle* leaf_tris, uint32_t n, const float* pos, const uint32_t* idx, uint32_t ninput,
+                     uint32_t* perm) {
+    struct Key {
+        uint32_t w[9];
+    };
+    auto key_of_input = [&](uint32_t t) {
+        Key k;
+        for (int c = 0; c < 3; ++c) std::memcpy(k.w + 3 * c, pos + 3ull * idx[3ull * t + c], 12);
+        return k;
+    };
+    auto key_of_leaf = [&](uint32_t i) {
+        Key k;
+        std::memcpy(k.w, leaf_tris[i].v0, 12);
+        std::memcpy(k.w + 3, leaf_tris[i].v1, 12);
+        std::memcpy(k.w + 6, leaf_tris[i].v2, 12);
+        return k;
+    };
+    auto less = [](const Key& a, const Key& b) { return std::memcmp(a.w, b.w, 36) < 0; };
+    std::vector<std::pair<Key, uint32_t>> in(ninput);
+    for (uint32_t t = 0; t < ninput; ++t) in[t] = {key_of_input(t), t};
+    std::sort(in.begin(), in.end(), [&](const auto& a, const auto& b) { return less(a.first, b.first); });
+    for (uint32_t t = 1; t < ninput; ++t)
+        if (!less(in[t - 1].first, in[t].first)) return 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        const Key k = key_of_leaf(i);
+        auto it = std::lower_bound(in.begin(), in.end(), k, [&](const auto& a, const Key& b) { return less(a.first, b); });
+        if (it == in.end() || std::memcmp(it->first.w, k.w, 36) != 0) return 1;
+        perm[i] = it->second;
+    }
+    return 0;
+}
+
+// The benchmark workloads' height-field grid, restated from the engine's
+// host generator so the reference arm of the benchmark can build its inputs
+// without the engine: vertices on a (qx+1) x (qy+1) lattice over
+// [x0,x1] x [y0,y1], z = amp sin(freq x) cos(freq y) + N(0, sigma) (SplitMix64
+// draws through Box-Muller in double, rounded to float once); each quad
+// (i, j) gives triangles (v00, v10, v01) and (v10, v11, v01), row-major.
+int orc_scene_grid(uint32_t qx, uint32_t qy, float x0, float x1, float y0, float y1, float amp, float freq,
+                   float sigma, uint64_t seed, float* pos, uint32_t* idx) {
+    if (qx == 0 || qy == 0) return 1;
+    const uint32_t nvx = qx + 1, nvy = qy + 1;
+    if (pos) {
+        SplitMix64 rng{seed};
+        const double two_pi = 6.283185307179586476925286766559;
+        double spare = 0.0;
+        bool have_spare = false;
+        for (uint32_t j = 0; j < nvy; ++j) {
+            const double y = double(y0) + (double(y1) - double(y0)) * double(j) / double(qy);
+            for (uint32_t i = 0; i < nvx; ++i) {
+                const double x = double(x0) + (double(x1) - double(x0)) * double(i) / double(qx);
+                double g;
+                if (have_spare) {
+                    g = spare;
+                    have_spare = false;
+                } else {
+                    const double u1 = rng.uniform(), u2 = rng.uniform();
+                    const double r = std::sqrt(-2.0 * std::log(u1));
+                    g = r * std::cos(two_pi * u2);
+                    spare = r * std::sin(two_pi * u2);
+                    have_spare = true;
+                }
+                const double z = double(amp) * std::sin(double(freq) * x) * std::cos(double(freq) * y) +
+                                 double(sigma) * g;
+                float* p = pos + 3ull * (size_t(j) * nvx + i);
+                p[0] = float(x);
+                p[1] = float(y);
+                p[2] = float(z);
+            }
+        }
+    }
+    if (idx) {
+        uint32_t* o = idx;
+        for (uint32_t j = 0; j < qy; ++j)
+            for (uint32_t i = 0; i < qx; ++i) {
+                const uint32_t v00 = j * nvx + i, v10 = v00 + 1, v01 = v00 + nvx, v11 = v01 + 1;
+                o[0] = v00;
+                o[1] = v10;
+                o[2] = v01;
+                o[3] = v10;
+                o[4] = v11;
+                o[5] = v01;
+                o += 6;
+            }
+    }
+    return 0;
+}
+
+// The benchmark camera (restated from the engine's host helper): right-handed
+// look-at view and a Vulkan perspective (depth 0..1, y flipped, near 0.1,
+// far 100), multiplied and inverted in double, stored column-major as float.
+int orc_camera_look_at(const float eye[3], const float target[3], const float up[3], float fovy_deg, uint32_t width,
+                       uint32_t height, rq_camera* out) {
+    double e[3] = {eye[0], eye[1], eye[2]}, t[3] = {target[0], target[1], target[2]}, u0[3] = {up[0], up[1], up[2]};
+    auto norm = [](double* v) {
+        const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        v[0] /= l;
+        v[1] /= l;
+        v[2] /= l;
+    };
+    auto cross3 = [](const double* a, const double* b, double* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    double f[3] = {t[0] - e[0], t[1] - e[1], t[2] - e[2]};
+    norm(f);
+    double sx[3], ux[3];
+    cross3(f, u0, sx);
+    norm(sx);
+    cross3(sx, f, ux);
+    const double V[4][4] = {{sx[0], ux[0], -f[0], 0}, {sx[1], ux[1], -f[1], 0}, {sx[2], ux[2], -f[2], 0},
+                            {-(sx[0] * e[0] + sx[1] * e[1] + sx[2] * e[2]),
+                             -(ux[0] * e[0] + ux[1] * e[1] + ux[2] * e[2]), f[0] * e[0] + f[1] * e[1] + f[2] * e[2], 1}};
+    const double aspect = double(width) / double(height);
+    const double th = std::tan(double(fovy_deg) * 3.14159265358979323846 / 360.0);
+    const double zn = 0.1, zf = 100.0;
+    const double Pm[4][4] = {{1.0 / (aspect * th), 0, 0, 0},
+                             {0, -1.0 / th, 0, 0},
+                             {0, 0, zf / (zn - zf), -1},
+                             {0, 0, -(zf * zn) / (zf - zn), 0}};
+    double A[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            double acc = 0;
+            for (int k = 0; k < 4; ++k) acc += Pm[k][r] * V[c][k];
+            A[r][c] = acc;
+            A[r][4 + c] = r == c ? 1.0 : 0.0;
+        }
+    for (int col = 0; col < 4; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 4; ++r)
+            if (std::fabs(A[r][col]) > std::fabs(A[piv][col])) piv = r;
+        if (std::fabs(A[piv][col]) < 1e-300) return 1;
+        if (piv != col)
+            for (int k = 0; k < 8; ++k) std::swap(A[piv][k], A[col][k]);
+        const double d = A[col][col];
+        for (int k = 0; k < 8; ++k) A[col][k] /= d;
+        for (int r = 0; r < 4; ++r)
+            if (r != col) {
+                const double m = A[r][col];
+                for (int k = 0; k < 8; ++k) A[r][k] -= m * A[col][k];
+            }
+    }
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r) out->inv_view_proj[4 * c + r] = float(A[r][4 + c]);
+    out->cam_pos[0] = eye[0];
+    out->cam_pos[1] = eye[1];
+    out->cam_pos[2] = eye[2];
+    out->width = width;
+    out->height = height;
+    out->jitter = 0;
+    out->seed = 0;
+    out->tmin = 0.01f;
+    out->tmax = 10000.0f;
+    out->flags = 0;
+    return 0;
 }
 
 }  // extern "C"

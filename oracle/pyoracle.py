@@ -51,7 +51,7 @@ def lib():
         L.orc_collapse4.restype = C.c_int
         L.orc_radv_build.argtypes = [_P, C.c_uint32, _P]
         L.orc_radv_build.restype = C.c_int
-        L.orc_trace_ref_bvh4.argtypes = [_P, _P, _P, C.c_uint32, _P, _P, C.c_int]
+        L.orc_trace_ref_bvh4.argtypes = [_P, _P, _P, C.c_uint32, _P, _P, _P, C.c_int]
         L.orc_trace_ref_bvh2.argtypes = [_P, _P, _P, C.c_uint32, C.c_float, _P, C.c_int]
         L.orc_trace_bvh4.argtypes = [_P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, C.c_int]
         L.orc_trace_radv.argtypes = [_P, _P, C.c_uint32, C.c_uint32, _P, _P, C.c_int]
@@ -62,6 +62,21 @@ def lib():
         L.orc_blur_ao.argtypes = [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_float]
         L.orc_tlas_trace.argtypes = [_P, _P, _P, _P, _P, _P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32,
                                      C.c_uint32, _P, C.c_int]
+        L.orc_render_gbuffer.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, C.c_int]
+        L.orc_render_shadow_ao.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, _P, _P, C.c_int]
+        L.orc_camera_rays.argtypes = [_P, _P, C.c_uint32, _P]
+        L.orc_shade_rays.argtypes = [_P, _P, _P, C.c_uint32, _P, _P, _P, C.c_uint64, _P]
+        L.orc_render_reflect.argtypes = [_P, _P, _P, _P, _P, _P, C.c_uint32, _P, _P, C.c_int]
+        L.orc_render_ao_depth.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, _P, C.c_int]
+        L.orc_ao_depth_rays.argtypes = [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint64, _P]
+        L.orc_refit.argtypes = [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32]
+        L.orc_recover_perm.argtypes = [_P, C.c_uint32, _P, _P, C.c_uint32, _P]
+        L.orc_recover_perm.restype = C.c_int
+        L.orc_scene_grid.argtypes = [C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                     C.c_float, C.c_float, C.c_uint64, _P, _P]
+        L.orc_scene_grid.restype = C.c_int
+        L.orc_camera_look_at.argtypes = [_P, _P, _P, C.c_float, C.c_uint32, C.c_uint32, _P]
+        L.orc_camera_look_at.restype = C.c_int
         _lib = L
     return _lib
 
@@ -150,13 +165,16 @@ def radv_build(tri9):
 
 # ------------------------------------------------------------ traversal --
 
-def trace_ref_bvh4(nodes4, tris, rays):
+def trace_ref_bvh4(nodes4, tris, rays, return_dropped=False):
+    """software_bvh_bvh4.comp as published: (stats, hits[, dropped]) where
+    dropped counts the pushes per ray its 24-entry stack could not hold."""
     rays = np.ascontiguousarray(rays)
     stats = np.empty(len(rays), STATS)
     hits = np.empty(len(rays), HIT)
+    dropped = np.empty(len(rays), np.uint32) if return_dropped else None
     lib().orc_trace_ref_bvh4(_ptr(np.ascontiguousarray(nodes4)), _ptr(np.ascontiguousarray(tris)), _ptr(rays),
-                             len(rays), _ptr(stats), _ptr(hits), threads())
-    return stats, hits
+                             len(rays), _ptr(stats), _ptr(hits), _ptr(dropped), threads())
+    return (stats, hits, dropped) if return_dropped else (stats, hits)
 
 
 def trace_ref_bvh2(nodes2, tris, rays, t_eps=0.001):
@@ -245,10 +263,10 @@ GBUFFER_PX = np.dtype([("pos", "<f4", 3), ("vis", "<u4"), ("nrm", "<f4", 3), ("t
 
 
 def render_gbuffer(nodes4, tris, perm, cam, pixels=None):
-    """cam: an rq.Camera ctypes structure; pixels: uint32 indices or None."""
+    """cam: a Camera (this module's or rq's) ctypes structure; pixels: uint32
+    indices or None."""
     import ctypes as CC
     L = lib()
-    L.orc_render_gbuffer.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, C.c_int]
     npix = cam.width * cam.height if pixels is None else len(pixels)
     out = np.empty(npix, GBUFFER_PX)
     px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
@@ -261,7 +279,6 @@ def render_gbuffer(nodes4, tris, perm, cam, pixels=None):
 def render_shadow_ao(nodes4, tris, gbuf_full, params, pixels=None):
     import ctypes as CC
     L = lib()
-    L.orc_render_shadow_ao.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, _P, _P, C.c_int]
     npix = params.width * params.height if pixels is None else len(pixels)
     mask = np.empty(npix, np.uint32)
     ao = np.empty(npix, np.float32)
@@ -357,16 +374,190 @@ def recover_perm(tris_leaf_order, pos, idx):
     """The reference discards the leaf-order permutation
     (common/software_bvh.hpp:60-63); recover it by matching the 9 float bit
     patterns of every leaf triangle to the input triangles.  Asserts unique."""
-    p = pos.reshape(-1, 3).view(np.uint32)
-    ii = idx.reshape(-1, 3)
-    inp = np.concatenate([p[ii[:, 0]], p[ii[:, 1]], p[ii[:, 2]]], axis=1)  # (n, 9)
-    lt = np.concatenate([tris_leaf_order["v0"][:, :3], tris_leaf_order["v1"][:, :3], tris_leaf_order["v2"][:, :3]],
-                        axis=1).view(np.uint32)
-    key_in = np.ascontiguousarray(inp).view([("k", "V36")]).ravel()
-    key_lt = np.ascontiguousarray(lt).view([("k", "V36")]).ravel()
-    order = np.argsort(key_in, kind="stable")
-    srt = key_in[order]
-    assert len(np.unique(srt)) == len(srt), "input triangles are not unique by vertex bits"
-    pos_in = np.searchsorted(srt, key_lt)
-    assert np.all(srt[pos_in] == key_lt)
-    return order[pos_in].astype(np.uint32)
+    tl = np.ascontiguousarray(tris_leaf_order)
+    pos = np.ascontiguousarray(pos, np.float32).reshape(-1)
+    idx = np.ascontiguousarray(idx, np.uint32).reshape(-1)
+    perm = np.empty(len(tl), np.uint32)
+    rc = lib().orc_recover_perm(_ptr(tl), len(tl), _ptr(pos), _ptr(idx), idx.size // 3, _ptr(perm))
+    assert rc == 0, "input triangles are not unique by vertex bits, or a leaf triangle is not an input triangle"
+    return perm
+
+
+# ------------------------------------------------------- frame ray makers --
+
+class Camera(C.Structure):
+    """rq_camera (include/rq.h)."""
+    _fields_ = [("inv_view_proj", C.c_float * 16), ("cam_pos", C.c_float * 3), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("jitter", C.c_uint32), ("seed", C.c_uint32), ("tmin", C.c_float),
+                ("tmax", C.c_float), ("flags", C.c_uint32)]
+
+
+class Light(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("radius", C.c_float)]
+
+
+class ShadeParams(C.Structure):
+    """rq_shade_params (include/rq.h)."""
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("num_lights", C.c_uint32), ("ao_spp", C.c_uint32),
+                ("ao_tmax", C.c_float), ("ao_tmin", C.c_float), ("ao_bias", C.c_float), ("shadow_tmin", C.c_float),
+                ("shadow_bias", C.c_float), ("flags", C.c_uint32), ("lights", Light * 32)]
+
+
+class ReflectParams(C.Structure):
+    """rq_reflect_params (include/rq.h)."""
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("cam_pos", C.c_float * 3), ("tmin", C.c_float),
+                ("tmax", C.c_float), ("bias", C.c_float), ("flags", C.c_uint32)]
+
+
+class AoDepthParams(C.Structure):
+    """rq_ao_depth_params (include/rq.h)."""
+    _fields_ = [("inv_view_proj", C.c_float * 16), ("cam_pos", C.c_float * 3), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("spp", C.c_uint32), ("max_distance", C.c_float), ("tmin", C.c_float),
+                ("bias", C.c_float), ("flags", C.c_uint32)]
+
+
+def _ref_of(s):
+    return C.cast(C.byref(s), _P)
+
+
+def scene_grid(qx, qy, x0=-1.0, x1=1.0, y0=-1.0, y1=1.0, amp=0.2, freq=3.0, sigma=0.01, seed=0):
+    """The benchmark's height-field grid, generated by the oracle's own copy of
+    the generator: float32 [V,3] positions, uint32 [T,3] indices."""
+    pos = np.empty(((qx + 1) * (qy + 1), 3), np.float32)
+    idx = np.empty((2 * qx * qy, 3), np.uint32)
+    assert lib().orc_scene_grid(qx, qy, x0, x1, y0, y1, amp, freq, sigma, seed, _ptr(pos), _ptr(idx)) == 0
+    return pos, idx
+
+
+def camera_look_at(eye, target, up, fovy_deg, width, height, jitter=False, seed=0, flags=0):
+    cam = Camera()
+    f3 = C.c_float * 3
+    assert lib().orc_camera_look_at(C.cast(f3(*eye), _P), C.cast(f3(*target), _P), C.cast(f3(*up), _P), fovy_deg,
+                                    width, height, _ref_of(cam)) == 0
+    cam.jitter, cam.seed, cam.flags = (1 if jitter else 0), seed, flags
+    return cam
+
+
+def shade_params(width, height, lights, ao_spp=1, ao_tmax=0.5, flags=0):
+    p = ShadeParams()
+    p.width, p.height, p.num_lights, p.ao_spp = width, height, len(lights), ao_spp
+    p.ao_tmax, p.ao_tmin, p.ao_bias = ao_tmax, 0.01, 0.03
+    p.shadow_tmin, p.shadow_bias, p.flags = 0.01, 0.04, flags
+    for k, (x, y, z, r) in enumerate(lights):
+        p.lights[k].pos[0], p.lights[k].pos[1], p.lights[k].pos[2], p.lights[k].radius = x, y, z, r
+    return p
+
+
+def reflect_params(cam, flags=0, tmin=0.02, tmax=100.0, bias=0.04):
+    p = ReflectParams()
+    p.width, p.height = cam.width, cam.height
+    for k in range(3):
+        p.cam_pos[k] = cam.cam_pos[k]
+    p.tmin, p.tmax, p.bias, p.flags = tmin, tmax, bias, flags
+    return p
+
+
+def ao_depth_params(cam, spp=1, max_distance=0.5, flags=0, tmin=0.01, bias=0.03):
+    p = AoDepthParams()
+    for k in range(16):
+        p.inv_view_proj[k] = cam.inv_view_proj[k]
+    for k in range(3):
+        p.cam_pos[k] = cam.cam_pos[k]
+    p.width, p.height, p.spp, p.max_distance = cam.width, cam.height, spp, max_distance
+    p.tmin, p.bias, p.flags = tmin, bias, flags
+    return p
+
+
+# The 1080p shadows + AO frame (the benchmark's headline workload), built
+# here from the oracle's generators so a process can set it up without the
+# engine.  The same constants define it in the engine's workload module; a
+# CPU test checks that both give the same bytes.
+SHADOW_QUADS, SHADOW_SEED = 1118, 1
+SHADOW_EYE, SHADOW_TARGET, SHADOW_UP, SHADOW_FOVY = (0.0, -0.6, 2.6), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 20.0
+
+
+def shadow_lights(n=16, seed=1):
+    rng = np.random.default_rng(seed)
+    xy = rng.uniform(-1.0, 1.0, size=(n, 2))
+    z = rng.uniform(2.0, 2.5, size=n)
+    return [(float(xy[k, 0]), float(xy[k, 1]), float(z[k]), 100.0) for k in range(n)]
+
+
+def shadow_frame_inputs(width=1920, height=1080):
+    """(positions, indices, camera, shade params) of the 1080p frame."""
+    pos, idx = scene_grid(SHADOW_QUADS, SHADOW_QUADS, seed=SHADOW_SEED)
+    cam = camera_look_at(SHADOW_EYE, SHADOW_TARGET, SHADOW_UP, SHADOW_FOVY, width, height)
+    params = shade_params(width, height, shadow_lights(16), ao_spp=1, ao_tmax=0.5)
+    return pos, idx, cam, params
+
+
+def camera_rays(cam, pixels=None):
+    npix = cam.width * cam.height if pixels is None else len(pixels)
+    px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    rays = np.empty(npix, RAY)
+    lib().orc_camera_rays(_ref_of(cam), _ptr(px), npix, _ptr(rays))
+    return rays
+
+
+def shade_rays(gbuf_full, params, pixels):
+    """The frame's secondary rays of the listed pixels, in casting order:
+    (rays, index into pixels, slot: light k or 32 + AO sample)."""
+    g = np.ascontiguousarray(gbuf_full)
+    px = np.ascontiguousarray(pixels, np.uint32)
+    cap = len(px) * (params.num_lights + params.ao_spp)
+    rays = np.empty(max(1, cap), RAY)
+    rpx = np.empty(max(1, cap), np.uint32)
+    slot = np.empty(max(1, cap), np.uint32)
+    cnt = np.zeros(1, np.uint64)
+    lib().orc_shade_rays(_ptr(g), _ref_of(params), _ptr(px), len(px), _ptr(rays), _ptr(rpx), _ptr(slot), cap,
+                         _ptr(cnt))
+    n = int(cnt[0])
+    return rays[:n].copy(), rpx[:n].copy(), slot[:n].copy()
+
+
+def render_reflect(nodes4, tris, perm, gbuf_full, params, pixels=None, want_rays=False):
+    g = np.ascontiguousarray(gbuf_full)
+    npix = params.width * params.height if pixels is None else len(pixels)
+    px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    hits = np.empty(npix, HIT)
+    rays = np.empty(npix, RAY) if want_rays else None
+    lib().orc_render_reflect(_ptr(np.ascontiguousarray(nodes4)), _ptr(np.ascontiguousarray(tris)),
+                             _ptr(None if perm is None else np.ascontiguousarray(perm, np.uint32)), _ptr(g),
+                             _ref_of(params), _ptr(px), npix, _ptr(hits), _ptr(rays), threads())
+    return (hits, rays) if want_rays else hits
+
+
+def render_ao_depth(nodes4, tris, depth, params, pixels=None):
+    d = np.ascontiguousarray(depth, np.float32)
+    npix = params.width * params.height if pixels is None else len(pixels)
+    px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+    ao = np.empty(npix, np.float32)
+    rays = np.zeros(1, np.uint64)
+    lib().orc_render_ao_depth(_ptr(np.ascontiguousarray(nodes4)), _ptr(np.ascontiguousarray(tris)), _ptr(d),
+                              _ref_of(params), _ptr(px), npix, _ptr(ao), _ptr(rays), threads())
+    return ao, int(rays[0])
+
+
+def ao_depth_rays(depth, params, pixels):
+    d = np.ascontiguousarray(depth, np.float32)
+    px = np.ascontiguousarray(pixels, np.uint32)
+    cap = len(px) * max(1, params.spp)
+    rays = np.empty(max(1, cap), RAY)
+    rpx = np.empty(max(1, cap), np.uint32)
+    cnt = np.zeros(1, np.uint64)
+    lib().orc_ao_depth_rays(_ptr(d), _ref_of(params), _ptr(px), len(px), _ptr(rays), _ptr(rpx), cap, _ptr(cnt))
+    n = int(cnt[0])
+    return rays[:n].copy(), rpx[:n].copy()
+
+
+def refit(pos, idx, perm, nodes2, nodes4):
+    """Boxes and leaf triangles of a built tree moved to new vertex
+    positions, topology kept: (tris, nodes2, nodes4) as new arrays."""
+    pos = np.ascontiguousarray(pos, np.float32).reshape(-1)
+    idx = np.ascontiguousarray(idx, np.uint32).reshape(-1)
+    perm = np.ascontiguousarray(perm, np.uint32)
+    n2 = np.array(nodes2, copy=True)
+    n4 = np.array(nodes4, copy=True)
+    tris = np.empty(len(perm), TRIANGLE)
+    lib().orc_refit(_ptr(pos), _ptr(idx), _ptr(perm), len(perm), _ptr(tris), _ptr(n2), len(n2), _ptr(n4), len(n4))
+    return tris, n2, n4

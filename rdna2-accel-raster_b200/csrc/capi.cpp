@@ -217,6 +217,7 @@ int rq_ctx_trace_tuning_set(rq_ctx* ctx, const rq_trace_tuning* t) {
     if (!ctx || !t) return RQ_ERR_INVALID_ARG;
     if (!rq_shade_shape_ok(*t)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
     if (t->refill_min > 32) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "refill_min above 32");
+    if (t->leaf_batch > 32) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "leaf_batch above 32");
     ctx->shade_shape = *t;
     if (ctx->shade_shape.refill_min == 0) ctx->shade_shape.refill_min = 1;
     return RQ_OK;
@@ -553,6 +554,31 @@ int rq_render_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
     return rq_launch_shadow_ao(ctx, bvh, gbuf, *params, light_mask, ao, counters, S(stream));
 }
 
+int rq_render_reflect(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_reflect_params* params,
+                      rq_hit* hits, rq_stream stream) {
+    if (!ctx || !bvh || !gbuf || !params || !hits) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (params->width == 0 || params->height == 0 || (params->flags & ~RQ_TRI_MT))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad reflection parameters");
+    if (!aligned(gbuf, 16) || !aligned(hits, 16)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "misaligned buffer");
+    cudaSetDevice(ctx->device);
+    int rc = frame_checks(ctx, bvh);
+    if (rc) return rc;
+    return rq_launch_reflect(ctx, bvh, gbuf, *params, hits, S(stream));
+}
+
+int rq_render_ao_depth(rq_ctx* ctx, const rq_bvh* bvh, const float* depth, const rq_ao_depth_params* params, float* ao,
+                       unsigned long long* counters, rq_stream stream) {
+    if (!ctx || !bvh || !depth || !params || !ao) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "null argument");
+    if (params->width == 0 || params->height == 0 || params->spp > 32 || (params->flags & ~RQ_TRI_MT))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad AO parameters");
+    if (!aligned(depth, 4) || !aligned(ao, 4) || (counters && !aligned(counters, 8)))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "misaligned buffer");
+    cudaSetDevice(ctx->device);
+    int rc = frame_checks(ctx, bvh);
+    if (rc) return rc;
+    return rq_launch_ao_depth(ctx, bvh, depth, *params, ao, counters, S(stream));
+}
+
 // ---------------------------------------------------------------- RADV
 
 int rq_radv_layout_get(uint32_t n, rq_radv_layout* out) {
@@ -593,6 +619,7 @@ int rq_build_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* 
     if (num_triangles > (1u << 25))
         return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "RADV node offsets are 32-bit: at most 2^25 triangles");
     if (!aligned(as_image, 16)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "image must be 16-byte aligned");
+    if (!aligned(tri9, 4)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "vertex buffer must be 4-byte aligned");
     rq_radv_layout L;
     if (rq_radv_layout_get(num_triangles, &L)) return RQ_ERR_UNSUPPORTED;
     if (as_bytes < L.total_as_size) return rq_set_error(ctx, RQ_ERR_SIZE, "image buffer smaller than rq_radv_size");
@@ -607,6 +634,7 @@ int rq_refit_radv(rq_ctx* ctx, const float* tri9, uint32_t num_triangles, void* 
     if (num_triangles > (1u << 25))
         return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "RADV node offsets are 32-bit: at most 2^25 triangles");
     if (!aligned(as_image, 16)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "image must be 16-byte aligned");
+    if (!aligned(tri9, 4)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "vertex buffer must be 4-byte aligned");
     rq_radv_layout L;
     if (rq_radv_layout_get(num_triangles, &L)) return RQ_ERR_UNSUPPORTED;
     if (as_bytes < L.total_as_size) return rq_set_error(ctx, RQ_ERR_SIZE, "image buffer smaller than rq_radv_size");

@@ -17,7 +17,16 @@
 //               light / escapes sets bit k of its pixel's 64-bit result word
 //               (lights in bits 0..31, AO samples in bits 32..63).
 //  k_shade_finish  result words -> light mask and AO fraction per pixel.
-// No ray or hit buffer touches HBM.
+//  k_reflect    the closest-hit reflection ray of
+//               shaders/tiled_lighting_ra.comp:91-113 per G-buffer pixel,
+//               on the refilling schedule (reflections off a rough surface
+//               scatter), writing one hit record per pixel.
+//  k_ao_depth   the AO rays of shaders/rq_ao.comp:47-97 from a depth buffer:
+//               surface position and normal reconstructed from the pixel's
+//               and its right and upper neighbours' depths, then the
+//               cosine-hemisphere any-hit rays; k_ao_depth_finish turns the
+//               per-pixel result bits into the AO fraction.
+// No ray buffer touches HBM.
 #include "rq_device.cuh"
 #include "rq_internal.h"
 #include "trace_core.cuh"
@@ -213,12 +222,14 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
 // TT threads per block, CHUNK ray ids per refill, REGS: launch bounds that
 // hold registers to REGS (0: none) — the tuned shapes; `stack` rows per lane;
 // idle lanes are refilled once `refill_min` of a warp's lanes are idle.
-template <bool MT, bool STATS, int TT, int CHUNK, int REGS, int TOP, bool SPEC>
+// INLOOP: rays finish and lanes refill inside the node loop (leaf_batch
+// parked leaves end it).
+template <bool MT, bool STATS, int TT, int CHUNK, int REGS, int TOP, bool SPEC, bool INLOOP = false>
 __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     k_shadow_ao(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
                 const rq_gbuffer_px* __restrict__ gbuf, const __grid_constant__ ShadeArgs sa,
                 unsigned long long* words, unsigned long long* counters, uint32_t* ctr, uint32_t* err, int stack,
-                int refill_min) {
+                int refill_min, int leaf_batch) {
     extern __shared__ __align__(16) int32_t s_stack[];
     // shared memory: the stack (stack rows x TT), then the staged top levels
     float4* s_top = reinterpret_cast<float4*>(s_stack + stack * TT);
@@ -230,9 +241,8 @@ __global__ void __launch_bounds__(TT, 65536 / (TT * (REGS ? REGS : 65536 / TT)))
     src.s = &sa;
     src.gbuf = gbuf;
     src.words = words;
-    rq::trace_persistent<1, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK, TOP, SPEC>(nodes, tris, src, ctr,
-                                                                              s_stack + threadIdx.x, err, stack,
-                                                                              s_top, refill_min);
+    rq::trace_persistent<1, MT, STATS, 128, TT, ShadeSrc<STATS>, CHUNK, TOP, SPEC, INLOOP>(
+        nodes, tris, src, ctr, s_stack + threadIdx.x, err, stack, s_top, refill_min, leaf_batch);
     if (counters) {
         const uint32_t r = __reduce_add_sync(rq::kFull, src.rays);
         if ((threadIdx.x & 31u) == 0 && r) atomicAdd(counters, (unsigned long long)r);
@@ -257,6 +267,163 @@ __global__ void __launch_bounds__(256) k_shade_finish(const rq_gbuffer_px* __res
     const bool vis = reinterpret_cast<const uint4*>(gbuf + p)->w != 0u;
     mask[p] = uint32_t(w);
     ao[p] = (vis && spp) ? __uint2float_rn(uint32_t(__popcll(w >> 32))) / __uint2float_rn(spp) : 1.0f;
+}
+
+// ------------------------------------------------------------- reflection
+struct ReflSrc {
+    struct Meta {
+        uint32_t pixel;
+    };
+    uint32_t total;
+    uint32_t tiles_x;
+    uint32_t w, h;
+    float cx, cy, cz, tmin, tmax, bias;
+    const rq_gbuffer_px* gbuf;
+    const uint32_t* perm;
+    rq_hit* hits;
+
+    __device__ bool make(uint32_t id, rq::Ray& r, Meta& m) const {
+        uint32_t pixel;
+        if (!tile_pixel(id >> 5, id & 31u, tiles_x, w, h, pixel)) return false;
+        const float4* gp = reinterpret_cast<const float4*>(gbuf + pixel);
+        const float4 g0 = __ldg(gp);
+        if (__float_as_uint(g0.w) == 0u) {  // no surface: the shader casts nothing
+            reinterpret_cast<uint4*>(hits)[pixel] = make_uint4(0u, __float_as_uint(-1.0f), 0xffffffffu, 0xffffffffu);
+            return false;
+        }
+        const float4 g1 = __ldg(gp + 1);
+        const rq::F3 P{g0.x, g0.y, g0.z}, N{g1.x, g1.y, g1.z};
+        const rq::F3 V = rq::f3norm(rq::f3sub(P, rq::F3{cx, cy, cz}));
+        const float k = 2.0f * rq::f3dot(N, V);  // reflect(V, N) = V - 2 dot(N, V) N
+        r.d = rq::F3{V.x - k * N.x, V.y - k * N.y, V.z - k * N.z};
+        r.o = rq::F3{P.x + N.x * bias, P.y + N.y * bias, P.z + N.z * bias};
+        r.tmin = tmin;
+        r.tmax = tmax;
+        m.pixel = pixel;
+        return true;
+    }
+
+    __device__ void finish(uint32_t, const Meta& m, const rq::Ray&, const rq::Hit& h) const {
+        const uint4 rec = h.hit ? make_uint4(1u, __float_as_uint(h.t), 0u, perm ? __ldg(perm + h.idx) : h.idx)
+                                : make_uint4(0u, __float_as_uint(-1.0f), 0xffffffffu, 0xffffffffu);
+        reinterpret_cast<uint4*>(hits)[m.pixel] = rec;
+    }
+};
+
+template <bool MT, int TT, int REGS>
+__global__ void __launch_bounds__(TT, 65536 / (TT * REGS))
+    k_reflect(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
+              const __grid_constant__ ReflSrc src0, uint32_t* ctr, uint32_t* err, int stack) {
+    extern __shared__ __align__(16) int32_t s_stack[];
+    ReflSrc src = src0;
+    rq::trace_persistent<0, MT, false, 128, TT, ReflSrc>(nodes, tris, src, ctr, s_stack + threadIdx.x, err, stack);
+}
+
+// ------------------------------------------------------------ AO from depth
+struct AoDepthArgs {
+    float m[16];
+    float cx, cy, cz;
+    uint32_t w, h, spp;  // spp >= 1
+    float maxd, tmin, bias;
+};
+
+// inv_view_proj * (u*2-1, v*2-1, d, 1), divided by w.
+__device__ __forceinline__ rq::F3 unproject(const float* m, float u, float v, float d) {
+    const float n[4] = {u * 2.0f - 1.0f, v * 2.0f - 1.0f, d, 1.0f};
+    float o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = ((m[k] * n[0] + m[4 + k] * n[1]) + m[8 + k] * n[2]) + m[12 + k] * n[3];
+    return rq::F3{o[0] / o[3], o[1] / o[3], o[2] / o[3]};
+}
+
+// rq_ao.comp:51-68: position from the depth at the pixel centre, normal from
+// the right and upper neighbours (depth clamped at the edge), turned toward
+// the camera.  False where depth >= 1.
+__device__ __forceinline__ bool depth_surface(const AoDepthArgs& a, const float* __restrict__ depth, uint32_t px,
+                                              uint32_t py, rq::F3& P, rq::F3& N) {
+    const float d = __ldg(depth + size_t(py) * a.w + px);
+    if (d >= 1.0f) return false;
+    const float fw = __uint2float_rn(a.w), fh = __uint2float_rn(a.h);
+    const float u = (__uint2float_rn(px) + 0.5f) / fw, v = (__uint2float_rn(py) + 0.5f) / fh;
+    const float tx = 1.0f / fw, ty = 1.0f / fh;
+    const float dr = __ldg(depth + size_t(py) * a.w + (px + 1 < a.w ? px + 1 : a.w - 1));
+    const float du = __ldg(depth + size_t(py + 1 < a.h ? py + 1 : a.h - 1) * a.w + px);
+    P = unproject(a.m, u, v, d);
+    const rq::F3 pr = unproject(a.m, u + tx, v, dr);
+    const rq::F3 pu = unproject(a.m, u, v + ty, du);
+    N = rq::f3norm(rq::f3cross(rq::f3sub(pr, P), rq::f3sub(pu, P)));
+    if (rq::f3dot(N, rq::f3sub(rq::F3{a.cx, a.cy, a.cz}, P)) < 0.0f) N = {-N.x, -N.y, -N.z};
+    return true;
+}
+
+struct AoDepthSrc {
+    struct Meta {
+        uint32_t pixel, bit;
+    };
+    uint32_t total;
+    uint32_t tiles_x;
+    const AoDepthArgs* a;
+    const float* depth;
+    uint32_t* words;
+    uint32_t rays = 0;
+
+    // id = ((tile * spp + sample) << 5) | pixel in the 8x4 tile
+    __device__ bool make(uint32_t id, rq::Ray& r, Meta& m) {
+        const uint32_t q = id >> 5, k = q % a->spp;
+        uint32_t pixel;
+        if (!tile_pixel(q / a->spp, id & 31u, tiles_x, a->w, a->h, pixel)) return false;
+        rq::F3 P, N;
+        if (!depth_surface(*a, depth, pixel % a->w, pixel / a->w, P, N)) return false;
+        m.pixel = pixel;
+        m.bit = k;
+        r.o = rq::F3{P.x + N.x * a->bias, P.y + N.y * a->bias, P.z + N.z * a->bias};
+        r.d = hemisphere(N, pixel, k);
+        r.tmin = a->tmin;
+        r.tmax = a->maxd;
+        ++rays;
+        return true;
+    }
+
+    __device__ void finish(uint32_t, const Meta& m, const rq::Ray&, const rq::Hit& h) {
+        if (!h.hit) atomicOr(words + m.pixel, 1u << m.bit);
+    }
+};
+
+template <bool MT, int TT, int REGS>
+__global__ void __launch_bounds__(TT, 65536 / (TT * REGS))
+    k_ao_depth(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
+               const float* __restrict__ depth, const __grid_constant__ AoDepthArgs a, uint32_t* words,
+               unsigned long long* counters, uint32_t* ctr, uint32_t* err, int stack) {
+    extern __shared__ __align__(16) int32_t s_stack[];
+    AoDepthSrc src;
+    src.tiles_x = (a.w + kTileW - 1) / kTileW;
+    src.total = src.tiles_x * ((a.h + kTileH - 1) / kTileH) * a.spp * 32u;
+    src.a = &a;
+    src.depth = depth;
+    src.words = words;
+    rq::trace_persistent<1, MT, false, 128, TT, AoDepthSrc>(nodes, tris, src, ctr, s_stack + threadIdx.x, err, stack);
+    if (counters) {
+        const uint32_t r = __reduce_add_sync(rq::kFull, src.rays);
+        if ((threadIdx.x & 31u) == 0 && r) atomicAdd(counters, (unsigned long long)r);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_ao_depth_finish(const float* __restrict__ depth,
+                                                         const uint32_t* __restrict__ words, uint32_t npix,
+                                                         uint32_t spp, float* __restrict__ ao) {
+    const uint32_t p = blockIdx.x * 256 + threadIdx.x;
+    if (p >= npix) return;
+    ao[p] = __ldg(depth + p) >= 1.0f ? 1.0f : __uint2float_rn(uint32_t(__popc(words[p]))) / __uint2float_rn(spp);
+}
+
+// Grid of a persistent traversal kernel: every SM filled to its occupancy.
+cudaError_t persistent_grid(rq_ctx* ctx, const void* k, int threads, size_t smem, uint32_t& blocks) {
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+    blocks = uint32_t(ctx->num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+    return e;
 }
 
 template <class F>
@@ -292,9 +459,28 @@ const void* shade_kernel(const rq_trace_tuning& t) {
     return nullptr;
 }
 
+// Shapes with in-loop refill (speculative, leaf_batch > 0).
+template <bool MT, bool STATS>
+const void* shade_kernel_inloop(const rq_trace_tuning& t) {
+#define RQ_SHAPE(T, C, R)                                                                      \
+    if (t.threads == T && t.chunk == C && t.reg_cap == R && t.top_levels == 0 && t.speculative) \
+        return reinterpret_cast<const void*>(k_shadow_ao<MT, STATS, T, C, R, 0, true, true>);
+    if constexpr (!MT && !STATS) {
+        RQ_SHAPE(64, 32, 64) RQ_SHAPE(64, 64, 64) RQ_SHAPE(128, 32, 64) RQ_SHAPE(128, 64, 64) RQ_SHAPE(256, 32, 64)
+        RQ_SHAPE(256, 64, 64) RQ_SHAPE(128, 64, 72) RQ_SHAPE(256, 64, 72)
+    }
+#undef RQ_SHAPE
+    return nullptr;
+}
+
+template <bool MT, bool STATS>
+const void* shade_kernel_any(const rq_trace_tuning& t) {
+    return t.leaf_batch ? shade_kernel_inloop<MT, STATS>(t) : shade_kernel<MT, STATS>(t);
+}
+
 }  // namespace
 
-bool rq_shade_shape_ok(const rq_trace_tuning& t) { return shade_kernel<false, false>(t) != nullptr; }
+bool rq_shade_shape_ok(const rq_trace_tuning& t) { return shade_kernel_any<false, false>(t) != nullptr; }
 
 int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_gbuffer_px* gbuf, cudaStream_t st) {
     GbufSrc src;
@@ -362,10 +548,10 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
     if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
     if (e == cudaSuccess && p.num_lights + p.ao_spp > 0) {
         // the counting and reference-arithmetic variants run in the default shape
-        const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0, 0, 1} : ctx->shade_shape;
+        const rq_trace_tuning shape = (mt || stats) ? rq_trace_tuning{128, 32, 0, 0, 0, 1, 0} : ctx->shade_shape;
         const size_t top_bytes = shape.top_levels == 4 ? rq::TopLevels<4>::kBytes : 0;
-        const void* k = mt ? (stats ? shade_kernel<true, true>(shape) : shade_kernel<true, false>(shape))
-                           : (stats ? shade_kernel<false, true>(shape) : shade_kernel<false, false>(shape));
+        const void* k = mt ? (stats ? shade_kernel_any<true, true>(shape) : shade_kernel_any<true, false>(shape))
+                           : (stats ? shade_kernel_any<false, true>(shape) : shade_kernel_any<false, false>(shape));
         if (!k) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "no traversal kernel for this shape");
         // stack rows: the bound for the tree's depth, rounded up to 4
         const int stack = int((bound + 3u) & ~3u);
@@ -379,8 +565,9 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
             const rq_triangle* tris = bvh->tris;
             uint32_t* err = ctx->d_err;
             int refill_min = int(shape.refill_min ? shape.refill_min : 1u);
+            int leaf_batch = int(shape.leaf_batch ? shape.leaf_batch : 32u);
             void* args[] = {&nodes, &tris, &gbuf, &s, &words, &counter, &ctr, &err, const_cast<int*>(&stack),
-                            &refill_min};
+                            &refill_min, &leaf_batch};
             e = cudaLaunchKernel(k, dim3(blocks), dim3(shape.threads), args, smem, st);
         }
     }
@@ -389,4 +576,89 @@ int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbu
         e = cudaGetLastError();
     }
     return rq_cuda_status(ctx, e, "shadow/AO launch");
+}
+
+// Launch shapes of the reflection and depth-AO traversals: 128-thread
+// blocks held to 64 registers (8 blocks, 32 warps per SM).
+constexpr int kReflThreads = 128, kReflRegs = 64;
+constexpr int kAoThreads = 128, kAoRegs = 64;
+
+int rq_launch_reflect(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_reflect_params& p,
+                      rq_hit* hits, cudaStream_t st) {
+    ReflSrc src;
+    src.w = p.width;
+    src.h = p.height;
+    src.tiles_x = (p.width + kTileW - 1) / kTileW;
+    src.total = src.tiles_x * ((p.height + kTileH - 1) / kTileH) * 32u;
+    src.cx = p.cam_pos[0];
+    src.cy = p.cam_pos[1];
+    src.cz = p.cam_pos[2];
+    src.tmin = p.tmin;
+    src.tmax = p.tmax;
+    src.bias = p.bias;
+    src.gbuf = gbuf;
+    src.perm = bvh->perm;
+    src.hits = hits;
+    const uint32_t bound = 3u * (bvh->h_counts[2] + 2u) + 1u;
+    const int stack = int((bound + 3u) & ~3u);
+    const bool mt = p.flags & RQ_TRI_MT;
+    const void* k = mt ? reinterpret_cast<const void*>(k_reflect<true, kReflThreads, kReflRegs>)
+                       : reinterpret_cast<const void*>(k_reflect<false, kReflThreads, kReflRegs>);
+    const size_t smem = size_t(stack) * kReflThreads * sizeof(int32_t);
+    uint32_t blocks = 0;
+    cudaError_t e = cudaMemsetAsync(ctx->d_ctr, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = persistent_grid(ctx, k, kReflThreads, smem, blocks);
+    if (e == cudaSuccess) {
+        const rq_bvh4_node* nodes = bvh->nodes4;
+        const rq_triangle* tris = bvh->tris;
+        uint32_t* ctr = ctx->d_ctr;
+        uint32_t* err = ctx->d_err;
+        int stk = stack;
+        void* args[] = {&nodes, &tris, &src, &ctr, &err, &stk};
+        e = cudaLaunchKernel(k, dim3(blocks), dim3(kReflThreads), args, smem, st);
+    }
+    return rq_cuda_status(ctx, e, "reflection launch");
+}
+
+int rq_launch_ao_depth(rq_ctx* ctx, const rq_bvh* bvh, const float* depth, const rq_ao_depth_params& p, float* ao,
+                       unsigned long long* counters, cudaStream_t st) {
+    AoDepthArgs a;
+    for (int i = 0; i < 16; ++i) a.m[i] = p.inv_view_proj[i];
+    a.cx = p.cam_pos[0];
+    a.cy = p.cam_pos[1];
+    a.cz = p.cam_pos[2];
+    a.w = p.width;
+    a.h = p.height;
+    a.spp = p.spp > 1u ? p.spp : 1u;  // rq_ao.comp:71: max(1u, samplesPerPixel)
+    a.maxd = p.max_distance;
+    a.tmin = p.tmin;
+    a.bias = p.bias;
+    const uint32_t npix = p.width * p.height;
+    int rc = rq_ensure_scratch(ctx, sizeof(uint32_t) * size_t(npix) + 256, st);
+    if (rc) return rc;
+    uint32_t* words = static_cast<uint32_t*>(ctx->scratch);
+    const uint32_t bound = 3u * (bvh->h_counts[2] + 2u) + 1u;
+    const int stack = int((bound + 3u) & ~3u);
+    const bool mt = p.flags & RQ_TRI_MT;
+    const void* k = mt ? reinterpret_cast<const void*>(k_ao_depth<true, kAoThreads, kAoRegs>)
+                       : reinterpret_cast<const void*>(k_ao_depth<false, kAoThreads, kAoRegs>);
+    const size_t smem = size_t(stack) * kAoThreads * sizeof(int32_t);
+    uint32_t blocks = 0;
+    cudaError_t e = cudaMemsetAsync(words, 0, sizeof(uint32_t) * size_t(npix), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_ctr, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = persistent_grid(ctx, k, kAoThreads, smem, blocks);
+    if (e == cudaSuccess) {
+        const rq_bvh4_node* nodes = bvh->nodes4;
+        const rq_triangle* tris = bvh->tris;
+        uint32_t* ctr = ctx->d_ctr;
+        uint32_t* err = ctx->d_err;
+        int stk = stack;
+        void* args[] = {&nodes, &tris, &depth, &a, &words, &counters, &ctr, &err, &stk};
+        e = cudaLaunchKernel(k, dim3(blocks), dim3(kAoThreads), args, smem, st);
+    }
+    if (e == cudaSuccess) {
+        k_ao_depth_finish<<<(npix + 255) / 256, 256, 0, st>>>(depth, words, npix, a.spp, ao);
+        e = cudaGetLastError();
+    }
+    return rq_cuda_status(ctx, e, "depth AO launch");
 }

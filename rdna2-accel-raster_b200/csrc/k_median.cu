@@ -20,8 +20,14 @@
 // leaf offsets and counts equal the reference's; the order inside a leaf
 // (left unspecified by nth_element) is the x order.  Sizes and boxes then
 // go bottom-up and pre-order positions top-down, level by level.
+//
+// Everything is stream-ordered (no host synchronisation, so the build can be
+// captured in a CUDA graph): splits at mid give children of floor and ceil
+// half the count, so the host knows from n and max_leaf alone the deepest
+// level a split can reach; it launches every level up to there, and each
+// kernel reads the level's frontier size and node range from device memory
+// (levels past the tree's real depth find nothing to do).
 #include <algorithm>
-#include <vector>
 
 #include "build_core.cuh"
 #include "rq_device.cuh"
@@ -55,7 +61,9 @@ struct MedScratch {
     uint32_t* nsize;    // nodes in the subtree
     uint32_t* npre;     // pre-order position
     float4* nbox;       // 2 per node
-    uint32_t* ctl;      // [0] node count, [1] next frontier size
+    uint32_t* ctl;      // [0] node count
+    uint32_t* fcount;   // kMaxLevels + 1: frontier size of each level
+    uint32_t* lstart;   // kMaxLevels + 2: first node id of each level
 };
 
 size_t carve_med(uintptr_t base, uint32_t n, MedScratch& m) {
@@ -81,6 +89,8 @@ size_t carve_med(uintptr_t base, uint32_t n, MedScratch& m) {
     m.npre = c.take<uint32_t>(M);
     m.nbox = c.take<float4>(2 * M);
     m.ctl = c.take<uint32_t>(8);
+    m.fcount = c.take<uint32_t>(kMaxLevels + 1);
+    m.lstart = c.take<uint32_t>(kMaxLevels + 2);
     return c.off + 256;
 }
 
@@ -116,20 +126,24 @@ __global__ void __launch_bounds__(kT) k_med_keys(const float4* __restrict__ cent
 
 __global__ void __launch_bounds__(kT) k_med_init(uint32_t n, MedScratch m) {
     for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) m.pos_seg[i] = 0;
+    for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < kMaxLevels + 1; i += gridDim.x * kT) m.fcount[i] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         m.front[0][0] = Seg{0u, n, 0u};
         m.ns[0] = 0;
         m.ne[0] = n;
         m.ctl[0] = 1;
-        m.ctl[1] = 0;
+        m.fcount[0] = 1;
+        m.lstart[0] = 0;
+        m.lstart[1] = 1;
     }
 }
 
-// One frontier node: leaf, or split on the longest centroid axis at mid.
-__global__ void __launch_bounds__(kT) k_med_decide(const Seg* __restrict__ cur, uint32_t nf, uint32_t max_leaf,
+// One frontier node of level L: leaf, or split on the longest centroid axis
+// at mid.  The level's frontier size is fcount[L]; children go to level L+1.
+__global__ void __launch_bounds__(kT) k_med_decide(const Seg* __restrict__ cur, uint32_t L, uint32_t max_leaf,
                                                    const float4* __restrict__ cent, MedScratch m, Seg* next) {
     const uint32_t j = blockIdx.x * kT + threadIdx.x;
-    if (j >= nf) return;
+    if (j >= m.fcount[L]) return;
     const Seg g = cur[j];
     m.seg_split[j] = 0;
     const uint32_t cnt = g.e - g.s;
@@ -162,7 +176,7 @@ __global__ void __launch_bounds__(kT) k_med_decide(const Seg* __restrict__ cur, 
     m.ne[id] = mid;
     m.ns[id + 1] = mid;
     m.ne[id + 1] = g.e;
-    const uint32_t f = atomicAdd(m.ctl + 1, 2u);
+    const uint32_t f = atomicAdd(m.fcount + L + 1, 2u);
     next[f] = Seg{g.s, mid, id};
     next[f + 1] = Seg{mid, g.e, id + 1};
     m.seg_axis[j] = axis;
@@ -202,7 +216,10 @@ __global__ void __launch_bounds__(kT) k_med_scatter(uint32_t n, const uint32_t* 
     }
 }
 
-__global__ void __launch_bounds__(kT) k_med_posseg(uint32_t n, MedScratch m) {
+// Positions move to their child segment (or leave the frontier); the nodes
+// level L's splits created end at the node count, which starts level L+2.
+__global__ void __launch_bounds__(kT) k_med_posseg(uint32_t n, uint32_t L, MedScratch m) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) m.lstart[L + 2] = m.ctl[0];
     for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
         const int32_t j = m.pos_seg[i];
         if (j < 0) continue;
@@ -213,11 +230,12 @@ __global__ void __launch_bounds__(kT) k_med_posseg(uint32_t n, MedScratch m) {
     }
 }
 
-// Nodes [lo, hi) of one level: subtree sizes and boxes from the level below.
-__global__ void __launch_bounds__(kT) k_med_up(uint32_t lo, uint32_t hi, MedScratch m,
-                                               const float4* __restrict__ pbox, uint32_t* counts) {
-    const uint32_t v = lo + blockIdx.x * kT + threadIdx.x;
-    if (v >= hi) return;
+// Nodes of level L, [lstart[L], lstart[L+1]): subtree sizes and boxes from
+// the level below.
+__global__ void __launch_bounds__(kT) k_med_up(uint32_t L, MedScratch m, const float4* __restrict__ pbox,
+                                               uint32_t* counts) {
+    const uint32_t v = m.lstart[L] + blockIdx.x * kT + threadIdx.x;
+    if (v >= m.lstart[L + 1]) return;
     float4 a, b;
     if (m.nl[v] < 0) {
         a = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
@@ -241,16 +259,16 @@ __global__ void __launch_bounds__(kT) k_med_up(uint32_t lo, uint32_t hi, MedScra
     m.nbox[2 * v + 1] = b;
 }
 
-__global__ void __launch_bounds__(kT) k_med_down(uint32_t lo, uint32_t hi, MedScratch m) {
-    const uint32_t v = lo + blockIdx.x * kT + threadIdx.x;
-    if (v >= hi || m.nl[v] < 0) return;
+__global__ void __launch_bounds__(kT) k_med_down(uint32_t L, MedScratch m) {
+    const uint32_t v = m.lstart[L] + blockIdx.x * kT + threadIdx.x;
+    if (v >= m.lstart[L + 1] || m.nl[v] < 0) return;
     const uint32_t l = uint32_t(m.nl[v]), r = uint32_t(m.nr[v]);
     m.npre[l] = m.npre[v] + 1;
     m.npre[r] = m.npre[v] + 1 + m.nsize[l];
 }
 
-__global__ void __launch_bounds__(kT) k_med_emit(uint32_t nodes, MedScratch m, rq_bvh2_node* __restrict__ out,
-                                                 uint32_t* counts) {
+__global__ void __launch_bounds__(kT) k_med_emit(MedScratch m, rq_bvh2_node* __restrict__ out, uint32_t* counts) {
+    const uint32_t nodes = m.ctl[0];
     for (uint32_t v = blockIdx.x * kT + threadIdx.x; v < nodes; v += gridDim.x * kT) {
         const bool leaf = m.nl[v] < 0;
         const int32_t lc = leaf ? int32_t(~m.ns[v]) : int32_t(m.npre[m.nl[v]]);
@@ -307,12 +325,20 @@ int rq_launch_build_median(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t 
     }
     if (e != cudaSuccess) return rq_cuda_status(ctx, e, "median build setup");
     k_med_init<<<g, kT, 0, st>>>(n, m);
-    // top-down, one level per round; the host reads the frontier size
-    std::vector<uint32_t> level_start{0u, 1u};
-    uint32_t nf = 1, cur = 0, ctl[2] = {1u, 0u};
-    for (uint32_t level = 0; nf > 0; ++level) {
-        if (level >= kMaxLevels) return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "median tree deeper than 96 levels");
-        k_med_decide<<<(nf + kT - 1) / kT, kT, 0, st>>>(m.front[cur], nf, max_leaf, s.cent, m, m.front[cur ^ 1]);
+    // the deepest level a split can reach: children hold floor and ceil
+    // half their parent's count, so the largest count of level L is n halved
+    // (rounded up) L times; the level whose largest count fits a leaf is the
+    // last one
+    uint32_t levels = 1;
+    for (uint32_t c = n; c > max_leaf; c = (c + 1) / 2) ++levels;
+    if (levels > kMaxLevels) return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "median tree deeper than 96 levels");
+    // widest possible frontier / level of level L: min(2^L, n) segments
+    auto width = [&](uint32_t L) { return L >= 31 ? n : std::min(n, 1u << L); };
+    // top-down, one level per round, no host synchronisation
+    uint32_t cur = 0;
+    for (uint32_t L = 0; L < levels; ++L) {
+        k_med_decide<<<(width(L) + kT - 1) / kT, kT, 0, st>>>(m.front[cur], L, max_leaf, s.cent, m,
+                                                              m.front[cur ^ 1]);
         k_med_flags<<<g, kT, 0, st>>>(n, m);
         for (int a = 0; a < 3; ++a) {
             // exclusive scan of the membership flags in this axis's order
@@ -321,28 +347,18 @@ int rq_launch_build_median(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t 
             k_med_scatter<<<g, kT, 0, st>>>(n, m.order[a], m.alt[a], m.front[cur], m);
             std::swap(m.order[a], m.alt[a]);
         }
-        k_med_posseg<<<g, kT, 0, st>>>(n, m);
-        e = cudaMemcpyAsync(ctl, m.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(m.ctl + 1, 0, sizeof(uint32_t), st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return rq_cuda_status(ctx, e, "median build level");
-        nf = ctl[1];
-        level_start.push_back(ctl[0]);
+        k_med_posseg<<<g, kT, 0, st>>>(n, L, m);
         cur ^= 1u;
     }
-    const uint32_t nodes = ctl[0];
-    // bottom-up sizes and boxes, top-down pre-order positions
-    const size_t levels = level_start.size() - 1;
-    for (size_t L = levels; L-- > 0;) {
-        const uint32_t lo = level_start[L], hi = level_start[L + 1];
-        if (hi > lo) k_med_up<<<(hi - lo + kT - 1) / kT, kT, 0, st>>>(lo, hi, m, s.box_lf, bvh->d_counts);
-    }
+    // bottom-up sizes and boxes, top-down pre-order positions (nodes lie on
+    // levels 0 .. levels-1, at most min(2^L, n) on level L; a level past the
+    // tree's real depth is empty)
+    for (uint32_t L = levels; L-- > 0;)
+        k_med_up<<<(width(L) + kT - 1) / kT, kT, 0, st>>>(L, m, s.box_lf, bvh->d_counts);
     e = cudaMemsetAsync(m.npre, 0, sizeof(uint32_t), st);
-    for (size_t L = 0; L < levels && e == cudaSuccess; ++L) {
-        const uint32_t lo = level_start[L], hi = level_start[L + 1];
-        if (hi > lo) k_med_down<<<(hi - lo + kT - 1) / kT, kT, 0, st>>>(lo, hi, m);
-    }
-    k_med_emit<<<grid(nodes, sms), kT, 0, st>>>(nodes, m, bvh->nodes2, bvh->d_counts);
+    for (uint32_t L = 0; L < levels && e == cudaSuccess; ++L)
+        k_med_down<<<(width(L) + kT - 1) / kT, kT, 0, st>>>(L, m);
+    k_med_emit<<<grid(2 * n, sms), kT, 0, st>>>(m, bvh->nodes2, bvh->d_counts);
     k_med_tris<<<g, kT, 0, st>>>(pos, sf, idx, n, m.order[0], bvh->tris, bvh->perm);
     rc = rq_cuda_status(ctx, e == cudaSuccess ? cudaGetLastError() : e, "median build");
     if (rc) return rc;

@@ -20,7 +20,6 @@
 // subtrees are 64 leaf boxes (a 4,096-triangle image is 16 blocks of one
 // round), from 4,194,304 on 1024, 256 between.
 #include <algorithm>
-#include <mutex>
 
 #include "rq_device.cuh"
 #include "rq_internal.h"
@@ -497,17 +496,18 @@ __global__ void __launch_bounds__(kT, LB == 256 ? 6 : 4) k_radv(RadvArgs A) {
     }
 }
 
-void launch_radv(const RadvArgs& a, uint32_t leaf_cnt, cudaStream_t st) {
+// Launches the build; returns this launch's own error (cudaLaunchKernel
+// reports the launch it was given, not an earlier call's pending error).
+cudaError_t launch_radv(const RadvArgs& a, uint32_t leaf_cnt, cudaStream_t st) {
     const uint32_t lb = radv_leaf_boxes(leaf_cnt);
     const uint32_t blocks = radv_blocks(leaf_cnt, lb);
-    if (lb == 1024u)
-        k_radv<1024, true><<<blocks, kT, 0, st>>>(a);
-    else if (lb == 256u)
-        k_radv<256, true><<<blocks, kT, 0, st>>>(a);
-    else if (blocks > 1)
-        k_radv<64, true><<<blocks, kT, 0, st>>>(a);
-    else
-        k_radv<64, false><<<1, kT, 0, st>>>(a);
+    const void* k = lb == 1024u  ? reinterpret_cast<const void*>(k_radv<1024, true>)
+                    : lb == 256u ? reinterpret_cast<const void*>(k_radv<256, true>)
+                    : blocks > 1 ? reinterpret_cast<const void*>(k_radv<64, true>)
+                                 : reinterpret_cast<const void*>(k_radv<64, false>);
+    RadvArgs arg = a;
+    void* args[] = {&arg};
+    return cudaLaunchKernel(k, dim3(blocks), dim3(kT), args, 0, st);
 }
 
 }  // namespace
@@ -522,7 +522,12 @@ void launch_radv(const RadvArgs& a, uint32_t leaf_cnt, cudaStream_t st) {
 // device array below, sized for at most RQ_RADV_NOALLOC_MAX_TRIANGLES
 // triangles (256 KiB).  Every GPU that loads librq.so holds the array until
 // the process exits.  The array starts at zero and every build leaves the
-// ticket at zero.
+// ticket at zero.  Host code cannot pass the array's name to a kernel (on
+// the host it names a stand-in, not device memory), so every call looks up
+// the array's device address on the current device with
+// cudaGetSymbolAddress, which allocates nothing.  Looking it up each time
+// (rather than caching it per device) stays right after a device reset,
+// which gives the array a new address.
 // The most blocks a build of at most RQ_RADV_NOALLOC_MAX_TRIANGLES takes:
 // 1024-leaf-box subtrees at the largest size, fewer than 4 * kLargeBlocksMin
 // of 256 leaf boxes, or at most kSmallBlocksMax of 64.
@@ -530,35 +535,22 @@ constexpr uint32_t kNoallocBlocks = std::max<uint32_t>(
     {(RQ_RADV_NOALLOC_MAX_TRIANGLES / 4 + 1023u) / 1024u, 4 * kLargeBlocksMin, kSmallBlocksMax});
 static __device__ __align__(256) unsigned char rq_radv_noalloc_scratch[256 + 4 * sizeof(float4) * kNoallocBlocks];
 
-namespace {
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[256] = {};  // device address of the array, per device ordinal
-}  // namespace
-
 extern "C" int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, void* as_image, uint64_t as_bytes,
                                      rq_stream stream) {
     if (!tri9 || !as_image || num_triangles == 0) return RQ_ERR_INVALID_ARG;
     if (num_triangles > RQ_RADV_NOALLOC_MAX_TRIANGLES) return RQ_ERR_UNSUPPORTED;
-    if (reinterpret_cast<uintptr_t>(as_image) & 15u) return RQ_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(as_image) & 15u) || (reinterpret_cast<uintptr_t>(tri9) & 3u))
+        return RQ_ERR_INVALID_ARG;
     rq_radv_layout L;
     if (rq_radv_layout_get(num_triangles, &L) != RQ_OK) return RQ_ERR_UNSUPPORTED;
     if (as_bytes < L.total_as_size) return RQ_ERR_SIZE;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return RQ_ERR_NO_DEVICE;
+    // the array's device address on the current device (the first call on a
+    // device, or after a reset, also loads the library's device code there)
     void* base = nullptr;
-    {
-        // set-up once per device, with that device current: the host-side
-        // name of the array is not a device address
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, rq_radv_noalloc_scratch) != cudaSuccess || !p) {
-                cudaGetLastError();
-                return RQ_ERR_CUDA;
-            }
-            g_noalloc_ptr[dev] = p;
-        }
-        base = g_noalloc_ptr[dev];
+    const cudaError_t ge = cudaGetSymbolAddress(&base, rq_radv_noalloc_scratch);
+    if (ge != cudaSuccess || !base) {
+        if (ge == cudaErrorNoDevice || ge == cudaErrorInsufficientDriver) return RQ_ERR_NO_DEVICE;
+        return RQ_ERR_CUDA;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     RadvArgs a;
@@ -575,9 +567,7 @@ extern "C" int rq_build_radv_noalloc(const float* tri9, uint32_t num_triangles, 
     a.top = reinterpret_cast<float4*>(static_cast<char*>(base) + 256);
     a.size = L.total_as_size;
     const uint32_t leaf_cnt = L.level_counts[L.num_levels - 1];
-    launch_radv(a, leaf_cnt, st);
-    if (cudaGetLastError() != cudaSuccess) return RQ_ERR_CUDA;
-    return RQ_OK;
+    return launch_radv(a, leaf_cnt, st) == cudaSuccess ? RQ_OK : RQ_ERR_CUDA;
 }
 
 int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st,
@@ -602,8 +592,7 @@ int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const 
     a.size = L.total_as_size;
     a.check_header = refit ? 1u : 0u;
     a.err = ctx->d_err;
-    launch_radv(a, leaf_cnt, st);
-    return rq_cuda_status(ctx, cudaGetLastError(), "radv build launch");
+    return rq_cuda_status(ctx, launch_radv(a, leaf_cnt, st), "radv build launch");
 }
 
 // ------------------------------------------------------------ validation

@@ -37,7 +37,7 @@ struct rq_ctx {
     uint32_t* d_ctr = nullptr;      // work counters of persistent launches (zeroed per launch)
     std::string last_error;
     int collapse_blocks = 0;        // co-resident blocks of the collapse kernel
-    rq_trace_tuning shade_shape{128, 32, 80, 0, 0, 1};  // shadow/AO traversal launch shape
+    rq_trace_tuning shade_shape{128, 32, 80, 0, 0, 1, 0};  // shadow/AO traversal launch shape
 };
 
 struct rq_bvh {
@@ -153,6 +153,10 @@ int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_g
 bool rq_shade_shape_ok(const rq_trace_tuning& t);
 int rq_launch_shadow_ao(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_shade_params& p,
                         uint32_t* mask, float* ao, unsigned long long* counter, cudaStream_t st);
+int rq_launch_reflect(rq_ctx* ctx, const rq_bvh* bvh, const rq_gbuffer_px* gbuf, const rq_reflect_params& p,
+                      rq_hit* hits, cudaStream_t st);
+int rq_launch_ao_depth(rq_ctx* ctx, const rq_bvh* bvh, const float* depth, const rq_ao_depth_params& p, float* ao,
+                       unsigned long long* counters, cudaStream_t st);
 
 // ---------------------------------------------------------------- k_radv
 int rq_launch_radv(rq_ctx* ctx, const float* tri9, uint32_t n, void* img, const rq_radv_layout& L, cudaStream_t st,

@@ -12,6 +12,10 @@
 //   2. leaf phase — lanes test their parked leaf's triangles in order;
 //   3. lanes whose stack is empty, or whose any-hit ray found a hit, report
 //      the result to the ray source and become idle.
+// With INLOOP, lanes whose stack runs out during the inner phase report at
+// once and idle lanes are refilled inside the inner phase too, which then
+// ends only when no lane searches or `leaf_batch` lanes hold a parked leaf:
+// rays that need few nodes no longer wait for the warp's longest one.
 // Per ray this visits stack entries in exactly the order of a sequential
 // pop-process-push traversal, so results do not depend on which lane or
 // round a ray runs in and match the oracle's traversal bit for bit.  The
@@ -161,14 +165,19 @@ __device__ __forceinline__ void stage_top(const rq_bvh4_node* __restrict__ nodes
 // (Aila and Laine 2009) — it changes the order in which a ray meets its
 // nodes, so it is only for any-hit rays whose result is hit or miss alone
 // (which triangle was found first is not reported by such sources).
+// INLOOP: finish and refill inside the inner phase (above); leaf_batch: the
+// parked leaves that end an INLOOP inner phase (1..32).  Neither changes a
+// ray's order of nodes.
 template <int ANY, bool MT, bool STATS, int STACK, int STRIDE, class Src, int CHUNK = int(kChunk), int TOP = 0,
-          bool SPEC = false>
+          bool SPEC = false, bool INLOOP = false>
 __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict__ nodes,
                                                  const rq_triangle* __restrict__ tris, Src& src, uint32_t* ctr,
                                                  int32_t* stk, uint32_t* err, int stack_cap = STACK,
-                                                 const float4* s_top = nullptr, int refill_min = 1) {
+                                                 const float4* s_top = nullptr, int refill_min = 1,
+                                                 int leaf_batch = 32) {
     static_assert(TOP == 0 || !IsMulti<Src>::value, "top-level staging needs one BVH per launch");
     static_assert(!SPEC || ANY == 1, "speculative traversal changes which hit an any-hit ray finds first");
+    static_assert(!INLOOP || !HasRoundEnd<Src>::value, "in-loop refill reports rays outside the round hooks");
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     // warp-uniform chunk of ray ids
@@ -192,11 +201,15 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
     h.u = h.v = 0.0f;
     h.boxes = h.tris = 0;
 
-    for (;;) {
-        // ---- refill idle lanes
+    int32_t leaf = kNoLeaf;  // the lane's parked leaf entry
+    bool stalled = false;    // SPEC: a second leaf waits in `top`
+
+    // hand the next ray ids to idle lanes once refill_min of them are idle
+    // (called by all 32 lanes together)
+    auto refill = [&]() {
         uint32_t idle = __ballot_sync(kFull, !active);
-        const bool refill = __popc(idle) >= refill_min || idle == kFull;
-        while (refill && idle && !exhausted) {
+        const bool go = __popc(idle) >= refill_min || idle == kFull;
+        while (go && idle && !exhausted) {
             if (next == end) {
                 uint32_t base = 0;
                 if (lane == 0) base = atomicAdd(ctr, uint32_t(CHUNK));
@@ -230,6 +243,8 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
                     top = TOP > 0 ? kStaged : 0;  // the root (slot 0 when staged)
                     has_top = true;
                     sp = 0;
+                    leaf = kNoLeaf;
+                    stalled = false;
                 }
             }
             next += take;
@@ -237,6 +252,11 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
             // empty pixel) take the next id at once
             idle = __ballot_sync(kFull, !active);
         }
+    };
+
+    for (;;) {
+        // ---- refill idle lanes
+        refill();
         if (!__any_sync(kFull, active)) {
             if (exhausted) break;
             continue;
@@ -245,12 +265,24 @@ __device__ __forceinline__ void trace_persistent(const rq_bvh4_node* __restrict_
         // ---- inner phase (SPEC: lanes holding a leaf keep taking inner
         // nodes while other lanes still search; a second leaf stays on the
         // stack and stalls the lane until the leaf phase)
-        int32_t leaf = kNoLeaf;
-        bool stalled = false;
+        leaf = kNoLeaf;
+        stalled = false;
         for (;;) {
+            if constexpr (INLOOP) {
+                // a ray whose stack ran out with no leaf pending is done
+                if (active && !(has_top || sp > 0) && leaf == kNoLeaf) {
+                    h.t = best;
+                    src.finish(rid, meta, ray, h);
+                    active = false;
+                }
+                refill();
+            }
             const bool left = has_top || sp > 0;
             const bool searching = active && left && leaf == kNoLeaf;
             if (!__any_sync(kFull, searching)) break;
+            if constexpr (INLOOP) {
+                if (__popc(__ballot_sync(kFull, active && leaf != kNoLeaf)) >= leaf_batch) break;
+            }
             const bool want = SPEC ? (active && left && !stalled) : searching;
             if (!want) continue;
             int32_t e;

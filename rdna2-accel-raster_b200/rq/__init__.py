@@ -93,6 +93,17 @@ class ShadeParams(C.Structure):
                 ("shadow_bias", C.c_float), ("flags", C.c_uint32), ("lights", Light * MAX_LIGHTS)]
 
 
+class ReflectParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("cam_pos", C.c_float * 3), ("tmin", C.c_float),
+                ("tmax", C.c_float), ("bias", C.c_float), ("flags", C.c_uint32)]
+
+
+class AoDepthParams(C.Structure):
+    _fields_ = [("inv_view_proj", C.c_float * 16), ("cam_pos", C.c_float * 3), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("spp", C.c_uint32), ("max_distance", C.c_float), ("tmin", C.c_float),
+                ("bias", C.c_float), ("flags", C.c_uint32)]
+
+
 GBUFFER_PX = np.dtype([("pos", "<f4", 3), ("vis", "<u4"), ("nrm", "<f4", 3), ("t", "<f4")])
 
 
@@ -108,7 +119,7 @@ class Instance(C.Structure):
 
 class TraceTuning(C.Structure):
     _fields_ = [("threads", C.c_uint32), ("chunk", C.c_uint32), ("reg_cap", C.c_uint32), ("top_levels", C.c_uint32),
-                ("speculative", C.c_uint32), ("refill_min", C.c_uint32)]
+                ("speculative", C.c_uint32), ("refill_min", C.c_uint32), ("leaf_batch", C.c_uint32)]
 
 
 class BatchTuning(C.Structure):
@@ -176,6 +187,8 @@ SIGNATURES = [
     ("rq_camera_look_at", C.c_int, [_P, _P, _P, C.c_float, _U32, _U32, C.POINTER(Camera)]),
     ("rq_render_gbuffer", C.c_int, [_P, _P, C.POINTER(Camera), _P, _P]),
     ("rq_render_shadow_ao", C.c_int, [_P, _P, _P, C.POINTER(ShadeParams), _P, _P, _P, _P]),
+    ("rq_render_reflect", C.c_int, [_P, _P, _P, C.POINTER(ReflectParams), _P, _P]),
+    ("rq_render_ao_depth", C.c_int, [_P, _P, _P, C.POINTER(AoDepthParams), _P, _P, _P]),
     ("rq_gbuffer_depth", C.c_int, [_P, _P, _U32, _P, _P, _P]),
     ("rq_blur_ao", C.c_int, [_P, _P, _P, _P, _U32, _U32, C.c_int, C.c_int, C.c_float, _P]),
     ("rq_radv_layout_get", C.c_int, [_U32, C.POINTER(RadvLayout)]),
@@ -308,14 +321,15 @@ class Context:
         t = TraceTuning()
         self.check(lib().rq_ctx_trace_tuning_get(self.h, C.byref(t)), "rq_ctx_trace_tuning_get")
         return {"threads": t.threads, "chunk": t.chunk, "reg_cap": t.reg_cap, "top_levels": t.top_levels,
-                "speculative": t.speculative, "refill_min": t.refill_min}
+                "speculative": t.speculative, "refill_min": t.refill_min, "leaf_batch": t.leaf_batch}
 
     def debug_wait_timeout(self, flag, limit, stream=None):
         """One bounded device wait on flag (int32 CUDA tensor) leaving 0."""
         self.check(lib().rq_debug_wait_timeout(self.h, _ptr(flag), limit, _stream(stream)), "rq_debug_wait_timeout")
 
-    def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80, top_levels=0, speculative=0, refill_min=1):
-        t = TraceTuning(threads, chunk, reg_cap, top_levels, speculative, refill_min)
+    def set_trace_tuning(self, threads=128, chunk=32, reg_cap=80, top_levels=0, speculative=0, refill_min=1,
+                         leaf_batch=0):
+        t = TraceTuning(threads, chunk, reg_cap, top_levels, speculative, refill_min, leaf_batch)
         self.check(lib().rq_ctx_trace_tuning_set(self.h, C.byref(t)), "rq_ctx_trace_tuning_set")
 
 
@@ -691,6 +705,53 @@ def render_gbuffer(ctx, bvh, cam, gbuf=None, stream=None):
         gbuf = torch.empty((cam.width * cam.height, 8), dtype=torch.int32, device="cuda")
     ctx.check(lib().rq_render_gbuffer(ctx.h, bvh.h, C.byref(cam), _ptr(gbuf), _stream(stream)), "rq_render_gbuffer")
     return gbuf
+
+
+def reflect_params(cam, flags=0, tmin=0.02, tmax=100.0, bias=0.04):
+    """Reflection rays of shaders/tiled_lighting_ra.comp:91-113 for a camera's
+    G-buffer (tmin 0.02, tmax 100, offset 0.04 as the shader)."""
+    p = ReflectParams()
+    p.width, p.height = cam.width, cam.height
+    for k in range(3):
+        p.cam_pos[k] = cam.cam_pos[k]
+    p.tmin, p.tmax, p.bias, p.flags = tmin, tmax, bias, flags
+    return p
+
+
+def render_reflect(ctx, bvh, gbuf, params, hits=None, stream=None):
+    """Closest-hit reflection ray per G-buffer pixel -> int32 [H*W, 4] hit
+    records (rq_hit) as a CUDA tensor."""
+    import torch
+    npix = params.width * params.height
+    if hits is None:
+        hits = torch.empty((npix, 4), dtype=torch.int32, device=gbuf.device)
+    ctx.check(lib().rq_render_reflect(ctx.h, bvh.h, _ptr(gbuf), C.byref(params), _ptr(hits), _stream(stream)),
+              "rq_render_reflect")
+    return hits
+
+
+def ao_depth_params(cam, spp=1, max_distance=0.5, flags=0, tmin=0.01, bias=0.03):
+    """rq_ao.comp's push constants for a camera (inv_view_proj, cam_pos,
+    resolution) with its fixed tmin 0.01 and 0.03 normal offset."""
+    p = AoDepthParams()
+    for k in range(16):
+        p.inv_view_proj[k] = cam.inv_view_proj[k]
+    for k in range(3):
+        p.cam_pos[k] = cam.cam_pos[k]
+    p.width, p.height, p.spp, p.max_distance = cam.width, cam.height, spp, max_distance
+    p.tmin, p.bias, p.flags = tmin, bias, flags
+    return p
+
+
+def render_ao_depth(ctx, bvh, depth, params, ao=None, counters=None, stream=None):
+    """rq_ao.comp from a depth buffer (float32 CUDA tensor, width*height) ->
+    float32 AO per pixel."""
+    import torch
+    if ao is None:
+        ao = torch.empty(params.width * params.height, dtype=torch.float32, device=depth.device)
+    ctx.check(lib().rq_render_ao_depth(ctx.h, bvh.h, _ptr(depth), C.byref(params), _ptr(ao), _ptr(counters),
+                                       _stream(stream)), "rq_render_ao_depth")
+    return ao
 
 
 def view_proj_of(cam):

@@ -3,7 +3,9 @@
 `python -m rq.tune --out FILE` times, on the device:
   - the 1080p shadows + AO frame's traversal (rq_render_shadow_ao) in every
     block size x refill chunk x register budget, with and without staged top
-    levels and speculative traversal (median of 5 runs each);
+    levels and speculative traversal, then the refill threshold, then the
+    in-loop refill shapes x refill threshold x leaf batch (median of 5 runs
+    each);
   - the batched workload (512 deforming grids, 4,096 any-hit + 4,096
     closest-hit rays per mesh) through rq_batch_autotune: every build block
     size x blocks per SM, every traversal block size x chunk x register budget;
@@ -50,6 +52,13 @@ SHADE_SHAPES = ([(t, c, r, 0, 0) for t in (64, 128, 256) for c in (32, 64) for r
 # speculation, for the fastest block size / chunk / register budgets
 REFILL_MINS = (4, 8, 12, 16, 20, 24)
 REFILL_TOP = 4
+# third stage: in-loop refill (speculative shapes): (threads, chunk, register
+# budget) x refill threshold x leaf batch
+INLOOP_SHAPES = [(64, 32, 64), (64, 64, 64), (128, 32, 64), (128, 64, 64), (256, 32, 64), (256, 64, 64),
+                 (128, 64, 72), (256, 64, 72)]
+INLOOP_REFILL = (4, 8, 12, 16)
+INLOOP_LEAF_BATCH = (4, 8, 12, 16, 24)
+SHAPE_KEYS = ("threads", "chunk", "reg_cap", "top_levels", "speculative", "refill_min", "leaf_batch")
 
 
 def shadow_key(ntri, params):
@@ -69,8 +78,8 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
     ao = torch.empty(n, dtype=torch.float32, device="cuda")
     trials = []
 
-    def timed(t, c, r, top, spec, refill):
-        ctx.set_trace_tuning(t, c, r, top, spec, refill)
+    def timed(t, c, r, top, spec, refill, leaf_batch=0):
+        ctx.set_trace_tuning(t, c, r, top, spec, refill, leaf_batch)
         rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao)
         ms = []
         for _ in range(reps):
@@ -82,7 +91,7 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
             ms.append(a.elapsed_time(b))
         ctx.sync_check()
         trials.append({"threads": t, "chunk": c, "reg_cap": r, "top_levels": top, "speculative": spec,
-                       "refill_min": refill, "ms": statistics.median(ms)})
+                       "refill_min": refill, "leaf_batch": leaf_batch, "ms": statistics.median(ms)})
 
     for t, c, r, top, spec in SHADE_SHAPES:
         timed(t, c, r, top, spec, 1)
@@ -97,10 +106,13 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
                 continue
             for refill in REFILL_MINS:
                 timed(t, c, r, top, spec, refill)
+    for t, c, r in INLOOP_SHAPES:
+        for refill in INLOOP_REFILL:
+            for lb in INLOOP_LEAF_BATCH:
+                timed(t, c, r, 0, 1, refill, lb)
     best = min(trials, key=lambda x: x["ms"])
-    keys = ("threads", "chunk", "reg_cap", "top_levels", "speculative", "refill_min")
-    ctx.set_trace_tuning(**{k: best[k] for k in keys})
-    return {k: best[k] for k in keys}, trials
+    ctx.set_trace_tuning(**{k: best.get(k, 0) for k in SHAPE_KEYS})
+    return {k: best.get(k, 0) for k in SHAPE_KEYS}, trials
 
 
 def lookup_shadow(key, path=TABLE):
@@ -125,10 +137,24 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--only", choices=["shadow", "batched"], help="tune one workload, keep the other's entry")
     args = ap.parse_args()
     ctx = rq.Context(0)
     table = load(args.out) if os.path.exists(args.out) else {}
     table.setdefault("device", torch.cuda.get_device_name(0))
+    if args.only != "batched":
+        tune_frame(ctx, table, args)
+    if args.only != "shadow":
+        tune_batch_entry(ctx, table, args)
+    with open(args.out, "w") as fo:
+        json.dump(table, fo, indent=1)
+
+
+def tune_frame(ctx, table, args):
+    import numpy as np
+    import torch
+    import rq
+    from rq import workloads as W
     # the 1080p shadows + AO frame
     pos, idx = W.shadow_mesh()
     p = torch.from_numpy(pos).cuda()
@@ -142,7 +168,13 @@ def main():
         "shape": shape, "ms": min(t["ms"] for t in trials), "trials": trials}
     print(json.dumps({"shadow_shape": shape, "ms": min(t["ms"] for t in trials)}))
     bvh.destroy()
-    del p, i, gbuf
+
+
+def tune_batch_entry(ctx, table, args):
+    import numpy as np
+    import torch
+    import rq
+    from rq import workloads as W
     sizes = W.batched_sizes(512, seed=2)
     pos, idx, descs = W.batched_meshes(sizes, seed=2)
     rays, mesh, flags = W.batched_rays(descs, 4096, 4096, seed=2)
@@ -159,8 +191,6 @@ def main():
         "build_ms": shape["build_ms"], "trace_ms": shape["trace_ms"],
         "trials": trials,
     }
-    with open(args.out, "w") as fo:
-        json.dump(table, fo, indent=1)
     print(json.dumps({"shape": table["entries"][workload_key(descs, 8192)]["shape"],
                       "build_ms": shape["build_ms"], "trace_ms": shape["trace_ms"]}))
 

@@ -4,7 +4,12 @@
 // the wrapper exactly as a reference call site would, and writes the bytes the
 // reference would upload:
 //
-//   software_bvh_wrapper MESH OUT_PREFIX MAX_LEAF SPLIT(0 morton, 1 median)
+//   software_bvh_wrapper MESH OUT_PREFIX MAX_LEAF SPLIT(0 morton, 1 median,
+//                                                    2 the reference's call shape)
+//
+// SPLIT 2 calls rq::SoftwareBVH::build(mesh, maxPrimsPerLeaf) and
+// rq::SoftwareBVH4::fromBVH2(bvh) with no engine argument, as
+// benchmarks/exp0_probe/microbench_main.cpp:175,185 call the reference.
 //
 // MESH: uint32 nv, uint32 ni, nv x 3 float32 positions, ni uint32 indices.
 // Writes OUT_PREFIX.nodes2 / .tris / .nodes4 / .perm; exit status 0 on
@@ -68,11 +73,19 @@ int main(int argc, char** argv) {
     }
     const std::string out = argv[2];
     const uint32_t max_leaf = uint32_t(std::strtoul(argv[3], nullptr, 10));
-    const rq::Split split = std::atoi(argv[4]) ? rq::Split::Median : rq::Split::Morton;
+    const int mode = std::atoi(argv[4]);
+    const rq::Split split = mode == 1 ? rq::Split::Median : rq::Split::Morton;
     try {
-        rq::Engine eng(0);
-        rq::SoftwareBVH b2 = rq::SoftwareBVH::build(eng, mesh, max_leaf, split);
-        rq::SoftwareBVH4 b4 = rq::SoftwareBVH4::fromBVH2(eng, b2);
+        rq::SoftwareBVH b2;
+        rq::SoftwareBVH4 b4;
+        if (mode == 2) {
+            b2 = rq::SoftwareBVH::build(mesh, max_leaf);
+            b4 = rq::SoftwareBVH4::fromBVH2(b2);
+        } else {
+            rq::Engine eng(0);
+            b2 = rq::SoftwareBVH::build(eng, mesh, max_leaf, split);
+            b4 = rq::SoftwareBVH4::fromBVH2(eng, b2);
+        }
         const bool ok = write_vec(out + ".nodes2", b2.nodes) && write_vec(out + ".tris", b2.triangles) &&
                         write_vec(out + ".nodes4", b4.nodes) && write_vec(out + ".perm", b2.perm);
         if (!ok) {

@@ -1,8 +1,12 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference.
 
-Run in a container that has the reference tree (default /root/reference) and
-the oracle built (`make -C oracle`).  The GPU box never needs the reference:
-the tests read only the files this script writes.
+Run where the reference tree exists, with the oracle built against it:
+
+  make -C oracle REF=<reference root>
+  python tests/golden/make_golden.py <reference root>
+
+(or set RQ_REFERENCE instead of the argument).  The GPU box never needs the
+reference: the tests read only the files this script writes.
 
   exp0_ray_stats.json   published SW BVH4 statistics, results/exp0_ray_stats.csv
   radv_layouts.json     compute_tree_layout (include/radv_bvh.hpp:193-215)
@@ -26,10 +30,15 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import pyoracle as O  # noqa: E402
 
-REF = os.environ.get("RQ_REFERENCE", "/root/reference")
+def reference_root():
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RQ_REFERENCE")
+    if not ref or not os.path.isfile(os.path.join(ref, "common", "software_bvh.hpp")):
+        sys.exit("usage: make_golden.py <reference root>  (or RQ_REFERENCE=<reference root>)")
+    return ref
 
 
 def main():
+    REF = reference_root()
     rows = []
     with open(os.path.join(REF, "results", "exp0_ray_stats.csv")) as f:
         for r in csv.DictReader(f):

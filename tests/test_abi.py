@@ -104,3 +104,18 @@ def test_server_refuses_bad_configs_without_a_device():
 def test_server_mesh_bytes_is_host_only():
     b = rq.Server.mesh_bytes(1000, 2000)
     assert b >= 12 * 1000 + 12 * 2000 + 2000 * (64 + 48 + 8 + 128)
+
+
+def test_noalloc_radv_checks_arguments_before_any_device_call():
+    # misaligned or missing buffers and oversized counts are refused on the
+    # host: these pointers are never dereferenced and no CUDA call is made
+    L = rq.lib()
+    f = L.rq_build_radv_noalloc
+    big = C.c_uint64(1 << 40)
+    assert f(C.c_void_p(0x1002), 1, C.c_void_p(0x10000), big, None) == rq.RQ_ERR_INVALID_ARG
+    assert f(C.c_void_p(0x1000), 1, C.c_void_p(0x10008), big, None) == rq.RQ_ERR_INVALID_ARG
+    assert f(None, 1, C.c_void_p(0x10000), big, None) == rq.RQ_ERR_INVALID_ARG
+    assert f(C.c_void_p(0x1000), 0, C.c_void_p(0x10000), big, None) == rq.RQ_ERR_INVALID_ARG
+    assert f(C.c_void_p(0x1000), rq.RADV_NOALLOC_MAX_TRIANGLES + 1, C.c_void_p(0x10000), big,
+             None) == rq.RQ_ERR_UNSUPPORTED
+    assert f(C.c_void_p(0x1000), 5, C.c_void_p(0x10000), C.c_uint64(100), None) == rq.RQ_ERR_SIZE

@@ -52,15 +52,17 @@ def wrapper(tmp_path_factory):
     return str(exe)
 
 
-def run(exe, tmp_path, pos, idx, max_leaf, median):
+def run(exe, tmp_path, pos, idx, max_leaf, median, mode=None):
+    """mode: 0 Morton, 1 median (from `median`), 2 the reference's call shape
+    (no engine argument)."""
     mesh = tmp_path / "mesh.bin"
     with open(mesh, "wb") as f:
         np.array([len(pos), idx.size], np.uint32).tofile(f)
         np.ascontiguousarray(pos, np.float32).tofile(f)
         np.ascontiguousarray(idx, np.uint32).tofile(f)
     out = str(tmp_path / "out")
-    r = subprocess.run([exe, str(mesh), out, str(max_leaf), "1" if median else "0"], capture_output=True,
-                       text=True, timeout=120)
+    mode = (1 if median else 0) if mode is None else mode
+    r = subprocess.run([exe, str(mesh), out, str(max_leaf), str(mode)], capture_output=True, text=True, timeout=120)
     if r.returncode:
         return r.returncode, r.stderr
     rd = lambda ext, dt: np.fromfile(out + ext, dtype=dt)  # noqa: E731
@@ -92,10 +94,13 @@ def test_wrapper_median_equals_reference_live(wrapper, tmp_path):
 
 
 @pytest.mark.gpu
-def test_wrapper_morton_equals_binding(ctx, wrapper, tmp_path):
+@pytest.mark.parametrize("mode", [0, 2], ids=["engine_argument", "reference_call_shape"])
+def test_wrapper_morton_equals_binding(ctx, wrapper, tmp_path, mode):
+    # mode 2 calls SoftwareBVH::build(mesh, 4) / SoftwareBVH4::fromBVH2(bvh)
+    # exactly as the reference's microbench_main.cpp:175,185 does
     import torch
     pos, idx = rq.scene_grid(96, 64, seed=5)
-    rc, res = run(wrapper, tmp_path, pos, idx.reshape(-1), 4, False)
+    rc, res = run(wrapper, tmp_path, pos, idx.reshape(-1), 4, False, mode)
     assert rc == 0, res
     b = rq.Bvh.build(ctx, torch.from_numpy(pos).cuda(), torch.from_numpy(idx.view(np.int32)).cuda())
     ctx.sync_check()

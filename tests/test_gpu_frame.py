@@ -96,7 +96,8 @@ def test_every_shadow_launch_shape_gives_identical_results(ctx):
     params = rq.shade_params(w, h, W.shadow_lights(16), ao_spp=2, ao_tmax=0.5)
     gb = rq.render_gbuffer(ctx, b, cam)
     base = ctx.trace_tuning()
-    assert base == {"threads": 128, "chunk": 32, "reg_cap": 80, "top_levels": 0, "speculative": 0, "refill_min": 1}
+    assert base == {"threads": 128, "chunk": 32, "reg_cap": 80, "top_levels": 0, "speculative": 0, "refill_min": 1,
+                    "leaf_batch": 0}
     want_m, want_a = [x.cpu().numpy() for x in rq.render_shadow_ao(ctx, b, gb, params)]
     for t, c, r, top, spec in T.SHADE_SHAPES:
         ctx.set_trace_tuning(t, c, r, top, spec)
@@ -108,6 +109,18 @@ def test_every_shadow_launch_shape_gives_identical_results(ctx):
         m, a = rq.render_shadow_ao(ctx, b, gb, params)
         ctx.sync_check()
         assert np.array_equal(m.cpu().numpy(), want_m) and a.cpu().numpy().tobytes() == want_a.tobytes(), refill
+    # in-loop refill: rays finish and lanes refill inside the node loop
+    for t, c, r in T.INLOOP_SHAPES:
+        for refill, lb in ((1, 1), (8, 8), (16, 4), (4, 32)):
+            ctx.set_trace_tuning(t, c, r, 0, 1, refill, lb)
+            m, a = rq.render_shadow_ao(ctx, b, gb, params)
+            ctx.sync_check()
+            assert np.array_equal(m.cpu().numpy(), want_m) and a.cpu().numpy().tobytes() == want_a.tobytes(), (
+                t, c, r, refill, lb)
+    with pytest.raises(rq.RqError):
+        ctx.set_trace_tuning(128, 32, 0, 0, 0, 1, 8)  # in-loop refill needs a speculative shape
+    with pytest.raises(rq.RqError):
+        ctx.set_trace_tuning(128, 64, 64, 0, 1, 8, 33)
     with pytest.raises(rq.RqError):
         ctx.set_trace_tuning(96, 32, 0)
     with pytest.raises(rq.RqError):
@@ -146,4 +159,62 @@ def test_ao_blur_chain_bit_exact(ctx):
     assert torch.equal(same, ao)
     with pytest.raises(rq.RqError):
         rq.blur_ao(ctx, ao, depth, w, h, 1, 1, 0.01)
+    b.destroy()
+
+
+def wide_camera(w, h, flags=0):
+    # looks past the mesh edge at the horizon: part of the image is empty
+    return rq.camera_look_at((0.0, -2.2, 0.9), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 50.0, w, h, flags=flags)
+
+
+@pytest.mark.parametrize("flags", [0, rq.RQ_TRI_MT])
+@pytest.mark.parametrize("view", ["shadow", "wide"])
+def test_reflection_rays_bit_exact(ctx, flags, view):
+    # tiled_lighting_ra.comp:91-113: R = reflect(normalize(P - cam), N) from
+    # P + 0.04 N over [0.02, 100], closest hit, one record per pixel
+    pos, idx = rq.scene_grid(128, 128, seed=1)
+    b = build(ctx, pos, idx)
+    n2, tr, n4, perm = b.download()
+    w, h = 320, 180
+    cam = W.shadow_camera(w, h, flags=flags) if view == "shadow" else wide_camera(w, h, flags)
+    gb = rq.render_gbuffer(ctx, b, cam)
+    hits = rq.render_reflect(ctx, b, gb, rq.reflect_params(cam, flags=flags))
+    ctx.sync_check()
+    gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    oh = O.render_reflect(n4, tr, perm, gbn, O.reflect_params(cam, flags=flags))
+    hn = rq.hits_numpy(hits)
+    assert hn.tobytes() == oh.tobytes()
+    vis = gbn["vis"] > 0
+    assert 0.0 < hn["hit"][vis].mean() < 1.0
+    if view == "wide":
+        assert (~vis).any() and (hn["hit"][~vis] == 0).all() and (hn["primitive_id"][~vis] == 0xFFFFFFFF).all()
+    b.destroy()
+
+
+@pytest.mark.parametrize("flags", [0, rq.RQ_TRI_MT])
+@pytest.mark.parametrize("view", ["shadow", "wide"])
+def test_depth_ao_bit_exact(ctx, flags, view):
+    # rq_ao.comp from the depth buffer: position from depth x invViewProj,
+    # normal from the right and upper neighbours, AO 1 at depth >= 1
+    pos, idx = rq.scene_grid(128, 128, seed=1)
+    b = build(ctx, pos, idx)
+    n2, tr, n4, perm = b.download()
+    w, h = 320, 180
+    cam = W.shadow_camera(w, h) if view == "shadow" else wide_camera(w, h)
+    gb = rq.render_gbuffer(ctx, b, cam)
+    depth = rq.gbuffer_depth(ctx, gb, rq.view_proj_of(cam))
+    dn = depth.cpu().numpy()
+    for spp in (0, 1, 3):
+        ap = rq.ao_depth_params(cam, spp=spp, max_distance=0.5, flags=flags)
+        counters = torch.zeros(4, dtype=torch.int64, device="cuda")
+        ao = rq.render_ao_depth(ctx, b, depth, ap, counters=counters)
+        ctx.sync_check()
+        oa, orays = O.render_ao_depth(n4, tr, dn, O.ao_depth_params(cam, spp=spp, max_distance=0.5, flags=flags))
+        assert ao.cpu().numpy().tobytes() == oa.tobytes(), spp
+        assert int(counters[0]) == orays
+    if view == "wide":
+        assert (dn >= 1.0).any() and (oa[dn >= 1.0] == 1.0).all()
+    assert 0.0 < oa[dn < 1.0].mean() < 1.0
+    with pytest.raises(rq.RqError):
+        rq.render_ao_depth(ctx, b, depth, rq.ao_depth_params(cam, spp=33))
     b.destroy()

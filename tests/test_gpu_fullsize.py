@@ -1,0 +1,242 @@
+"""GPU parity at the full sizes of the benchmark configurations.
+
+  c2  the 1080p shadows + AO frame: 2,499,848 triangles (1118x1118 quads,
+      seed 1), 16 lights, 1 SPP AO;
+  c4  subpixel visibility: 8,323,200 triangles (2040x2040 quads, seed 3),
+      jittered primary rays, the tree built at frame 0 and refitted at
+      frame 199 of the deformation z = z0 + 0.05 sin(0.1 f + x).
+
+At each size:
+  - the LBVH build equals Oracle B byte for byte (Morton keys, sort
+    permutation, binary nodes, leaf-ordered triangles, 4-wide nodes), and a
+    refit equals the oracle's refit of the same topology;
+  - the engine's rays at 20,000 sampled pixels equal the oracle's
+    statement bit for bit, and are checked against the reference pipeline:
+    the reference's own SoftwareBVH tree (oracle/_ref, compiled from
+    common/software_bvh.hpp) traversed by the restated
+    software_bvh_bvh4.comp.  With the engine in the shader's arithmetic
+    (RQ_TRI_MT) hit flags and closest-hit primitive ids agree except edge
+    grazes, under 1e-5 of the rays, t within 1e-6 relative; with the default
+    watertight test every disagreement must also be explained, and the rays
+    the shader's |a| < 1e-7 test culls as parallel are counted."""
+import numpy as np
+import pytest
+import torch
+
+import pyoracle as O
+import rq
+from parity_util import GRAZE_FRACTION, assert_t_close, graze_report
+from rq import workloads as W
+
+pytestmark = pytest.mark.gpu
+SAMPLE = 20000
+WIDTH, HEIGHT = 1920, 1080
+
+
+def device_mesh(pos, idx):
+    return torch.from_numpy(pos).cuda(), torch.from_numpy(idx.view(np.int32)).cuda()
+
+
+def assert_build_equals_oracle(b, pos, idx):
+    n2, tr, n4, perm = b.download()
+    keys, ids = b.download_sort()
+    o = O.lbvh_build(pos.reshape(-1), idx.reshape(-1))
+    assert np.array_equal(ids, o["sorted"]) and np.array_equal(perm, o["sorted"]), "sort permutation"
+    assert np.array_equal(keys, o["codes"][o["sorted"]]), "Morton keys"
+    assert len(n2) == len(o["nodes2"]) and n2.tobytes() == o["nodes2"].tobytes(), "binary nodes"
+    assert tr.tobytes() == o["tris"].tobytes(), "leaf-ordered triangles"
+    assert len(n4) == len(o["nodes4"]) and n4.tobytes() == o["nodes4"].tobytes(), "4-wide nodes"
+    assert b.info()["depth4"] == o["depth4"]
+    return n2, tr, n4, perm
+
+
+class RefPipeline:
+    """The reference's SoftwareBVH::build + fromBVH2 on a mesh, traversed by
+    the restated software_bvh_bvh4.comp; primitive ids mapped back to the
+    input order."""
+
+    def __init__(self, pos, idx):
+        _, self.tris, self.nodes4 = O.ref_build(pos.reshape(-1), idx.reshape(-1))
+        self.perm = O.recover_perm(self.tris, pos, idx)
+
+    def trace(self, rays):
+        _, h, dropped = O.trace_ref_bvh4(self.nodes4, self.tris, rays, return_dropped=True)
+        prim = np.where(h["hit"] == 1, self.perm[np.minimum(h["primitive_id"], len(self.perm) - 1)], 0xFFFFFFFF)
+        return h, prim, dropped
+
+
+def sample_pixels(seed):
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(WIDTH * HEIGHT, SAMPLE, replace=False)).astype(np.uint32)
+
+
+def check_primary(pos, idx, ref, cam, gbn, pixels, mt):
+    """G-buffer hits at the sampled pixels against the reference pipeline."""
+    rays = O.camera_rays(cam, pixels)
+    rh, rprim, dropped = ref.trace(rays)
+    g = gbn[pixels]
+    ours_hit = (g["vis"] > 0).astype(np.uint32)
+    ours_prim = g["vis"].astype(np.int64) - 1
+    dis, kinds, unexplained = graze_report(pos, idx, rays, ours_hit, ours_prim, rh["hit"], rprim,
+                                           ours_t=g["t"], ref_t=rh["t"])
+    assert not unexplained, [(i, int(dropped[i])) for i in unexplained[:10]]
+    assert kinds["edge"] < GRAZE_FRACTION * len(rays) + 1, kinds
+    if mt:
+        assert kinds["parallel"] == 0, kinds
+    both = (ours_hit == 1) & (rh["hit"] == 1) & (ours_prim == rprim)
+    assert both.mean() > 0.99
+    assert_t_close(g["t"], rh["t"], both)
+    return kinds
+
+
+def check_secondary(pos, idx, ref, n4, tr, perm, gbn, mask, ao, params, pixels, mt):
+    """Shadow and AO hit flags at the sampled pixels against the reference
+    pipeline (rays re-made by the oracle from the engine's G-buffer)."""
+    rays, rpx, slot = O.shade_rays(gbn, params, pixels)
+    px = pixels[rpx]
+    occluded = np.where(slot < 32, ((mask[px] >> np.minimum(slot, 31)) & 1) == 0, ao[px] == 0).astype(np.uint32)
+    rh, rprim, dropped = ref.trace(rays)
+    # the triangle the engine found for the rays where the flags differ
+    diff = np.nonzero(occluded != rh["hit"])[0]
+    ours_prim = np.full(len(rays), 0xFFFFFFFF, np.int64)
+    if len(diff):
+        ch, _, _ = O.trace_bvh4(n4, tr, perm, rays[diff], rq.RQ_TRI_MT if mt else 0)
+        ours_prim[diff] = ch["primitive_id"]
+    dis, kinds, unexplained = graze_report(pos, idx, rays, occluded, ours_prim, rh["hit"], rprim, closest=False)
+    assert not unexplained, [(i, int(dropped[i])) for i in unexplained[:10]]
+    assert kinds["edge"] < GRAZE_FRACTION * len(rays) + 1, kinds
+    if mt:
+        assert kinds["parallel"] == 0, kinds
+    assert len(rays) > 10 * len(pixels) and 0.02 < occluded.mean() < 0.5
+    return kinds
+
+
+@pytest.fixture(scope="module")
+def c2(ctx):
+    pos, idx = W.shadow_mesh()
+    assert len(idx) == 2499848
+    p_d, i_d = device_mesh(pos, idx)
+    b = rq.Bvh.build(ctx, p_d, i_d)
+    ctx.sync_check()
+    yield pos, idx, b
+    b.destroy()
+
+
+def test_c2_build_equals_oracle(c2):
+    pos, idx, b = c2
+    assert_build_equals_oracle(b, pos, idx)
+
+
+@pytest.mark.parametrize("mt", [True, False], ids=["mt", "watertight"])
+def test_c2_frame_vs_oracle_and_reference_pipeline(ctx, c2, mt, have_ref):
+    if not have_ref:
+        pytest.skip("needs oracle/_ref (the reference's SoftwareBVH)")
+    pos, idx, b = c2
+    flags = rq.RQ_TRI_MT if mt else 0
+    cam = W.shadow_camera(flags=flags)
+    params = W.shadow_params(flags=flags)
+    gb = rq.render_gbuffer(ctx, b, cam)
+    mask, ao = rq.render_shadow_ao(ctx, b, gb, params)
+    ctx.sync_check()
+    gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    maskn, aon = mask.cpu().numpy().astype(np.uint32), ao.cpu().numpy()
+    n2, tr, n4, perm = b.download()
+    pixels = sample_pixels(11)
+    # bit-exact against the oracle's statement of the same frame
+    og = O.render_gbuffer(n4, tr, perm, cam, pixels)
+    assert gbn[pixels].tobytes() == og.tobytes()
+    om, oa, _ = O.render_shadow_ao(n4, tr, gbn, params, pixels)
+    assert np.array_equal(maskn[pixels], om) and aon[pixels].tobytes() == oa.tobytes()
+    # against the reference pipeline
+    ref = RefPipeline(pos, idx)
+    check_primary(pos, idx, ref, cam, gbn, pixels, mt)
+    check_secondary(pos, idx, ref, n4, tr, perm, gbn, maskn, aon, params, pixels, mt)
+
+
+def test_c2_reflection_and_depth_ao_sampled(ctx, c2):
+    # the two remaining ray kinds of the consumer shaders at full size:
+    # reflection rays (tiled_lighting_ra.comp:91-113) and AO from depth
+    # (rq_ao.comp), bit-exact with the oracle at the sampled pixels
+    pos, idx, b = c2
+    cam = W.shadow_camera()
+    gb = rq.render_gbuffer(ctx, b, cam)
+    rp = rq.reflect_params(cam)
+    hits = rq.render_reflect(ctx, b, gb, rp)
+    depth = rq.gbuffer_depth(ctx, gb, rq.view_proj_of(cam))
+    ap = rq.ao_depth_params(cam, spp=1, max_distance=0.5)
+    counters = torch.zeros(4, dtype=torch.int64, device="cuda")
+    ao = rq.render_ao_depth(ctx, b, depth, ap, counters=counters)
+    ctx.sync_check()
+    n2, tr, n4, perm = b.download()
+    gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    pixels = sample_pixels(12)
+    oh = O.render_reflect(n4, tr, perm, gbn, O.reflect_params(cam), pixels)
+    hn = rq.hits_numpy(hits)
+    assert hn[pixels].tobytes() == oh.tobytes()
+    assert 0.0 < hn["hit"].mean() < 1.0
+    dn = depth.cpu().numpy()
+    oa, _ = O.render_ao_depth(n4, tr, dn, O.ao_depth_params(cam, spp=1, max_distance=0.5), pixels)
+    an = ao.cpu().numpy()
+    assert an[pixels].tobytes() == oa.tobytes()
+    assert int(counters[0]) == int((dn < 1.0).sum())
+    assert 0.0 < an.mean() < 1.0
+
+
+@pytest.fixture(scope="module")
+def c4(ctx):
+    pos0, idx = W.visibility_mesh()
+    assert len(idx) == 8323200
+    base, i_d = device_mesh(pos0, idx)
+    cur = torch.empty_like(base)
+    yield pos0, idx, base, cur, i_d
+
+
+def deformed(ctx, base, cur, frame):
+    rq.deform_wave(ctx, base, cur, W.deform_time(frame), W.DEFORM_AMP, W.DEFORM_FREQ)
+    ctx.sync_check()
+    return cur.cpu().numpy()
+
+
+def check_visibility(ctx, b, pos, idx, n4, tr, perm, frame, have_ref):
+    """Jittered primary rays of one visibility frame: bit-exact with the
+    oracle on the engine's tree, and against the reference pipeline on the
+    same (deformed) mesh in the shader's arithmetic."""
+    pixels = sample_pixels(100 + frame)
+    for mt in (False, True):
+        cam = W.visibility_camera(seed=3 + frame, flags=rq.RQ_TRI_MT if mt else 0)
+        gb = rq.render_gbuffer(ctx, b, cam)
+        ctx.sync_check()
+        gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+        og = O.render_gbuffer(n4, tr, perm, cam, pixels)
+        assert gbn[pixels].tobytes() == og.tobytes(), (frame, mt)
+        assert (gbn["vis"] > 0).all()
+        if have_ref:
+            ref = RefPipeline(pos, idx)
+            check_primary(pos, idx, ref, cam, gbn, pixels, mt)
+
+
+def test_c4_fresh_build_refit_and_rebuild(ctx, c4, have_ref):
+    pos0, idx, base, cur, i_d = c4
+    # frame 0: the bench builds here and then refits every frame
+    p0 = deformed(ctx, base, cur, 0)
+    b = rq.Bvh.build(ctx, cur, i_d)
+    ctx.sync_check()
+    n2, tr, n4, perm = assert_build_equals_oracle(b, p0, idx)
+    check_visibility(ctx, b, p0, idx, n4, tr, perm, 0, have_ref)
+    # frame 199, refitted: topology kept, boxes and triangles the oracle's refit
+    p199 = deformed(ctx, base, cur, 199)
+    b.refit(cur, i_d)
+    ctx.sync_check()
+    n2f, trf, n4f, permf = b.download()
+    otr, on2, on4 = O.refit(p199, idx, perm, n2, n4)
+    assert np.array_equal(permf, perm)
+    assert trf.tobytes() == otr.tobytes(), "refitted triangles"
+    assert n2f.tobytes() == on2.tobytes(), "refitted binary nodes"
+    assert n4f.tobytes() == on4.tobytes(), "refitted 4-wide nodes"
+    assert not np.array_equal(n4f["max_z"], n4["max_z"])
+    check_visibility(ctx, b, p199, idx, n4f, trf, permf, 199, have_ref)
+    # a rebuild on the deformed mesh equals Oracle B on it
+    rq.Bvh.build(ctx, cur, i_d, into=b)
+    ctx.sync_check()
+    assert_build_equals_oracle(b, p199, idx)
+    b.destroy()

@@ -92,3 +92,37 @@ def test_median_traces_like_lbvh(ctx):
     assert (hm["primitive_id"] != hl["primitive_id"]).mean() < 1e-4
     bm.destroy()
     bl.destroy()
+
+
+def test_median_build_replayed_from_a_graph(ctx):
+    # the median build is stream-ordered (it launches every level a split can
+    # reach and reads each level's size on the device), so a rebuild can be
+    # captured in a CUDA graph beside an LBVH rebuild and replayed after the
+    # vertices move; each replay equals a build outside the graph
+    pos_a = tie_free_soup(30000, 61)
+    n = len(pos_a) // 3
+    pos_b = tie_free_soup(40000, 62)[: 3 * n]
+    p = torch.from_numpy(pos_a).cuda()
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        bm = rq.Bvh.build(ctx, p, None, median=True, stream=side)  # arrays and scratch before the capture
+        bl = rq.Bvh.build(ctx, p, None, stream=side)
+        side.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            rq.Bvh.build(ctx, p, None, median=True, into=bm, stream=side)
+            rq.Bvh.build(ctx, p, None, into=bl, stream=side)
+    for pos in (pos_b, pos_a):
+        p.copy_(torch.from_numpy(pos))
+        g.replay()
+        torch.cuda.synchronize()
+        ctx.sync_check()
+        got_m, got_l = bm.download(), bl.download()
+        want_m = gpu_median(ctx, pos, 4)
+        o = O.lbvh_build(pos.reshape(-1), None)
+        for a, b in zip(got_m, want_m):
+            assert a.tobytes() == b.tobytes()
+        assert got_l[0].tobytes() == o["nodes2"].tobytes() and got_l[2].tobytes() == o["nodes4"].tobytes()
+    del g
+    bm.destroy()
+    bl.destroy()

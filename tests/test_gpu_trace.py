@@ -19,6 +19,7 @@ import torch
 
 import pyoracle as O
 import rq
+from parity_util import assert_t_close, graze_report
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -65,41 +66,6 @@ def test_trace_larger_mesh_vs_oracle(ctx):
     b.destroy()
 
 
-def edge_distance(ray, v):
-    """Smallest barycentric coordinate (float64) of the ray's crossing of the
-    triangle's plane: ~0 means the ray passes along an edge."""
-    o, d = ray[0:3].astype(np.float64), ray[4:7].astype(np.float64)
-    v = v.astype(np.float64)
-    e1, e2 = v[1] - v[0], v[2] - v[0]
-    n = np.cross(e1, e2)
-    t = np.dot(v[0] - o, n) / np.dot(d, n)
-    p = o + t * d
-    area = np.dot(n, n)
-    b1 = np.dot(np.cross(p - v[0], e2), -n) / area
-    b2 = np.dot(np.cross(e1, p - v[0]), n) / area
-    return min(abs(1 - b1 - b2), abs(b1), abs(b2))
-
-
-def graze_report(pos, idx, rays, ours, ref_hit, ref_prim_orig):
-    """Rays where the engine and the reference pipeline disagree.  Each must
-    graze a shared edge: either both hit triangles share a vertex, or only one
-    side hits and its crossing lies within 1e-5 (barycentric) of an edge —
-    the cracks a non-watertight test leaves between neighbours."""
-    tri = idx.reshape(-1, 3)
-    dis = np.nonzero((ours["hit"] != ref_hit) | ((ours["hit"] == 1) & (ours["primitive_id"] != ref_prim_orig)))[0]
-    unexplained = []
-    for i in dis:
-        if ours["hit"][i] != ref_hit[i]:
-            pid = ours["primitive_id"][i] if ours["hit"][i] else ref_prim_orig[i]
-            if edge_distance(rays[i], pos[tri[pid]]) > 1e-5:
-                unexplained.append(i)
-            continue
-        a, b = tri[ours["primitive_id"][i]], tri[ref_prim_orig[i]]
-        if not set(a.tolist()) & set(b.tolist()):
-            unexplained.append(i)
-    return dis, unexplained
-
-
 @pytest.mark.parametrize("flags", [rq.RQ_TRI_MT, rq.RQ_TRI_WATERTIGHT])
 def test_closest_hit_vs_reference_pipeline(ctx, flags, have_ref):
     if not have_ref:
@@ -113,12 +79,12 @@ def test_closest_hit_vs_reference_pipeline(ctx, flags, have_ref):
     perm_r = O.recover_perm(trr, pos.reshape(-1), idx.reshape(-1))
     st, rh = O.trace_ref_bvh4(n4r, trr, rays_np.view(O.RAY).reshape(-1))
     ref_prim = np.where(rh["hit"] == 1, perm_r[np.minimum(rh["primitive_id"], len(perm_r) - 1)], 0xFFFFFFFF)
-    dis, unexplained = graze_report(pos, idx, rays_np, ours, rh["hit"], ref_prim)
+    dis, kinds, unexplained = graze_report(pos, idx, rays_np, ours["hit"], ours["primitive_id"], rh["hit"], ref_prim,
+                                           ours_t=ours["t"], ref_t=rh["t"])
     assert len(unexplained) == 0, unexplained[:10]
-    assert len(dis) < 1e-5 * n, len(dis)
+    assert len(dis) < 1e-5 * n, (len(dis), kinds)
     both = (ours["hit"] == 1) & (rh["hit"] == 1) & (ours["primitive_id"] == ref_prim)
-    rel = np.abs(ours["t"][both] - rh["t"][both]) / rh["t"][both]
-    assert rel.max() <= 1e-6
+    assert_t_close(ours["t"], rh["t"], both)
     b.destroy()
 
 
