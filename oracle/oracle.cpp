@@ -272,6 +272,150 @@ int32_t emit(LbvhState& S, bool is_leaf, int64_t id) {
     return me;
 }
 
+// ------------------------------------- LBVH with SAH-rebuilt subtrees --
+// The LBVH's Karras hierarchy above every node of at most K primitives; each
+// such subtree (a contiguous range of the Morton-sorted order) rebuilt top
+// down by binned SAH: 16 bins per axis over the node's centroid bounds, bin
+// b = min(15, int((c - cmin) * (16 / extent))), split cost
+// float(nL) * SA(left) + float(nR) * SA(right) with SA = 2((dx dy + dy dz) + dz dx),
+// the smallest cost wins (strict <: the lower axis, then the lower bin, on
+// ties), a stable partition of the range; leaves of at most max_leaf
+// primitives; the middle of the range where no axis has a centroid extent
+// or the subtree is kSahDepthCap levels deep.  Nodes in depth-first pre-order.
+constexpr int kSahBins = 16;
+constexpr uint32_t kSahDepthCap = 24;
+
+struct SahState {
+    LbvhState* S;
+    uint32_t K;
+    std::vector<uint32_t> order;  // leaf position -> original primitive
+};
+
+inline float sah_area(const float mn[3], const float mx[3]) {
+    const float dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+    return 2.0f * ((dx * dy + dy * dz) + dz * dx);
+}
+
+inline int sah_bin(float c, float cmin, float scale) {
+    const int b = int((c - cmin) * scale);
+    return b < kSahBins - 1 ? b : kSahBins - 1;
+}
+
+int32_t emit_sah(SahState& T, uint32_t s, uint32_t e, uint32_t depth) {
+    LbvhState& S = *T.S;
+    const int32_t me = int32_t(S.out.size());
+    S.out.emplace_back();
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = s; i < e; ++i) {
+        const Prim& p = S.prims[T.order[i]];
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fmin_(mn[k], p.mn[k]);
+            mx[k] = fmax_(mx[k], p.mx[k]);
+            cmn[k] = fmin_(cmn[k], p.c[k]);
+            cmx[k] = fmax_(cmx[k], p.c[k]);
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        S.out[me].aabb_min[k] = mn[k];
+        S.out[me].aabb_max[k] = mx[k];
+    }
+    const uint32_t n = e - s;
+    if (n <= S.max_leaf) {
+        S.out[me].left_child = ~int32_t(s);
+        S.out[me].right_child = int32_t(n);
+        return me;
+    }
+    float best = INFINITY, best_scale = 0.0f;
+    int best_axis = -1, best_bin = -1;
+    uint32_t best_nl = 0;
+    if (depth < kSahDepthCap) {
+        for (int a = 0; a < 3; ++a) {
+            const float ext = cmx[a] - cmn[a];
+            if (!(ext > 0.0f)) continue;
+            const float scale = float(kSahBins) / ext;
+            if (!(scale < INFINITY)) continue;  // an extent too small to scale: no split there
+            uint32_t cnt[kSahBins] = {};
+            float bmn[kSahBins][3], bmx[kSahBins][3];
+            for (int b = 0; b < kSahBins; ++b)
+                for (int k = 0; k < 3; ++k) {
+                    bmn[b][k] = INFINITY;
+                    bmx[b][k] = -INFINITY;
+                }
+            for (uint32_t i = s; i < e; ++i) {
+                const Prim& p = S.prims[T.order[i]];
+                const int b = sah_bin(p.c[a], cmn[a], scale);
+                ++cnt[b];
+                for (int k = 0; k < 3; ++k) {
+                    bmn[b][k] = fmin_(bmn[b][k], p.mn[k]);
+                    bmx[b][k] = fmax_(bmx[b][k], p.mx[k]);
+                }
+            }
+            for (int split = 0; split < kSahBins - 1; ++split) {
+                float lmn[3] = {INFINITY, INFINITY, INFINITY}, lmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+                float rmn[3] = {INFINITY, INFINITY, INFINITY}, rmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+                uint32_t nl = 0, nr = 0;
+                for (int b = 0; b < kSahBins; ++b) {
+                    float* tmn = b <= split ? lmn : rmn;
+                    float* tmx = b <= split ? lmx : rmx;
+                    (b <= split ? nl : nr) += cnt[b];
+                    for (int k = 0; k < 3; ++k) {
+                        tmn[k] = fmin_(tmn[k], bmn[b][k]);
+                        tmx[k] = fmax_(tmx[k], bmx[b][k]);
+                    }
+                }
+                const float cost = float(nl) * sah_area(lmn, lmx) + float(nr) * sah_area(rmn, rmx);
+                if (cost < best) {
+                    best = cost;
+                    best_axis = a;
+                    best_bin = split;
+                    best_scale = scale;
+                    best_nl = nl;
+                }
+            }
+        }
+    }
+    uint32_t mid;
+    if (best_axis < 0) {
+        mid = s + n / 2;
+    } else {
+        std::vector<uint32_t> left, right;
+        for (uint32_t i = s; i < e; ++i) {
+            const uint32_t id = T.order[i];
+            (sah_bin(S.prims[id].c[best_axis], cmn[best_axis], best_scale) <= best_bin ? left : right).push_back(id);
+        }
+        std::copy(left.begin(), left.end(), T.order.begin() + s);
+        std::copy(right.begin(), right.end(), T.order.begin() + s + left.size());
+        mid = s + best_nl;
+    }
+    const int32_t l = emit_sah(T, s, mid, depth + 1);
+    const int32_t r = emit_sah(T, mid, e, depth + 1);
+    S.out[me].left_child = l;
+    S.out[me].right_child = r;
+    return me;
+}
+
+int32_t emit_top(SahState& T, bool is_leaf, int64_t id) {
+    LbvhState& S = *T.S;
+    const int64_t lo = is_leaf ? id : S.inner[size_t(id)].lo;
+    const int64_t hi = is_leaf ? id : S.inner[size_t(id)].hi;
+    if (uint64_t(hi - lo + 1) <= T.K) return emit_sah(T, uint32_t(lo), uint32_t(hi + 1), 0);
+    const int32_t me = int32_t(S.out.size());
+    S.out.emplace_back();
+    float mn[3], mx[3];
+    union_range(S, lo, hi, mn, mx);
+    for (int k = 0; k < 3; ++k) {
+        S.out[me].aabb_min[k] = mn[k];
+        S.out[me].aabb_max[k] = mx[k];
+    }
+    const KNode& kn = S.inner[size_t(id)];
+    const int32_t l = emit_top(T, kn.left_leaf, kn.left);
+    const int32_t r = emit_top(T, kn.right_leaf, kn.right);
+    S.out[me].left_child = l;
+    S.out[me].right_child = r;
+    return me;
+}
+
 // Greedy 4-wide collapse: restates SoftwareBVH4::collapse
 // (common/software_bvh.hpp:202-291) — open the inner candidate with the
 // largest surface area (strict >, first wins) until four candidates, emit in
@@ -729,6 +873,61 @@ int orc_lbvh_build(const float* pos, uint32_t stride_floats, const uint32_t* idx
             tr.v1[0] = p1.x; tr.v1[1] = p1.y; tr.v1[2] = p1.z; tr.v1[3] = 0.0f;
             tr.v2[0] = p2.x; tr.v2[1] = p2.y; tr.v2[2] = p2.z; tr.v2[3] = 0.0f;
             tris[k] = tr;
+        }
+    }
+    if (nodes4 || n4) {
+        std::vector<rq_bvh4_node> out4;
+        uint32_t md = 0;
+        collapse4(S.out.data(), 0, out4, 1, &md);
+        if (n4) *n4 = uint32_t(out4.size());
+        if (depth4) *depth4 = md;
+        if (nodes4) std::memcpy(nodes4, out4.data(), sizeof(rq_bvh4_node) * out4.size());
+    }
+    return 0;
+}
+
+// LBVH with SAH-rebuilt subtrees of at most `sah_max` primitives (see
+// emit_sah).  Codes and sort as orc_lbvh_build; perm_out[k] = the original
+// triangle at leaf position k (the sort permutation, permuted inside each
+// rebuilt subtree).
+int orc_lbvh_sah_build(const float* pos, uint32_t stride_floats, const uint32_t* idx, uint32_t n, uint32_t max_leaf,
+                       uint32_t sah_max, uint32_t* codes_out, uint32_t* sorted_out, rq_bvh2_node* nodes2, uint32_t* n2,
+                       rq_triangle* tris, uint32_t* perm_out, rq_bvh4_node* nodes4, uint32_t* n4, uint32_t* depth4) {
+    if (n == 0 || max_leaf == 0 || sah_max < max_leaf) return 1;
+    LbvhState S;
+    S.max_leaf = max_leaf;
+    S.prims.resize(n);
+    for (uint32_t t = 0; t < n; ++t) {
+        V3 p0, p1, p2;
+        tri_vertices(pos, stride_floats, idx, t, p0, p1, p2);
+        S.prims[t] = make_prim(p0, p1, p2);
+    }
+    morton_codes(S.prims, S.codes);
+    S.sorted.resize(n);
+    for (uint32_t i = 0; i < n; ++i) S.sorted[i] = i;
+    std::sort(S.sorted.begin(), S.sorted.end(), [&](uint32_t a, uint32_t b) {
+        return S.codes[a] != S.codes[b] ? S.codes[a] < S.codes[b] : a < b;
+    });
+    S.skeys.resize(n);
+    for (uint32_t i = 0; i < n; ++i) S.skeys[i] = S.codes[S.sorted[i]];
+    if (codes_out) std::memcpy(codes_out, S.codes.data(), 4ull * n);
+    if (sorted_out) std::memcpy(sorted_out, S.sorted.data(), 4ull * n);
+    Karras K{S.skeys, int64_t(n)};
+    if (n >= 2) {
+        S.inner.resize(n - 1);
+        for (uint32_t i = 0; i + 1 < n; ++i) S.inner[i] = karras_node(K, i);
+    }
+    SahState T{&S, sah_max, S.sorted};
+    S.out.reserve(2ull * n);
+    emit_top(T, n == 1, 0);
+    *n2 = uint32_t(S.out.size());
+    if (nodes2) std::memcpy(nodes2, S.out.data(), sizeof(rq_bvh2_node) * S.out.size());
+    if (perm_out) std::memcpy(perm_out, T.order.data(), 4ull * n);
+    if (tris) {
+        for (uint32_t k = 0; k < n; ++k) {
+            V3 p0, p1, p2;
+            tri_vertices(pos, stride_floats, idx, T.order[k], p0, p1, p2);
+            tris[k] = rq_triangle{{p0.x, p0.y, p0.z, 0.0f}, {p1.x, p1.y, p1.z, 0.0f}, {p2.x, p2.y, p2.z, 0.0f}};
         }
     }
     if (nodes4 || n4) {

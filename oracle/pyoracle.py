@@ -47,6 +47,9 @@ def lib():
         L = C.CDLL(ORACLE_SO)
         L.orc_lbvh_build.argtypes = [_P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P]
         L.orc_lbvh_build.restype = C.c_int
+        L.orc_lbvh_sah_build.argtypes = [_P, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P,
+                                         _P, _P, _P, _P]
+        L.orc_lbvh_sah_build.restype = C.c_int
         L.orc_collapse4.argtypes = [_P, C.c_uint32, _P, _P, _P]
         L.orc_collapse4.restype = C.c_int
         L.orc_radv_build.argtypes = [_P, C.c_uint32, _P]
@@ -134,6 +137,32 @@ def lbvh_build(pos, idx, max_leaf=4, stride_floats=3):
                               _ptr(nodes2), _ptr(n2), _ptr(tris), _ptr(nodes4), _ptr(n4), _ptr(d4))
     assert rc == 0
     return dict(codes=codes, sorted=srt, nodes2=nodes2[: n2[0]].copy(), tris=tris,
+                nodes4=nodes4[: n4[0]].copy(), depth4=int(d4[0]))
+
+
+def lbvh_sah_build(pos, idx, max_leaf=4, sah_max=1024, stride_floats=3):
+    """LBVH with SAH-rebuilt subtrees of at most sah_max primitives.  Returns
+    dict with codes, sorted ids, perm (leaf order -> original), nodes2,
+    tris, nodes4, depth4."""
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    if idx is not None:
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        n = idx.size // 3
+    else:
+        n = (pos.size // stride_floats) // 3
+    codes = np.empty(n, np.uint32)
+    srt = np.empty(n, np.uint32)
+    perm = np.empty(n, np.uint32)
+    nodes2 = np.empty(2 * n, BVH2_NODE)
+    tris = np.empty(n, TRIANGLE)
+    nodes4 = np.empty(max(1, n), BVH4_NODE)
+    n2 = np.zeros(1, np.uint32)
+    n4 = np.zeros(1, np.uint32)
+    d4 = np.zeros(1, np.uint32)
+    rc = lib().orc_lbvh_sah_build(_ptr(pos), stride_floats, _ptr(idx), n, max_leaf, sah_max, _ptr(codes), _ptr(srt),
+                                  _ptr(nodes2), _ptr(n2), _ptr(tris), _ptr(perm), _ptr(nodes4), _ptr(n4), _ptr(d4))
+    assert rc == 0
+    return dict(codes=codes, sorted=srt, perm=perm, nodes2=nodes2[: n2[0]].copy(), tris=tris,
                 nodes4=nodes4[: n4[0]].copy(), depth4=int(d4[0]))
 
 

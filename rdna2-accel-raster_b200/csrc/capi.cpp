@@ -247,7 +247,10 @@ int rq_build(rq_ctx* ctx, const float* positions, uint32_t stride_bytes, uint32_
     if (num_triangles >= RQ_MAX_TRIANGLES) return rq_set_error(ctx, RQ_ERR_UNSUPPORTED, "more than 2^27 triangles");
     if (stride_bytes < 12 || stride_bytes % 4) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad vertex stride");
     if (max_leaf < 1 || max_leaf > 16) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "max_leaf must be 1..16");
-    if (flags & ~(RQ_BUILD_BVH4 | RQ_BUILD_MEDIAN)) return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "unknown build flags");
+    if (flags & ~(RQ_BUILD_BVH4 | RQ_BUILD_MEDIAN | RQ_BUILD_SAH))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "unknown build flags");
+    if ((flags & RQ_BUILD_MEDIAN) && (flags & RQ_BUILD_SAH))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "RQ_BUILD_MEDIAN and RQ_BUILD_SAH exclude each other");
     if (!indices && uint64_t(num_vertices) < 3ull * num_triangles)
         return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "non-indexed mesh needs 3 vertices per triangle");
     cudaSetDevice(ctx->device);
@@ -277,7 +280,8 @@ int rq_build(rq_ctx* ctx, const float* positions, uint32_t stride_bytes, uint32_
     int rc = (flags & RQ_BUILD_MEDIAN)
                  ? rq_launch_build_median(ctx, b, positions, stride_bytes, indices, num_triangles, max_leaf, want4,
                                           S(stream))
-                 : rq_launch_build(ctx, b, positions, stride_bytes, indices, num_triangles, max_leaf, want4, S(stream));
+                 : rq_launch_build(ctx, b, positions, stride_bytes, indices, num_triangles, max_leaf, want4, S(stream),
+                                   (flags & RQ_BUILD_SAH) ? RQ_SAH_SUBTREE_MAX : 0u);
     if (rc) {
         if (fresh) {
             free_arrays(b);

@@ -175,6 +175,448 @@ __global__ void __launch_bounds__(kT) k_emit2(uint32_t n, uint32_t max_leaf, con
     }
 }
 
+// ------------------------------------------------- SAH-rebuilt subtrees
+// RQ_BUILD_SAH: the Karras hierarchy above every node of at most K
+// primitives stays; each such subtree (a contiguous range of the sorted
+// order) is rebuilt top down by binned SAH inside one block: 16 bins per axis
+// over the node's centroid bounds, bin = min(15, int((c - cmin) * (16 /
+// extent))), cost float(nL) * SA(left) + float(nR) * SA(right), the smallest
+// cost first by axis then bin, a stable partition of the node's range, leaves
+// of at most max_leaf primitives, the middle of the range where no axis has
+// a centroid extent or the subtree is kSahDepthCap levels deep.  Every node
+// still covers a contiguous range of leaf positions, so the pre-order
+// position of every node is A[lo(v)] + L(v) as in the plain LBVH: the subtree
+// blocks write one record per node (box, first position, L, and the right
+// child's first position or the leaf count) and the emission counts of their
+// leaves; after the scan, k_sah_emit writes the records and the top nodes.
+constexpr uint32_t kSahMax = RQ_SAH_SUBTREE_MAX;  // largest subtree a block rebuilds
+constexpr int kSahT = 256;
+constexpr int kSahWarps = kSahT / 32;
+constexpr int kSahBins = 16;
+constexpr uint32_t kSahDepthCap = 24;
+constexpr uint32_t kNoRecord = 0xffffffffu;
+
+// Subtree roots: every child of at most K primitives of a node of more (or
+// the root itself when n <= K), marked at its first sorted position with its
+// last position, the left-child links above it and its Karras index.
+__global__ void __launch_bounds__(kT) k_sah_roots(uint32_t n, uint32_t K, const int32_t* __restrict__ kl,
+                                                  const int32_t* __restrict__ kr, const uint32_t* __restrict__ klo,
+                                                  const uint32_t* __restrict__ khi,
+                                                  const uint32_t* __restrict__ par_in, uint32_t* __restrict__ sflag,
+                                                  uint32_t* __restrict__ shi, uint32_t* __restrict__ sL,
+                                                  uint32_t* __restrict__ snode) {
+    if (n <= K) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            sflag[0] = 1u;
+            shi[0] = n - 1u;
+            sL[0] = 0u;
+            snode[0] = n == 1u ? 0x80000000u : 0u;
+        }
+        return;
+    }
+    for (uint32_t p = blockIdx.x * kT + threadIdx.x; p + 1u < n; p += gridDim.x * kT) {
+        if (rq::count_in(klo, khi, p) <= K) continue;
+        uint32_t L = 0, par = par_in[p];
+        while (par != rq::kNoParent && (par & 1u) == 0u) {
+            ++L;
+            par = par_in[par >> 1];
+        }
+        const int32_t ch[2] = {kl[p], kr[p]};
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const bool leaf = ch[side] < 0;
+            const uint32_t ci = uint32_t(ch[side]) & 0x7fffffffu;
+            const uint32_t lo = leaf ? ci : klo[ci], hi = leaf ? ci : khi[ci];
+            if (hi - lo + 1u > K) continue;
+            sflag[lo] = 1u;
+            shi[lo] = hi;
+            sL[lo] = side == 0 ? L + 1u : 0u;
+            snode[lo] = leaf ? (0x80000000u | ci) : ci;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kT) k_sah_list(uint32_t n, const uint32_t* __restrict__ sflag,
+                                                 const uint32_t* __restrict__ sidx, uint32_t* __restrict__ list,
+                                                 uint32_t* __restrict__ count) {
+    for (uint32_t x = blockIdx.x * kT + threadIdx.x; x < n; x += gridDim.x * kT) {
+        if (sflag[x]) list[sidx[x]] = x;
+        if (x == n - 1u) *count = sidx[x] + sflag[x];
+    }
+}
+
+struct SahArgs {
+    const float* pos;
+    uint32_t sf;
+    const uint32_t* idx;
+    uint32_t n, max_leaf;
+    const float4* cent;
+    const uint32_t* skeys;
+    const uint32_t* sids;
+    const int32_t* kl;
+    const int32_t* kr;
+    const uint32_t* par_in;
+    const uint32_t* par_lf;
+    float4* box_in;
+    float4* box_lf;
+    uint32_t* refit_flag;
+    const uint32_t* shi;
+    const uint32_t* sL;
+    const uint32_t* snode;
+    const uint32_t* list;
+    const uint32_t* count;
+    uint32_t* next;
+    float4* rec;
+    uint32_t* rec_l;
+    uint32_t* c;
+    rq_triangle* tris;
+    uint32_t* perm;
+    uint32_t* keys_out;
+    uint32_t* err;
+};
+
+// Shared memory of one subtree block (kSahMax primitives): boxes with the x
+// and y centroid in w, z centroids, triangle ids, the leaf order of two
+// consecutive levels (local indices), the node lists of two levels, and one
+// set of bins per warp (3 axes x 16 bins x (count, min xyz, max xyz) as
+// ordered integers).
+struct SahShared {
+    float4 lo[kSahMax];
+    float4 hi[kSahMax];
+    float cz[kSahMax];
+    uint32_t id[kSahMax];
+    uint16_t ord[2][kSahMax];
+    uint2 list[2][kSahMax];
+    uint32_t bins[kSahWarps][3 * kSahBins * 7];
+    uint32_t cnt[2];
+    uint32_t slots;
+    uint32_t job;
+    float4 root_lo, root_hi;
+};
+
+__device__ __forceinline__ int sah_bin(float c, float cmin, float scale) {
+    const int b = __float2int_rz((c - cmin) * scale);
+    return b < kSahBins - 1 ? b : kSahBins - 1;
+}
+
+__device__ __forceinline__ float sah_area(float mnx, float mny, float mnz, float mxx, float mxy, float mxz) {
+    const float dx = mxx - mnx, dy = mxy - mny, dz = mxz - mnz;
+    return 2.0f * ((dx * dy + dy * dz) + dz * dx);
+}
+
+__device__ __forceinline__ float sah_centroid(const SahShared& S, uint32_t p, int a) {
+    return a == 0 ? S.lo[p].w : (a == 1 ? S.hi[p].w : S.cz[p]);
+}
+
+// Node list entry: x = s | e << 11 | depth << 22, y = slot | L << 12.
+__device__ __forceinline__ uint2 sah_entry(uint32_t s, uint32_t e, uint32_t depth, uint32_t slot, uint32_t L) {
+    return make_uint2(s | (e << 11) | (depth << 22), slot | (L << 12));
+}
+
+// One node of a subtree, by one warp: box and centroid bounds, then a leaf
+// (its record, emission counts, triangles) or the binned split, the stable
+// partition of its range into the next level's order, its record and its two
+// children appended to the next level's list.
+__device__ void sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t nsub, uint2 ent, int cur,
+                         uint32_t lane, uint32_t warp) {
+    const uint32_t s = ent.x & 0x7ffu, e = (ent.x >> 11) & 0x7ffu, depth = ent.x >> 22;
+    const uint32_t slot = ent.y & 0xfffu, L = ent.y >> 12;
+    const uint16_t* ord = S.ord[cur];
+    uint16_t* nxt = S.ord[cur ^ 1];
+    const uint32_t n = e - s;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = s + lane; i < e; i += 32) {
+        const uint32_t p = ord[i];
+        const float4 a = S.lo[p], b = S.hi[p];
+        mn[0] = fminf(mn[0], a.x);
+        mn[1] = fminf(mn[1], a.y);
+        mn[2] = fminf(mn[2], a.z);
+        mx[0] = fmaxf(mx[0], b.x);
+        mx[1] = fmaxf(mx[1], b.y);
+        mx[2] = fmaxf(mx[2], b.z);
+        const float c[3] = {a.w, b.w, S.cz[p]};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            cmn[k] = fminf(cmn[k], c[k]);
+            cmx[k] = fmaxf(cmx[k], c[k]);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+            cmn[k] = fminf(cmn[k], __shfl_xor_sync(0xffffffffu, cmn[k], o));
+            cmx[k] = fmaxf(cmx[k], __shfl_xor_sync(0xffffffffu, cmx[k], o));
+        }
+    const size_t r = 2ull * lo + slot;  // record index
+    if (slot == 0 && lane == 0) {       // the subtree root's box, for the top refit
+        S.root_lo = make_float4(mn[0], mn[1], mn[2], 0.0f);
+        S.root_hi = make_float4(mx[0], mx[1], mx[2], 0.0f);
+    }
+    if (n <= A.max_leaf) {
+        if (lane == 0) {
+            A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+            A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
+            A.rec_l[r] = L;
+        }
+        for (uint32_t i = s + lane; i < e; i += 32) {
+            const uint32_t k = lo + i, gid = S.id[ord[i]];
+            rq::F3 p0, p1, p2;
+            rq::load_tri(A.pos, A.sf, A.idx, gid, p0, p1, p2);
+            float4* tp = reinterpret_cast<float4*>(A.tris + k);
+            tp[0] = make_float4(p0.x, p0.y, p0.z, 0.0f);
+            tp[1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
+            tp[2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
+            A.perm[k] = gid;
+            A.keys_out[k] = A.skeys[k];
+            A.c[k] = i == s ? 1u + L : 0u;
+        }
+        return;
+    }
+    // binned SAH over the axes with a centroid extent
+    int best_axis = -1, best_split = -1;
+    uint32_t best_nl = 0;
+    float best_scale = 0.0f;
+    if (depth < kSahDepthCap) {
+        uint32_t* bins = S.bins[warp];
+        for (uint32_t w = lane; w < 3u * kSahBins * 7u; w += 32) {
+            const uint32_t f = w % 7u;
+            bins[w] = f == 0 ? 0u : (f <= 3 ? rq::f2o(INFINITY) : rq::f2o(-INFINITY));
+        }
+        float scale[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float ext = cmx[a] - cmn[a];
+            scale[a] = ext > 0.0f ? float(kSahBins) / ext : 0.0f;
+            if (!(scale[a] < INFINITY)) scale[a] = 0.0f;  // an extent too small to scale: no split there
+        }
+        __syncwarp();
+        for (uint32_t i = s + lane; i < e; i += 32) {
+            const uint32_t p = ord[i];
+            const float4 a4 = S.lo[p], b4 = S.hi[p];
+            const float c[3] = {a4.w, b4.w, S.cz[p]};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (!(scale[a] > 0.0f)) continue;
+                uint32_t* bn = bins + (a * kSahBins + sah_bin(c[a], cmn[a], scale[a])) * 7;
+                atomicAdd(bn, 1u);
+                atomicMin(bn + 1, rq::f2o(a4.x));
+                atomicMin(bn + 2, rq::f2o(a4.y));
+                atomicMin(bn + 3, rq::f2o(a4.z));
+                atomicMax(bn + 4, rq::f2o(b4.x));
+                atomicMax(bn + 5, rq::f2o(b4.y));
+                atomicMax(bn + 6, rq::f2o(b4.z));
+            }
+        }
+        __syncwarp();
+        // 45 candidates (axis, split after bin k): lanes take candidates lane and lane + 32
+        float bc = INFINITY;
+        uint32_t bi = 0xffffffffu, bnl = 0;
+        for (uint32_t cand = lane; cand < 3u * (kSahBins - 1); cand += 32) {
+            const uint32_t a = cand / (kSahBins - 1), k = cand % (kSahBins - 1);
+            if (!(scale[a] > 0.0f)) continue;
+            float l[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+            float rr[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+            uint32_t nl = 0, nr = 0;
+            for (uint32_t b = 0; b < kSahBins; ++b) {
+                const uint32_t* bn = bins + (a * kSahBins + b) * 7;
+                float* t = b <= k ? l : rr;
+                (b <= k ? nl : nr) += bn[0];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    t[q] = fminf(t[q], rq::o2f(bn[1 + q]));
+                    t[3 + q] = fmaxf(t[3 + q], rq::o2f(bn[4 + q]));
+                }
+            }
+            const float cost = float(nl) * sah_area(l[0], l[1], l[2], l[3], l[4], l[5]) +
+                               float(nr) * sah_area(rr[0], rr[1], rr[2], rr[3], rr[4], rr[5]);
+            if (cost < bc) {  // candidates of one lane rise in index
+                bc = cost;
+                bi = cand;
+                bnl = nl;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+            const uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            const uint32_t on = __shfl_xor_sync(0xffffffffu, bnl, o);
+            if (oc < bc || (oc == bc && oi < bi)) {
+                bc = oc;
+                bi = oi;
+                bnl = on;
+            }
+        }
+        if (bi != 0xffffffffu) {
+            best_axis = int(bi / (kSahBins - 1));
+            best_split = int(bi % (kSahBins - 1));
+            best_nl = bnl;
+            best_scale = scale[best_axis];
+        }
+        __syncwarp();  // the bins are read before the next node reuses them
+    }
+    uint32_t mid;
+    if (best_axis < 0) {
+        mid = s + n / 2u;
+        for (uint32_t i = s + lane; i < e; i += 32) nxt[i] = ord[i];
+    } else {
+        mid = s + best_nl;
+        const uint32_t lt = (1u << lane) - 1u;
+        uint32_t nl = 0, nr = 0;
+        for (uint32_t b = s; b < e; b += 32) {
+            const uint32_t i = b + lane;
+            const bool in = i < e;
+            const uint32_t p = in ? ord[i] : 0u;
+            const bool left =
+                in && sah_bin(sah_centroid(S, p, best_axis), cmn[best_axis], best_scale) <= best_split;
+            const uint32_t ml = __ballot_sync(0xffffffffu, left), mr = __ballot_sync(0xffffffffu, in && !left);
+            if (left)
+                nxt[s + nl + __popc(ml & lt)] = uint16_t(p);
+            else if (in)
+                nxt[mid + nr + __popc(mr & lt)] = uint16_t(p);
+            nl += __popc(ml);
+            nr += __popc(mr);
+        }
+    }
+    uint32_t base = 0;
+    if (lane == 0) {
+        A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+        A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(lo + mid));
+        A.rec_l[r] = L;
+        const uint32_t cs = atomicAdd(&S.slots, 2u);
+        base = atomicAdd(&S.cnt[cur ^ 1], 2u);
+        S.list[cur ^ 1][base] = sah_entry(s, mid, depth + 1u, cs, L + 1u);
+        S.list[cur ^ 1][base + 1] = sah_entry(mid, e, depth + 1u, cs + 1u, 0u);
+    }
+    (void)nsub;
+}
+
+// One block per subtree (taken from a counter): load its primitives, build
+// it level by level (a warp per node), mark its unused record slots, then
+// refit the top of the tree from its root upward (the second arrival at a
+// top node computes its box, as refit_walk).
+__global__ void __launch_bounds__(kSahT) k_sah_build(const SahArgs A) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    SahShared& S = *reinterpret_cast<SahShared*>(s_raw);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t nsubtrees = *A.count;
+    for (;;) {
+        if (threadIdx.x == 0) S.job = atomicAdd(A.next, 1u);
+        __syncthreads();
+        const uint32_t j = S.job;
+        if (j >= nsubtrees) break;
+        const uint32_t lo = A.list[j];
+        const uint32_t nsub = A.shi[lo] - lo + 1u;
+        for (uint32_t i = threadIdx.x; i < nsub; i += kSahT) {
+            const uint32_t gid = A.sids[lo + i];
+            rq::F3 p0, p1, p2;
+            rq::load_tri(A.pos, A.sf, A.idx, gid, p0, p1, p2);
+            const float4 c = A.cent[gid];
+            S.lo[i] = make_float4(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)),
+                                  fminf(p0.z, fminf(p1.z, p2.z)), c.x);
+            S.hi[i] = make_float4(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)),
+                                  fmaxf(p0.z, fmaxf(p1.z, p2.z)), c.y);
+            S.cz[i] = c.z;
+            S.id[i] = gid;
+            S.ord[0][i] = uint16_t(i);
+        }
+        if (threadIdx.x == 0) {
+            S.cnt[0] = 1u;
+            S.cnt[1] = 0u;
+            S.slots = 1u;
+            S.list[0][0] = sah_entry(0u, nsub, 0u, 0u, A.sL[lo]);
+        }
+        __syncthreads();
+        int cur = 0;
+        for (uint32_t guard = 0;; ++guard) {
+            const uint32_t m = S.cnt[cur];
+            if (m == 0u || guard > 64u) break;
+            for (uint32_t k = warp; k < m; k += kSahWarps) sah_node(S, A, lo, nsub, S.list[cur][k], cur, lane, warp);
+            __syncthreads();
+            if (threadIdx.x == 0) S.cnt[cur] = 0u;
+            cur ^= 1;
+            __syncthreads();
+        }
+        for (uint32_t k = S.slots + threadIdx.x; k < 2u * nsub; k += kSahT) A.rec_l[2ull * lo + k] = kNoRecord;
+        if (threadIdx.x == 0) {
+            // the root's box where its parent's union reads it, then the walk up
+            const uint32_t rn = A.snode[lo];
+            const bool rleaf = (rn >> 31) != 0u;
+            const uint32_t ri = rn & 0x7fffffffu;
+            float4* dst = rleaf ? A.box_lf + 2 * size_t(ri) : A.box_in + 2 * size_t(ri);
+            __stcg(dst, S.root_lo);
+            __stcg(dst + 1, S.root_hi);
+            uint32_t par = rleaf ? A.par_lf[ri] : A.par_in[ri];
+            for (uint32_t guard = 0; par != rq::kNoParent; ++guard) {
+                const uint32_t p = par >> 1;
+                if (rq::atom_add_acq_rel(&A.refit_flag[p], 1u) == 0u) break;
+                const int32_t a = A.kl[p], b = A.kr[p];
+                const float4* ba = a < 0 ? A.box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : A.box_in + 2 * size_t(a);
+                const float4* bb = b < 0 ? A.box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : A.box_in + 2 * size_t(b);
+                const float4 alo = rq::ld_cg4(ba), ahi = rq::ld_cg4(ba + 1), blo = rq::ld_cg4(bb),
+                             bhi = rq::ld_cg4(bb + 1);
+                __stcg(A.box_in + 2 * size_t(p),
+                       make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f));
+                __stcg(A.box_in + 2 * size_t(p) + 1,
+                       make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f));
+                par = A.par_in[p];
+                if (guard > 128u) {
+                    rq::set_err(A.err, RQ_DERR_REFIT);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Node writes: every record at A[first] + L (left child next to it, right
+// child at A[its first position]; leaves as ~first / count), every top node
+// (more than K primitives) likewise from its Karras range and refitted box.
+__global__ void __launch_bounds__(kT) k_sah_emit(uint32_t n, uint32_t K, uint32_t max_leaf,
+                                                 const float4* __restrict__ rec, const uint32_t* __restrict__ rec_l,
+                                                 const int32_t* __restrict__ kr, const uint32_t* __restrict__ klo,
+                                                 const uint32_t* __restrict__ khi,
+                                                 const uint32_t* __restrict__ par_in, const float4* box_in,
+                                                 const uint32_t* __restrict__ c, const uint32_t* __restrict__ A,
+                                                 rq_bvh2_node* __restrict__ out, uint32_t* __restrict__ counts) {
+    for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < 2u * n; i += gridDim.x * kT) {
+        const uint32_t L = rec_l[i];
+        if (L == kNoRecord) continue;
+        const float4 a = rec[2 * size_t(i)], b = rec[2 * size_t(i) + 1];
+        const uint32_t first = __float_as_uint(a.w), aux = __float_as_uint(b.w);
+        const uint32_t pre = A[first] + L;
+        const bool leaf = (aux >> 31) != 0u;
+        const int32_t lc = leaf ? ~int32_t(first) : int32_t(pre + 1u);
+        const int32_t rc = leaf ? int32_t(aux & 0x7fffffffu) : int32_t(A[aux]);
+        float4* o = reinterpret_cast<float4*>(out + pre);
+        o[0] = make_float4(a.x, a.y, a.z, __int_as_float(lc));
+        o[1] = make_float4(b.x, b.y, b.z, __int_as_float(rc));
+    }
+    for (uint32_t p = blockIdx.x * kT + threadIdx.x; p + 1u < n; p += gridDim.x * kT) {
+        if (rq::count_in(klo, khi, p) <= K) continue;
+        uint32_t L = 0, par = par_in[p];
+        while (par != rq::kNoParent && (par & 1u) == 0u) {
+            ++L;
+            par = par_in[par >> 1];
+        }
+        const uint32_t pre = A[klo[p]] + L;
+        const int32_t r = kr[p];
+        const uint32_t rlo = r < 0 ? (uint32_t(r) & 0x7fffffffu) : klo[r];
+        const float4 lo = rq::ld_cg4(box_in + 2 * size_t(p)), hi = rq::ld_cg4(box_in + 2 * size_t(p) + 1);
+        float4* o = reinterpret_cast<float4*>(out + pre);
+        o[0] = make_float4(lo.x, lo.y, lo.z, __int_as_float(int32_t(pre + 1u)));
+        o[1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(int32_t(A[rlo])));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counts[0] = A[n - 1u] + c[n - 1u];
+        counts[3] = max_leaf;
+    }
+}
+
 // ------------------------------------------------------------------ refit
 // Parent links of an emitted binary BVH (any layout with the root at 0).
 __global__ void __launch_bounds__(kT) k_parents2(const rq_bvh2_node* __restrict__ nodes, const uint32_t* counts,
@@ -272,7 +714,7 @@ inline uint32_t grid_for(uint32_t n, int sms) {
 
 }  // namespace
 
-size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s) {
+size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s, bool sah) {
     Carve c{reinterpret_cast<uintptr_t>(base), 0};
     const size_t N = n ? n : 1;
     const uint32_t tiles = rq_sort_tiles(uint32_t(N)), stiles = rq_scan_tiles(uint32_t(N));
@@ -304,16 +746,91 @@ size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s) {
     s.cpar = c.take<uint32_t>(N);
     s.cacc = c.take<unsigned long long>(N);
     s.coll_ctl = c.take<uint32_t>(256);
+    s.sah_flag = s.sah_idx = s.sah_hi = s.sah_L = s.sah_node = s.sah_list = s.sah_rec_l = nullptr;
+    s.sah_rec = nullptr;
+    if (sah) {
+        s.sah_flag = c.take<uint32_t>(N);
+        s.sah_idx = c.take<uint32_t>(N);
+        s.sah_hi = c.take<uint32_t>(N);
+        s.sah_L = c.take<uint32_t>(N);
+        s.sah_node = c.take<uint32_t>(N);
+        s.sah_list = c.take<uint32_t>(N);
+        s.sah_rec = c.take<float4>(4 * N);
+        s.sah_rec_l = c.take<uint32_t>(2 * N);
+    }
     return c.off + 256;
 }
 
+namespace {
+
+// Subtree roots, their list, the subtree blocks (with the top refit), the
+// scan of the emission counts and the node writes.
+int launch_sah(rq_ctx* ctx, rq_bvh* bvh, BuildScratch& s, const float* pos, uint32_t sf, const uint32_t* idx,
+               uint32_t n, uint32_t max_leaf, uint32_t K, const uint32_t* skeys, const uint32_t* sids,
+               cudaStream_t st) {
+    const int sms = ctx->num_sms;
+    static const size_t kSmem = sizeof(SahShared);
+    static int per_sm = [] {
+        cudaFuncSetAttribute(k_sah_build, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmem));
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sah_build, kSahT, kSmem);
+        return b > 0 ? b : 1;
+    }();
+    cudaError_t e = cudaMemsetAsync(s.sah_flag, 0, sizeof(uint32_t) * n, st);
+    k_sah_roots<<<grid_for(n, sms), kT, 0, st>>>(n, K, s.kl, s.kr, s.klo, s.khi, s.par_in, s.sah_flag, s.sah_hi,
+                                                 s.sah_L, s.sah_node);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.tile_ctr + 8, 0, sizeof(uint32_t), st);
+    rq_launch_scan(ctx, s.sah_flag, s.sah_idx, n, s.scan_status, s.tile_ctr + 8, st);
+    k_sah_list<<<grid_for(n, sms), kT, 0, st>>>(n, s.sah_flag, s.sah_idx, s.sah_list, s.tile_ctr + 13);
+    SahArgs a;
+    a.pos = pos;
+    a.sf = sf;
+    a.idx = idx;
+    a.n = n;
+    a.max_leaf = max_leaf;
+    a.cent = s.cent;
+    a.skeys = skeys;
+    a.sids = sids;
+    a.kl = s.kl;
+    a.kr = s.kr;
+    a.par_in = s.par_in;
+    a.par_lf = s.par_lf;
+    a.box_in = s.box_in;
+    a.box_lf = s.box_lf;
+    a.refit_flag = s.refit_flag;
+    a.shi = s.sah_hi;
+    a.sL = s.sah_L;
+    a.snode = s.sah_node;
+    a.list = s.sah_list;
+    a.count = s.tile_ctr + 13;
+    a.next = s.tile_ctr + 12;
+    a.rec = s.sah_rec;
+    a.rec_l = s.sah_rec_l;
+    a.c = s.c;
+    a.tris = bvh->tris;
+    a.perm = bvh->perm;
+    a.keys_out = bvh->skeys;
+    a.err = ctx->d_err;
+    k_sah_build<<<uint32_t(sms) * uint32_t(per_sm), kSahT, kSmem, st>>>(a);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.tile_ctr + 8, 0, sizeof(uint32_t), st);
+    rq_launch_scan(ctx, s.c, s.a, n, s.scan_status, s.tile_ctr + 8, st);
+    k_sah_emit<<<grid_for(2 * n, sms), kT, 0, st>>>(n, K, max_leaf, s.sah_rec, s.sah_rec_l, s.kr, s.klo, s.khi,
+                                                    s.par_in, s.box_in, s.c, s.a, bvh->nodes2, bvh->d_counts);
+    return rq_cuda_status(ctx, e == cudaSuccess ? cudaGetLastError() : e, "SAH-subtree build launch");
+}
+
+}  // namespace
+
 int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
-                    uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t st) {
+                    uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t st, uint32_t sah_max) {
     BuildScratch s;
-    const size_t need = rq_build_scratch_carve(nullptr, n, s);
+    const bool sah = sah_max > 0;
+    if (sah && (sah_max > kSahMax || sah_max < max_leaf))
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "SAH subtree size out of range");
+    const size_t need = rq_build_scratch_carve(nullptr, n, s, sah);
     int rc = rq_ensure_scratch(ctx, need, st);
     if (rc) return rc;
-    rq_build_scratch_carve(ctx->scratch, n, s);
+    rq_build_scratch_carve(ctx->scratch, n, s, sah);
     const uint32_t sf = stride_bytes / 4;
     const int sms = ctx->num_sms;
 
@@ -331,6 +848,12 @@ int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_
     const uint32_t* skeys = s.keys[rb];
     const uint32_t* sids = s.vals[rb];
     k_karras<<<grid_for(n, sms), kT, 0, st>>>(skeys, n, s.kl, s.kr, s.klo, s.khi, s.par_in, s.par_lf);
+    if (sah) {
+        rc = launch_sah(ctx, bvh, s, pos, sf, idx, n, max_leaf, sah_max, skeys, sids, st);
+        if (rc) return rc;
+        if (collapse) return rq_launch_collapse(ctx, bvh, s, st);
+        return RQ_OK;
+    }
     k_leaves_local<<<(n + kLocal - 1) / kLocal, kT, 0, st>>>(pos, sf, idx, n, max_leaf, skeys, sids, s.kl, s.kr,
                                                              s.klo, s.khi, s.par_in, s.par_lf, s.box_in, s.box_lf,
                                                              s.refit_flag, s.c, bvh->tris, bvh->perm, bvh->skeys,

@@ -112,13 +112,24 @@ struct BuildScratch {
     uint32_t* cpar;        // N parent link of each queue entry
     unsigned long long* cacc;  // N arrival counts and size sums
     uint32_t* coll_ctl;    // 256 words: [1] barrier count [2] barrier gen, [4..10] collapse control
+    // LBVH with SAH-rebuilt subtrees (RQ_BUILD_SAH; null otherwise)
+    uint32_t* sah_flag;    // N: 1 at the first sorted position of a subtree
+    uint32_t* sah_idx;     // N: exclusive scan of sah_flag
+    uint32_t* sah_hi;      // N: at a subtree's first position, its last
+    uint32_t* sah_L;       // N: at a subtree's first position, the left-child links above its root
+    uint32_t* sah_node;    // N: at a subtree's first position, its root (bit 31: a Karras leaf)
+    uint32_t* sah_list;    // N: first positions of the subtrees, in order
+    float4* sah_rec;       // 4N: two float4 per node record (box, first position, aux word)
+    uint32_t* sah_rec_l;   // 2N: left-child links above the node, or kNoRecord for an unused slot
 };
 
 // Carve the build scratch for n triangles out of `base`; returns its size
-// (base may be null to measure).
-size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s);
+// (base may be null to measure).  sah: also the SAH-subtree arrays.
+size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s, bool sah = false);
+// sah_max > 0: the LBVH above every node of at most sah_max triangles, each
+// such subtree rebuilt by binned SAH (RQ_BUILD_SAH); 0: the plain LBVH.
 int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
-                    uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t s);
+                    uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t s, uint32_t sah_max = 0);
 // The reference's median-split topology (k_median.cu); synchronises once per tree level.
 int rq_launch_build_median(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_bytes, const uint32_t* idx,
                            uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t s);

@@ -34,6 +34,8 @@ RQ_FAULT_LAUNCH = 2
 
 RQ_BUILD_BVH4 = 1
 RQ_BUILD_MEDIAN = 2
+RQ_BUILD_SAH = 4
+SAH_SUBTREE_MAX = 1024
 RQ_TRACE_CLOSEST = 0
 RQ_TRACE_ANY = 1
 RQ_TRI_WATERTIGHT = 0
@@ -341,14 +343,16 @@ class Bvh:
         self.h = handle
 
     @staticmethod
-    def build(ctx, pos, idx=None, max_leaf=4, bvh4=True, stride_bytes=12, stream=None, into=None, median=False):
+    def build(ctx, pos, idx=None, max_leaf=4, bvh4=True, stride_bytes=12, stream=None, into=None, median=False,
+              sah=False):
         """pos: float32 CUDA tensor of vertices; idx: int32/uint32 CUDA tensor
         [T, 3] or None (non-indexed: 3 consecutive vertices per triangle).
-        median: the reference's median-split topology (RQ_BUILD_MEDIAN)."""
+        median: the reference's median-split topology (RQ_BUILD_MEDIAN);
+        sah: the LBVH with SAH-rebuilt subtrees (RQ_BUILD_SAH)."""
         nverts = _count(pos, 4) * 4 // stride_bytes
         ntri = _count(idx, 12) if idx is not None else nverts // 3
         h = _P(into.h.value) if into is not None else _P()
-        flags = (RQ_BUILD_BVH4 if bvh4 else 0) | (RQ_BUILD_MEDIAN if median else 0)
+        flags = (RQ_BUILD_BVH4 if bvh4 else 0) | (RQ_BUILD_MEDIAN if median else 0) | (RQ_BUILD_SAH if sah else 0)
         rc = lib().rq_build(ctx.h, _ptr(pos), stride_bytes, nverts, _ptr(idx), ntri, max_leaf, flags, C.byref(h),
                             _stream(stream))
         ctx.check(rc, "rq_build")

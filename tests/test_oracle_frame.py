@@ -158,3 +158,51 @@ def test_recover_perm_inverts_the_leaf_order():
     dup = np.concatenate([idx, idx[:1]])
     with pytest.raises(AssertionError):
         O.recover_perm(o["tris"], pos, dup)
+
+
+@pytest.mark.parametrize("n,max_leaf", [(1, 4), (7, 4), (1500, 4), (5000, 2), (3000, 8)])
+def test_oracle_sah_subtree_build_invariants(n, max_leaf):
+    # the LBVH with SAH-rebuilt subtrees: a permutation of the triangles in
+    # leaf order, every node's range contiguous and its box the union of its
+    # leaves, leaves of at most max_leaf, Morton keys and sort as the LBVH's
+    from conftest import soup
+    v = soup(n, 900 + n).reshape(-1)
+    o = O.lbvh_sah_build(v, None, max_leaf, 1024)
+    ol = O.lbvh_build(v, None, max_leaf)
+    assert np.array_equal(o["codes"], ol["codes"]) and np.array_equal(o["sorted"], ol["sorted"])
+    assert np.array_equal(np.sort(o["perm"]), np.arange(n, dtype=np.uint32))
+    tri = v.reshape(-1, 3, 3)[o["perm"]]
+    assert np.array_equal(o["tris"]["v0"][:, :3], tri[:, 0])
+    lo, hi = tri.min(1), tri.max(1)
+    n2 = o["nodes2"]
+
+    def walk(k):
+        nd = n2[k]
+        if nd["left_child"] < 0:
+            f, c = ~int(nd["left_child"]), int(nd["right_child"])
+            assert 1 <= c <= max_leaf
+            rng = (f, f + c)
+        else:
+            a, b = walk(int(nd["left_child"])), walk(int(nd["right_child"]))
+            assert a[1] == b[0] and int(nd["left_child"]) == k + 1
+            rng = (a[0], b[1])
+        assert np.array_equal(nd["aabb_min"], lo[rng[0]:rng[1]].min(0))
+        assert np.array_equal(nd["aabb_max"], hi[rng[0]:rng[1]].max(0))
+        return rng
+
+    assert walk(0) == (0, n)
+
+
+def test_oracle_sah_subtrees_need_fewer_node_visits():
+    pos, idx = O.scene_grid(300, 300, seed=1)
+    o = O.lbvh_sah_build(pos.reshape(-1), idx.reshape(-1), 4, 1024)
+    ol = O.lbvh_build(pos.reshape(-1), idx.reshape(-1))
+    w, h = 160, 90
+    cam = O.camera_look_at(O.SHADOW_EYE, O.SHADOW_TARGET, O.SHADOW_UP, O.SHADOW_FOVY, w, h)
+    g = O.render_gbuffer(ol["nodes4"], ol["tris"], ol["sorted"], cam)
+    params = O.shade_params(w, h, O.shadow_lights(16), ao_spp=1, ao_tmax=0.5)
+    rays, _, _ = O.shade_rays(g, params, np.arange(w * h, dtype=np.uint32))
+    hs, _, ss = O.trace_bvh4(o["nodes4"], o["tris"], o["perm"], rays, 1, want_stats=True)
+    hl, _, sl = O.trace_bvh4(ol["nodes4"], ol["tris"], ol["sorted"], rays, 1, want_stats=True)
+    assert np.array_equal(hs["hit"], hl["hit"])  # any-hit results do not depend on the tree
+    assert ss["box_tests"].mean() < 0.95 * sl["box_tests"].mean()
