@@ -35,10 +35,13 @@ sys.path.insert(0, os.path.join(ROOT, "rdna2-accel-raster_b200"))
 
 WIDTH, HEIGHT = 1920, 1080
 METRIC = "Mrays/s + BVH Mtris/s on 1 B200; p50/p99 request latency batched vs plain"
-# kernels launched by one step of the default workload: build = centroids,
-# morton, hist, hist_scan, 4 onesweep passes, karras, leaves, scan, emit,
-# collapse (13); then gbuffer and shadow/AO
-KERNELS_PER_STEP = 15
+# kernels launched by one step of the frame: the build — centroids, morton,
+# hist, hist_scan, 4 onesweep passes, karras, then leaves, scan, emit (plain
+# LBVH) or subtree roots, scan, list, subtree build, scan, emit (SAH
+# subtrees), then collapse: 13 or 16 — then G-buffer, shadow/AO and the
+# shade finish (3)
+BUILD_KERNELS = {"lbvh": 13, "sah": 16}
+FRAME_KERNELS = 3
 
 
 def parse():
@@ -48,6 +51,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=200000, help="pixels in the CPU baseline sample")
+    ap.add_argument("--build", choices=["lbvh", "sah"], default="sah",
+                    help="the frame's per-step build: plain LBVH, or LBVH with SAH-rebuilt subtrees (RQ_BUILD_SAH)")
+    ap.add_argument("--serve-catalogue", type=int, default=256,
+                    help="meshes in the serving catalogue (fewer for a small profiling case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the visibility / batched / serving workloads")
     ap.add_argument("--extra", choices=["visibility", "batched", "serving", "radv"],
@@ -162,18 +169,23 @@ def replica_line(pg, rank, world, ms_local, rays_local):
     return {"ms_per_step": ms, "value": rays / (ms * 1e-3) / 1e6, "n_gpus": world} if rank == 0 else None
 
 
-def read_traffic(name):
-    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.md)."""
+def read_profile(name, key):
+    """A `key: value` figure from a committed ncu summary (profiles/<name>.md),
+    e.g. traffic_bytes_per_launch (DRAM read + write bytes of one launch)."""
     path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     for ln in open(path):
-        if ln.strip().startswith("traffic_bytes_per_launch:"):
+        if ln.strip().startswith(key + ":"):
             try:
                 return float(ln.split(":", 1)[1].strip())
             except ValueError:
                 return None
     return None
+
+
+def read_traffic(name):
+    return read_profile(name, "traffic_bytes_per_launch")
 
 
 def frame_config(world):
@@ -287,6 +299,7 @@ def run_ours(args, world, rank, local, pg):
     from rq import workloads as W
 
     ctx = rq.Context(local)
+    sah = args.build == "sah"
     pos, idx = W.shadow_mesh()
     ntri = len(idx)
     cam = W.shadow_camera()
@@ -302,10 +315,10 @@ def run_ours(args, world, rank, local, pg):
     mask = torch.empty(npx, dtype=torch.int32, device=dev)
     ao = torch.empty(npx, dtype=torch.float32, device=dev)
     counters = torch.zeros(4, dtype=torch.int64, device=dev)
-    bvh = rq.Bvh.build(ctx, p_d, i_d)
+    bvh = rq.Bvh.build(ctx, p_d, i_d, sah=sah)
 
     def step(count=None):
-        rq.Bvh.build(ctx, p_d, i_d, into=bvh)
+        rq.Bvh.build(ctx, p_d, i_d, into=bvh, sah=sah)
         rq.render_gbuffer(ctx, bvh, cam, gbuf)
         rq.render_shadow_ao(ctx, bvh, gbuf, params, mask, ao, count)
 
@@ -320,7 +333,7 @@ def run_ours(args, world, rank, local, pg):
     # launch shape of the shadow/AO traversal: committed autotuner table,
     # else tuned now (untimed)
     from rq import tune as T
-    skey = T.shadow_key(len(idx), params)
+    skey = T.shadow_key(len(idx), params, sah)
     sshape = T.lookup_shadow(skey)
     if sshape is not None:
         ctx.set_trace_tuning(**sshape)
@@ -352,7 +365,7 @@ def run_ours(args, world, rank, local, pg):
         for s in range(args.steps):
             e0, e1, e2, e3 = ev[1 + 4 * s: 5 + 4 * s]
             e0.record(stream)
-            rq.Bvh.build(ctx, p_d, i_d, into=bvh)
+            rq.Bvh.build(ctx, p_d, i_d, into=bvh, sah=sah)
             e1.record(stream)
             rq.render_gbuffer(ctx, bvh, cam, gbuf)
             e2.record(stream)
@@ -433,7 +446,7 @@ def run_ours(args, world, rank, local, pg):
             stream.wait_event(up[k])
             if out[k] is not None:
                 stream.wait_event(out[k])  # this result set has been downloaded
-            rq.Bvh.build(ctx, p2[k], i2[k], into=bvh)
+            rq.Bvh.build(ctx, p2[k], i2[k], into=bvh, sah=sah)
             used[k] = torch.cuda.Event()
             used[k].record(stream)
             rq.render_gbuffer(ctx, bvh, cam, gbuf)
@@ -529,6 +542,9 @@ def run_ours(args, world, rank, local, pg):
     comp_bytes = npx * (32 + 8)
     comp_gbs = comp_bytes / (shade_med * 1e-3) / 1e9
     traffic = read_traffic("k_shadow_ao_1080p.md")
+    # what binds the kernel, from the same capture: instruction issue and L1
+    binding = {k: read_profile("k_shadow_ao_1080p.md", k) for k in
+               ("issue_active_frac", "l1tex_busy_frac", "lanes_per_instruction", "dram_frac")}
     clocks = clk.summary()
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -552,6 +568,8 @@ def run_ours(args, world, rank, local, pg):
         "dtype": "f32",
         "data": "synthetic",
         "config": frame_config(world),
+        "build_mode": ("LBVH with SAH-rebuilt subtrees of at most 1,024 triangles (RQ_BUILD_SAH)" if sah
+                       else "LBVH (Karras hierarchy, Morton order)"),
         "frame": {"triangles": ntri, "rays_per_step": frame_rays, "primary_rays": npx, "secondary_rays": sec_rays,
                   "primary_hits": hits},
         "build_mtris_per_s": round(ntri / statistics.median(build_ms) / 1e3, 1),
@@ -573,13 +591,16 @@ def run_ours(args, world, rank, local, pg):
                      "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback",
                      "algorithmic_bytes_per_launch": round(alg_bytes),
+                     "binding": dict(binding, source="profiles/k_shadow_ao_1080p.md (ncu, same kernel and frame)",
+                                     what=("the algorithmic bytes are consumed from L1/L2: the kernel is bound by "
+                                           "instruction issue and the L1, not by HBM (dram_frac)")),
                      "compulsory": {"bytes_per_launch": comp_bytes, "achieved": round(comp_gbs, 2),
                                     "frac": round(comp_gbs / hbm, 5),
                                     "what": "G-buffer pixel in (32 B) + light mask / AO word out (8 B); rays are "
                                             "generated in the kernel, so no ray or hit record crosses HBM"}},
         "cpu_baseline": cpu,
         "clocks": clocks,
-        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "gpu_launches": (BUILD_KERNELS[args.build] + FRAME_KERNELS) * args.steps,
         "shadow_tuning": shade_tuning,
         "ao_blur": blur,
         "median_build": median_build,
@@ -1059,7 +1080,7 @@ def run_extra(args):
         out = run_radv_build(ctx, dev, load_peaks(), reps=max(1, args.steps),
                              meshes=(("frame_2.5M", W.shadow_mesh),))
     else:
-        out = run_serving(dev, duration_s=max(0.05, args.steps * 0.05))
+        out = run_serving(dev, duration_s=max(0.05, args.steps * 0.05), catalogue=args.serve_catalogue)
     print(json.dumps({"extra": args.extra, **out}))
 
 

@@ -61,9 +61,9 @@ INLOOP_LEAF_BATCH = (4, 8, 12, 16, 24)
 SHAPE_KEYS = ("threads", "chunk", "reg_cap", "top_levels", "speculative", "refill_min", "leaf_batch")
 
 
-def shadow_key(ntri, params):
+def shadow_key(ntri, params, sah=False):
     return (f"shadow_ao:tris={ntri},{params.width}x{params.height},lights={params.num_lights},"
-            f"ao_spp={params.ao_spp}")
+            f"ao_spp={params.ao_spp}" + (",build=sah" if sah else ""))
 
 
 def tune_shadow(ctx, bvh, gbuf, params, reps=5):
@@ -138,6 +138,7 @@ def main():
     ap.add_argument("--out", required=True)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--only", choices=["shadow", "batched"], help="tune one workload, keep the other's entry")
+    ap.add_argument("--build", choices=["lbvh", "sah"], default="sah", help="the frame's build for the shadow tuning")
     args = ap.parse_args()
     ctx = rq.Context(0)
     table = load(args.out) if os.path.exists(args.out) else {}
@@ -159,12 +160,14 @@ def tune_frame(ctx, table, args):
     pos, idx = W.shadow_mesh()
     p = torch.from_numpy(pos).cuda()
     i = torch.from_numpy(idx.view(np.int32)).cuda()
-    bvh = rq.Bvh.build(ctx, p, i)
+    sah = args.build == "sah"
+    bvh = rq.Bvh.build(ctx, p, i, sah=sah)
     params = W.shadow_params()
     gbuf = rq.render_gbuffer(ctx, bvh, W.shadow_camera())
     shape, trials = tune_shadow(ctx, bvh, gbuf, params, args.reps)
-    table.setdefault("shadow", {})[shadow_key(len(idx), params)] = {
-        "workload": "1080p shadows + AO frame (2.5M-triangle grid, seed 1, 16 lights, 1 AO ray)",
+    table.setdefault("shadow", {})[shadow_key(len(idx), params, sah)] = {
+        "workload": ("1080p shadows + AO frame (2.5M-triangle grid, seed 1, 16 lights, 1 AO ray)"
+                     + (", LBVH with SAH-rebuilt subtrees" if sah else ", LBVH")),
         "shape": shape, "ms": min(t["ms"] for t in trials), "trials": trials}
     print(json.dumps({"shadow_shape": shape, "ms": min(t["ms"] for t in trials)}))
     bvh.destroy()

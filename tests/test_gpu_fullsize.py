@@ -240,3 +240,41 @@ def test_c4_fresh_build_refit_and_rebuild(ctx, c4, have_ref):
     ctx.sync_check()
     assert_build_equals_oracle(b, p199, idx)
     b.destroy()
+
+
+def test_c2_sah_build_and_frame_equal_oracle(ctx, c2):
+    # the frame's build in the benchmark: the LBVH with SAH-rebuilt subtrees,
+    # byte-equal to the oracle's statement at 2.5M triangles, and the frame
+    # traced on it bit-exact with the oracle on that tree; its light masks
+    # and AO equal the plain LBVH frame's wherever the G-buffers agree (any-
+    # hit results do not depend on the tree)
+    pos, idx, b_lbvh = c2
+    p_d, i_d = device_mesh(pos, idx)
+    b = rq.Bvh.build(ctx, p_d, i_d, sah=True)
+    ctx.sync_check()
+    n2, tr, n4, perm = b.download()
+    keys, _ = b.download_sort()
+    o = O.lbvh_sah_build(pos.reshape(-1), idx.reshape(-1), 4, rq.SAH_SUBTREE_MAX)
+    assert np.array_equal(keys, o["codes"][o["sorted"]]) and np.array_equal(perm, o["perm"])
+    assert n2.tobytes() == o["nodes2"].tobytes() and tr.tobytes() == o["tris"].tobytes()
+    assert n4.tobytes() == o["nodes4"].tobytes()
+    assert len(n4) < 0.9 * len(b_lbvh.download()[2])
+    cam, params = W.shadow_camera(), W.shadow_params()
+    gb = rq.render_gbuffer(ctx, b, cam)
+    mask, ao = rq.render_shadow_ao(ctx, b, gb, params)
+    gb_l = rq.render_gbuffer(ctx, b_lbvh, cam)
+    mask_l, ao_l = rq.render_shadow_ao(ctx, b_lbvh, gb_l, params)
+    ctx.sync_check()
+    gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    pixels = sample_pixels(13)
+    og = O.render_gbuffer(n4, tr, perm, cam, pixels)
+    assert gbn[pixels].tobytes() == og.tobytes()
+    om, oa, _ = O.render_shadow_ao(n4, tr, gbn, params, pixels)
+    assert np.array_equal(mask.cpu().numpy().astype(np.uint32)[pixels], om)
+    assert ao.cpu().numpy()[pixels].tobytes() == oa.tobytes()
+    gl = gb_l.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
+    agree = (gbn["vis"] == gl["vis"]) & (gbn["t"] == gl["t"])
+    assert agree.mean() > 1 - 1e-4, agree.mean()
+    assert np.array_equal(mask.cpu().numpy()[agree], mask_l.cpu().numpy()[agree])
+    assert np.array_equal(ao.cpu().numpy()[agree], ao_l.cpu().numpy()[agree])
+    b.destroy()
