@@ -341,6 +341,12 @@ def run_ours(args, world, rank, local, pg):
     else:
         sshape, strials = T.tune_shadow(ctx, bvh, gbuf, params, reps=3)
         shade_tuning = {"source": f"autotuned in this run ({len(strials)} shapes timed)", **sshape}
+    cshape = T.lookup_camera(skey)
+    if cshape is not None:
+        ctx.set_camera_tuning(**cshape)
+        camera_tuning = {"source": "committed table rq/tuning_b200.json", **cshape}
+    else:
+        camera_tuning = {"source": "default (one ray per thread)", **ctx.camera_tuning()}
 
     # node / triangle tests per any-hit ray, for the algorithmic bytes
     cp = rq.shade_params(WIDTH, HEIGHT, W.shadow_lights(16), ao_spp=1, ao_tmax=0.5,
@@ -602,6 +608,7 @@ def run_ours(args, world, rank, local, pg):
         "clocks": clocks,
         "gpu_launches": (BUILD_KERNELS[args.build] + FRAME_KERNELS) * args.steps,
         "shadow_tuning": shade_tuning,
+        "camera_tuning": camera_tuning,
         "ao_blur": blur,
         "median_build": median_build,
         "reference_benchmarks": refbench,

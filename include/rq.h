@@ -82,6 +82,18 @@ int rq_ctx_trace_tuning_get(const rq_ctx* ctx, rq_trace_tuning* out);
 /* RQ_ERR_INVALID_ARG for a shape that has no kernel. */
 int rq_ctx_trace_tuning_set(rq_ctx* ctx, const rq_trace_tuning* t);
 
+/* Schedule of the context's camera traversal (rq_render_gbuffer).  Results
+ * do not depend on it. */
+typedef struct rq_camera_tuning {
+    uint32_t engine;      /* 0: one ray per thread, 8x4-pixel tiles per warp (default); 1: the
+                             persistent refilling engine with in-loop refill (128-thread blocks,
+                             64 registers) */
+    uint32_t refill_min;  /* engine: idle lanes before a refill, 1..32 (0 means 1) */
+    uint32_t leaf_batch;  /* engine: parked leaves that end the node loop, 1..32 (0 means 32) */
+} rq_camera_tuning;
+int rq_ctx_camera_tuning_get(const rq_ctx* ctx, rq_camera_tuning* out);
+int rq_ctx_camera_tuning_set(rq_ctx* ctx, const rq_camera_tuning* t);
+
 /* ------------------------------------------------------------------ */
 /* Mesh generation and deformation (inputs of the BVH path)            */
 /* ------------------------------------------------------------------ */

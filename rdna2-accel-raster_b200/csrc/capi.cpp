@@ -223,6 +223,22 @@ int rq_ctx_trace_tuning_set(rq_ctx* ctx, const rq_trace_tuning* t) {
     return RQ_OK;
 }
 
+int rq_ctx_camera_tuning_get(const rq_ctx* ctx, rq_camera_tuning* out) {
+    if (!ctx || !out) return RQ_ERR_INVALID_ARG;
+    *out = ctx->camera;
+    return RQ_OK;
+}
+
+int rq_ctx_camera_tuning_set(rq_ctx* ctx, const rq_camera_tuning* t) {
+    if (!ctx || !t) return RQ_ERR_INVALID_ARG;
+    if (t->engine > 1 || t->refill_min > 32 || t->leaf_batch > 32)
+        return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "bad camera schedule");
+    ctx->camera = *t;
+    if (ctx->camera.refill_min == 0) ctx->camera.refill_min = 1;
+    if (ctx->camera.leaf_batch == 0) ctx->camera.leaf_batch = 32;
+    return RQ_OK;
+}
+
 // ---------------------------------------------------------------- meshes
 
 int rq_deform_wave(rq_ctx* ctx, const float* base, float* out, uint32_t num_vertices, float t, float amp,

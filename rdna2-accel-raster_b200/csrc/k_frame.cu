@@ -219,6 +219,20 @@ __global__ void __launch_bounds__(kT) k_gbuffer_seq(const rq_bvh4_node* __restri
     src.finish(id, m, r, h);
 }
 
+// Camera rays on the refilling engine with in-loop refill (closest hit):
+// rays that need few nodes hand their lane to the next pixel instead of
+// waiting for the warp's longest ray.
+template <bool MT, int TT, int REGS>
+__global__ void __launch_bounds__(TT, 65536 / (TT * REGS))
+    k_gbuffer_eng(const rq_bvh4_node* __restrict__ nodes, const rq_triangle* __restrict__ tris,
+                  const __grid_constant__ GbufSrc src0, uint32_t* ctr, uint32_t* err, int stack, int refill_min,
+                  int leaf_batch) {
+    extern __shared__ __align__(16) int32_t s_stack[];
+    GbufSrc src = src0;
+    rq::trace_persistent<0, MT, false, 128, TT, GbufSrc, 32, 0, false, true>(
+        nodes, tris, src, ctr, s_stack + threadIdx.x, err, stack, nullptr, refill_min, leaf_batch);
+}
+
 // TT threads per block, CHUNK ray ids per refill, REGS: launch bounds that
 // hold registers to REGS (0: none) — the tuned shapes; `stack` rows per lane;
 // idle lanes are refilled once `refill_min` of a warp's lanes are idle.
@@ -502,6 +516,26 @@ int rq_launch_gbuffer(rq_ctx* ctx, const rq_bvh* bvh, const rq_camera& cam, rq_g
     src.gbuf = gbuf;
     const uint32_t bound = 3u * (bvh->h_counts[2] + 2u) + 1u;
     const bool mt = cam.flags & RQ_TRI_MT;
+    if (ctx->camera.engine) {
+        constexpr int kET = 128, kER = 64;
+        const int stack = int((bound + 3u) & ~3u);
+        const void* k = mt ? reinterpret_cast<const void*>(k_gbuffer_eng<true, kET, kER>)
+                           : reinterpret_cast<const void*>(k_gbuffer_eng<false, kET, kER>);
+        const size_t smem = size_t(stack) * kET * sizeof(int32_t);
+        uint32_t blocks = 0;
+        cudaError_t e = cudaMemsetAsync(ctx->d_ctr, 0, sizeof(uint32_t), st);
+        if (e == cudaSuccess) e = persistent_grid(ctx, k, kET, smem, blocks);
+        if (e == cudaSuccess) {
+            const rq_bvh4_node* nodes = bvh->nodes4;
+            const rq_triangle* tris = bvh->tris;
+            uint32_t* ctr = ctx->d_ctr;
+            uint32_t* err = ctx->d_err;
+            int stk = stack, rm = int(ctx->camera.refill_min), lb = int(ctx->camera.leaf_batch);
+            void* args[] = {&nodes, &tris, &src, &ctr, &err, &stk, &rm, &lb};
+            e = cudaLaunchKernel(k, dim3(blocks), dim3(kET), args, smem, st);
+        }
+        return rq_cuda_status(ctx, e, "gbuffer launch");
+    }
     dim3 grid((cam.width + 15) / 16, (cam.height + 7) / 8);
     cudaError_t e = with_stack(bound, [&](auto S) {
         constexpr int STACK = decltype(S)::value;

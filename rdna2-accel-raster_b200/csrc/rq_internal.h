@@ -38,6 +38,7 @@ struct rq_ctx {
     std::string last_error;
     int collapse_blocks = 0;        // co-resident blocks of the collapse kernel
     rq_trace_tuning shade_shape{128, 32, 80, 0, 0, 1, 0};  // shadow/AO traversal launch shape
+    rq_camera_tuning camera{0, 1, 32};                      // camera traversal schedule
 };
 
 struct rq_bvh {

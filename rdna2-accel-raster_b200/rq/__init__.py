@@ -119,6 +119,10 @@ class Instance(C.Structure):
                 ("blas", C.c_void_p)]
 
 
+class CameraTuning(C.Structure):
+    _fields_ = [("engine", C.c_uint32), ("refill_min", C.c_uint32), ("leaf_batch", C.c_uint32)]
+
+
 class TraceTuning(C.Structure):
     _fields_ = [("threads", C.c_uint32), ("chunk", C.c_uint32), ("reg_cap", C.c_uint32), ("top_levels", C.c_uint32),
                 ("speculative", C.c_uint32), ("refill_min", C.c_uint32), ("leaf_batch", C.c_uint32)]
@@ -166,6 +170,8 @@ SIGNATURES = [
     ("rq_ctx_scratch_bytes", C.c_uint64, [_P]),
     ("rq_ctx_trace_tuning_get", C.c_int, [_P, C.POINTER(TraceTuning)]),
     ("rq_ctx_trace_tuning_set", C.c_int, [_P, C.POINTER(TraceTuning)]),
+    ("rq_ctx_camera_tuning_get", C.c_int, [_P, C.POINTER(CameraTuning)]),
+    ("rq_ctx_camera_tuning_set", C.c_int, [_P, C.POINTER(CameraTuning)]),
     ("rq_debug_wait_timeout", C.c_int, [_P, _P, _U32, _P]),
     ("rq_scene_grid", C.c_int, [_U32, _U32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                 C.c_float, C.c_uint64, _P, _P]),
@@ -333,6 +339,15 @@ class Context:
                          leaf_batch=0):
         t = TraceTuning(threads, chunk, reg_cap, top_levels, speculative, refill_min, leaf_batch)
         self.check(lib().rq_ctx_trace_tuning_set(self.h, C.byref(t)), "rq_ctx_trace_tuning_set")
+
+    def camera_tuning(self):
+        t = CameraTuning()
+        self.check(lib().rq_ctx_camera_tuning_get(self.h, C.byref(t)), "rq_ctx_camera_tuning_get")
+        return {"engine": t.engine, "refill_min": t.refill_min, "leaf_batch": t.leaf_batch}
+
+    def set_camera_tuning(self, engine=0, refill_min=1, leaf_batch=32):
+        t = CameraTuning(engine, refill_min, leaf_batch)
+        self.check(lib().rq_ctx_camera_tuning_set(self.h, C.byref(t)), "rq_ctx_camera_tuning_set")
 
 
 class Bvh:

@@ -115,6 +115,49 @@ def tune_shadow(ctx, bvh, gbuf, params, reps=5):
     return {k: best.get(k, 0) for k in SHAPE_KEYS}, trials
 
 
+CAMERA_REFILL = (1, 4, 8, 16)
+CAMERA_LEAF_BATCH = (4, 8, 16, 32)
+
+
+def tune_camera(ctx, bvh, cam, reps=5):
+    """Time rq_render_gbuffer on one ray per thread and on the refilling
+    engine (refill threshold x leaf batch); keep the fastest.  Returns
+    (schedule, trials)."""
+    import statistics
+    import torch
+    import rq
+    gbuf = torch.empty((cam.width * cam.height, 8), dtype=torch.int32, device="cuda")
+    trials = []
+
+    def timed(engine, refill, lb):
+        ctx.set_camera_tuning(engine, refill, lb)
+        rq.render_gbuffer(ctx, bvh, cam, gbuf)
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            rq.render_gbuffer(ctx, bvh, cam, gbuf)
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        ctx.sync_check()
+        trials.append({"engine": engine, "refill_min": refill, "leaf_batch": lb, "ms": statistics.median(ms)})
+
+    timed(0, 1, 32)
+    for refill in CAMERA_REFILL:
+        for lb in CAMERA_LEAF_BATCH:
+            timed(1, refill, lb)
+    best = min(trials, key=lambda x: x["ms"])
+    keys = ("engine", "refill_min", "leaf_batch")
+    ctx.set_camera_tuning(**{k: best[k] for k in keys})
+    return {k: best[k] for k in keys}, trials
+
+
+def lookup_camera(key, path=TABLE):
+    e = load(path).get("camera", {}).get(key)
+    return e["shape"] if e else None
+
+
 def lookup_shadow(key, path=TABLE):
     e = load(path).get("shadow", {}).get(key)
     return e["shape"] if e else None
@@ -170,6 +213,11 @@ def tune_frame(ctx, table, args):
                      + (", LBVH with SAH-rebuilt subtrees" if sah else ", LBVH")),
         "shape": shape, "ms": min(t["ms"] for t in trials), "trials": trials}
     print(json.dumps({"shadow_shape": shape, "ms": min(t["ms"] for t in trials)}))
+    cshape, ctrials = tune_camera(ctx, bvh, W.shadow_camera(), args.reps)
+    table.setdefault("camera", {})[shadow_key(len(idx), params, sah)] = {
+        "workload": "1080p frame's primary rays (the shadows + AO frame's camera)",
+        "shape": cshape, "ms": min(t["ms"] for t in ctrials), "trials": ctrials}
+    print(json.dumps({"camera_schedule": cshape, "ms": min(t["ms"] for t in ctrials)}))
     bvh.destroy()
 
 

@@ -218,3 +218,25 @@ def test_depth_ao_bit_exact(ctx, flags, view):
     with pytest.raises(rq.RqError):
         rq.render_ao_depth(ctx, b, depth, rq.ao_depth_params(cam, spp=33))
     b.destroy()
+
+
+def test_every_camera_schedule_gives_identical_gbuffers(ctx):
+    # one ray per thread or the refilling engine with in-loop refill, every
+    # refill threshold and leaf batch: the same G-buffer bytes (closest hit,
+    # jittered, both triangle tests)
+    pos, idx = rq.scene_grid(160, 120, seed=6)
+    b = build(ctx, pos, idx)
+    base = ctx.camera_tuning()
+    assert base == {"engine": 0, "refill_min": 1, "leaf_batch": 32}
+    for flags in (0, rq.RQ_TRI_MT):
+        cam = W.visibility_camera(320, 200, jitter=True, seed=8, flags=flags)
+        want = rq.render_gbuffer(ctx, b, cam).cpu().numpy()
+        for refill, lb in ((1, 32), (1, 1), (8, 8), (16, 4), (32, 16)):
+            ctx.set_camera_tuning(1, refill, lb)
+            got = rq.render_gbuffer(ctx, b, cam)
+            ctx.sync_check()
+            assert got.cpu().numpy().tobytes() == want.tobytes(), (flags, refill, lb)
+        ctx.set_camera_tuning(**base)
+    with pytest.raises(rq.RqError):
+        ctx.set_camera_tuning(2, 1, 1)
+    b.destroy()
