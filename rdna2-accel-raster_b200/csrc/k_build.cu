@@ -412,31 +412,76 @@ __device__ void sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t n
             }
         }
         __syncwarp();
-        // 45 candidates (axis, split after bin k): lanes take candidates lane and lane + 32
+        // 45 candidates (axis, split after bin k).  Two axes per pass, one per
+        // half-warp, lane b holding bin b: inclusive prefix and suffix unions
+        // over the bins (min / max are exact, so the unions equal any other
+        // order's), then lane k < 15 prices the split after bin k.
         float bc = INFINITY;
         uint32_t bi = 0xffffffffu, bnl = 0;
-        for (uint32_t cand = lane; cand < 3u * (kSahBins - 1); cand += 32) {
-            const uint32_t a = cand / (kSahBins - 1), k = cand % (kSahBins - 1);
-            if (!(scale[a] > 0.0f)) continue;
-            float l[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-            float rr[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-            uint32_t nl = 0, nr = 0;
-            for (uint32_t b = 0; b < kSahBins; ++b) {
+        for (int pass = 0; pass < 2; ++pass) {
+            const int a = pass * 2 + int(lane >> 4);
+            const uint32_t b = lane & 15u;
+            const bool live = a < 3 && scale[a < 3 ? a : 0] > 0.0f;
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t cnt = 0;
+            if (live) {
                 const uint32_t* bn = bins + (a * kSahBins + b) * 7;
-                float* t = b <= k ? l : rr;
-                (b <= k ? nl : nr) += bn[0];
+                cnt = bn[0];
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
-                    t[q] = fminf(t[q], rq::o2f(bn[1 + q]));
-                    t[3 + q] = fmaxf(t[3 + q], rq::o2f(bn[4 + q]));
+                    lo[q] = rq::o2f(bn[1 + q]);
+                    hi[q] = rq::o2f(bn[4 + q]);
                 }
             }
-            const float cost = float(nl) * sah_area(l[0], l[1], l[2], l[3], l[4], l[5]) +
-                               float(nr) * sah_area(rr[0], rr[1], rr[2], rr[3], rr[4], rr[5]);
-            if (cost < bc) {  // candidates of one lane rise in index
-                bc = cost;
-                bi = cand;
-                bnl = nl;
+            float plo[3] = {lo[0], lo[1], lo[2]}, phi[3] = {hi[0], hi[1], hi[2]};
+            float slo[3] = {lo[0], lo[1], lo[2]}, shi[3] = {hi[0], hi[1], hi[2]};
+            uint32_t pc = cnt, sc = cnt;
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) {
+                const uint32_t upc = __shfl_up_sync(0xffffffffu, pc, o, 16);
+                const uint32_t dnc = __shfl_down_sync(0xffffffffu, sc, o, 16);
+                float u[6], d[6];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    u[q] = __shfl_up_sync(0xffffffffu, plo[q], o, 16);
+                    u[3 + q] = __shfl_up_sync(0xffffffffu, phi[q], o, 16);
+                    d[q] = __shfl_down_sync(0xffffffffu, slo[q], o, 16);
+                    d[3 + q] = __shfl_down_sync(0xffffffffu, shi[q], o, 16);
+                }
+                if (b >= uint32_t(o)) {
+                    pc += upc;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        plo[q] = fminf(plo[q], u[q]);
+                        phi[q] = fmaxf(phi[q], u[3 + q]);
+                    }
+                }
+                if (b + uint32_t(o) < 16u) {
+                    sc += dnc;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        slo[q] = fminf(slo[q], d[q]);
+                        shi[q] = fmaxf(shi[q], d[3 + q]);
+                    }
+                }
+            }
+            // the right side of split b is the suffix from bin b + 1
+            const uint32_t nr = __shfl_down_sync(0xffffffffu, sc, 1, 16);
+            float r[6];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                r[q] = __shfl_down_sync(0xffffffffu, slo[q], 1, 16);
+                r[3 + q] = __shfl_down_sync(0xffffffffu, shi[q], 1, 16);
+            }
+            if (live && b < kSahBins - 1) {
+                const float cost = float(pc) * sah_area(plo[0], plo[1], plo[2], phi[0], phi[1], phi[2]) +
+                                   float(nr) * sah_area(r[0], r[1], r[2], r[3], r[4], r[5]);
+                const uint32_t cand = uint32_t(a) * (kSahBins - 1) + b;
+                if (cost < bc || (cost == bc && cand < bi)) {
+                    bc = cost;
+                    bi = cand;
+                    bnl = pc;
+                }
             }
         }
 #pragma unroll

@@ -2,15 +2,18 @@
 compared with the reference pipeline (the reference's own SoftwareBVH tree
 traversed by the restated software_bvh_bvh4.comp).
 
-The two pipelines use different triangle tests (the engine's watertight test
-by default, the shader's Moller-Trumbore with |a| < 1e-7) and different
-trees, so they may disagree only on grazing rays: either both hit triangles
-that share a vertex, or one side misses where the other's crossing lies
-within 1e-5 (barycentric) of an edge of the triangle it hit, or the hit
-triangle is one the shader's test culls as parallel to the ray (its
-determinant |a| = |e1 . (d x e2)| below 1e-7, software_bvh_bvh4.comp:170).
-Those rays are counted and must stay under 1e-5 of the rays; every other
-disagreement is a failure."""
+In the shader's arithmetic (the engine's Moller-Trumbore mode) the two may
+differ only where two triangles that share a vertex are hit at the same t
+and the trees visit them in different orders (edge ties); those rays are
+counted and must stay under 1e-5 of the rays, and t agrees within 1e-6
+relative.  With the engine's default watertight test the triangle test
+itself differs: the shader's test culls triangles nearly parallel to the ray
+(|a| = |e1 . (d x e2)| < 1e-7, software_bvh_bvh4.comp:170), leaves cracks at
+shared edges, and loses the barycentrics to cancellation when the origin is
+far from a small triangle.  There, every disagreement must be reproduced by
+tracing the same ray with the engine in the shader's arithmetic on the same
+tree (the difference lies in the triangle test alone); such rays are counted
+by kind."""
 import numpy as np
 
 GRAZE_BARY = 1e-5
@@ -52,7 +55,8 @@ def ray_rows(rays):
     return r.view(np.float32).reshape(-1, 8)
 
 
-def graze_report(pos, idx, rays, ours_hit, ours_prim, ref_hit, ref_prim, closest=True, ours_t=None, ref_t=None):
+def graze_report(pos, idx, rays, ours_hit, ours_prim, ref_hit, ref_prim, closest=True, ours_t=None, ref_t=None,
+                 mt_hit=None, mt_prim=None):
     """Disagreements between the engine and the reference pipeline, sorted
     into explained kinds, and the rays no kind explains.
 
@@ -65,7 +69,11 @@ def graze_report(pos, idx, rays, ours_hit, ours_prim, ref_hit, ref_prim, closest
                  hit triangles share a vertex at equal t (a tie on the edge);
       "parallel" the engine hit a triangle, no farther than the reference's
                  hit, that the shader's Moller-Trumbore test culls as parallel
-                 to the ray (|a| < 1e-7, software_bvh_bvh4.comp:170).
+                 to the ray (|a| < 1e-7, software_bvh_bvh4.comp:170);
+      "test"     (mt_hit given: the engine's results for the same rays in the
+                 shader's arithmetic on the same tree) none of the above, but
+                 the engine in the shader's arithmetic gives the reference's
+                 result: the difference lies in the triangle test.
     Returns (indices of all disagreements, dict kind -> count, unexplained)."""
     pos = np.asarray(pos, np.float32).reshape(-1, 3)
     tri = np.asarray(idx, np.uint32).reshape(-1, 3)
@@ -76,7 +84,7 @@ def graze_report(pos, idx, rays, ours_hit, ours_prim, ref_hit, ref_prim, closest
     if closest:
         differ |= (ours_hit == 1) & (ref_hit == 1) & (ours_prim != ref_prim)
     dis = np.nonzero(differ)[0]
-    kinds = {"edge": 0, "parallel": 0}
+    kinds = {"edge": 0, "parallel": 0, "test": 0}
     unexplained = []
 
     def grazes(i, pid):
@@ -104,6 +112,10 @@ def graze_report(pos, idx, rays, ours_hit, ours_prim, ref_hit, ref_prim, closest
                 kind = "parallel" if culled(i, a) else "edge"
             elif to is not None and tr_ < to and grazes(i, b):
                 kind = "edge"
+        if kind is None and mt_hit is not None:
+            same_flag = int(mt_hit[i]) == int(ref_hit[i])
+            if same_flag and (not closest or ref_hit[i] == 0 or int(mt_prim[i]) == int(ref_prim[i])):
+                kind = "test"
         if kind is None:
             unexplained.append(int(i))
         else:
@@ -111,10 +123,19 @@ def graze_report(pos, idx, rays, ours_hit, ours_prim, ref_hit, ref_prim, closest
     return dis, kinds, unexplained
 
 
-def assert_t_close(ours_t, ref_t, mask):
+def assert_t_close(ours_t, ref_t, mask, mt_t=None):
     """Hit distances of rays both pipelines hit on the same primitive agree
-    within 1e-6 relative."""
+    within 1e-6 relative; with mt_t (the engine's t in the shader's
+    arithmetic), a ray off by more must have mt_t equal to the reference's t
+    (the two triangle tests round t differently on rays that graze the
+    triangle's plane).  Returns the number of such rays."""
     if not mask.any():
-        return
-    rel = np.abs(ours_t[mask].astype(np.float64) - ref_t[mask]) / np.abs(ref_t[mask].astype(np.float64))
-    assert rel.max() <= T_REL, rel.max()
+        return 0
+    rel = np.abs(ours_t.astype(np.float64) - ref_t) / np.abs(ref_t.astype(np.float64))
+    off = mask & (rel > T_REL)
+    if mt_t is None:
+        assert not off.any(), rel[mask].max()
+        return 0
+    assert np.array_equal(np.asarray(mt_t)[off].view(np.uint32), np.asarray(ref_t)[off].view(np.uint32)), \
+        rel[off].max()
+    return int(off.sum())
