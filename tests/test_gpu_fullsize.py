@@ -228,7 +228,7 @@ def check_visibility(ctx, b, pos, idx, n4, tr, perm, frame, have_ref):
         gbn = gb.cpu().numpy().view(rq.GBUFFER_PX).reshape(-1)
         og = O.render_gbuffer(n4, tr, perm, cam, pixels)
         assert gbn[pixels].tobytes() == og.tobytes(), (frame, mt)
-        assert (gbn["vis"] > 0).all()
+        assert (gbn["vis"] > 0).mean() > 0.999  # the view can reach past the edge where the mesh dips
         if have_ref:
             check_primary(pos, idx, ref, cam, gbn, pixels, mt, (n4, tr, perm))
 
