@@ -144,7 +144,8 @@ int rq_deform_wave_step(rq_ctx* ctx, const float* base, float* out, uint32_t num
 /* The LBVH's Karras hierarchy above every node of at most RQ_SAH_SUBTREE_MAX
  * triangles; each such subtree (a contiguous range of the Morton order) is
  * rebuilt top down by binned SAH (16 bins per axis over the node's centroid
- * bounds, the smallest float(nL)*SA(left) + float(nR)*SA(right), first by
+ * bounds for nodes of more than 32 triangles, 8 for smaller nodes; the
+ * smallest float(nL)*SA(left) + float(nR)*SA(right), first by
  * axis then by bin on ties, a stable partition, leaves of at most max_leaf
  * triangles; the middle of the range where no axis has a centroid extent or
  * 24 levels are reached).  Fewer node visits per ray than the plain LBVH

@@ -275,14 +275,16 @@ int32_t emit(LbvhState& S, bool is_leaf, int64_t id) {
 // ------------------------------------- LBVH with SAH-rebuilt subtrees --
 // The LBVH's Karras hierarchy above every node of at most K primitives; each
 // such subtree (a contiguous range of the Morton-sorted order) rebuilt top
-// down by binned SAH: 16 bins per axis over the node's centroid bounds, bin
-// b = min(15, int((c - cmin) * (16 / extent))), split cost
+// down by binned SAH: B bins per axis over the node's centroid bounds (B =
+// 16 for nodes of more than kSahSmallNode primitives, 8 for the others), bin
+// b = min(B - 1, int((c - cmin) * (B / extent))), split cost
 // float(nL) * SA(left) + float(nR) * SA(right) with SA = 2((dx dy + dy dz) + dz dx),
 // the smallest cost wins (strict <: the lower axis, then the lower bin, on
 // ties), a stable partition of the range; leaves of at most max_leaf
 // primitives; the middle of the range where no axis has a centroid extent
 // or the subtree is kSahDepthCap levels deep.  Nodes in depth-first pre-order.
-constexpr int kSahBins = 16;
+constexpr int kSahBinsMax = 16;
+constexpr uint32_t kSahSmallNode = 32;
 constexpr uint32_t kSahDepthCap = 24;
 
 struct SahState {
@@ -296,9 +298,9 @@ inline float sah_area(const float mn[3], const float mx[3]) {
     return 2.0f * ((dx * dy + dy * dz) + dz * dx);
 }
 
-inline int sah_bin(float c, float cmin, float scale) {
+inline int sah_bin(float c, float cmin, float scale, int bins) {
     const int b = int((c - cmin) * scale);
-    return b < kSahBins - 1 ? b : kSahBins - 1;
+    return b < bins - 1 ? b : bins - 1;
 }
 
 int32_t emit_sah(SahState& T, uint32_t s, uint32_t e, uint32_t depth) {
@@ -329,33 +331,34 @@ int32_t emit_sah(SahState& T, uint32_t s, uint32_t e, uint32_t depth) {
     float best = INFINITY, best_scale = 0.0f;
     int best_axis = -1, best_bin = -1;
     uint32_t best_nl = 0;
+    const int bins = n > kSahSmallNode ? 16 : 8;
     if (depth < kSahDepthCap) {
         for (int a = 0; a < 3; ++a) {
             const float ext = cmx[a] - cmn[a];
             if (!(ext > 0.0f)) continue;
-            const float scale = float(kSahBins) / ext;
+            const float scale = float(bins) / ext;
             if (!(scale < INFINITY)) continue;  // an extent too small to scale: no split there
-            uint32_t cnt[kSahBins] = {};
-            float bmn[kSahBins][3], bmx[kSahBins][3];
-            for (int b = 0; b < kSahBins; ++b)
+            uint32_t cnt[kSahBinsMax] = {};
+            float bmn[kSahBinsMax][3], bmx[kSahBinsMax][3];
+            for (int b = 0; b < bins; ++b)
                 for (int k = 0; k < 3; ++k) {
                     bmn[b][k] = INFINITY;
                     bmx[b][k] = -INFINITY;
                 }
             for (uint32_t i = s; i < e; ++i) {
                 const Prim& p = S.prims[T.order[i]];
-                const int b = sah_bin(p.c[a], cmn[a], scale);
+                const int b = sah_bin(p.c[a], cmn[a], scale, bins);
                 ++cnt[b];
                 for (int k = 0; k < 3; ++k) {
                     bmn[b][k] = fmin_(bmn[b][k], p.mn[k]);
                     bmx[b][k] = fmax_(bmx[b][k], p.mx[k]);
                 }
             }
-            for (int split = 0; split < kSahBins - 1; ++split) {
+            for (int split = 0; split < bins - 1; ++split) {
                 float lmn[3] = {INFINITY, INFINITY, INFINITY}, lmx[3] = {-INFINITY, -INFINITY, -INFINITY};
                 float rmn[3] = {INFINITY, INFINITY, INFINITY}, rmx[3] = {-INFINITY, -INFINITY, -INFINITY};
                 uint32_t nl = 0, nr = 0;
-                for (int b = 0; b < kSahBins; ++b) {
+                for (int b = 0; b < bins; ++b) {
                     float* tmn = b <= split ? lmn : rmn;
                     float* tmx = b <= split ? lmx : rmx;
                     (b <= split ? nl : nr) += cnt[b];
@@ -382,7 +385,7 @@ int32_t emit_sah(SahState& T, uint32_t s, uint32_t e, uint32_t depth) {
         std::vector<uint32_t> left, right;
         for (uint32_t i = s; i < e; ++i) {
             const uint32_t id = T.order[i];
-            (sah_bin(S.prims[id].c[best_axis], cmn[best_axis], best_scale) <= best_bin ? left : right).push_back(id);
+            (sah_bin(S.prims[id].c[best_axis], cmn[best_axis], best_scale, bins) <= best_bin ? left : right).push_back(id);
         }
         std::copy(left.begin(), left.end(), T.order.begin() + s);
         std::copy(right.begin(), right.end(), T.order.begin() + s + left.size());

@@ -178,9 +178,10 @@ __global__ void __launch_bounds__(kT) k_emit2(uint32_t n, uint32_t max_leaf, con
 // ------------------------------------------------- SAH-rebuilt subtrees
 // RQ_BUILD_SAH: the Karras hierarchy above every node of at most K
 // primitives stays; each such subtree (a contiguous range of the sorted
-// order) is rebuilt top down by binned SAH inside one block: 16 bins per axis
-// over the node's centroid bounds, bin = min(15, int((c - cmin) * (16 /
-// extent))), cost float(nL) * SA(left) + float(nR) * SA(right), the smallest
+// order) is rebuilt top down by binned SAH inside one block: B bins per axis
+// over the node's centroid bounds (B = 16 above kSahSmallNode primitives, 8 at
+// or below), bin = min(B - 1, int((c - cmin) * (B / extent))), cost
+// float(nL) * SA(left) + float(nR) * SA(right), the smallest
 // cost first by axis then bin, a stable partition of the node's range, leaves
 // of at most max_leaf primitives, the middle of the range where no axis has
 // a centroid extent or the subtree is kSahDepthCap levels deep.  Every node
@@ -192,7 +193,16 @@ __global__ void __launch_bounds__(kT) k_emit2(uint32_t n, uint32_t max_leaf, con
 constexpr uint32_t kSahMax = RQ_SAH_SUBTREE_MAX;  // largest subtree a block rebuilds
 constexpr int kSahT = 256;
 constexpr int kSahWarps = kSahT / 32;
-constexpr int kSahBins = 16;
+// Nodes of more than kSahSmallNode primitives are binned 16 ways per axis,
+// smaller ones 8 ways (as good for the small nodes, at half the pricing).
+constexpr uint32_t kSahSmallNode = 32;
+template <int NB>
+struct SahBinsOf {
+    static constexpr uint32_t slots = 3u * NB;       // (axis, bin) pairs of one node
+    static constexpr uint32_t words = 7u * slots;    // count, min xyz, max xyz: field-major
+    static constexpr int axes_per_pass = 32 / NB;    // axes one warp prices at a time
+    static_assert(words % 4u == 0u && slots % 4u == 0u, "bins are cleared with 16-byte stores");
+};
 constexpr uint32_t kSahDepthCap = 24;
 constexpr uint32_t kNoRecord = 0xffffffffu;
 
@@ -276,10 +286,10 @@ struct SahArgs {
 };
 
 // Shared memory of one subtree block (kSahMax primitives): boxes with the x
-// and y centroid in w, z centroids, triangle ids, the leaf order of two
-// consecutive levels (local indices), the node lists of two levels, and one
-// set of bins per warp (3 axes x 16 bins x (count, min xyz, max xyz) as
-// ordered integers).
+// and y centroid in w, z centroids, triangle ids, the leaf order at even and
+// odd depths (local indices), the node lists of two levels, and one set of
+// bins per warp (7 fields x 3 axes x 16 bins: count, min xyz, max xyz as
+// ordered integers, field-major).
 struct SahShared {
     float4 lo[kSahMax];
     float4 hi[kSahMax];
@@ -287,16 +297,27 @@ struct SahShared {
     uint32_t id[kSahMax];
     uint16_t ord[2][kSahMax];
     uint2 list[2][kSahMax];
-    uint32_t bins[kSahWarps][3 * kSahBins * 7];
+    alignas(16) uint32_t bins[kSahWarps][SahBinsOf<16>::words];
     uint32_t cnt[2];
     uint32_t slots;
     uint32_t job;
     float4 root_lo, root_hi;
 };
 
-__device__ __forceinline__ int sah_bin(float c, float cmin, float scale) {
-    const int b = __float2int_rz((c - cmin) * scale);
-    return b < kSahBins - 1 ? b : kSahBins - 1;
+// int((c - cmin) * scale) for a centroid c of the node: the product lies in
+// [0, ~bins] (scale = bins / the node's extent), and for x in [0, 2^23) the
+// sum 2^23 + x rounded toward zero is 2^23 + floor(x), so its low mantissa
+// bits are the truncation (an FADD instead of a float-to-int conversion, which
+// issues at a quarter of the rate).
+__device__ __forceinline__ uint32_t sah_floor(float c, float cmin, float scale) {
+    return __float_as_uint(__fadd_rz((c - cmin) * scale, 8388608.0f)) & 0x7fffffu;
+}
+
+// The bin: the truncation clamped to the last of NB bins.
+template <int NB>
+__device__ __forceinline__ uint32_t sah_bin(float c, float cmin, float scale) {
+    const uint32_t b = sah_floor(c, cmin, scale);
+    return b < uint32_t(NB - 1) ? b : uint32_t(NB - 1);
 }
 
 __device__ __forceinline__ float sah_area(float mnx, float mny, float mnz, float mxx, float mxy, float mxz) {
@@ -304,25 +325,207 @@ __device__ __forceinline__ float sah_area(float mnx, float mny, float mnz, float
     return 2.0f * ((dx * dy + dy * dz) + dz * dx);
 }
 
+__device__ __forceinline__ float sah_pick(const float (&v)[3], int a) {
+    return a == 0 ? v[0] : (a == 1 ? v[1] : v[2]);
+}
+
 __device__ __forceinline__ float sah_centroid(const SahShared& S, uint32_t p, int a) {
     return a == 0 ? S.lo[p].w : (a == 1 ? S.hi[p].w : S.cz[p]);
 }
 
-// Node list entry: x = s | e << 11 | depth << 22, y = slot | L << 12.
+// Node list entry: x = s | e << 11 | depth << 22, y = slot | L << 12 (slot:
+// the node's record slot; L: the consecutive left-child links above it).
 __device__ __forceinline__ uint2 sah_entry(uint32_t s, uint32_t e, uint32_t depth, uint32_t slot, uint32_t L) {
     return make_uint2(s | (e << 11) | (depth << 22), slot | (L << 12));
 }
 
+// The bins of one node (7 fields x 3 axes x NB bins, field-major: count,
+// min xyz, max xyz as ordered integers), cleared by one warp with 16-byte
+// stores (a field is a whole number of them).
+template <int NB>
+__device__ __forceinline__ void sah_bins_clear(uint32_t* bins, uint32_t lane) {
+    using B = SahBinsOf<NB>;
+    uint4* b4 = reinterpret_cast<uint4*>(bins);
+    for (uint32_t w = lane; w < B::words / 4u; w += 32) {
+        const uint32_t f = w / (B::slots / 4u);
+        const uint32_t v = f == 0 ? 0u : (f <= 3 ? rq::f2o(INFINITY) : rq::f2o(-INFINITY));
+        b4[w] = make_uint4(v, v, v, v);
+    }
+}
+
+// NB / extent per axis, 0 where the centroids have no extent or the extent is
+// too small to scale (no split on that axis).
+template <int NB>
+__device__ __forceinline__ void sah_scales(const float (&cmn)[3], const float (&cmx)[3], float (&scale)[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float ext = cmx[a] - cmn[a];
+        scale[a] = ext > 0.0f ? float(NB) / ext : 0.0f;
+        if (!(scale[a] < INFINITY)) scale[a] = 0.0f;
+    }
+}
+
+// Bins the primitives at ord[s, e) into `bins` (one warp).  Each lane bins a
+// run of C consecutive primitives: consecutive primitives are close in space
+// and mostly share a bin, so lanes on far-apart runs update different bins
+// (with the lanes on consecutive primitives, the warp's atomics serialise on
+// one address).  C is odd, so the 16-byte box loads of 8 lanes at stride C
+// fall in distinct banks.
+template <int NB>
+__device__ __forceinline__ void sah_bin_range(const SahShared& S, uint32_t* bins, const uint16_t* ord, uint32_t s,
+                                              uint32_t e, uint32_t lane, const float (&cmn)[3],
+                                              const float (&scale)[3]) {
+    const uint32_t run = ((e - s + 31u) >> 5) | 1u;
+    for (uint32_t j = 0; j < run; ++j) {
+        const uint32_t i = s + lane * run + j;
+        if (i >= e) break;
+        const uint32_t p = ord[i];
+        const float4 a4 = S.lo[p], b4 = S.hi[p];
+        const float c[3] = {a4.w, b4.w, S.cz[p]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (!(scale[a] > 0.0f)) continue;
+            constexpr uint32_t F = SahBinsOf<NB>::slots;
+            uint32_t* bn = bins + a * NB + sah_bin<NB>(c[a], cmn[a], scale[a]);
+            atomicAdd(bn, 1u);
+            atomicMin(bn + 1 * F, rq::f2o(a4.x));
+            atomicMin(bn + 2 * F, rq::f2o(a4.y));
+            atomicMin(bn + 3 * F, rq::f2o(a4.z));
+            atomicMax(bn + 4 * F, rq::f2o(b4.x));
+            atomicMax(bn + 5 * F, rq::f2o(b4.y));
+            atomicMax(bn + 6 * F, rq::f2o(b4.z));
+        }
+    }
+}
+
+// The split of the filled bins (one warp, every lane gets the result):
+// 3 x (NB - 1) candidates (axis, split after bin k).  32 / NB axes per pass,
+// one per lane segment, lane b of a segment holding bin b: inclusive prefix
+// and suffix unions over the bins (min / max are exact, so the unions equal
+// any other order's), then lane k < NB - 1 prices the split after bin k.  The
+// winner is the smallest finite cost, the lowest candidate among equal costs.
+// axis < 0: no split.
+template <int NB>
+__device__ __forceinline__ void sah_choose(const uint32_t* bins, const float (&scale)[3], uint32_t lane, int& axis,
+                                           int& split, uint32_t& nl_out) {
+    constexpr uint32_t F = SahBinsOf<NB>::slots;
+    float bc = INFINITY;
+    uint32_t bi = 0xffffffffu, bnl = 0;
+    for (int pass = 0; pass * SahBinsOf<NB>::axes_per_pass < 3; ++pass) {
+        const int a = pass * SahBinsOf<NB>::axes_per_pass + int(lane / NB);
+        const uint32_t b = lane % NB;
+        const bool live = a < 3 && sah_pick(scale, a) > 0.0f;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        uint32_t cnt = 0;
+        if (live) {
+            const uint32_t* bn = bins + a * NB + b;
+            cnt = bn[0];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                lo[q] = rq::o2f(bn[(1 + q) * F]);
+                hi[q] = rq::o2f(bn[(4 + q) * F]);
+            }
+        }
+        float plo[3] = {lo[0], lo[1], lo[2]}, phi[3] = {hi[0], hi[1], hi[2]};
+        float slo[3] = {lo[0], lo[1], lo[2]}, shi[3] = {hi[0], hi[1], hi[2]};
+        uint32_t pc = cnt, sc = cnt;
+#pragma unroll
+        for (int o = 1; o < NB; o <<= 1) {
+            const uint32_t upc = __shfl_up_sync(0xffffffffu, pc, o, NB);
+            const uint32_t dnc = __shfl_down_sync(0xffffffffu, sc, o, NB);
+            float u[6], d[6];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                u[q] = __shfl_up_sync(0xffffffffu, plo[q], o, NB);
+                u[3 + q] = __shfl_up_sync(0xffffffffu, phi[q], o, NB);
+                d[q] = __shfl_down_sync(0xffffffffu, slo[q], o, NB);
+                d[3 + q] = __shfl_down_sync(0xffffffffu, shi[q], o, NB);
+            }
+            if (b >= uint32_t(o)) {
+                pc += upc;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    plo[q] = fminf(plo[q], u[q]);
+                    phi[q] = fmaxf(phi[q], u[3 + q]);
+                }
+            }
+            if (b + uint32_t(o) < uint32_t(NB)) {
+                sc += dnc;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    slo[q] = fminf(slo[q], d[q]);
+                    shi[q] = fmaxf(shi[q], d[3 + q]);
+                }
+            }
+        }
+        // the right side of split b is the suffix from bin b + 1
+        const uint32_t nr = __shfl_down_sync(0xffffffffu, sc, 1, NB);
+        float r[6];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            r[q] = __shfl_down_sync(0xffffffffu, slo[q], 1, NB);
+            r[3 + q] = __shfl_down_sync(0xffffffffu, shi[q], 1, NB);
+        }
+        if (live && b < uint32_t(NB - 1)) {
+            const float cost = float(pc) * sah_area(plo[0], plo[1], plo[2], phi[0], phi[1], phi[2]) +
+                               float(nr) * sah_area(r[0], r[1], r[2], r[3], r[4], r[5]);
+            const uint32_t cand = uint32_t(a) * (NB - 1) + b;
+            if (cost < bc) {
+                bc = cost;
+                bi = cand;
+                bnl = pc;
+            }
+        }
+    }
+    // The smallest (cost, candidate): costs are +0, positive or +inf, so
+    // their bits order as their values.
+    const uint32_t cbits = __float_as_uint(bc);
+    const uint32_t cmin = __reduce_min_sync(0xffffffffu, cbits);
+    const uint32_t mine = cbits == cmin ? bi : 0xffffffffu;
+    const uint32_t win = __reduce_min_sync(0xffffffffu, mine);
+    const uint32_t holder = __ballot_sync(0xffffffffu, win != 0xffffffffu && mine == win);
+    bnl = __shfl_sync(0xffffffffu, bnl, holder ? uint32_t(__ffs(holder) - 1) : 0u);
+    axis = -1;
+    split = -1;
+    nl_out = 0;
+    if (win != 0xffffffffu) {
+        axis = int(win / (NB - 1));
+        split = int(win % (NB - 1));
+        nl_out = bnl;
+    }
+}
+
+// The binned split of a node (one warp): clear the warp's bins, bin the
+// node's primitives, price the candidates; the chosen axis's scale for the
+// partition.
+template <int NB>
+__device__ __forceinline__ void sah_split(const SahShared& S, uint32_t* bins, const uint16_t* ord, uint32_t s,
+                                          uint32_t e, uint32_t lane, const float (&cmn)[3], const float (&cmx)[3],
+                                          int& axis, int& split, uint32_t& nl, float& axis_scale) {
+    float scale[3];
+    sah_bins_clear<NB>(bins, lane);
+    sah_scales<NB>(cmn, cmx, scale);
+    __syncwarp();
+    sah_bin_range<NB>(S, bins, ord, s, e, lane, cmn, scale);
+    __syncwarp();
+    sah_choose<NB>(bins, scale, lane, axis, split, nl);
+    __syncwarp();  // the bins are read before the next node reuses them
+    axis_scale = axis < 0 ? 0.0f : sah_pick(scale, axis);
+}
+
 // One node of a subtree, by one warp: box and centroid bounds, then a leaf
-// (its record, emission counts, triangles) or the binned split, the stable
-// partition of its range into the next level's order, its record and its two
-// children appended to the next level's list.
-__device__ void sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t nsub, uint2 ent, int cur,
-                         uint32_t lane, uint32_t warp) {
+// (its record, emission counts, triangles; returns false) or the binned
+// split: the stable partition of its range into the order of the next depth,
+// its record, and its two children in every lane (returns true).  A node at
+// depth d reads ord[d & 1] and writes ord[(d + 1) & 1] over its own range:
+// ranges of nodes that are not ancestors of one another are disjoint, and a
+// node's range is complete before its children start.
+__device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent, uint32_t lane, uint32_t warp,
+                         uint2& left_child, uint2& right_child) {
     const uint32_t s = ent.x & 0x7ffu, e = (ent.x >> 11) & 0x7ffu, depth = ent.x >> 22;
     const uint32_t slot = ent.y & 0xfffu, L = ent.y >> 12;
-    const uint16_t* ord = S.ord[cur];
-    uint16_t* nxt = S.ord[cur ^ 1];
+    const uint16_t* ord = S.ord[depth & 1u];
+    uint16_t* nxt = S.ord[(depth + 1u) & 1u];
     const uint32_t n = e - s;
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     float cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -342,21 +545,37 @@ __device__ void sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t n
             cmx[k] = fmaxf(cmx[k], c[k]);
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
+    // Butterfly over the lanes that hold primitives (lanes n..31 hold the
+    // identities): ceil(log2(min(n, 32))) steps leave the bounds in lane 0.
+    // Leaves need only the box; a split needs the centroid bounds in every lane.
+    const uint32_t span = n < 32u ? n : 32u;
+    const bool leaf = n <= A.max_leaf;
+    for (uint32_t o = 1; o < span; o <<= 1)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
             mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
-            cmn[k] = fminf(cmn[k], __shfl_xor_sync(0xffffffffu, cmn[k], o));
-            cmx[k] = fmaxf(cmx[k], __shfl_xor_sync(0xffffffffu, cmx[k], o));
         }
+    if (!leaf) {
+        for (uint32_t o = 1; o < span; o <<= 1)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                cmn[k] = fminf(cmn[k], __shfl_xor_sync(0xffffffffu, cmn[k], o));
+                cmx[k] = fmaxf(cmx[k], __shfl_xor_sync(0xffffffffu, cmx[k], o));
+            }
+        if (span < 32u)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                cmn[k] = __shfl_sync(0xffffffffu, cmn[k], 0);
+                cmx[k] = __shfl_sync(0xffffffffu, cmx[k], 0);
+            }
+    }
     const size_t r = 2ull * lo + slot;  // record index
     if (slot == 0 && lane == 0) {       // the subtree root's box, for the top refit
         S.root_lo = make_float4(mn[0], mn[1], mn[2], 0.0f);
         S.root_hi = make_float4(mx[0], mx[1], mx[2], 0.0f);
     }
-    if (n <= A.max_leaf) {
+    if (leaf) {
         if (lane == 0) {
             A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
             A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
@@ -374,134 +593,17 @@ __device__ void sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t n
             A.keys_out[k] = A.skeys[k];
             A.c[k] = i == s ? 1u + L : 0u;
         }
-        return;
+        return false;
     }
     // binned SAH over the axes with a centroid extent
     int best_axis = -1, best_split = -1;
     uint32_t best_nl = 0;
-    float best_scale = 0.0f;
+    float bscale = 0.0f;
     if (depth < kSahDepthCap) {
-        uint32_t* bins = S.bins[warp];
-        for (uint32_t w = lane; w < 3u * kSahBins * 7u; w += 32) {
-            const uint32_t f = w % 7u;
-            bins[w] = f == 0 ? 0u : (f <= 3 ? rq::f2o(INFINITY) : rq::f2o(-INFINITY));
-        }
-        float scale[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float ext = cmx[a] - cmn[a];
-            scale[a] = ext > 0.0f ? float(kSahBins) / ext : 0.0f;
-            if (!(scale[a] < INFINITY)) scale[a] = 0.0f;  // an extent too small to scale: no split there
-        }
-        __syncwarp();
-        for (uint32_t i = s + lane; i < e; i += 32) {
-            const uint32_t p = ord[i];
-            const float4 a4 = S.lo[p], b4 = S.hi[p];
-            const float c[3] = {a4.w, b4.w, S.cz[p]};
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (!(scale[a] > 0.0f)) continue;
-                uint32_t* bn = bins + (a * kSahBins + sah_bin(c[a], cmn[a], scale[a])) * 7;
-                atomicAdd(bn, 1u);
-                atomicMin(bn + 1, rq::f2o(a4.x));
-                atomicMin(bn + 2, rq::f2o(a4.y));
-                atomicMin(bn + 3, rq::f2o(a4.z));
-                atomicMax(bn + 4, rq::f2o(b4.x));
-                atomicMax(bn + 5, rq::f2o(b4.y));
-                atomicMax(bn + 6, rq::f2o(b4.z));
-            }
-        }
-        __syncwarp();
-        // 45 candidates (axis, split after bin k).  Two axes per pass, one per
-        // half-warp, lane b holding bin b: inclusive prefix and suffix unions
-        // over the bins (min / max are exact, so the unions equal any other
-        // order's), then lane k < 15 prices the split after bin k.
-        float bc = INFINITY;
-        uint32_t bi = 0xffffffffu, bnl = 0;
-        for (int pass = 0; pass < 2; ++pass) {
-            const int a = pass * 2 + int(lane >> 4);
-            const uint32_t b = lane & 15u;
-            const bool live = a < 3 && scale[a < 3 ? a : 0] > 0.0f;
-            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-            uint32_t cnt = 0;
-            if (live) {
-                const uint32_t* bn = bins + (a * kSahBins + b) * 7;
-                cnt = bn[0];
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    lo[q] = rq::o2f(bn[1 + q]);
-                    hi[q] = rq::o2f(bn[4 + q]);
-                }
-            }
-            float plo[3] = {lo[0], lo[1], lo[2]}, phi[3] = {hi[0], hi[1], hi[2]};
-            float slo[3] = {lo[0], lo[1], lo[2]}, shi[3] = {hi[0], hi[1], hi[2]};
-            uint32_t pc = cnt, sc = cnt;
-#pragma unroll
-            for (int o = 1; o < 16; o <<= 1) {
-                const uint32_t upc = __shfl_up_sync(0xffffffffu, pc, o, 16);
-                const uint32_t dnc = __shfl_down_sync(0xffffffffu, sc, o, 16);
-                float u[6], d[6];
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    u[q] = __shfl_up_sync(0xffffffffu, plo[q], o, 16);
-                    u[3 + q] = __shfl_up_sync(0xffffffffu, phi[q], o, 16);
-                    d[q] = __shfl_down_sync(0xffffffffu, slo[q], o, 16);
-                    d[3 + q] = __shfl_down_sync(0xffffffffu, shi[q], o, 16);
-                }
-                if (b >= uint32_t(o)) {
-                    pc += upc;
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        plo[q] = fminf(plo[q], u[q]);
-                        phi[q] = fmaxf(phi[q], u[3 + q]);
-                    }
-                }
-                if (b + uint32_t(o) < 16u) {
-                    sc += dnc;
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        slo[q] = fminf(slo[q], d[q]);
-                        shi[q] = fmaxf(shi[q], d[3 + q]);
-                    }
-                }
-            }
-            // the right side of split b is the suffix from bin b + 1
-            const uint32_t nr = __shfl_down_sync(0xffffffffu, sc, 1, 16);
-            float r[6];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                r[q] = __shfl_down_sync(0xffffffffu, slo[q], 1, 16);
-                r[3 + q] = __shfl_down_sync(0xffffffffu, shi[q], 1, 16);
-            }
-            if (live && b < kSahBins - 1) {
-                const float cost = float(pc) * sah_area(plo[0], plo[1], plo[2], phi[0], phi[1], phi[2]) +
-                                   float(nr) * sah_area(r[0], r[1], r[2], r[3], r[4], r[5]);
-                const uint32_t cand = uint32_t(a) * (kSahBins - 1) + b;
-                if (cost < bc || (cost == bc && cand < bi)) {
-                    bc = cost;
-                    bi = cand;
-                    bnl = pc;
-                }
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
-            const uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            const uint32_t on = __shfl_xor_sync(0xffffffffu, bnl, o);
-            if (oc < bc || (oc == bc && oi < bi)) {
-                bc = oc;
-                bi = oi;
-                bnl = on;
-            }
-        }
-        if (bi != 0xffffffffu) {
-            best_axis = int(bi / (kSahBins - 1));
-            best_split = int(bi % (kSahBins - 1));
-            best_nl = bnl;
-            best_scale = scale[best_axis];
-        }
-        __syncwarp();  // the bins are read before the next node reuses them
+        if (n > kSahSmallNode)
+            sah_split<16>(S, S.bins[warp], ord, s, e, lane, cmn, cmx, best_axis, best_split, best_nl, bscale);
+        else
+            sah_split<8>(S, S.bins[warp], ord, s, e, lane, cmn, cmx, best_axis, best_split, best_nl, bscale);
     }
     uint32_t mid;
     if (best_axis < 0) {
@@ -509,14 +611,15 @@ __device__ void sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t n
         for (uint32_t i = s + lane; i < e; i += 32) nxt[i] = ord[i];
     } else {
         mid = s + best_nl;
+        const float bmin = sah_pick(cmn, best_axis);
         const uint32_t lt = (1u << lane) - 1u;
         uint32_t nl = 0, nr = 0;
         for (uint32_t b = s; b < e; b += 32) {
             const uint32_t i = b + lane;
             const bool in = i < e;
             const uint32_t p = in ? ord[i] : 0u;
-            const bool left =
-                in && sah_bin(sah_centroid(S, p, best_axis), cmn[best_axis], best_scale) <= best_split;
+            // the clamp to the last bin cannot move a centroid across a split
+            const bool left = in && sah_floor(sah_centroid(S, p, best_axis), bmin, bscale) <= uint32_t(best_split);
             const uint32_t ml = __ballot_sync(0xffffffffu, left), mr = __ballot_sync(0xffffffffu, in && !left);
             if (left)
                 nxt[s + nl + __popc(ml & lt)] = uint16_t(p);
@@ -526,24 +629,24 @@ __device__ void sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t n
             nr += __popc(mr);
         }
     }
-    uint32_t base = 0;
+    uint32_t cs = 0;
     if (lane == 0) {
         A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
         A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(lo + mid));
         A.rec_l[r] = L;
-        const uint32_t cs = atomicAdd(&S.slots, 2u);
-        base = atomicAdd(&S.cnt[cur ^ 1], 2u);
-        S.list[cur ^ 1][base] = sah_entry(s, mid, depth + 1u, cs, L + 1u);
-        S.list[cur ^ 1][base + 1] = sah_entry(mid, e, depth + 1u, cs + 1u, 0u);
+        cs = atomicAdd(&S.slots, 2u);
     }
-    (void)nsub;
+    cs = __shfl_sync(0xffffffffu, cs, 0);
+    left_child = sah_entry(s, mid, depth + 1u, cs, L + 1u);
+    right_child = sah_entry(mid, e, depth + 1u, cs + 1u, 0u);
+    return true;
 }
 
 // One block per subtree (taken from a counter): load its primitives, build
 // it level by level (a warp per node), mark its unused record slots, then
 // refit the top of the tree from its root upward (the second arrival at a
 // top node computes its box, as refit_walk).
-__global__ void __launch_bounds__(kSahT) k_sah_build(const SahArgs A) {
+__global__ void __launch_bounds__(kSahT, 3) k_sah_build(const SahArgs A) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SahShared& S = *reinterpret_cast<SahShared*>(s_raw);
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -575,11 +678,20 @@ __global__ void __launch_bounds__(kSahT) k_sah_build(const SahArgs A) {
             S.list[0][0] = sah_entry(0u, nsub, 0u, 0u, A.sL[lo]);
         }
         __syncthreads();
+        // Level by level, a warp per node; a node at depth d reads the leaf
+        // order at parity d and writes its partition to parity d + 1.
         int cur = 0;
         for (uint32_t guard = 0;; ++guard) {
             const uint32_t m = S.cnt[cur];
             if (m == 0u || guard > 64u) break;
-            for (uint32_t k = warp; k < m; k += kSahWarps) sah_node(S, A, lo, nsub, S.list[cur][k], cur, lane, warp);
+            for (uint32_t k = warp; k < m; k += kSahWarps) {
+                uint2 lc, rc;
+                if (sah_node(S, A, lo, S.list[cur][k], lane, warp, lc, rc) && lane == 0) {
+                    const uint32_t b = atomicAdd(&S.cnt[cur ^ 1], 2u);
+                    S.list[cur ^ 1][b] = lc;
+                    S.list[cur ^ 1][b + 1] = rc;
+                }
+            }
             __syncthreads();
             if (threadIdx.x == 0) S.cnt[cur] = 0u;
             cur ^= 1;
