@@ -2,7 +2,8 @@
 RQ_BUILD_SAH) against the oracle's statement of the same build
 (orc_lbvh_sah_build): Morton keys, leaf-order permutation, binary nodes,
 leaf-ordered triangles and 4-wide nodes byte for byte, at sizes around the
-1,024-triangle subtree limit and the one-subtree case, for every leaf size,
+1,024-triangle subtree limit, the one-subtree case and the 32-triangle switch
+from 16 to 8 bins, for every leaf size,
 degenerate inputs (equal centroids), a grid mesh, and a refit; traversal on
 the rebuilt tree bit-exact with the oracle's traversal of it."""
 import numpy as np
@@ -40,9 +41,16 @@ def assert_same_as_oracle(ctx, pos, idx, max_leaf=4):
     return o
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 17, 100, 1000, 1023, 1024, 1025, 2049, 4097, 50000])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 17, 31, 32, 33, 64, 65, 100, 1000, 1023, 1024, 1025, 2049, 4097, 50000])
 def test_sah_soup_parity(ctx, n):
     assert_same_as_oracle(ctx, soup(n, 300 + n), None)
+
+
+@pytest.mark.parametrize("n", [33, 65, 700])
+def test_sah_bin_count_boundary(ctx, n):
+    # leaves of one triangle: every node is split, so nodes of 33 triangles
+    # (16 bins) and of 32 (8 bins) meet under each other
+    assert_same_as_oracle(ctx, soup(n, 900 + n), None, max_leaf=1)
 
 
 @pytest.mark.parametrize("max_leaf", [1, 2, 4, 8, 16])
