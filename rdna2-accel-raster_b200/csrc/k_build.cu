@@ -513,6 +513,127 @@ __device__ __forceinline__ void sah_split(const SahShared& S, uint32_t* bins, co
     axis_scale = axis < 0 ? 0.0f : sah_pick(scale, axis);
 }
 
+// A node of at most 32 primitives (every leaf, and most inner nodes), by one
+// warp with lane i holding primitive s + i: the same bounds, 8-way bins,
+// pricing and stable partition as sah_node's loops, without the loops.
+__device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t s, uint32_t n,
+                                               uint32_t depth, uint32_t slot, uint32_t L, uint32_t lane,
+                                               uint32_t warp, uint2& left_child, uint2& right_child) {
+    static_assert(kSahSmallNode == 32u, "one primitive per lane");
+    const uint16_t* ord = S.ord[depth & 1u];
+    uint16_t* nxt = S.ord[(depth + 1u) & 1u];
+    const bool in = lane < n;
+    const uint32_t p = ord[s + (in ? lane : 0u)];
+    const float4 a = S.lo[p], b = S.hi[p];
+    float mn[3] = {in ? a.x : INFINITY, in ? a.y : INFINITY, in ? a.z : INFINITY};
+    float mx[3] = {in ? b.x : -INFINITY, in ? b.y : -INFINITY, in ? b.z : -INFINITY};
+    // butterfly over lanes 0..n-1 (the others hold the identities): the bounds end in lane 0
+    for (uint32_t o = 1; o < n; o <<= 1)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+    const size_t r = 2ull * lo + slot;  // record index
+    if (slot == 0 && lane == 0) {       // the subtree root's box, for the top refit
+        S.root_lo = make_float4(mn[0], mn[1], mn[2], 0.0f);
+        S.root_hi = make_float4(mx[0], mx[1], mx[2], 0.0f);
+    }
+    if (n <= A.max_leaf) {
+        if (lane == 0) {
+            A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+            A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
+            A.rec_l[r] = L;
+        }
+        if (in) {
+            const uint32_t k = lo + s + lane, gid = S.id[p];
+            rq::F3 p0, p1, p2;
+            rq::load_tri(A.pos, A.sf, A.idx, gid, p0, p1, p2);
+            float4* tp = reinterpret_cast<float4*>(A.tris + k);
+            tp[0] = make_float4(p0.x, p0.y, p0.z, 0.0f);
+            tp[1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
+            tp[2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
+            A.perm[k] = gid;
+            A.keys_out[k] = A.skeys[k];
+            A.c[k] = lane == 0 ? 1u + L : 0u;
+        }
+        return false;
+    }
+    const float c[3] = {a.w, b.w, S.cz[p]};
+    float cmn[3], cmx[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        cmn[k] = in ? c[k] : INFINITY;
+        cmx[k] = in ? c[k] : -INFINITY;
+    }
+    for (uint32_t o = 1; o < n; o <<= 1)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            cmn[k] = fminf(cmn[k], __shfl_xor_sync(0xffffffffu, cmn[k], o));
+            cmx[k] = fmaxf(cmx[k], __shfl_xor_sync(0xffffffffu, cmx[k], o));
+        }
+    if (n < 32u)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            cmn[k] = __shfl_sync(0xffffffffu, cmn[k], 0);
+            cmx[k] = __shfl_sync(0xffffffffu, cmx[k], 0);
+        }
+    int best_axis = -1, best_split = -1;
+    uint32_t best_nl = 0;
+    float scale[3] = {0.0f, 0.0f, 0.0f};
+    if (depth < kSahDepthCap) {
+        uint32_t* bins = S.bins[warp];
+        sah_bins_clear<8>(bins, lane);
+        sah_scales<8>(cmn, cmx, scale);
+        __syncwarp();
+        if (in) {
+            constexpr uint32_t F = SahBinsOf<8>::slots;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (!(scale[k] > 0.0f)) continue;
+                uint32_t* bn = bins + k * 8 + sah_bin<8>(c[k], cmn[k], scale[k]);
+                atomicAdd(bn, 1u);
+                atomicMin(bn + 1 * F, rq::f2o(a.x));
+                atomicMin(bn + 2 * F, rq::f2o(a.y));
+                atomicMin(bn + 3 * F, rq::f2o(a.z));
+                atomicMax(bn + 4 * F, rq::f2o(b.x));
+                atomicMax(bn + 5 * F, rq::f2o(b.y));
+                atomicMax(bn + 6 * F, rq::f2o(b.z));
+            }
+        }
+        __syncwarp();
+        sah_choose<8>(bins, scale, lane, best_axis, best_split, best_nl);
+        __syncwarp();  // the bins are read before the next node reuses them
+    }
+    uint32_t mid;
+    if (best_axis < 0) {
+        mid = s + n / 2u;
+        if (in) nxt[s + lane] = uint16_t(p);
+    } else {
+        mid = s + best_nl;
+        // the clamp to the last bin cannot move a centroid across a split
+        const bool left = in && sah_floor(sah_pick(c, best_axis), sah_pick(cmn, best_axis),
+                                          sah_pick(scale, best_axis)) <= uint32_t(best_split);
+        const uint32_t lt = (1u << lane) - 1u;
+        const uint32_t ml = __ballot_sync(0xffffffffu, left), mr = __ballot_sync(0xffffffffu, in && !left);
+        if (left)
+            nxt[s + __popc(ml & lt)] = uint16_t(p);
+        else if (in)
+            nxt[mid + __popc(mr & lt)] = uint16_t(p);
+    }
+    uint32_t cs = 0;
+    if (lane == 0) {
+        A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+        A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(lo + mid));
+        A.rec_l[r] = L;
+        cs = atomicAdd(&S.slots, 2u);
+    }
+    cs = __shfl_sync(0xffffffffu, cs, 0);
+    left_child = sah_entry(s, mid, depth + 1u, cs, L + 1u);
+    right_child = sah_entry(mid, s + n, depth + 1u, cs + 1u, 0u);
+    return true;
+}
+
 // One node of a subtree, by one warp: box and centroid bounds, then a leaf
 // (its record, emission counts, triangles; returns false) or the binned
 // split: the stable partition of its range into the order of the next depth,
@@ -524,9 +645,10 @@ __device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent,
                          uint2& left_child, uint2& right_child) {
     const uint32_t s = ent.x & 0x7ffu, e = (ent.x >> 11) & 0x7ffu, depth = ent.x >> 22;
     const uint32_t slot = ent.y & 0xfffu, L = ent.y >> 12;
+    const uint32_t n = e - s;
+    if (n <= kSahSmallNode) return sah_node_small(S, A, lo, s, n, depth, slot, L, lane, warp, left_child, right_child);
     const uint16_t* ord = S.ord[depth & 1u];
     uint16_t* nxt = S.ord[(depth + 1u) & 1u];
-    const uint32_t n = e - s;
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     float cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (uint32_t i = s + lane; i < e; i += 32) {
