@@ -287,15 +287,16 @@ struct SahArgs {
 
 // Shared memory of one subtree block (kSahMax primitives): boxes with the x
 // and y centroid in w, z centroids, triangle ids, the leaf order at even and
-// odd depths (local indices), the node lists of two levels, and one set of
-// bins per warp (7 fields x 3 axes x 16 bins: count, min xyz, max xyz as
-// ordered integers, field-major).
+// odd depths and the final one (local indices), the node lists of two levels,
+// and one set of bins per warp (7 fields x 3 axes x 16 bins: count, min xyz,
+// max xyz as ordered integers, field-major).
 struct SahShared {
     float4 lo[kSahMax];
     float4 hi[kSahMax];
     float cz[kSahMax];
     uint32_t id[kSahMax];
     uint16_t ord[2][kSahMax];
+    uint16_t fin[kSahMax];  // the final leaf order: each leaf writes its range
     uint2 list[2][kSahMax];
     alignas(16) uint32_t bins[kSahWarps][SahBinsOf<16>::words];
     uint32_t cnt[2];
@@ -545,17 +546,10 @@ __device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, u
             A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
             A.rec_l[r] = L;
         }
+        // the triangles are written once the subtree is done (sah_leaves)
         if (in) {
-            const uint32_t k = lo + s + lane, gid = S.id[p];
-            rq::F3 p0, p1, p2;
-            rq::load_tri(A.pos, A.sf, A.idx, gid, p0, p1, p2);
-            float4* tp = reinterpret_cast<float4*>(A.tris + k);
-            tp[0] = make_float4(p0.x, p0.y, p0.z, 0.0f);
-            tp[1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
-            tp[2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
-            A.perm[k] = gid;
-            A.keys_out[k] = A.skeys[k];
-            A.c[k] = lane == 0 ? 1u + L : 0u;
+            S.fin[s + lane] = uint16_t(p);
+            A.c[lo + s + lane] = lane == 0 ? 1u + L : 0u;
         }
         return false;
     }
@@ -704,16 +698,8 @@ __device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent,
             A.rec_l[r] = L;
         }
         for (uint32_t i = s + lane; i < e; i += 32) {
-            const uint32_t k = lo + i, gid = S.id[ord[i]];
-            rq::F3 p0, p1, p2;
-            rq::load_tri(A.pos, A.sf, A.idx, gid, p0, p1, p2);
-            float4* tp = reinterpret_cast<float4*>(A.tris + k);
-            tp[0] = make_float4(p0.x, p0.y, p0.z, 0.0f);
-            tp[1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
-            tp[2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
-            A.perm[k] = gid;
-            A.keys_out[k] = A.skeys[k];
-            A.c[k] = i == s ? 1u + L : 0u;
+            S.fin[i] = ord[i];
+            A.c[lo + i] = i == s ? 1u + L : 0u;
         }
         return false;
     }
@@ -818,6 +804,21 @@ __global__ void __launch_bounds__(kSahT, 3) k_sah_build(const SahArgs A) {
             if (threadIdx.x == 0) S.cnt[cur] = 0u;
             cur ^= 1;
             __syncthreads();
+        }
+        // The leaf-ordered triangles, permutation and keys of the whole subtree
+        // by the whole block (every leaf recorded its range of the final order):
+        // the index and vertex fetches of all its triangles are in flight
+        // together instead of a leaf's few at a time.
+        for (uint32_t i = threadIdx.x; i < nsub; i += kSahT) {
+            const uint32_t k = lo + i, gid = S.id[S.fin[i]];
+            rq::F3 p0, p1, p2;
+            rq::load_tri(A.pos, A.sf, A.idx, gid, p0, p1, p2);
+            float4* tp = reinterpret_cast<float4*>(A.tris + k);
+            tp[0] = make_float4(p0.x, p0.y, p0.z, 0.0f);
+            tp[1] = make_float4(p1.x, p1.y, p1.z, 0.0f);
+            tp[2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
+            A.perm[k] = gid;
+            A.keys_out[k] = A.skeys[k];
         }
         for (uint32_t k = S.slots + threadIdx.x; k < 2u * nsub; k += kSahT) A.rec_l[2ull * lo + k] = kNoRecord;
         if (threadIdx.x == 0) {
