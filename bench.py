@@ -37,9 +37,9 @@ WIDTH, HEIGHT = 1920, 1080
 METRIC = "Mrays/s + BVH Mtris/s on 1 B200; p50/p99 request latency batched vs plain"
 # kernels launched by one step of the frame: the build — centroids, morton,
 # hist, hist_scan, 4 onesweep passes, karras, then leaves, scan, emit (plain
-# LBVH) or subtree roots, scan, list, subtree build, scan, emit (SAH
-# subtrees), then collapse: 13 or 16 — then G-buffer, shadow/AO and the
-# shade finish (3)
+# LBVH) or per-position boxes, SAH roots, the node queue above the block
+# size, the block subtrees, scan, emit (SAH subtrees), then collapse: 13 or
+# 16 — then G-buffer, shadow/AO and the shade finish (3)
 BUILD_KERNELS = {"lbvh": 13, "sah": 16}
 FRAME_KERNELS = 3
 
@@ -580,7 +580,7 @@ def run_ours(args, world, rank, local, pg):
         "dtype": "f32",
         "data": "synthetic",
         "config": frame_config(world),
-        "build_mode": ("LBVH with SAH-rebuilt subtrees of at most 1,024 triangles (RQ_BUILD_SAH)" if sah
+        "build_mode": ("LBVH with SAH-rebuilt subtrees of at most 65,536 triangles (RQ_BUILD_SAH)" if sah
                        else "LBVH (Karras hierarchy, Morton order)"),
         "frame": {"triangles": ntri, "rays_per_step": frame_rays, "primary_rays": npx, "secondary_rays": sec_rays,
                   "primary_hits": hits},

@@ -190,7 +190,8 @@ __global__ void __launch_bounds__(kT) k_emit2(uint32_t n, uint32_t max_leaf, con
 // blocks write one record per node (box, first position, L, and the right
 // child's first position or the leaf count) and the emission counts of their
 // leaves; after the scan, k_sah_emit writes the records and the top nodes.
-constexpr uint32_t kSahMax = RQ_SAH_SUBTREE_MAX;  // largest subtree a block rebuilds
+constexpr uint32_t kSahMax = 1024;  // largest subtree a block rebuilds in shared memory
+constexpr uint32_t kSahNone = 0xffffffffu;  // no Karras node above (no top refit from here)
 constexpr int kSahT = 256;
 constexpr int kSahWarps = kSahT / 32;
 // Nodes of more than kSahSmallNode primitives are binned 16 ways per axis,
@@ -204,24 +205,80 @@ struct SahBinsOf {
     static_assert(words % 4u == 0u && slots % 4u == 0u, "bins are cleared with 16-byte stores");
 };
 constexpr uint32_t kSahDepthCap = 24;
+// depths at which a node of more than kSahMax triangles can lie (the queue's capacity)
+constexpr uint32_t kSahMidDepths = kSahDepthCap + 8u;
+static_assert(RQ_SAH_SUBTREE_MAX <= 64u * kSahMax, "kSahMidDepths allows 6 halvings after the SAH levels");
 constexpr uint32_t kNoRecord = 0xffffffffu;
 
-// Subtree roots: every child of at most K primitives of a node of more (or
-// the root itself when n <= K), marked at its first sorted position with its
-// last position, the left-child links above it and its Karras index.
+// Per sorted position: the triangle's box with its x and y centroid in w, its
+// z centroid, and the identity order (the order of every SAH root at depth 0).
+__global__ void __launch_bounds__(kT) k_sah_pbox(const float* __restrict__ pos, uint32_t sf,
+                                                 const uint32_t* __restrict__ idx, uint32_t n,
+                                                 const uint32_t* __restrict__ sids, const float4* __restrict__ cent,
+                                                 float4* __restrict__ plo, float4* __restrict__ phi,
+                                                 float* __restrict__ pcz, uint32_t* __restrict__ ord0) {
+    for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
+        const uint32_t gid = sids[i];
+        rq::F3 p0, p1, p2;
+        rq::load_tri(pos, sf, idx, gid, p0, p1, p2);
+        const float4 c = cent[gid];
+        plo[i] = make_float4(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)),
+                             fminf(p0.z, fminf(p1.z, p2.z)), c.x);
+        phi[i] = make_float4(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)),
+                             fmaxf(p0.z, fmaxf(p1.z, p2.z)), c.y);
+        pcz[i] = c.z;
+        ord0[i] = i;
+    }
+}
+
+// Where a finished SAH root's subtree goes next: a block subtree (at most
+// kSahMax triangles: recorded at its first sorted position — last position,
+// left-child links above it, depth, Karras node above or kSahNone — and
+// appended to the block list) or the node queue of k_sah_mid.
+struct SahOut {
+    uint32_t* list;
+    uint32_t* count;
+    uint32_t* shi;
+    uint32_t* sL;
+    uint32_t* sdepth;
+    uint32_t* snode;
+    uint4* mq;
+    uint32_t* mready;
+    uint32_t mcap;
+    uint32_t* ctl;
+    uint32_t* err;
+};
+
+__device__ __forceinline__ void sah_route(const SahOut& O, uint32_t s, uint32_t e, uint32_t depth, uint32_t L,
+                                          uint32_t node) {
+    if (e - s <= kSahMax) {
+        O.shi[s] = e - 1u;
+        O.sL[s] = L;
+        O.sdepth[s] = depth;
+        O.snode[s] = node;
+        O.list[atomicAdd(O.count, 1u)] = s;
+        return;
+    }
+    const uint32_t k = atomicAdd(O.ctl + 1, 1u);
+    if (k >= O.mcap) {  // cannot happen (the queue holds every node of more than kSahMax)
+        rq::set_err(O.err, RQ_DERR_QUEUE);
+        return;
+    }
+    __stcg(O.mq + k, make_uint4(s, e, depth | (L << 8), node));
+    __threadfence();
+    rq::st_release(O.mready + k, 1u);
+}
+
+// SAH roots: every child of at most K primitives of a Karras node of more (or
+// the root itself when n <= K), in any order (a subtree's output depends on
+// its own primitives only), routed with the left-child links above it and its
+// Karras node.
 __global__ void __launch_bounds__(kT) k_sah_roots(uint32_t n, uint32_t K, const int32_t* __restrict__ kl,
                                                   const int32_t* __restrict__ kr, const uint32_t* __restrict__ klo,
                                                   const uint32_t* __restrict__ khi,
-                                                  const uint32_t* __restrict__ par_in, uint32_t* __restrict__ sflag,
-                                                  uint32_t* __restrict__ shi, uint32_t* __restrict__ sL,
-                                                  uint32_t* __restrict__ snode) {
+                                                  const uint32_t* __restrict__ par_in, SahOut O) {
     if (n <= K) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            sflag[0] = 1u;
-            shi[0] = n - 1u;
-            sL[0] = 0u;
-            snode[0] = n == 1u ? 0x80000000u : 0u;
-        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) sah_route(O, 0u, n, 0u, 0u, n == 1u ? 0x80000000u : 0u);
         return;
     }
     for (uint32_t p = blockIdx.x * kT + threadIdx.x; p + 1u < n; p += gridDim.x * kT) {
@@ -238,29 +295,52 @@ __global__ void __launch_bounds__(kT) k_sah_roots(uint32_t n, uint32_t K, const 
             const uint32_t ci = uint32_t(ch[side]) & 0x7fffffffu;
             const uint32_t lo = leaf ? ci : klo[ci], hi = leaf ? ci : khi[ci];
             if (hi - lo + 1u > K) continue;
-            sflag[lo] = 1u;
-            shi[lo] = hi;
-            sL[lo] = side == 0 ? L + 1u : 0u;
-            snode[lo] = leaf ? (0x80000000u | ci) : ci;
+            sah_route(O, lo, hi + 1u, 0u, side == 0 ? L + 1u : 0u, leaf ? (0x80000000u | ci) : ci);
         }
     }
 }
 
-__global__ void __launch_bounds__(kT) k_sah_list(uint32_t n, const uint32_t* __restrict__ sflag,
-                                                 const uint32_t* __restrict__ sidx, uint32_t* __restrict__ list,
-                                                 uint32_t* __restrict__ count) {
-    for (uint32_t x = blockIdx.x * kT + threadIdx.x; x < n; x += gridDim.x * kT) {
-        if (sflag[x]) list[sidx[x]] = x;
-        if (x == n - 1u) *count = sidx[x] + sflag[x];
+// A finished SAH root's box where its Karras parent's union reads it, then the
+// walk up the Karras nodes above it (the second arrival at a node computes its
+// box, as refit_walk).  One thread.
+__device__ void sah_refit_up(uint32_t rn, float4 rlo, float4 rhi, const int32_t* __restrict__ kl,
+                             const int32_t* __restrict__ kr, const uint32_t* __restrict__ par_in,
+                             const uint32_t* __restrict__ par_lf, float4* box_in, float4* box_lf,
+                             uint32_t* refit_flag, uint32_t* err) {
+    const bool rleaf = (rn >> 31) != 0u;
+    const uint32_t ri = rn & 0x7fffffffu;
+    float4* dst = rleaf ? box_lf + 2 * size_t(ri) : box_in + 2 * size_t(ri);
+    __stcg(dst, rlo);
+    __stcg(dst + 1, rhi);
+    uint32_t par = rleaf ? par_lf[ri] : par_in[ri];
+    for (uint32_t guard = 0; par != rq::kNoParent; ++guard) {
+        const uint32_t p = par >> 1;
+        if (rq::atom_add_acq_rel(&refit_flag[p], 1u) == 0u) break;
+        const int32_t a = kl[p], b = kr[p];
+        const float4* ba = a < 0 ? box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : box_in + 2 * size_t(a);
+        const float4* bb = b < 0 ? box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : box_in + 2 * size_t(b);
+        const float4 alo = rq::ld_cg4(ba), ahi = rq::ld_cg4(ba + 1), blo = rq::ld_cg4(bb), bhi = rq::ld_cg4(bb + 1);
+        __stcg(box_in + 2 * size_t(p), make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f));
+        __stcg(box_in + 2 * size_t(p) + 1,
+               make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f));
+        par = par_in[p];
+        if (guard > 128u) {
+            rq::set_err(err, RQ_DERR_REFIT);
+            break;
+        }
     }
 }
 
 struct SahArgs {
+    uint32_t n, max_leaf;
+    const float4* plo;  // per sorted position: box min, centroid x
+    const float4* phi;  // box max, centroid y
+    const float* pcz;   // centroid z
+    const uint32_t* ord[2];  // the order of the sorted positions at even / odd depths
+    const uint32_t* sdepth;
     const float* pos;
     uint32_t sf;
     const uint32_t* idx;
-    uint32_t n, max_leaf;
-    const float4* cent;
     const uint32_t* skeys;
     const uint32_t* sids;
     const int32_t* kl;
@@ -750,10 +830,339 @@ __device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent,
     return true;
 }
 
-// One block per subtree (taken from a counter): load its primitives, build
-// it level by level (a warp per node), mark its unused record slots, then
-// refit the top of the tree from its root upward (the second arrival at a
-// top node computes its box, as refit_walk).
+// ---- nodes of more than kSahMax triangles (below the Karras top)
+// A persistent launch of blocks of kMidT threads takes them from the node
+// queue, one node per block at a time: bounds over the node's range (in the
+// order of its depth's parity), 16-bin SAH with one set of bins per warp
+// merged before the pricing, a stable partition into the other parity's
+// order (each warp counts its slice's left side first), the node's record,
+// and its children routed (queue or block list).  A block waits for the next
+// entry until it is written, or until every created node is finished (read
+// in that order: equal counts mean no node was in progress, and only a node
+// in progress creates nodes); every wait is bounded.
+constexpr int kMidT = 512;
+constexpr int kMidWarps = kMidT / 32;
+constexpr uint32_t kMidSpin = 1u << 22;  // polls of a waiting block, at most 1 us apart
+constexpr int kMidU = 4;     // positions per thread whose gathers are in flight together
+constexpr int kMidBinU = 2;  // the same in the binning pass (its run sums hold 24 registers)
+
+struct MidArgs {
+    const float4* plo;
+    const float4* phi;
+    const float* pcz;
+    uint32_t* ord[2];
+    uint4* mq;
+    const uint32_t* mready;
+    float4* mrec;
+    uint32_t* mrec_l;
+    SahOut out;
+    const int32_t* kl;
+    const int32_t* kr;
+    const uint32_t* par_in;
+    const uint32_t* par_lf;
+    float4* box_in;
+    float4* box_lf;
+    uint32_t* refit_flag;
+};
+
+// One thread: entry h of the queue once written (true), or false once every
+// created node is finished (or the wait gave up: RQ_DERR_QUEUE).
+__device__ bool mid_take(const MidArgs& A, uint32_t h, uint4& ent) {
+    const uint32_t* ctl = A.out.ctl;
+    uint32_t nap = 32;
+    for (uint32_t it = 0;; ++it) {
+        if (h < A.out.mcap && rq::ld_acquire(A.mready + h) != 0u) {
+            ent = __ldcg(A.mq + h);
+            return true;
+        }
+        const uint32_t done = rq::ld_acquire(ctl + 2);
+        const uint32_t tail = rq::ld_acquire(ctl + 1);
+        if (done == tail) return false;
+        if (it > kMidSpin) {
+            rq::set_err(A.out.err, RQ_DERR_QUEUE);
+            return false;
+        }
+        __nanosleep(nap);
+        if (nap < 1024u) nap <<= 1;
+    }
+}
+
+__global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
+    using B16 = SahBinsOf<16>;
+    __shared__ alignas(16) uint32_t bins[kMidWarps][B16::words];
+    __shared__ float red[kMidWarps][12];
+    __shared__ float redf[12];
+    __shared__ uint32_t part[kMidWarps];
+    __shared__ uint4 s_ent;
+    __shared__ uint32_t s_got;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint4 ent = make_uint4(0u, 0u, 0u, 0u);
+            s_got = mid_take(A, atomicAdd(A.out.ctl, 1u), ent) ? 1u : 0u;
+            s_ent = ent;
+        }
+        __syncthreads();
+        if (!s_got) break;
+        const uint32_t s = s_ent.x, e = s_ent.y, depth = s_ent.z & 0xffu, L = s_ent.z >> 8, rn = s_ent.w;
+        const uint32_t n = e - s;
+        const uint32_t* in = A.ord[depth & 1u];
+        uint32_t* out = A.ord[(depth + 1u) & 1u];
+        // bounds
+        float v[12];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = INFINITY;
+            v[3 + k] = -INFINITY;
+            v[6 + k] = INFINITY;
+            v[9 + k] = -INFINITY;
+        }
+        // kMidU positions per thread per step, their order entries and then
+        // their boxes all in flight before the first is used
+        for (uint32_t i0 = s + threadIdx.x; i0 < e; i0 += kMidT * kMidU) {
+            uint32_t p[kMidU];
+#pragma unroll
+            for (int u = 0; u < kMidU; ++u) {
+                const uint32_t i = i0 + uint32_t(u) * kMidT;
+                p[u] = i < e ? __ldcg(in + i) : kSahNone;
+            }
+            float4 a[kMidU], b[kMidU];
+            float cz[kMidU];
+#pragma unroll
+            for (int u = 0; u < kMidU; ++u) {
+                const uint32_t q = p[u] != kSahNone ? p[u] : 0u;  // position 0 exists (n > kSahMax)
+                a[u] = __ldg(A.plo + q);
+                b[u] = __ldg(A.phi + q);
+                cz[u] = __ldg(A.pcz + q);
+            }
+#pragma unroll
+            for (int u = 0; u < kMidU; ++u) {
+                if (p[u] == kSahNone) continue;
+                const float c[3] = {a[u].w, b[u].w, cz[u]};
+                v[0] = fminf(v[0], a[u].x);
+                v[1] = fminf(v[1], a[u].y);
+                v[2] = fminf(v[2], a[u].z);
+                v[3] = fmaxf(v[3], b[u].x);
+                v[4] = fmaxf(v[4], b[u].y);
+                v[5] = fmaxf(v[5], b[u].z);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    v[6 + k] = fminf(v[6 + k], c[k]);
+                    v[9 + k] = fmaxf(v[9 + k], c[k]);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                const float w = __shfl_xor_sync(0xffffffffu, v[k], o);
+                v[k] = (k < 3 || (k >= 6 && k < 9)) ? fminf(v[k], w) : fmaxf(v[k], w);
+            }
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < 12; ++k) red[warp][k] = v[k];
+        __syncthreads();
+        if (threadIdx.x < 12u) {
+            const uint32_t k = threadIdx.x;
+            const bool is_min = k < 3u || (k >= 6u && k < 9u);
+            float x = red[0][k];
+            for (uint32_t w = 1; w < uint32_t(kMidWarps); ++w) x = is_min ? fminf(x, red[w][k]) : fmaxf(x, red[w][k]);
+            redf[k] = x;
+        }
+        __syncthreads();
+        float mn[3], mx[3], cmn[3], cmx[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = redf[k];
+            mx[k] = redf[3 + k];
+            cmn[k] = redf[6 + k];
+            cmx[k] = redf[9 + k];
+        }
+        // binned SAH (the same bins and pricing as the block subtrees' nodes
+        // of more than 32 triangles)
+        int best_axis = -1, best_split = -1;
+        uint32_t best_nl = 0;
+        float scale[3] = {0.0f, 0.0f, 0.0f};
+        if (depth < kSahDepthCap) {
+            sah_scales<16>(cmn, cmx, scale);
+            sah_bins_clear<16>(bins[warp], lane);
+            __syncwarp();
+            const uint32_t q = (n + kMidWarps - 1u) / kMidWarps;
+            const uint32_t ws = s + min(n, warp * q), we = s + min(n, (warp + 1u) * q);
+            // Each lane a run of consecutive positions, kMidBinU of them in flight
+            // at a time.  Consecutive triangles mostly share a bin, so a lane
+            // sums its current bin per axis in registers and adds it to the
+            // warp's bins only when the bin changes (and at the end): min and
+            // max of the partial boxes are exact, so the bins are the same.
+            const uint32_t run = ((we - ws + 31u) >> 5) | 1u;
+            const uint32_t r0 = ws + lane * run, r1 = min(we, r0 + run);
+            constexpr uint32_t F = B16::slots;
+            uint32_t cb[3] = {kSahNone, kSahNone, kSahNone}, cn[3] = {0u, 0u, 0u};
+            float bl[3][3], bh[3][3];
+            auto flush = [&](int k) {
+                uint32_t* bn = bins[warp] + k * 16 + cb[k];
+                atomicAdd(bn, cn[k]);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    atomicMin(bn + (1 + q) * F, rq::f2o(bl[k][q]));
+                    atomicMax(bn + (4 + q) * F, rq::f2o(bh[k][q]));
+                }
+            };
+            for (uint32_t i0 = r0; i0 < r1; i0 += kMidBinU) {
+                uint32_t p[kMidBinU];
+#pragma unroll
+                for (int u = 0; u < kMidBinU; ++u) {
+                    const uint32_t i = i0 + uint32_t(u);
+                    p[u] = i < r1 ? __ldcg(in + i) : kSahNone;
+                }
+                float4 a4[kMidBinU], b4[kMidBinU];
+                float cz[kMidBinU];
+#pragma unroll
+                for (int u = 0; u < kMidBinU; ++u) {
+                    const uint32_t q = p[u] != kSahNone ? p[u] : 0u;  // position 0 exists (n > kSahMax)
+                    a4[u] = __ldg(A.plo + q);
+                    b4[u] = __ldg(A.phi + q);
+                    cz[u] = __ldg(A.pcz + q);
+                }
+#pragma unroll
+                for (int u = 0; u < kMidBinU; ++u) {
+                    if (p[u] == kSahNone) continue;
+                    const float c[3] = {a4[u].w, b4[u].w, cz[u]};
+                    const float lo3[3] = {a4[u].x, a4[u].y, a4[u].z}, hi3[3] = {b4[u].x, b4[u].y, b4[u].z};
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        if (!(scale[k] > 0.0f)) continue;
+                        const uint32_t bin = sah_bin<16>(c[k], cmn[k], scale[k]);
+                        if (bin != cb[k]) {
+                            if (cb[k] != kSahNone) flush(k);
+                            cb[k] = bin;
+                            cn[k] = 0u;
+#pragma unroll
+                            for (int q = 0; q < 3; ++q) {
+                                bl[k][q] = INFINITY;
+                                bh[k][q] = -INFINITY;
+                            }
+                        }
+                        ++cn[k];
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            bl[k][q] = fminf(bl[k][q], lo3[q]);
+                            bh[k][q] = fmaxf(bh[k][q], hi3[q]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if (cb[k] != kSahNone) flush(k);
+            __syncthreads();
+            for (uint32_t w = threadIdx.x; w < B16::words; w += kMidT) {
+                const uint32_t f = w / B16::slots;
+                uint32_t x = bins[0][w];
+                for (uint32_t c = 1; c < uint32_t(kMidWarps); ++c) {
+                    const uint32_t y = bins[c][w];
+                    x = f == 0 ? x + y : (f <= 3 ? min(x, y) : max(x, y));
+                }
+                bins[0][w] = x;
+            }
+            __syncthreads();
+            sah_choose<16>(bins[0], scale, lane, best_axis, best_split, best_nl);  // every warp, the same result
+        }
+        uint32_t mid;
+        if (best_axis < 0) {
+            mid = s + n / 2u;
+            for (uint32_t i = s + threadIdx.x; i < e; i += kMidT) out[i] = __ldcg(in + i);
+        } else {
+            mid = s + best_nl;
+            const float bmin = sah_pick(cmn, best_axis), bscale = sah_pick(scale, best_axis);
+            const float* cax = best_axis == 2 ? A.pcz : reinterpret_cast<const float*>(best_axis == 0 ? A.plo : A.phi);
+            const uint32_t cstride = best_axis == 2 ? 1u : 4u, coff = best_axis == 2 ? 0u : 3u;
+            // warp slices of a multiple of 32 positions, in order
+            const uint32_t q32 = ((n + 32u * kMidWarps - 1u) / (32u * kMidWarps)) * 32u;
+            const uint32_t ws = s + min(n, warp * q32), we = s + min(n, (warp + 1u) * q32);
+            uint32_t nl = 0;
+            for (uint32_t b = ws; b < we; b += 32u * kMidU) {
+                uint32_t p[kMidU];
+#pragma unroll
+                for (int u = 0; u < kMidU; ++u) {
+                    const uint32_t i = b + uint32_t(u) * 32u + lane;
+                    p[u] = i < we ? __ldcg(in + i) : kSahNone;
+                }
+                float c[kMidU];
+#pragma unroll
+                for (int u = 0; u < kMidU; ++u)
+                    c[u] = __ldg(cax + size_t(p[u] != kSahNone ? p[u] : 0u) * cstride + coff);
+#pragma unroll
+                for (int u = 0; u < kMidU; ++u) {
+                    const bool left =
+                        p[u] != kSahNone && sah_floor(c[u], bmin, bscale) <= uint32_t(best_split);
+                    nl += __popc(__ballot_sync(0xffffffffu, left));
+                }
+            }
+            if (lane == 0) part[warp] = nl;
+            __syncthreads();
+            uint32_t offl = 0, offr = 0;
+            for (uint32_t w = 0; w < warp; ++w) {
+                const uint32_t len = min(n, (w + 1u) * q32) - min(n, w * q32);
+                offl += part[w];
+                offr += len - part[w];
+            }
+            const uint32_t lt = (1u << lane) - 1u;
+            for (uint32_t b = ws; b < we; b += 32u * kMidU) {
+                uint32_t p[kMidU];
+#pragma unroll
+                for (int u = 0; u < kMidU; ++u) {
+                    const uint32_t i = b + uint32_t(u) * 32u + lane;
+                    p[u] = i < we ? __ldcg(in + i) : kSahNone;
+                }
+                float c[kMidU];
+#pragma unroll
+                for (int u = 0; u < kMidU; ++u)
+                    c[u] = __ldg(cax + size_t(p[u] != kSahNone ? p[u] : 0u) * cstride + coff);
+#pragma unroll
+                for (int u = 0; u < kMidU; ++u) {
+                    const bool in_range = p[u] != kSahNone;
+                    const bool left = in_range && sah_floor(c[u], bmin, bscale) <= uint32_t(best_split);
+                    const uint32_t ml = __ballot_sync(0xffffffffu, left),
+                                   mr = __ballot_sync(0xffffffffu, in_range && !left);
+                    if (left)
+                        out[s + offl + __popc(ml & lt)] = p[u];
+                    else if (in_range)
+                        out[mid + offr + __popc(mr & lt)] = p[u];
+                    offl += __popc(ml);
+                    offr += __popc(mr);
+                }
+            }
+        }
+        __threadfence();  // the new order before the children are published
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t k = atomicAdd(A.out.ctl + 3, 1u);
+            if (k < A.out.mcap) {
+                A.mrec[2 * size_t(k)] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(s));
+                A.mrec[2 * size_t(k) + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(mid));
+                A.mrec_l[k] = L;
+            } else {
+                rq::set_err(A.out.err, RQ_DERR_QUEUE);
+            }
+            sah_route(A.out, s, mid, depth + 1u, L + 1u, kSahNone);
+            sah_route(A.out, mid, e, depth + 1u, 0u, kSahNone);
+            if (rn != kSahNone)
+                sah_refit_up(rn, make_float4(mn[0], mn[1], mn[2], 0.0f), make_float4(mx[0], mx[1], mx[2], 0.0f), A.kl,
+                             A.kr, A.par_in, A.par_lf, A.box_in, A.box_lf, A.refit_flag, A.out.err);
+            __threadfence();
+            atomicAdd(A.out.ctl + 2, 1u);  // finished, after its children were created
+        }
+        __syncthreads();
+    }
+}
+
+// One block per subtree of at most kSahMax triangles (taken from a counter):
+// load its primitives in the order and at the depth it was handed over, build
+// it level by level (a warp per node), write its leaf-ordered triangles, mark
+// its unused record slots, then, under a Karras node, refit the Karras nodes
+// above it.
 __global__ void __launch_bounds__(kSahT, 3) k_sah_build(const SahArgs A) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SahShared& S = *reinterpret_cast<SahShared*>(s_raw);
@@ -766,24 +1175,25 @@ __global__ void __launch_bounds__(kSahT, 3) k_sah_build(const SahArgs A) {
         if (j >= nsubtrees) break;
         const uint32_t lo = A.list[j];
         const uint32_t nsub = A.shi[lo] - lo + 1u;
+        // depth below the SAH root and starting order: from the node queue's
+        // partitions (k_sah_mid) or, under a Karras node, 0 and the Morton order.
+        // Slot i holds the primitive at position i of that order (a sorted
+        // position anywhere in the parent's range, after a partition).
+        const uint32_t d0 = A.sdepth[lo];
+        const uint32_t* g = A.ord[d0 & 1u];
         for (uint32_t i = threadIdx.x; i < nsub; i += kSahT) {
-            const uint32_t gid = A.sids[lo + i];
-            rq::F3 p0, p1, p2;
-            rq::load_tri(A.pos, A.sf, A.idx, gid, p0, p1, p2);
-            const float4 c = A.cent[gid];
-            S.lo[i] = make_float4(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)),
-                                  fminf(p0.z, fminf(p1.z, p2.z)), c.x);
-            S.hi[i] = make_float4(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)),
-                                  fmaxf(p0.z, fmaxf(p1.z, p2.z)), c.y);
-            S.cz[i] = c.z;
-            S.id[i] = gid;
-            S.ord[0][i] = uint16_t(i);
+            const uint32_t p = __ldcg(g + lo + i);
+            S.lo[i] = __ldg(A.plo + p);
+            S.hi[i] = __ldg(A.phi + p);
+            S.cz[i] = __ldg(A.pcz + p);
+            S.id[i] = A.sids[p];
+            S.ord[d0 & 1u][i] = uint16_t(i);
         }
         if (threadIdx.x == 0) {
             S.cnt[0] = 1u;
             S.cnt[1] = 0u;
             S.slots = 1u;
-            S.list[0][0] = sah_entry(0u, nsub, 0u, 0u, A.sL[lo]);
+            S.list[0][0] = sah_entry(0u, nsub, d0, 0u, A.sL[lo]);
         }
         __syncthreads();
         // Level by level, a warp per node; a node at depth d reads the leaf
@@ -821,43 +1231,35 @@ __global__ void __launch_bounds__(kSahT, 3) k_sah_build(const SahArgs A) {
             A.keys_out[k] = A.skeys[k];
         }
         for (uint32_t k = S.slots + threadIdx.x; k < 2u * nsub; k += kSahT) A.rec_l[2ull * lo + k] = kNoRecord;
-        if (threadIdx.x == 0) {
-            // the root's box where its parent's union reads it, then the walk up
-            const uint32_t rn = A.snode[lo];
-            const bool rleaf = (rn >> 31) != 0u;
-            const uint32_t ri = rn & 0x7fffffffu;
-            float4* dst = rleaf ? A.box_lf + 2 * size_t(ri) : A.box_in + 2 * size_t(ri);
-            __stcg(dst, S.root_lo);
-            __stcg(dst + 1, S.root_hi);
-            uint32_t par = rleaf ? A.par_lf[ri] : A.par_in[ri];
-            for (uint32_t guard = 0; par != rq::kNoParent; ++guard) {
-                const uint32_t p = par >> 1;
-                if (rq::atom_add_acq_rel(&A.refit_flag[p], 1u) == 0u) break;
-                const int32_t a = A.kl[p], b = A.kr[p];
-                const float4* ba = a < 0 ? A.box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : A.box_in + 2 * size_t(a);
-                const float4* bb = b < 0 ? A.box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : A.box_in + 2 * size_t(b);
-                const float4 alo = rq::ld_cg4(ba), ahi = rq::ld_cg4(ba + 1), blo = rq::ld_cg4(bb),
-                             bhi = rq::ld_cg4(bb + 1);
-                __stcg(A.box_in + 2 * size_t(p),
-                       make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f));
-                __stcg(A.box_in + 2 * size_t(p) + 1,
-                       make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f));
-                par = A.par_in[p];
-                if (guard > 128u) {
-                    rq::set_err(A.err, RQ_DERR_REFIT);
-                    break;
-                }
-            }
-        }
+        if (threadIdx.x == 0 && A.snode[lo] != kSahNone)
+            sah_refit_up(A.snode[lo], S.root_lo, S.root_hi, A.kl, A.kr, A.par_in, A.par_lf, A.box_in, A.box_lf,
+                         A.refit_flag, A.err);
         __syncthreads();
     }
 }
 
-// Node writes: every record at A[first] + L (left child next to it, right
-// child at A[its first position]; leaves as ~first / count), every top node
-// (more than K primitives) likewise from its Karras range and refitted box.
+// Node writes: every record (the block subtrees' and the node queue's) at
+// A[first] + L (left child next to it, right child at A[its first position];
+// leaves as ~first / count), every Karras node above the SAH roots (more
+// than K primitives) likewise from its Karras range and refitted box.
+// One node record (box, first position in w; box, the right child's first
+// position or bit 31 | the leaf count in w) at its pre-order position.
+__device__ __forceinline__ void sah_emit_record(float4 a, float4 b, uint32_t L, const uint32_t* __restrict__ A,
+                                                rq_bvh2_node* __restrict__ out) {
+    const uint32_t first = __float_as_uint(a.w), aux = __float_as_uint(b.w);
+    const uint32_t pre = A[first] + L;
+    const bool leaf = (aux >> 31) != 0u;
+    const int32_t lc = leaf ? ~int32_t(first) : int32_t(pre + 1u);
+    const int32_t rc = leaf ? int32_t(aux & 0x7fffffffu) : int32_t(A[aux]);
+    float4* o = reinterpret_cast<float4*>(out + pre);
+    o[0] = make_float4(a.x, a.y, a.z, __int_as_float(lc));
+    o[1] = make_float4(b.x, b.y, b.z, __int_as_float(rc));
+}
+
 __global__ void __launch_bounds__(kT) k_sah_emit(uint32_t n, uint32_t K, uint32_t max_leaf,
                                                  const float4* __restrict__ rec, const uint32_t* __restrict__ rec_l,
+                                                 const float4* __restrict__ mrec, const uint32_t* __restrict__ mrec_l,
+                                                 const uint32_t* __restrict__ mcount, uint32_t mcap,
                                                  const int32_t* __restrict__ kr, const uint32_t* __restrict__ klo,
                                                  const uint32_t* __restrict__ khi,
                                                  const uint32_t* __restrict__ par_in, const float4* box_in,
@@ -866,16 +1268,11 @@ __global__ void __launch_bounds__(kT) k_sah_emit(uint32_t n, uint32_t K, uint32_
     for (uint32_t i = blockIdx.x * kT + threadIdx.x; i < 2u * n; i += gridDim.x * kT) {
         const uint32_t L = rec_l[i];
         if (L == kNoRecord) continue;
-        const float4 a = rec[2 * size_t(i)], b = rec[2 * size_t(i) + 1];
-        const uint32_t first = __float_as_uint(a.w), aux = __float_as_uint(b.w);
-        const uint32_t pre = A[first] + L;
-        const bool leaf = (aux >> 31) != 0u;
-        const int32_t lc = leaf ? ~int32_t(first) : int32_t(pre + 1u);
-        const int32_t rc = leaf ? int32_t(aux & 0x7fffffffu) : int32_t(A[aux]);
-        float4* o = reinterpret_cast<float4*>(out + pre);
-        o[0] = make_float4(a.x, a.y, a.z, __int_as_float(lc));
-        o[1] = make_float4(b.x, b.y, b.z, __int_as_float(rc));
+        sah_emit_record(rec[2 * size_t(i)], rec[2 * size_t(i) + 1], L, A, out);
     }
+    const uint32_t m = min(*mcount, mcap);
+    for (uint32_t k = blockIdx.x * kT + threadIdx.x; k < m; k += gridDim.x * kT)
+        sah_emit_record(mrec[2 * size_t(k)], mrec[2 * size_t(k) + 1], mrec_l[k], A, out);
     for (uint32_t p = blockIdx.x * kT + threadIdx.x; p + 1u < n; p += gridDim.x * kT) {
         if (rq::count_in(klo, khi, p) <= K) continue;
         uint32_t L = 0, par = par_in[p];
@@ -1026,25 +1423,44 @@ size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s, bool sah)
     s.cpar = c.take<uint32_t>(N);
     s.cacc = c.take<unsigned long long>(N);
     s.coll_ctl = c.take<uint32_t>(256);
-    s.sah_flag = s.sah_idx = s.sah_hi = s.sah_L = s.sah_node = s.sah_list = s.sah_rec_l = nullptr;
-    s.sah_rec = nullptr;
+    s.sah_hi = s.sah_L = s.sah_node = s.sah_list = s.sah_depth = s.sah_rec_l = nullptr;
+    s.sah_rec = s.sah_plo = s.sah_phi = s.sah_mrec = nullptr;
+    s.sah_pcz = nullptr;
+    s.sah_ord[0] = s.sah_ord[1] = s.sah_mready = s.sah_mrec_l = s.sah_ctl = nullptr;
+    s.sah_mq = nullptr;
+    s.sah_mcap = 0;
     if (sah) {
-        s.sah_flag = c.take<uint32_t>(N);
-        s.sah_idx = c.take<uint32_t>(N);
         s.sah_hi = c.take<uint32_t>(N);
         s.sah_L = c.take<uint32_t>(N);
         s.sah_node = c.take<uint32_t>(N);
         s.sah_list = c.take<uint32_t>(N);
+        s.sah_depth = c.take<uint32_t>(N);
         s.sah_rec = c.take<float4>(4 * N);
         s.sah_rec_l = c.take<uint32_t>(2 * N);
+        s.sah_plo = c.take<float4>(N);
+        s.sah_phi = c.take<float4>(N);
+        s.sah_pcz = c.take<float>(N);
+        s.sah_ord[0] = c.take<uint32_t>(N);
+        s.sah_ord[1] = c.take<uint32_t>(N);
+        // nodes of more than kSahMax triangles: those at one depth hold disjoint
+        // ranges of more than kSahMax positions (at most N / kSahMax of them),
+        // and they lie at most kSahDepthCap + 6 deep (SAH splits to the depth
+        // cap, then halvings from RQ_SAH_SUBTREE_MAX = 64 x kSahMax down)
+        s.sah_mcap = uint32_t(kSahMidDepths * (N / kSahMax) + 64);
+        s.sah_mq = c.take<uint4>(s.sah_mcap);
+        s.sah_mready = c.take<uint32_t>(s.sah_mcap);
+        s.sah_mrec = c.take<float4>(2 * size_t(s.sah_mcap));
+        s.sah_mrec_l = c.take<uint32_t>(s.sah_mcap);
+        s.sah_ctl = c.take<uint32_t>(16);
     }
     return c.off + 256;
 }
 
 namespace {
 
-// Subtree roots, their list, the subtree blocks (with the top refit), the
-// scan of the emission counts and the node writes.
+// Per-position boxes, the SAH roots, the nodes of more than kSahMax triangles
+// (node queue), the block subtrees (with the top refit), the scan of the
+// emission counts and the node writes.
 int launch_sah(rq_ctx* ctx, rq_bvh* bvh, BuildScratch& s, const float* pos, uint32_t sf, const uint32_t* idx,
                uint32_t n, uint32_t max_leaf, uint32_t K, const uint32_t* skeys, const uint32_t* sids,
                cudaStream_t st) {
@@ -1056,19 +1472,61 @@ int launch_sah(rq_ctx* ctx, rq_bvh* bvh, BuildScratch& s, const float* pos, uint
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sah_build, kSahT, kSmem);
         return b > 0 ? b : 1;
     }();
-    cudaError_t e = cudaMemsetAsync(s.sah_flag, 0, sizeof(uint32_t) * n, st);
-    k_sah_roots<<<grid_for(n, sms), kT, 0, st>>>(n, K, s.kl, s.kr, s.klo, s.khi, s.par_in, s.sah_flag, s.sah_hi,
-                                                 s.sah_L, s.sah_node);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s.tile_ctr + 8, 0, sizeof(uint32_t), st);
-    rq_launch_scan(ctx, s.sah_flag, s.sah_idx, n, s.scan_status, s.tile_ctr + 8, st);
-    k_sah_list<<<grid_for(n, sms), kT, 0, st>>>(n, s.sah_flag, s.sah_idx, s.sah_list, s.tile_ctr + 13);
+    static int mid_per_sm = [] {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sah_mid, kMidT, 0);
+        return b > 0 ? b : 1;
+    }();
+    // queue counters and written flags; the block list's count is tile_ctr[13]
+    // (zeroed with the build's counters)
+    cudaError_t e = cudaMemsetAsync(s.sah_ctl, 0, 16 * sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.sah_mready, 0, sizeof(uint32_t) * s.sah_mcap, st);
+    k_sah_pbox<<<grid_for(n, sms), kT, 0, st>>>(pos, sf, idx, n, sids, s.cent, s.sah_plo, s.sah_phi, s.sah_pcz,
+                                                s.sah_ord[0]);
+    SahOut o;
+    o.list = s.sah_list;
+    o.count = s.tile_ctr + 13;
+    o.shi = s.sah_hi;
+    o.sL = s.sah_L;
+    o.sdepth = s.sah_depth;
+    o.snode = s.sah_node;
+    o.mq = s.sah_mq;
+    o.mready = s.sah_mready;
+    o.mcap = s.sah_mcap;
+    o.ctl = s.sah_ctl;
+    o.err = ctx->d_err;
+    k_sah_roots<<<grid_for(n, sms), kT, 0, st>>>(n, K, s.kl, s.kr, s.klo, s.khi, s.par_in, o);
+    MidArgs m;
+    m.plo = s.sah_plo;
+    m.phi = s.sah_phi;
+    m.pcz = s.sah_pcz;
+    m.ord[0] = s.sah_ord[0];
+    m.ord[1] = s.sah_ord[1];
+    m.mq = s.sah_mq;
+    m.mready = s.sah_mready;
+    m.mrec = s.sah_mrec;
+    m.mrec_l = s.sah_mrec_l;
+    m.out = o;
+    m.kl = s.kl;
+    m.kr = s.kr;
+    m.par_in = s.par_in;
+    m.par_lf = s.par_lf;
+    m.box_in = s.box_in;
+    m.box_lf = s.box_lf;
+    m.refit_flag = s.refit_flag;
+    if (n > kSahMax) k_sah_mid<<<uint32_t(sms) * uint32_t(mid_per_sm), kMidT, 0, st>>>(m);
     SahArgs a;
+    a.n = n;
+    a.max_leaf = max_leaf;
+    a.plo = s.sah_plo;
+    a.phi = s.sah_phi;
+    a.pcz = s.sah_pcz;
+    a.ord[0] = s.sah_ord[0];
+    a.ord[1] = s.sah_ord[1];
+    a.sdepth = s.sah_depth;
     a.pos = pos;
     a.sf = sf;
     a.idx = idx;
-    a.n = n;
-    a.max_leaf = max_leaf;
-    a.cent = s.cent;
     a.skeys = skeys;
     a.sids = sids;
     a.kl = s.kl;
@@ -1094,8 +1552,9 @@ int launch_sah(rq_ctx* ctx, rq_bvh* bvh, BuildScratch& s, const float* pos, uint
     k_sah_build<<<uint32_t(sms) * uint32_t(per_sm), kSahT, kSmem, st>>>(a);
     if (e == cudaSuccess) e = cudaMemsetAsync(s.tile_ctr + 8, 0, sizeof(uint32_t), st);
     rq_launch_scan(ctx, s.c, s.a, n, s.scan_status, s.tile_ctr + 8, st);
-    k_sah_emit<<<grid_for(2 * n, sms), kT, 0, st>>>(n, K, max_leaf, s.sah_rec, s.sah_rec_l, s.kr, s.klo, s.khi,
-                                                    s.par_in, s.box_in, s.c, s.a, bvh->nodes2, bvh->d_counts);
+    k_sah_emit<<<grid_for(2 * n, sms), kT, 0, st>>>(n, K, max_leaf, s.sah_rec, s.sah_rec_l, s.sah_mrec, s.sah_mrec_l,
+                                                    s.sah_ctl + 3, s.sah_mcap, s.kr, s.klo, s.khi, s.par_in,
+                                                    s.box_in, s.c, s.a, bvh->nodes2, bvh->d_counts);
     return rq_cuda_status(ctx, e == cudaSuccess ? cudaGetLastError() : e, "SAH-subtree build launch");
 }
 
@@ -1105,7 +1564,7 @@ int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_
                     uint32_t n, uint32_t max_leaf, bool collapse, cudaStream_t st, uint32_t sah_max) {
     BuildScratch s;
     const bool sah = sah_max > 0;
-    if (sah && (sah_max > kSahMax || sah_max < max_leaf))
+    if (sah && (sah_max > RQ_SAH_SUBTREE_MAX || sah_max < max_leaf))
         return rq_set_error(ctx, RQ_ERR_INVALID_ARG, "SAH subtree size out of range");
     const size_t need = rq_build_scratch_carve(nullptr, n, s, sah);
     int rc = rq_ensure_scratch(ctx, need, st);

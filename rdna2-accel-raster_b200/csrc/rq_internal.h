@@ -114,14 +114,23 @@ struct BuildScratch {
     unsigned long long* cacc;  // N arrival counts and size sums
     uint32_t* coll_ctl;    // 256 words: [1] barrier count [2] barrier gen, [4..10] collapse control
     // LBVH with SAH-rebuilt subtrees (RQ_BUILD_SAH; null otherwise)
-    uint32_t* sah_flag;    // N: 1 at the first sorted position of a subtree
-    uint32_t* sah_idx;     // N: exclusive scan of sah_flag
     uint32_t* sah_hi;      // N: at a subtree's first position, its last
     uint32_t* sah_L;       // N: at a subtree's first position, the left-child links above its root
     uint32_t* sah_node;    // N: at a subtree's first position, its root (bit 31: a Karras leaf)
-    uint32_t* sah_list;    // N: first positions of the subtrees, in order
+    uint32_t* sah_list;    // N: first positions of the block subtrees (in the order they were found)
+    uint32_t* sah_depth;   // N: at a block subtree's first position, its depth below its SAH root
     float4* sah_rec;       // 4N: two float4 per node record (box, first position, aux word)
     uint32_t* sah_rec_l;   // 2N: left-child links above the node, or kNoRecord for an unused slot
+    float4* sah_plo;       // N: per sorted position, the triangle's box min and centroid x
+    float4* sah_phi;       // N: box max and centroid y
+    float* sah_pcz;        // N: centroid z
+    uint32_t* sah_ord[2];  // N each: the order of the sorted positions at even / odd depths
+    uint4* sah_mq;         // node queue of the nodes above a block's size: s, e, depth | L << 8, Karras node
+    uint32_t* sah_mready;  // per queue entry: written
+    float4* sah_mrec;      // two float4 per such node's record
+    uint32_t* sah_mrec_l;  // left-child links above it
+    uint32_t sah_mcap;     // capacity of the queue and of the records
+    uint32_t* sah_ctl;     // 16 words: [0] queue head [1] queue tail [2] nodes done [3] records
 };
 
 // Carve the build scratch for n triangles out of `base`; returns its size
