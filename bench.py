@@ -580,7 +580,7 @@ def run_ours(args, world, rank, local, pg):
         "dtype": "f32",
         "data": "synthetic",
         "config": frame_config(world),
-        "build_mode": ("LBVH with SAH-rebuilt subtrees of at most 65,536 triangles (RQ_BUILD_SAH)" if sah
+        "build_mode": ("LBVH with SAH-rebuilt subtrees of at most 16,384 triangles (RQ_BUILD_SAH)" if sah
                        else "LBVH (Karras hierarchy, Morton order)"),
         "frame": {"triangles": ntri, "rays_per_step": frame_rays, "primary_rays": npx, "secondary_rays": sec_rays,
                   "primary_hits": hits},

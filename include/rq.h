@@ -149,12 +149,12 @@ int rq_deform_wave_step(rq_ctx* ctx, const float* base, float* out, uint32_t num
  * axis then by bin on ties, a stable partition, leaves of at most max_leaf
  * triangles; the middle of the range where no axis has a centroid extent or
  * 24 levels are reached).  Fewer node visits per ray than the plain LBVH
- * (about 25 % on the 1080p frame's shadow rays, within 0.1 % of a binned SAH
- * over the whole mesh); Morton keys and the sort are the LBVH's, the
+ * (about 23 % on the 1080p frame's shadow rays; a binned SAH over the whole
+ * mesh: 25 %); Morton keys and the sort are the LBVH's, the
  * permutation differs inside the rebuilt subtrees.  Not with
  * RQ_BUILD_MEDIAN. */
 #define RQ_BUILD_SAH 4u
-#define RQ_SAH_SUBTREE_MAX 65536u
+#define RQ_SAH_SUBTREE_MAX 16384u
 
 /* Build a binary BVH over `num_triangles` triangles.  Device pointers.
  * `positions`: float xyz per vertex with `stride_bytes` between vertices

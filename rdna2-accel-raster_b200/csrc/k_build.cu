@@ -249,8 +249,12 @@ struct SahOut {
     uint32_t* err;
 };
 
+// bnd (queue entries only, may be null): the node's bounds, 12 floats: box
+// min, box max, centroid min, centroid max.  A queue entry is 4 uint4: s, e,
+// depth | L << 8, Karras node; then the bounds; its written flag is 2 with the
+// bounds, 1 without.
 __device__ __forceinline__ void sah_route(const SahOut& O, uint32_t s, uint32_t e, uint32_t depth, uint32_t L,
-                                          uint32_t node) {
+                                          uint32_t node, const float* bnd = nullptr) {
     if (e - s <= kSahMax) {
         O.shi[s] = e - 1u;
         O.sL[s] = L;
@@ -264,9 +268,16 @@ __device__ __forceinline__ void sah_route(const SahOut& O, uint32_t s, uint32_t 
         rq::set_err(O.err, RQ_DERR_QUEUE);
         return;
     }
-    __stcg(O.mq + k, make_uint4(s, e, depth | (L << 8), node));
+    uint4* q = O.mq + 4 * size_t(k);
+    __stcg(q, make_uint4(s, e, depth | (L << 8), node));
+    if (bnd) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            __stcg(q + 1 + j, make_uint4(__float_as_uint(bnd[4 * j]), __float_as_uint(bnd[4 * j + 1]),
+                                         __float_as_uint(bnd[4 * j + 2]), __float_as_uint(bnd[4 * j + 3])));
+    }
     __threadfence();
-    rq::st_release(O.mready + k, 1u);
+    rq::st_release(O.mready + k, bnd ? 2u : 1u);
 }
 
 // SAH roots: every child of at most K primitives of a Karras node of more (or
@@ -844,7 +855,8 @@ constexpr int kMidT = 512;
 constexpr int kMidWarps = kMidT / 32;
 constexpr uint32_t kMidSpin = 1u << 22;  // polls of a waiting block, at most 1 us apart
 constexpr int kMidU = 4;     // positions per thread whose gathers are in flight together
-constexpr int kMidBinU = 2;  // the same in the binning pass (its run sums hold 24 registers)
+constexpr int kMidBinU = 2;   // the same in the binning pass (its run sums hold 24 registers)
+constexpr int kMidPartU = 1;  // and in the partition pass (its children's bounds hold 24)
 
 struct MidArgs {
     const float4* plo;
@@ -865,112 +877,136 @@ struct MidArgs {
     uint32_t* refit_flag;
 };
 
-// One thread: entry h of the queue once written (true), or false once every
-// created node is finished (or the wait gave up: RQ_DERR_QUEUE).
-__device__ bool mid_take(const MidArgs& A, uint32_t h, uint4& ent) {
+// One thread: entry h of the queue once written (its written flag: 1 without
+// bounds, 2 with), or 0 once every created node is finished (or the wait gave
+// up: RQ_DERR_QUEUE).
+__device__ uint32_t mid_take(const MidArgs& A, uint32_t h) {
     const uint32_t* ctl = A.out.ctl;
     uint32_t nap = 32;
     for (uint32_t it = 0;; ++it) {
-        if (h < A.out.mcap && rq::ld_acquire(A.mready + h) != 0u) {
-            ent = __ldcg(A.mq + h);
-            return true;
+        if (h < A.out.mcap) {
+            const uint32_t r = rq::ld_acquire(A.mready + h);
+            if (r != 0u) return r;
         }
         const uint32_t done = rq::ld_acquire(ctl + 2);
         const uint32_t tail = rq::ld_acquire(ctl + 1);
-        if (done == tail) return false;
+        if (done == tail) return 0u;
         if (it > kMidSpin) {
             rq::set_err(A.out.err, RQ_DERR_QUEUE);
-            return false;
+            return 0u;
         }
         __nanosleep(nap);
         if (nap < 1024u) nap <<= 1;
     }
 }
 
+// Bounds accumulators: box min, box max, centroid min, centroid max.
+__device__ __forceinline__ void bnd_init(float (&v)[12]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = INFINITY;
+        v[3 + k] = -INFINITY;
+        v[6 + k] = INFINITY;
+        v[9 + k] = -INFINITY;
+    }
+}
+__device__ __forceinline__ void bnd_add(float (&v)[12], float4 a, float4 b, float cz) {
+    v[0] = fminf(v[0], a.x);
+    v[1] = fminf(v[1], a.y);
+    v[2] = fminf(v[2], a.z);
+    v[3] = fmaxf(v[3], b.x);
+    v[4] = fmaxf(v[4], b.y);
+    v[5] = fmaxf(v[5], b.z);
+    v[6] = fminf(v[6], a.w);
+    v[7] = fminf(v[7], b.w);
+    v[8] = fminf(v[8], cz);
+    v[9] = fmaxf(v[9], a.w);
+    v[10] = fmaxf(v[10], b.w);
+    v[11] = fmaxf(v[11], cz);
+}
+__device__ __forceinline__ bool bnd_is_min(int k) { return k < 3 || (k >= 6 && k < 9); }
+
+// Block reduction of NV bounds values per thread (sets of 12), into out (shared).
+template <int NV>
+__device__ __forceinline__ void bnd_reduce(float (&v)[NV], float (*red)[NV], float* out, uint32_t lane, uint32_t warp) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const float w = __shfl_xor_sync(0xffffffffu, v[k], o);
+            v[k] = bnd_is_min(k % 12) ? fminf(v[k], w) : fmaxf(v[k], w);
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < uint32_t(NV)) {
+        const uint32_t k = threadIdx.x;
+        float x = red[0][k];
+        for (uint32_t w = 1; w < uint32_t(kMidWarps); ++w)
+            x = bnd_is_min(int(k % 12u)) ? fminf(x, red[w][k]) : fmaxf(x, red[w][k]);
+        out[k] = x;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
     using B16 = SahBinsOf<16>;
-    __shared__ alignas(16) uint32_t bins[kMidWarps][B16::words];
-    __shared__ float red[kMidWarps][12];
-    __shared__ float redf[12];
+    __shared__ alignas(16) uint32_t bins[kMidWarps][B16::words];  // per warp slice
+    __shared__ alignas(16) uint32_t mbins[B16::words];             // merged
+    __shared__ float red[kMidWarps][24];
+    __shared__ float redf[24];
     __shared__ uint32_t part[kMidWarps];
-    __shared__ uint4 s_ent;
+    __shared__ uint4 s_ent[4];
     __shared__ uint32_t s_got;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     for (;;) {
         if (threadIdx.x == 0) {
-            uint4 ent = make_uint4(0u, 0u, 0u, 0u);
-            s_got = mid_take(A, atomicAdd(A.out.ctl, 1u), ent) ? 1u : 0u;
-            s_ent = ent;
-        }
-        __syncthreads();
-        if (!s_got) break;
-        const uint32_t s = s_ent.x, e = s_ent.y, depth = s_ent.z & 0xffu, L = s_ent.z >> 8, rn = s_ent.w;
-        const uint32_t n = e - s;
-        const uint32_t* in = A.ord[depth & 1u];
-        uint32_t* out = A.ord[(depth + 1u) & 1u];
-        // bounds
-        float v[12];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            v[k] = INFINITY;
-            v[3 + k] = -INFINITY;
-            v[6 + k] = INFINITY;
-            v[9 + k] = -INFINITY;
-        }
-        // kMidU positions per thread per step, their order entries and then
-        // their boxes all in flight before the first is used
-        for (uint32_t i0 = s + threadIdx.x; i0 < e; i0 += kMidT * kMidU) {
-            uint32_t p[kMidU];
-#pragma unroll
-            for (int u = 0; u < kMidU; ++u) {
-                const uint32_t i = i0 + uint32_t(u) * kMidT;
-                p[u] = i < e ? __ldcg(in + i) : kSahNone;
-            }
-            float4 a[kMidU], b[kMidU];
-            float cz[kMidU];
-#pragma unroll
-            for (int u = 0; u < kMidU; ++u) {
-                const uint32_t q = p[u] != kSahNone ? p[u] : 0u;  // position 0 exists (n > kSahMax)
-                a[u] = __ldg(A.plo + q);
-                b[u] = __ldg(A.phi + q);
-                cz[u] = __ldg(A.pcz + q);
-            }
-#pragma unroll
-            for (int u = 0; u < kMidU; ++u) {
-                if (p[u] == kSahNone) continue;
-                const float c[3] = {a[u].w, b[u].w, cz[u]};
-                v[0] = fminf(v[0], a[u].x);
-                v[1] = fminf(v[1], a[u].y);
-                v[2] = fminf(v[2], a[u].z);
-                v[3] = fmaxf(v[3], b[u].x);
-                v[4] = fmaxf(v[4], b[u].y);
-                v[5] = fmaxf(v[5], b[u].z);
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    v[6 + k] = fminf(v[6 + k], c[k]);
-                    v[9 + k] = fmaxf(v[9 + k], c[k]);
+            const uint32_t h = atomicAdd(A.out.ctl, 1u);
+            const uint32_t r = mid_take(A, h);
+            s_got = r;
+            if (r != 0u) {
+                const uint4* q = A.mq + 4 * size_t(h);
+                s_ent[0] = __ldcg(q);
+                if (r == 2u) {
+                    s_ent[1] = __ldcg(q + 1);
+                    s_ent[2] = __ldcg(q + 2);
+                    s_ent[3] = __ldcg(q + 3);
                 }
             }
         }
+        __syncthreads();
+        const uint32_t got = s_got;
+        if (got == 0u) break;
+        const uint4 hdr = s_ent[0];
+        const uint32_t s = hdr.x, e = hdr.y, depth = hdr.z & 0xffu, L = hdr.z >> 8, rn = hdr.w;
+        const uint32_t n = e - s;
+        const uint32_t* in = A.ord[depth & 1u];
+        uint32_t* out = A.ord[(depth + 1u) & 1u];
+        // the node's bounds: from its entry, or (a SAH root) over its range
+        if (got == 2u) {
+            if (threadIdx.x < 12u) redf[threadIdx.x] = __uint_as_float((&s_ent[1].x)[threadIdx.x]);
+            __syncthreads();
+        } else {
+            float v[12];
+            bnd_init(v);
+            for (uint32_t i0 = s + threadIdx.x; i0 < e; i0 += kMidT * kMidU) {
+                uint32_t p[kMidU];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
+                for (int u = 0; u < kMidU; ++u) {
+                    const uint32_t i = i0 + uint32_t(u) * kMidT;
+                    p[u] = i < e ? __ldcg(in + i) : kSahNone;
+                }
 #pragma unroll
-            for (int k = 0; k < 12; ++k) {
-                const float w = __shfl_xor_sync(0xffffffffu, v[k], o);
-                v[k] = (k < 3 || (k >= 6 && k < 9)) ? fminf(v[k], w) : fmaxf(v[k], w);
+                for (int u = 0; u < kMidU; ++u) {
+                    const uint32_t q = p[u] != kSahNone ? p[u] : 0u;  // position 0 exists (n > kSahMax)
+                    const float4 a = __ldg(A.plo + q), b = __ldg(A.phi + q);
+                    const float cz = __ldg(A.pcz + q);
+                    if (p[u] != kSahNone) bnd_add(v, a, b, cz);
+                }
             }
-        if (lane == 0)
-#pragma unroll
-            for (int k = 0; k < 12; ++k) red[warp][k] = v[k];
-        __syncthreads();
-        if (threadIdx.x < 12u) {
-            const uint32_t k = threadIdx.x;
-            const bool is_min = k < 3u || (k >= 6u && k < 9u);
-            float x = red[0][k];
-            for (uint32_t w = 1; w < uint32_t(kMidWarps); ++w) x = is_min ? fminf(x, red[w][k]) : fmaxf(x, red[w][k]);
-            redf[k] = x;
+            bnd_reduce<12>(v, reinterpret_cast<float (*)[12]>(&red[0][0]), redf, lane, warp);
         }
-        __syncthreads();
         float mn[3], mx[3], cmn[3], cmx[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -979,8 +1015,11 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
             cmn[k] = redf[6 + k];
             cmx[k] = redf[9 + k];
         }
-        // binned SAH (the same bins and pricing as the block subtrees' nodes
-        // of more than 32 triangles)
+        __syncthreads();  // redf is reused below
+        // warp slices of a multiple of 32 positions, in order: the same slices
+        // are binned and partitioned, so a warp's left count is in its bins
+        const uint32_t q32 = ((n + 32u * kMidWarps - 1u) / (32u * kMidWarps)) * 32u;
+        const uint32_t ws = s + min(n, warp * q32), we = s + min(n, (warp + 1u) * q32);
         int best_axis = -1, best_split = -1;
         uint32_t best_nl = 0;
         float scale[3] = {0.0f, 0.0f, 0.0f};
@@ -988,13 +1027,11 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
             sah_scales<16>(cmn, cmx, scale);
             sah_bins_clear<16>(bins[warp], lane);
             __syncwarp();
-            const uint32_t q = (n + kMidWarps - 1u) / kMidWarps;
-            const uint32_t ws = s + min(n, warp * q), we = s + min(n, (warp + 1u) * q);
-            // Each lane a run of consecutive positions, kMidBinU of them in flight
-            // at a time.  Consecutive triangles mostly share a bin, so a lane
-            // sums its current bin per axis in registers and adds it to the
-            // warp's bins only when the bin changes (and at the end): min and
-            // max of the partial boxes are exact, so the bins are the same.
+            // Each lane a run of consecutive positions, kMidBinU of them in
+            // flight at a time.  Consecutive triangles mostly share a bin, so
+            // a lane sums its current bin per axis in registers and adds it to
+            // the warp's bins only when the bin changes (and at the end): min
+            // and max of the partial boxes are exact, so the bins are the same.
             const uint32_t run = ((we - ws + 31u) >> 5) | 1u;
             const uint32_t r0 = ws + lane * run, r1 = min(we, r0 + run);
             constexpr uint32_t F = B16::slots;
@@ -1020,7 +1057,7 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
                 float cz[kMidBinU];
 #pragma unroll
                 for (int u = 0; u < kMidBinU; ++u) {
-                    const uint32_t q = p[u] != kSahNone ? p[u] : 0u;  // position 0 exists (n > kSahMax)
+                    const uint32_t q = p[u] != kSahNone ? p[u] : 0u;
                     a4[u] = __ldg(A.plo + q);
                     b4[u] = __ldg(A.phi + q);
                     cz[u] = __ldg(A.pcz + q);
@@ -1064,43 +1101,34 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
                     const uint32_t y = bins[c][w];
                     x = f == 0 ? x + y : (f <= 3 ? min(x, y) : max(x, y));
                 }
-                bins[0][w] = x;
+                mbins[w] = x;
             }
             __syncthreads();
-            sah_choose<16>(bins[0], scale, lane, best_axis, best_split, best_nl);  // every warp, the same result
+            sah_choose<16>(mbins, scale, lane, best_axis, best_split, best_nl);  // every warp, the same result
         }
+        // the stable partition, and both children's bounds
         uint32_t mid;
+        float cv[24];
+        bnd_init(*reinterpret_cast<float (*)[12]>(&cv[0]));
+        bnd_init(*reinterpret_cast<float (*)[12]>(&cv[12]));
         if (best_axis < 0) {
             mid = s + n / 2u;
-            for (uint32_t i = s + threadIdx.x; i < e; i += kMidT) out[i] = __ldcg(in + i);
+            for (uint32_t i = s + threadIdx.x; i < e; i += kMidT) {
+                const uint32_t p = __ldcg(in + i);
+                out[i] = p;
+                const float4 a = __ldg(A.plo + p), b = __ldg(A.phi + p);
+                bnd_add(*reinterpret_cast<float (*)[12]>(&cv[i < mid ? 0 : 12]), a, b, __ldg(A.pcz + p));
+            }
         } else {
             mid = s + best_nl;
             const float bmin = sah_pick(cmn, best_axis), bscale = sah_pick(scale, best_axis);
-            const float* cax = best_axis == 2 ? A.pcz : reinterpret_cast<const float*>(best_axis == 0 ? A.plo : A.phi);
-            const uint32_t cstride = best_axis == 2 ? 1u : 4u, coff = best_axis == 2 ? 0u : 3u;
-            // warp slices of a multiple of 32 positions, in order
-            const uint32_t q32 = ((n + 32u * kMidWarps - 1u) / (32u * kMidWarps)) * 32u;
-            const uint32_t ws = s + min(n, warp * q32), we = s + min(n, (warp + 1u) * q32);
-            uint32_t nl = 0;
-            for (uint32_t b = ws; b < we; b += 32u * kMidU) {
-                uint32_t p[kMidU];
-#pragma unroll
-                for (int u = 0; u < kMidU; ++u) {
-                    const uint32_t i = b + uint32_t(u) * 32u + lane;
-                    p[u] = i < we ? __ldcg(in + i) : kSahNone;
-                }
-                float c[kMidU];
-#pragma unroll
-                for (int u = 0; u < kMidU; ++u)
-                    c[u] = __ldg(cax + size_t(p[u] != kSahNone ? p[u] : 0u) * cstride + coff);
-#pragma unroll
-                for (int u = 0; u < kMidU; ++u) {
-                    const bool left =
-                        p[u] != kSahNone && sah_floor(c[u], bmin, bscale) <= uint32_t(best_split);
-                    nl += __popc(__ballot_sync(0xffffffffu, left));
-                }
+            // this warp's left count: its slice's bins up to the split on the axis
+            {
+                const uint32_t* bw = bins[warp] + best_axis * 16;
+                const uint32_t cnt = lane < 16u && lane <= uint32_t(best_split) ? bw[lane] : 0u;
+                const uint32_t nl = __reduce_add_sync(0xffffffffu, cnt);
+                if (lane == 0) part[warp] = nl;
             }
-            if (lane == 0) part[warp] = nl;
             __syncthreads();
             uint32_t offl = 0, offr = 0;
             for (uint32_t w = 0; w < warp; ++w) {
@@ -1109,34 +1137,43 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
                 offr += len - part[w];
             }
             const uint32_t lt = (1u << lane) - 1u;
-            for (uint32_t b = ws; b < we; b += 32u * kMidU) {
-                uint32_t p[kMidU];
+            for (uint32_t b = ws; b < we; b += 32u * kMidPartU) {
+                uint32_t p[kMidPartU];
 #pragma unroll
-                for (int u = 0; u < kMidU; ++u) {
+                for (int u = 0; u < kMidPartU; ++u) {
                     const uint32_t i = b + uint32_t(u) * 32u + lane;
                     p[u] = i < we ? __ldcg(in + i) : kSahNone;
                 }
-                float c[kMidU];
+                float4 a4[kMidPartU], b4[kMidPartU];
+                float cz[kMidPartU];
 #pragma unroll
-                for (int u = 0; u < kMidU; ++u)
-                    c[u] = __ldg(cax + size_t(p[u] != kSahNone ? p[u] : 0u) * cstride + coff);
+                for (int u = 0; u < kMidPartU; ++u) {
+                    const uint32_t q = p[u] != kSahNone ? p[u] : 0u;
+                    a4[u] = __ldg(A.plo + q);
+                    b4[u] = __ldg(A.phi + q);
+                    cz[u] = __ldg(A.pcz + q);
+                }
 #pragma unroll
-                for (int u = 0; u < kMidU; ++u) {
+                for (int u = 0; u < kMidPartU; ++u) {
                     const bool in_range = p[u] != kSahNone;
-                    const bool left = in_range && sah_floor(c[u], bmin, bscale) <= uint32_t(best_split);
+                    const float c = best_axis == 0 ? a4[u].w : (best_axis == 1 ? b4[u].w : cz[u]);
+                    const bool left = in_range && sah_floor(c, bmin, bscale) <= uint32_t(best_split);
                     const uint32_t ml = __ballot_sync(0xffffffffu, left),
                                    mr = __ballot_sync(0xffffffffu, in_range && !left);
-                    if (left)
+                    if (left) {
                         out[s + offl + __popc(ml & lt)] = p[u];
-                    else if (in_range)
+                        bnd_add(*reinterpret_cast<float (*)[12]>(&cv[0]), a4[u], b4[u], cz[u]);
+                    } else if (in_range) {
                         out[mid + offr + __popc(mr & lt)] = p[u];
+                        bnd_add(*reinterpret_cast<float (*)[12]>(&cv[12]), a4[u], b4[u], cz[u]);
+                    }
                     offl += __popc(ml);
                     offr += __popc(mr);
                 }
             }
         }
         __threadfence();  // the new order before the children are published
-        __syncthreads();
+        bnd_reduce<24>(cv, red, redf, lane, warp);
         if (threadIdx.x == 0) {
             const uint32_t k = atomicAdd(A.out.ctl + 3, 1u);
             if (k < A.out.mcap) {
@@ -1146,8 +1183,14 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
             } else {
                 rq::set_err(A.out.err, RQ_DERR_QUEUE);
             }
-            sah_route(A.out, s, mid, depth + 1u, L + 1u, kSahNone);
-            sah_route(A.out, mid, e, depth + 1u, 0u, kSahNone);
+            float lb[12], rb[12];
+#pragma unroll
+            for (int k2 = 0; k2 < 12; ++k2) {
+                lb[k2] = redf[k2];
+                rb[k2] = redf[12 + k2];
+            }
+            sah_route(A.out, s, mid, depth + 1u, L + 1u, kSahNone, lb);
+            sah_route(A.out, mid, e, depth + 1u, 0u, kSahNone, rb);
             if (rn != kSahNone)
                 sah_refit_up(rn, make_float4(mn[0], mn[1], mn[2], 0.0f), make_float4(mx[0], mx[1], mx[2], 0.0f), A.kl,
                              A.kr, A.par_in, A.par_lf, A.box_in, A.box_lf, A.refit_flag, A.out.err);
@@ -1445,9 +1488,9 @@ size_t rq_build_scratch_carve(void* base, uint32_t n, BuildScratch& s, bool sah)
         // nodes of more than kSahMax triangles: those at one depth hold disjoint
         // ranges of more than kSahMax positions (at most N / kSahMax of them),
         // and they lie at most kSahDepthCap + 6 deep (SAH splits to the depth
-        // cap, then halvings from RQ_SAH_SUBTREE_MAX = 64 x kSahMax down)
+        // cap, then halvings from at most RQ_SAH_SUBTREE_MAX <= 64 x kSahMax down)
         s.sah_mcap = uint32_t(kSahMidDepths * (N / kSahMax) + 64);
-        s.sah_mq = c.take<uint4>(s.sah_mcap);
+        s.sah_mq = c.take<uint4>(4 * size_t(s.sah_mcap));
         s.sah_mready = c.take<uint32_t>(s.sah_mcap);
         s.sah_mrec = c.take<float4>(2 * size_t(s.sah_mcap));
         s.sah_mrec_l = c.take<uint32_t>(s.sah_mcap);

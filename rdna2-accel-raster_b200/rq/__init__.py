@@ -35,7 +35,7 @@ RQ_FAULT_LAUNCH = 2
 RQ_BUILD_BVH4 = 1
 RQ_BUILD_MEDIAN = 2
 RQ_BUILD_SAH = 4
-SAH_SUBTREE_MAX = 65536
+SAH_SUBTREE_MAX = 16384
 RQ_TRACE_CLOSEST = 0
 RQ_TRACE_ANY = 1
 RQ_TRI_WATERTIGHT = 0

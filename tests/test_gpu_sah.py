@@ -3,7 +3,7 @@ RQ_BUILD_SAH) against the oracle's statement of the same build
 (orc_lbvh_sah_build): Morton keys, leaf-order permutation, binary nodes,
 leaf-ordered triangles and 4-wide nodes byte for byte, at sizes around the
 1,024 triangles a block rebuilds in shared memory (larger nodes are split by
-the node queue first), the 65,536-triangle subtree limit, the one-subtree case
+the node queue first), the 16,384-triangle subtree limit, the one-subtree case
 and the 32-triangle switch from 16 to 8 bins, for every leaf size,
 degenerate inputs (equal centroids), a grid mesh, and a refit; traversal on
 the rebuilt tree bit-exact with the oracle's traversal of it."""
@@ -42,8 +42,8 @@ def assert_same_as_oracle(ctx, pos, idx, max_leaf=4):
     return o
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 17, 31, 32, 33, 64, 65, 100, 1000, 1023, 1024, 1025, 2049, 4097, 50000,
-                               65535, 65536, 65537, 131073, 300000])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 17, 31, 32, 33, 64, 65, 100, 1000, 1023, 1024, 1025, 2049, 4097, 16383,
+                               16384, 16385, 50000, 65537, 300000])
 def test_sah_soup_parity(ctx, n):
     assert_same_as_oracle(ctx, soup(n, 300 + n), None)
 
