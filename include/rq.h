@@ -346,13 +346,19 @@ typedef struct rq_batch_tuning {
     float trace_ms;
     uint32_t trace_refill_min;    /* idle lanes of a traversal warp get new rays once at least this
                                      many of 32 are idle (or all are): 1..32; 0 means 1 */
+    uint32_t build_cluster;       /* build blocks per thread-block cluster: 0 or 1 (none), 2 or 4;
+                                     a cluster builds one large mesh with all its blocks */
+    uint32_t cluster_min_tris;    /* meshes of at least this many triangles are built by a whole
+                                     cluster (build_cluster > 1), the others by single blocks */
 } rq_batch_tuning;
 
 int rq_batch_tuning_get(const rq_batch* batch, rq_batch_tuning* out);
 /* Validates the shape (RQ_ERR_INVALID_ARG for one that has no kernel). */
 int rq_batch_tuning_set(rq_batch* batch, const rq_batch_tuning* t);
 /* Autotuner: builds the batch and traces the given rays once per candidate
- * shape — every build block size with 1..occupancy blocks per SM, every
+ * shape — every build block size with 1..occupancy blocks per SM, clusters
+ * of 2 and 4 blocks of 512 and 1,024 threads for the meshes of at least
+ * 8,192 or 32,768 triangles, every
  * traversal block size x refill chunk x register cap, then refill thresholds
  * for the fastest traversal shape — timing each with CUDA events (median of
  * `reps`), and keeps the fastest build and traversal shape.

@@ -48,6 +48,8 @@ rq_batch_tuning default_tuning(rq_ctx* ctx, uint32_t slices) {
     t.stack_entries = 0;
     t.max_build_blocks = slices;
     t.trace_refill_min = 1;
+    t.build_cluster = 1;
+    t.cluster_min_tris = 16384;
     return t;
 }
 
@@ -94,8 +96,10 @@ int rq_batch_tuning_set(rq_batch* batch, const rq_batch_tuning* t) {
     if (!batch || !t) return RQ_ERR_INVALID_ARG;
     if ((t->build_threads != 256 && t->build_threads != 512 && t->build_threads != 1024) || t->build_blocks == 0 ||
         !rq_batch_trace_shape_ok(t->trace_threads, t->trace_chunk, t->trace_reg_cap) || t->stack_entries > 128 ||
-        t->trace_refill_min > 32)
+        t->trace_refill_min > 32 || (t->build_cluster > 1 && t->build_cluster != 2 && t->build_cluster != 4))
         return rq_set_error(batch->ctx, RQ_ERR_INVALID_ARG, "no kernel for this batch shape");
+    if (t->build_cluster > 1 && rq_batch_build_clusters(t->build_threads, t->build_cluster) < 1)
+        return rq_set_error(batch->ctx, RQ_ERR_UNSUPPORTED, "no resident cluster of this build shape");
     const float bm = batch->tune.build_ms, tm = batch->tune.trace_ms;
     batch->tune = *t;
     batch->tune.build_ms = bm;
@@ -132,6 +136,7 @@ int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint
             rq_batch_tuning t = start;
             t.build_threads = bt;
             t.build_blocks = std::min<uint32_t>(batch->build_slices, uint32_t(ctx->num_sms) * uint32_t(k));
+            t.build_cluster = 1;
             if (k > 1 && t.build_blocks == std::min<uint32_t>(batch->build_slices, uint32_t(ctx->num_sms) * (k - 1)))
                 continue;  // clamped to the same grid as k - 1
             batch->tune = t;
@@ -149,6 +154,35 @@ int rq_batch_autotune(rq_ctx* ctx, rq_batch* batch, const float* positions, uint
             }
         }
         if (rc) break;
+    }
+    // clusters for the largest meshes, at full occupancy
+    for (uint32_t bt : {512u, 1024u}) {
+        if (rc) break;
+        const int occ = rq_batch_build_occupancy(bt);
+        for (uint32_t cl : {2u, 4u}) {
+            if (rc || occ < 1 || rq_batch_build_clusters(bt, cl) < 1) continue;
+            for (uint32_t min_tris : {8192u, 32768u}) {
+                rq_batch_tuning t = start;
+                t.build_threads = bt;
+                t.build_blocks = std::min<uint32_t>(batch->build_slices, uint32_t(ctx->num_sms) * uint32_t(occ));
+                t.build_cluster = cl;
+                t.cluster_min_tris = min_tris;
+                if (t.build_blocks < cl) continue;
+                batch->tune = t;
+                float ms = 0.0f;
+                rc = time_median(ctx, st, reps,
+                                 [&] { return rq_launch_batch_build(ctx, batch, positions, stride_bytes, indices, st); },
+                                 &ms);
+                if (rc) break;
+                t.build_ms = ms;
+                t.trace_ms = 0.0f;
+                record(t);
+                if (ms < best_bms) {
+                    best_bms = ms;
+                    best_b = t;
+                }
+            }
+        }
     }
     // traversal shapes (on the batch as built)
     rq_batch_tuning best_t = start;

@@ -30,7 +30,7 @@ struct rq_batch {
     uint32_t* d_counts = nullptr;  // 4 per mesh: nodes2, nodes4, depth4, max leaf
     rq_mesh_desc* d_meshes = nullptr;
     uint32_t* d_order = nullptr;   // build order: largest mesh first
-    uint32_t* d_ctr = nullptr;     // build queue counter
+    uint32_t* d_ctr = nullptr;     // build queue counters: [0] clusters, [1] single blocks
     // per-block build scratch, sized for the largest mesh
     void* scratch = nullptr;
     size_t scratch_stride = 0;
@@ -46,6 +46,8 @@ struct rq_batch {
 size_t rq_batch_block_scratch(uint32_t max_tris);
 // Resident build blocks per SM for a build block size (0 if none).
 int rq_batch_build_occupancy(uint32_t threads);
+// Resident clusters of `cluster` (2 or 4) build blocks of `threads` (0 if none).
+int rq_batch_build_clusters(uint32_t threads, uint32_t cluster);
 // Whether a traversal kernel exists for this shape.
 bool rq_batch_trace_shape_ok(uint32_t threads, uint32_t chunk, uint32_t regs);
 int rq_launch_batch_build(rq_ctx* ctx, rq_batch* b, const float* pos, uint32_t stride_bytes, const uint32_t* idx,

@@ -132,7 +132,8 @@ class BatchTuning(C.Structure):
     _fields_ = [("build_threads", C.c_uint32), ("build_blocks", C.c_uint32), ("trace_threads", C.c_uint32),
                 ("trace_chunk", C.c_uint32), ("trace_reg_cap", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
                 ("stack_entries", C.c_uint32), ("max_build_blocks", C.c_uint32), ("build_ms", C.c_float),
-                ("trace_ms", C.c_float), ("trace_refill_min", C.c_uint32)]
+                ("trace_ms", C.c_float), ("trace_refill_min", C.c_uint32), ("build_cluster", C.c_uint32),
+                ("cluster_min_tris", C.c_uint32)]
 
 
 class ServerConfig(C.Structure):
@@ -494,7 +495,7 @@ class Batch:
         return hits, s
 
     TUNING_KEYS = ("build_threads", "build_blocks", "trace_threads", "trace_chunk", "trace_reg_cap",
-                   "trace_blocks_per_sm", "stack_entries", "trace_refill_min")
+                   "trace_blocks_per_sm", "stack_entries", "trace_refill_min", "build_cluster", "cluster_min_tris")
 
     def tuning(self):
         t = BatchTuning()

@@ -88,6 +88,21 @@ def test_batched_workload_sampled(ctx):
         o = O.lbvh_build(pos[vo:vo + nv].reshape(-1), idx[to:to + nt].reshape(-1))
         n2, tr, n4, pm = b.download(int(m))
         assert n2.tobytes() == o["nodes2"].tobytes() and n4.tobytes() == o["nodes4"].tobytes(), m
+    # the same batch built with clusters for its large meshes: every mesh's
+    # bytes unchanged, and the largest against the oracle
+    want = [b.download(m) for m in range(len(descs))]
+    for bt, cl, min_tris in ((1024, 2, 16384), (512, 4, 8192)):
+        b.set_tuning({"build_threads": bt, "build_blocks": b.tuning()["max_build_blocks"], "build_cluster": cl,
+                      "cluster_min_tris": min_tris})
+        b.build(p, i)
+        ctx.sync_check()
+        for m in range(len(descs)):
+            assert all(x.tobytes() == y.tobytes() for x, y in zip(want[m], b.download(m))), (bt, cl, m)
+    m = int(np.argmax(sizes))
+    vo, nv, to, nt = descs[m]
+    o = O.lbvh_build(pos[vo:vo + nv].reshape(-1), idx[to:to + nt].reshape(-1))
+    n2, tr, n4, pm = b.download(m)
+    assert n2.tobytes() == o["nodes2"].tobytes() and n4.tobytes() == o["nodes4"].tobytes(), m
     b.destroy()
 
 
@@ -105,15 +120,29 @@ def test_every_launch_shape_gives_identical_results(ctx):
     mesh_t = torch.from_numpy(mesh.view(np.int32)).cuda()
     flags_t = torch.from_numpy(flags.view(np.int32)).cuda()
     want_tree = [b.download(m) for m in range(len(descs))]
+    depths = [b.info(m)["depth4"] for m in range(len(descs))]
     want_hits = b.trace(rays_t, mesh_t, flags_t)[0].cpu().numpy()
     base = b.tuning()
+    assert base["build_cluster"] == 1
     assert base["build_threads"] == 512 and base["trace_threads"] == 128 and base["max_build_blocks"] >= 1
     for bt, blocks in ((256, 1), (1024, 3), (512, base["max_build_blocks"])):
-        b.set_tuning({"build_threads": bt, "build_blocks": blocks})
+        b.set_tuning({"build_threads": bt, "build_blocks": blocks, "build_cluster": 1})
         b.build(p, i)
         ctx.sync_check()
         for m in range(len(descs)):
             assert all(x.tobytes() == y.tobytes() for x, y in zip(want_tree[m], b.download(m))), (bt, blocks, m)
+    # thread-block clusters: every mesh (threshold 0, the 2-triangle ones
+    # included), the large ones only, and grids that round down to whole
+    # clusters or hold fewer blocks than one cluster
+    for bt, blocks, cl, min_tris in ((1024, 8, 2, 0), (256, 8, 4, 0), (512, 5, 2, 1000), (1024, 11, 4, 20000),
+                                     (512, base["max_build_blocks"], 4, 4096), (256, 1, 4, 0)):
+        b.set_tuning({"build_threads": bt, "build_blocks": blocks, "build_cluster": cl, "cluster_min_tris": min_tris})
+        b.build(p, i)
+        ctx.sync_check()
+        for m in range(len(descs)):
+            got = b.download(m)
+            assert all(x.tobytes() == y.tobytes() for x, y in zip(want_tree[m], got)), (bt, blocks, cl, min_tris, m)
+        assert [b.info(m)["depth4"] for m in range(len(descs))] == depths
     for tt in (64, 128, 256):
         for chunk in (32, 64):
             for cap in (0, 64, 80):
@@ -123,6 +152,8 @@ def test_every_launch_shape_gives_identical_results(ctx):
                 assert got.tobytes() == want_hits.tobytes(), (tt, chunk, cap)
     with pytest.raises(rq.RqError):
         b.set_tuning({"trace_threads": 96})
+    with pytest.raises(rq.RqError):
+        b.set_tuning({"build_cluster": 3})
     b.destroy()
 
 
