@@ -241,35 +241,62 @@ __device__ __forceinline__ N2 load_n2(const rq_bvh2_node* n2, int32_t i) {
 
 // Greedy candidates of SoftwareBVH4::collapse (software_bvh.hpp:225-247)
 // for inner binary node u: open the inner candidate with the largest
-// surface area (strict >, first wins) until four.  Returns the count.
+// surface area (strict >, first wins) until four.  Returns the count;
+// inner[i]: candidate i is an inner binary node.
 template <bool NC>
-__device__ __forceinline__ int greedy_candidates(const rq_bvh2_node* n2, int32_t u, int32_t c[4]) {
+__device__ __forceinline__ int greedy_candidates(const rq_bvh2_node* n2, int32_t u, int32_t c[4], bool inner[4]) {
+    // each candidate's children and surface area, loaded once (slots are
+    // static indices, so the records stay in registers)
+    int32_t cl[4], cr[4];
+    float sa[4];
+    auto set = [&](int i, int32_t id, const N2& nd) {
+        c[i] = id;
+        cl[i] = nd.l;
+        cr[i] = nd.r;
+        const float dx = nd.mx[0] - nd.mn[0];
+        const float dy = nd.mx[1] - nd.mn[1];
+        const float dz = nd.mx[2] - nd.mn[2];
+        sa[i] = 2.0f * ((dx * dy + dy * dz) + dz * dx);
+    };
     const N2 nd = load_n2<NC>(n2, u);
-    c[0] = nd.l;
-    c[1] = nd.r;
+    {
+        const N2 a = load_n2<NC>(n2, nd.l), b = load_n2<NC>(n2, nd.r);
+        set(0, nd.l, a);
+        set(1, nd.r, b);
+    }
     c[2] = c[3] = -1;
+    cl[2] = cl[3] = -1;
+    cr[2] = cr[3] = -1;
+    sa[2] = sa[3] = 0.0f;
     int nc = 2;
-    while (nc < 4) {
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
         int best = -1;
         float best_sa = -1.0f;
-        for (int i = 0; i < nc; ++i) {
-            const N2 ci = load_n2<NC>(n2, c[i]);
-            if (ci.l >= 0) {
-                const float dx = ci.mx[0] - ci.mn[0];
-                const float dy = ci.mx[1] - ci.mn[1];
-                const float dz = ci.mx[2] - ci.mn[2];
-                const float sa = 2.0f * ((dx * dy + dy * dz) + dz * dx);
-                if (sa > best_sa) {
-                    best_sa = sa;
-                    best = i;
-                }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (i < nc && cl[i] >= 0 && sa[i] > best_sa) {
+                best_sa = sa[i];
+                best = i;
             }
-        }
         if (best < 0) break;
-        const N2 ex = load_n2<NC>(n2, c[best]);
-        c[best] = ex.l;
-        c[nc++] = ex.r;
+        int32_t l = 0, r = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (i == best) {
+                l = cl[i];
+                r = cr[i];
+            }
+        const N2 a = load_n2<NC>(n2, l), b = load_n2<NC>(n2, r);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (i == best) set(i, l, a);
+            if (i == nc) set(i, r, b);
+        }
+        ++nc;
     }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) inner[i] = i < nc && cl[i] >= 0;
     return nc;
 }
 
@@ -369,22 +396,37 @@ __device__ __forceinline__ bool collapse_levels(const CollapseIO& io, uint32_t t
     // count while the next level appends to another one, and the one after
     // that is cleared during level L, two syncs after its last reader.
     uint32_t* lvl_cnt = io.tail + 4;
+    // Inner candidates take consecutive queue entries: one atomic per warp
+    // (the lanes that expand together), each lane's entries after the lower
+    // lanes'.  Entry numbers only name queue records; the output does not
+    // depend on them.
     auto expand = [&](uint32_t e, uint32_t end, uint32_t depth) {
         const int32_t u = int32_t(__ldcg(io.q + e));
         int32_t c[4] = {-1, -1, -1, -1};
+        bool inner[4] = {false, false, false, false};
         if (root_leaf)
             c[0] = 0;
         else
-            greedy_candidates<NC>(io.n2, u, c);
+            greedy_candidates<NC>(io.n2, u, c, inner);
+        const uint32_t cnt = uint32_t(inner[0]) + uint32_t(inner[1]) + uint32_t(inner[2]) + uint32_t(inner[3]);
+        const uint32_t act = __activemask();
+        const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+        const uint32_t b0 = __ballot_sync(act, cnt & 1u), b1 = __ballot_sync(act, cnt & 2u),
+                       b2 = __ballot_sync(act, cnt & 4u);
+        const uint32_t below = __popc(b0 & lt) + 2u * __popc(b1 & lt) + 4u * __popc(b2 & lt);
+        const uint32_t total = __popc(b0) + 2u * __popc(b1) + 4u * __popc(b2);
+        const uint32_t leader = __ffs(act) - 1u;
+        uint32_t base = 0;
+        if (lane == leader && total) base = atomicAdd(lvl_cnt + depth % 3u, total);
+        uint32_t pos = end + __shfl_sync(act, base, leader) + below;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             int32_t cq = -1;
-            if (c[k] >= 0 && !root_leaf && load_n2<NC>(io.n2, c[k]).l >= 0) {
-                const uint32_t pos = end + atomicAdd(lvl_cnt + depth % 3u, 1u);
+            if (inner[k]) {
                 __stcg(io.q + pos, uint32_t(c[k]));
                 __stcg(io.par + pos, (e << 2) | uint32_t(k));
                 __stcg(io.acc + pos, 0ull);
-                cq = int32_t(pos);
+                cq = int32_t(pos++);
             }
             __stcg(io.cand + 4 * size_t(e) + k, c[k]);
             __stcg(io.child_q + 4 * size_t(e) + k, cq);
