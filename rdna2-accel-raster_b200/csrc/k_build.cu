@@ -425,10 +425,32 @@ __device__ __forceinline__ float sah_centroid(const SahShared& S, uint32_t p, in
     return a == 0 ? S.lo[p].w : (a == 1 ? S.hi[p].w : S.cz[p]);
 }
 
-// Node list entry: x = s | e << 11 | depth << 22, y = slot | L << 12 (slot:
-// the node's record slot; L: the consecutive left-child links above it).
-__device__ __forceinline__ uint2 sah_entry(uint32_t s, uint32_t e, uint32_t depth, uint32_t slot, uint32_t L) {
-    return make_uint2(s | (e << 11) | (depth << 22), slot | (L << 12));
+// Node list entry: x = s | e << 11 | depth << 22, y = slot | boxed << 11 |
+// L << 12 (slot: the node's record slot, below 2 x kSahMax; boxed: the
+// parent wrote the node's box into its record; L: the consecutive left-child
+// links above it).
+__device__ __forceinline__ uint2 sah_entry(uint32_t s, uint32_t e, uint32_t depth, uint32_t slot, uint32_t L,
+                                           bool boxed = false) {
+    return make_uint2(s | (e << 11) | (depth << 22), slot | (boxed ? 0x800u : 0u) | (L << 12));
+}
+
+// Record r's box (min xyz, max xyz) without its w words, and its w words
+// (first position; right child's first position or bit 31 | leaf count)
+// without the box: a parent that knows a child's box writes the one, the
+// child the other.
+__device__ __forceinline__ void sah_rec_box(float4* rec, size_t r, const float (&b)[6]) {
+    float* f = reinterpret_cast<float*>(rec + 2 * r);
+    f[0] = b[0];
+    f[1] = b[1];
+    f[2] = b[2];
+    f[4] = b[3];
+    f[5] = b[4];
+    f[6] = b[5];
+}
+__device__ __forceinline__ void sah_rec_aux(float4* rec, size_t r, uint32_t first, uint32_t aux) {
+    float* f = reinterpret_cast<float*>(rec + 2 * r);
+    f[3] = __uint_as_float(first);
+    f[7] = __uint_as_float(aux);
 }
 
 // The bins of one node (7 fields x 3 axes x NB bins, field-major: count,
@@ -499,10 +521,13 @@ __device__ __forceinline__ void sah_bin_range(const SahShared& S, uint32_t* bins
 // axis < 0: no split.
 template <int NB>
 __device__ __forceinline__ void sah_choose(const uint32_t* bins, const float (&scale)[3], uint32_t lane, int& axis,
-                                           int& split, uint32_t& nl_out) {
+                                           int& split, uint32_t& nl_out, float (&lbox)[6], float (&rbox)[6]) {
     constexpr uint32_t F = SahBinsOf<NB>::slots;
     float bc = INFINITY;
     uint32_t bi = 0xffffffffu, bnl = 0;
+    float blb[6], brb[6];  // this lane's best candidate's left and right boxes
+#pragma unroll
+    for (int q = 0; q < 6; ++q) blb[q] = brb[q] = 0.0f;
     for (int pass = 0; pass * SahBinsOf<NB>::axes_per_pass < 3; ++pass) {
         const int a = pass * SahBinsOf<NB>::axes_per_pass + int(lane / NB);
         const uint32_t b = lane % NB;
@@ -566,6 +591,13 @@ __device__ __forceinline__ void sah_choose(const uint32_t* bins, const float (&s
                 bc = cost;
                 bi = cand;
                 bnl = pc;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    blb[q] = plo[q];
+                    blb[3 + q] = phi[q];
+                    brb[q] = r[q];
+                    brb[3 + q] = r[3 + q];
+                }
             }
         }
     }
@@ -576,7 +608,15 @@ __device__ __forceinline__ void sah_choose(const uint32_t* bins, const float (&s
     const uint32_t mine = cbits == cmin ? bi : 0xffffffffu;
     const uint32_t win = __reduce_min_sync(0xffffffffu, mine);
     const uint32_t holder = __ballot_sync(0xffffffffu, win != 0xffffffffu && mine == win);
-    bnl = __shfl_sync(0xffffffffu, bnl, holder ? uint32_t(__ffs(holder) - 1) : 0u);
+    const uint32_t hl = holder ? uint32_t(__ffs(holder) - 1) : 0u;
+    bnl = __shfl_sync(0xffffffffu, bnl, hl);
+    // the winner's prefix and suffix unions: exactly the children's boxes
+    // (min and max are exact in any order)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        lbox[q] = __shfl_sync(0xffffffffu, blb[q], hl);
+        rbox[q] = __shfl_sync(0xffffffffu, brb[q], hl);
+    }
     axis = -1;
     split = -1;
     nl_out = 0;
@@ -593,14 +633,15 @@ __device__ __forceinline__ void sah_choose(const uint32_t* bins, const float (&s
 template <int NB>
 __device__ __forceinline__ void sah_split(const SahShared& S, uint32_t* bins, const uint16_t* ord, uint32_t s,
                                           uint32_t e, uint32_t lane, const float (&cmn)[3], const float (&cmx)[3],
-                                          int& axis, int& split, uint32_t& nl, float& axis_scale) {
+                                          int& axis, int& split, uint32_t& nl, float& axis_scale,
+                                          float (&lbox)[6], float (&rbox)[6]) {
     float scale[3];
     sah_bins_clear<NB>(bins, lane);
     sah_scales<NB>(cmn, cmx, scale);
     __syncwarp();
     sah_bin_range<NB>(S, bins, ord, s, e, lane, cmn, scale);
     __syncwarp();
-    sah_choose<NB>(bins, scale, lane, axis, split, nl);
+    sah_choose<NB>(bins, scale, lane, axis, split, nl, lbox, rbox);
     __syncwarp();  // the bins are read before the next node reuses them
     axis_scale = axis < 0 ? 0.0f : sah_pick(scale, axis);
 }
@@ -608,9 +649,16 @@ __device__ __forceinline__ void sah_split(const SahShared& S, uint32_t* bins, co
 // A node of at most 32 primitives (every leaf, and most inner nodes), by one
 // warp with lane i holding primitive s + i: the same bounds, 8-way bins,
 // pricing and stable partition as sah_node's loops, without the loops.
-__device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t s, uint32_t n,
-                                               uint32_t depth, uint32_t slot, uint32_t L, uint32_t lane,
-                                               uint32_t warp, uint2& left_child, uint2& right_child) {
+// boxed: the parent wrote this node's box into its record (no box
+// reduction here).  After a binned split the children's boxes are the
+// winning candidate's unions: they go into the children's records, and a
+// child of at most max_leaf primitives is written as a leaf here (record,
+// final order, emission count) instead of being listed.  Returns the
+// children to list (bit 0 left, bit 1 right).
+__device__ __forceinline__ uint32_t sah_node_small(SahShared& S, const SahArgs& A, uint32_t lo, uint32_t s, uint32_t n,
+                                                   uint32_t depth, uint32_t slot, uint32_t L, bool boxed,
+                                                   uint32_t lane, uint32_t warp, uint2& left_child,
+                                                   uint2& right_child) {
     static_assert(kSahSmallNode == 32u, "one primitive per lane");
     const uint16_t* ord = S.ord[depth & 1u];
     uint16_t* nxt = S.ord[(depth + 1u) & 1u];
@@ -619,22 +667,28 @@ __device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, u
     const float4 a = S.lo[p], b = S.hi[p];
     float mn[3] = {in ? a.x : INFINITY, in ? a.y : INFINITY, in ? a.z : INFINITY};
     float mx[3] = {in ? b.x : -INFINITY, in ? b.y : -INFINITY, in ? b.z : -INFINITY};
-    // butterfly over lanes 0..n-1 (the others hold the identities): the bounds end in lane 0
-    for (uint32_t o = 1; o < n; o <<= 1)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
-            mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
-        }
     const size_t r = 2ull * lo + slot;  // record index
-    if (slot == 0 && lane == 0) {       // the subtree root's box, for the top refit
-        S.root_lo = make_float4(mn[0], mn[1], mn[2], 0.0f);
-        S.root_hi = make_float4(mx[0], mx[1], mx[2], 0.0f);
+    if (!boxed) {
+        // butterfly over lanes 0..n-1 (the others hold the identities): the bounds end in lane 0
+        for (uint32_t o = 1; o < n; o <<= 1)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+                mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+            }
+        if (slot == 0 && lane == 0) {  // the subtree root's box, for the top refit
+            S.root_lo = make_float4(mn[0], mn[1], mn[2], 0.0f);
+            S.root_hi = make_float4(mx[0], mx[1], mx[2], 0.0f);
+        }
     }
     if (n <= A.max_leaf) {
         if (lane == 0) {
-            A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
-            A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
+            if (boxed) {
+                sah_rec_aux(A.rec, r, lo + s, 0x80000000u | n);
+            } else {
+                A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+                A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
+            }
             A.rec_l[r] = L;
         }
         // the triangles are written once the subtree is done (sah_leaves)
@@ -642,7 +696,7 @@ __device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, u
             S.fin[s + lane] = uint16_t(p);
             A.c[lo + s + lane] = lane == 0 ? 1u + L : 0u;
         }
-        return false;
+        return 0u;
     }
     const float c[3] = {a.w, b.w, S.cz[p]};
     float cmn[3], cmx[3];
@@ -666,6 +720,7 @@ __device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, u
     int best_axis = -1, best_split = -1;
     uint32_t best_nl = 0;
     float scale[3] = {0.0f, 0.0f, 0.0f};
+    float lbox[6], rbox[6];
     if (depth < kSahDepthCap) {
         uint32_t* bins = S.bins[warp];
         sah_bins_clear<8>(bins, lane);
@@ -687,36 +742,73 @@ __device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, u
             }
         }
         __syncwarp();
-        sah_choose<8>(bins, scale, lane, best_axis, best_split, best_nl);
+        sah_choose<8>(bins, scale, lane, best_axis, best_split, best_nl, lbox, rbox);
         __syncwarp();  // the bins are read before the next node reuses them
     }
+    const bool known = best_axis >= 0;  // the children's boxes are lbox, rbox
     uint32_t mid;
-    if (best_axis < 0) {
+    bool leaf_l = false, leaf_r = false;
+    if (!known) {
         mid = s + n / 2u;
         if (in) nxt[s + lane] = uint16_t(p);
     } else {
         mid = s + best_nl;
+        leaf_l = mid - s <= A.max_leaf;
+        leaf_r = s + n - mid <= A.max_leaf;
         // the clamp to the last bin cannot move a centroid across a split
         const bool left = in && sah_floor(sah_pick(c, best_axis), sah_pick(cmn, best_axis),
                                           sah_pick(scale, best_axis)) <= uint32_t(best_split);
         const uint32_t lt = (1u << lane) - 1u;
         const uint32_t ml = __ballot_sync(0xffffffffu, left), mr = __ballot_sync(0xffffffffu, in && !left);
-        if (left)
-            nxt[s + __popc(ml & lt)] = uint16_t(p);
-        else if (in)
-            nxt[mid + __popc(mr & lt)] = uint16_t(p);
+        if (left) {
+            const uint32_t q = s + __popc(ml & lt);
+            nxt[q] = uint16_t(p);
+            if (leaf_l) {  // the left child's leaf: final order and emission count (L + 1 left links)
+                S.fin[q] = uint16_t(p);
+                A.c[lo + q] = q == s ? 2u + L : 0u;
+            }
+        } else if (in) {
+            const uint32_t q = mid + __popc(mr & lt);
+            nxt[q] = uint16_t(p);
+            if (leaf_r) {  // the right child's leaf (no left link above it)
+                S.fin[q] = uint16_t(p);
+                A.c[lo + q] = q == mid ? 1u : 0u;
+            }
+        }
     }
     uint32_t cs = 0;
     if (lane == 0) {
-        A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
-        A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(lo + mid));
+        if (boxed) {
+            sah_rec_aux(A.rec, r, lo + s, lo + mid);
+        } else {
+            A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+            A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(lo + mid));
+        }
         A.rec_l[r] = L;
         cs = atomicAdd(&S.slots, 2u);
+        if (known) {
+            const size_t rl = 2ull * lo + cs, rr = rl + 1;
+            if (leaf_l) {
+                A.rec[2 * rl] = make_float4(lbox[0], lbox[1], lbox[2], __uint_as_float(lo + s));
+                A.rec[2 * rl + 1] = make_float4(lbox[3], lbox[4], lbox[5], __uint_as_float(0x80000000u | (mid - s)));
+                A.rec_l[rl] = L + 1u;
+            } else {
+                sah_rec_box(A.rec, rl, lbox);
+            }
+            if (leaf_r) {
+                A.rec[2 * rr] = make_float4(rbox[0], rbox[1], rbox[2], __uint_as_float(lo + mid));
+                A.rec[2 * rr + 1] =
+                    make_float4(rbox[3], rbox[4], rbox[5], __uint_as_float(0x80000000u | (s + n - mid)));
+                A.rec_l[rr] = 0u;
+            } else {
+                sah_rec_box(A.rec, rr, rbox);
+            }
+        }
     }
     cs = __shfl_sync(0xffffffffu, cs, 0);
-    left_child = sah_entry(s, mid, depth + 1u, cs, L + 1u);
-    right_child = sah_entry(mid, s + n, depth + 1u, cs + 1u, 0u);
-    return true;
+    left_child = sah_entry(s, mid, depth + 1u, cs, L + 1u, known);
+    right_child = sah_entry(mid, s + n, depth + 1u, cs + 1u, 0u, known);
+    return (leaf_l ? 0u : 1u) | (leaf_r ? 0u : 2u);
 }
 
 // One node of a subtree, by one warp: box and centroid bounds, then a leaf
@@ -725,13 +817,17 @@ __device__ __forceinline__ bool sah_node_small(SahShared& S, const SahArgs& A, u
 // its record, and its two children in every lane (returns true).  A node at
 // depth d reads ord[d & 1] and writes ord[(d + 1) & 1] over its own range:
 // ranges of nodes that are not ancestors of one another are disjoint, and a
-// node's range is complete before its children start.
-__device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent, uint32_t lane, uint32_t warp,
-                         uint2& left_child, uint2& right_child) {
+// node's range is complete before its children start.  Returns the children
+// to list (bit 0 left, bit 1 right); a node with a binned split writes its
+// children's boxes into their records (their entries are boxed).
+__device__ uint32_t sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent, uint32_t lane, uint32_t warp,
+                             uint2& left_child, uint2& right_child) {
     const uint32_t s = ent.x & 0x7ffu, e = (ent.x >> 11) & 0x7ffu, depth = ent.x >> 22;
-    const uint32_t slot = ent.y & 0xfffu, L = ent.y >> 12;
+    const uint32_t slot = ent.y & 0x7ffu, L = ent.y >> 12;
+    const bool boxed = (ent.y >> 11) & 1u;
     const uint32_t n = e - s;
-    if (n <= kSahSmallNode) return sah_node_small(S, A, lo, s, n, depth, slot, L, lane, warp, left_child, right_child);
+    if (n <= kSahSmallNode)
+        return sah_node_small(S, A, lo, s, n, depth, slot, L, boxed, lane, warp, left_child, right_child);
     const uint16_t* ord = S.ord[depth & 1u];
     uint16_t* nxt = S.ord[(depth + 1u) & 1u];
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -757,12 +853,13 @@ __device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent,
     // Leaves need only the box; a split needs the centroid bounds in every lane.
     const uint32_t span = n < 32u ? n : 32u;
     const bool leaf = n <= A.max_leaf;
-    for (uint32_t o = 1; o < span; o <<= 1)
+    if (!boxed)
+        for (uint32_t o = 1; o < span; o <<= 1)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
-            mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
-        }
+            for (int k = 0; k < 3; ++k) {
+                mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+                mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+            }
     if (!leaf) {
         for (uint32_t o = 1; o < span; o <<= 1)
 #pragma unroll
@@ -778,31 +875,38 @@ __device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent,
             }
     }
     const size_t r = 2ull * lo + slot;  // record index
-    if (slot == 0 && lane == 0) {       // the subtree root's box, for the top refit
+    if (slot == 0 && lane == 0 && !boxed) {  // the subtree root's box, for the top refit
         S.root_lo = make_float4(mn[0], mn[1], mn[2], 0.0f);
         S.root_hi = make_float4(mx[0], mx[1], mx[2], 0.0f);
     }
     if (leaf) {
         if (lane == 0) {
-            A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
-            A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
+            if (boxed) {
+                sah_rec_aux(A.rec, r, lo + s, 0x80000000u | n);
+            } else {
+                A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+                A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(0x80000000u | n));
+            }
             A.rec_l[r] = L;
         }
         for (uint32_t i = s + lane; i < e; i += 32) {
             S.fin[i] = ord[i];
             A.c[lo + i] = i == s ? 1u + L : 0u;
         }
-        return false;
+        return 0u;
     }
     // binned SAH over the axes with a centroid extent
     int best_axis = -1, best_split = -1;
     uint32_t best_nl = 0;
     float bscale = 0.0f;
+    float lbox[6], rbox[6];
     if (depth < kSahDepthCap) {
         if (n > kSahSmallNode)
-            sah_split<16>(S, S.bins[warp], ord, s, e, lane, cmn, cmx, best_axis, best_split, best_nl, bscale);
+            sah_split<16>(S, S.bins[warp], ord, s, e, lane, cmn, cmx, best_axis, best_split, best_nl, bscale, lbox,
+                          rbox);
         else
-            sah_split<8>(S, S.bins[warp], ord, s, e, lane, cmn, cmx, best_axis, best_split, best_nl, bscale);
+            sah_split<8>(S, S.bins[warp], ord, s, e, lane, cmn, cmx, best_axis, best_split, best_nl, bscale, lbox,
+                         rbox);
     }
     uint32_t mid;
     if (best_axis < 0) {
@@ -829,16 +933,25 @@ __device__ bool sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 ent,
         }
     }
     uint32_t cs = 0;
+    const bool known = best_axis >= 0;  // the children's boxes are lbox, rbox
     if (lane == 0) {
-        A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
-        A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(lo + mid));
+        if (boxed) {
+            sah_rec_aux(A.rec, r, lo + s, lo + mid);
+        } else {
+            A.rec[2 * r] = make_float4(mn[0], mn[1], mn[2], __uint_as_float(lo + s));
+            A.rec[2 * r + 1] = make_float4(mx[0], mx[1], mx[2], __uint_as_float(lo + mid));
+        }
         A.rec_l[r] = L;
         cs = atomicAdd(&S.slots, 2u);
+        if (known) {
+            sah_rec_box(A.rec, 2ull * lo + cs, lbox);
+            sah_rec_box(A.rec, 2ull * lo + cs + 1, rbox);
+        }
     }
     cs = __shfl_sync(0xffffffffu, cs, 0);
-    left_child = sah_entry(s, mid, depth + 1u, cs, L + 1u);
-    right_child = sah_entry(mid, e, depth + 1u, cs + 1u, 0u);
-    return true;
+    left_child = sah_entry(s, mid, depth + 1u, cs, L + 1u, known);
+    right_child = sah_entry(mid, e, depth + 1u, cs + 1u, 0u, known);
+    return 3u;
 }
 
 // ---- nodes of more than kSahMax triangles (below the Karras top)
@@ -1104,7 +1217,8 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
                 mbins[w] = x;
             }
             __syncthreads();
-            sah_choose<16>(mbins, scale, lane, best_axis, best_split, best_nl);  // every warp, the same result
+            float lbx[6], rbx[6];  // not needed: the partition pass sums the children's bounds
+            sah_choose<16>(mbins, scale, lane, best_axis, best_split, best_nl, lbx, rbx);  // every warp, the same result
         }
         // the stable partition, and both children's bounds
         uint32_t mid;
@@ -1247,10 +1361,11 @@ __global__ void __launch_bounds__(kSahT, 3) k_sah_build(const SahArgs A) {
             if (m == 0u || guard > 64u) break;
             for (uint32_t k = warp; k < m; k += kSahWarps) {
                 uint2 lc, rc;
-                if (sah_node(S, A, lo, S.list[cur][k], lane, warp, lc, rc) && lane == 0) {
-                    const uint32_t b = atomicAdd(&S.cnt[cur ^ 1], 2u);
-                    S.list[cur ^ 1][b] = lc;
-                    S.list[cur ^ 1][b + 1] = rc;
+                const uint32_t push = sah_node(S, A, lo, S.list[cur][k], lane, warp, lc, rc);
+                if (push && lane == 0) {
+                    uint32_t b = atomicAdd(&S.cnt[cur ^ 1], uint32_t(__popc(push)));
+                    if (push & 1u) S.list[cur ^ 1][b++] = lc;
+                    if (push & 2u) S.list[cur ^ 1][b] = rc;
                 }
             }
             __syncthreads();
