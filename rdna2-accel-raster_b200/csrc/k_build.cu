@@ -646,6 +646,24 @@ __device__ __forceinline__ void sah_split(const SahShared& S, uint32_t* bins, co
     axis_scale = axis < 0 ? 0.0f : sah_pick(scale, axis);
 }
 
+// Centroid bounds over a warp in every lane: warp min / max reductions of the
+// values as order-preserving integers (exact, as any min / max).  Lanes
+// without a primitive contribute the identities (+inf for the minimum,
+// -inf for the maximum).
+__device__ __forceinline__ void sah_warp_bounds2(const float (&lmn)[3], const float (&lmx)[3], float (&cmn)[3],
+                                                 float (&cmx)[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        cmn[k] = rq::o2f(__reduce_min_sync(0xffffffffu, rq::f2o(lmn[k])));
+        cmx[k] = rq::o2f(__reduce_max_sync(0xffffffffu, rq::f2o(lmx[k])));
+    }
+}
+__device__ __forceinline__ void sah_warp_bounds(const float (&c)[3], bool in, float (&cmn)[3], float (&cmx)[3]) {
+    const float lmn[3] = {in ? c[0] : INFINITY, in ? c[1] : INFINITY, in ? c[2] : INFINITY};
+    const float lmx[3] = {in ? c[0] : -INFINITY, in ? c[1] : -INFINITY, in ? c[2] : -INFINITY};
+    sah_warp_bounds2(lmn, lmx, cmn, cmx);
+}
+
 // A node of at most 32 primitives (every leaf, and most inner nodes), by one
 // warp with lane i holding primitive s + i: the same bounds, 8-way bins,
 // pricing and stable partition as sah_node's loops, without the loops.
@@ -700,23 +718,7 @@ __device__ __forceinline__ uint32_t sah_node_small(SahShared& S, const SahArgs& 
     }
     const float c[3] = {a.w, b.w, S.cz[p]};
     float cmn[3], cmx[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        cmn[k] = in ? c[k] : INFINITY;
-        cmx[k] = in ? c[k] : -INFINITY;
-    }
-    for (uint32_t o = 1; o < n; o <<= 1)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            cmn[k] = fminf(cmn[k], __shfl_xor_sync(0xffffffffu, cmn[k], o));
-            cmx[k] = fmaxf(cmx[k], __shfl_xor_sync(0xffffffffu, cmx[k], o));
-        }
-    if (n < 32u)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            cmn[k] = __shfl_sync(0xffffffffu, cmn[k], 0);
-            cmx[k] = __shfl_sync(0xffffffffu, cmx[k], 0);
-        }
+    sah_warp_bounds(c, in, cmn, cmx);
     int best_axis = -1, best_split = -1;
     uint32_t best_nl = 0;
     float scale[3] = {0.0f, 0.0f, 0.0f};
@@ -861,18 +863,8 @@ __device__ uint32_t sah_node(SahShared& S, const SahArgs& A, uint32_t lo, uint2 
                 mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
             }
     if (!leaf) {
-        for (uint32_t o = 1; o < span; o <<= 1)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                cmn[k] = fminf(cmn[k], __shfl_xor_sync(0xffffffffu, cmn[k], o));
-                cmx[k] = fmaxf(cmx[k], __shfl_xor_sync(0xffffffffu, cmx[k], o));
-            }
-        if (span < 32u)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                cmn[k] = __shfl_sync(0xffffffffu, cmn[k], 0);
-                cmx[k] = __shfl_sync(0xffffffffu, cmx[k], 0);
-            }
+        float lmn[3] = {cmn[0], cmn[1], cmn[2]}, lmx[3] = {cmx[0], cmx[1], cmx[2]};
+        sah_warp_bounds2(lmn, lmx, cmn, cmx);
     }
     const size_t r = 2ull * lo + slot;  // record index
     if (slot == 0 && lane == 0 && !boxed) {  // the subtree root's box, for the top refit
