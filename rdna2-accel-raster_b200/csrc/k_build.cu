@@ -468,15 +468,18 @@ __device__ __forceinline__ void sah_bins_clear(uint32_t* bins, uint32_t lane) {
 }
 
 // NB / extent per axis, 0 where the centroids have no extent or the extent is
-// too small to scale (no split on that axis).
+// too small to scale (no split on that axis).  Called by a whole warp with
+// the same bounds in every lane: lane a < 3 divides for axis a, one division
+// per lane instead of three.
 template <int NB>
-__device__ __forceinline__ void sah_scales(const float (&cmn)[3], const float (&cmx)[3], float (&scale)[3]) {
+__device__ __forceinline__ void sah_scales(const float (&cmn)[3], const float (&cmx)[3], float (&scale)[3],
+                                           uint32_t lane) {
+    const int a = lane < 3u ? int(lane) : 0;
+    const float ext = sah_pick(cmx, a) - sah_pick(cmn, a);
+    float sc = ext > 0.0f ? float(NB) / ext : 0.0f;
+    if (!(sc < INFINITY)) sc = 0.0f;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float ext = cmx[a] - cmn[a];
-        scale[a] = ext > 0.0f ? float(NB) / ext : 0.0f;
-        if (!(scale[a] < INFINITY)) scale[a] = 0.0f;
-    }
+    for (int k = 0; k < 3; ++k) scale[k] = __shfl_sync(0xffffffffu, sc, k);
 }
 
 // Bins the primitives at ord[s, e) into `bins` (one warp).  Each lane bins a
@@ -637,7 +640,7 @@ __device__ __forceinline__ void sah_split(const SahShared& S, uint32_t* bins, co
                                           float (&lbox)[6], float (&rbox)[6]) {
     float scale[3];
     sah_bins_clear<NB>(bins, lane);
-    sah_scales<NB>(cmn, cmx, scale);
+    sah_scales<NB>(cmn, cmx, scale, lane);
     __syncwarp();
     sah_bin_range<NB>(S, bins, ord, s, e, lane, cmn, scale);
     __syncwarp();
@@ -726,7 +729,7 @@ __device__ __forceinline__ uint32_t sah_node_small(SahShared& S, const SahArgs& 
     if (depth < kSahDepthCap) {
         uint32_t* bins = S.bins[warp];
         sah_bins_clear<8>(bins, lane);
-        sah_scales<8>(cmn, cmx, scale);
+        sah_scales<8>(cmn, cmx, scale, lane);
         __syncwarp();
         if (in) {
             constexpr uint32_t F = SahBinsOf<8>::slots;
@@ -1129,7 +1132,7 @@ __global__ void __launch_bounds__(kMidT, 2) k_sah_mid(const MidArgs A) {
         uint32_t best_nl = 0;
         float scale[3] = {0.0f, 0.0f, 0.0f};
         if (depth < kSahDepthCap) {
-            sah_scales<16>(cmn, cmx, scale);
+            sah_scales<16>(cmn, cmx, scale, lane);
             sah_bins_clear<16>(bins[warp], lane);
             __syncwarp();
             // Each lane a run of consecutive positions, kMidBinU of them in
