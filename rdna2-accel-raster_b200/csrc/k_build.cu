@@ -86,9 +86,12 @@ __global__ void __launch_bounds__(kT) k_karras(const uint32_t* __restrict__ keys
 // index is one end of its leaf range, so a node whose range lies inside the
 // block's has its index inside it too: such nodes take their arrival count
 // and box in shared memory (CTA-scope ordering), and write the box to global
-// memory once for the emission.  Only nodes whose range crosses a block
-// boundary (a few per block and level) use the device-scope acquire-release
-// count of refit_walk.  Unions are exact, so the boxes equal refit_walk's.
+// memory once for the emission.  A walk that reaches a node whose range
+// crosses a block boundary stops there and lists its parent link for
+// k_refit_top, which carries every such walk on with the device-scope
+// acquire-release count of refit_walk: a block is done once its own leaves
+// and local nodes are, instead of holding its slot while a walk climbs
+// through the tree's top.  Unions are exact, so the boxes equal refit_walk's.
 constexpr uint32_t kLocal = 256;  // 17 KB of shared memory per block (measured: faster than 512)
 
 __global__ void __launch_bounds__(kT) k_leaves_local(
@@ -97,13 +100,17 @@ __global__ void __launch_bounds__(kT) k_leaves_local(
     const int32_t* __restrict__ kr, const uint32_t* __restrict__ klo, const uint32_t* __restrict__ khi,
     const uint32_t* __restrict__ par_in, const uint32_t* __restrict__ par_lf, float4* box_in,
     float4* __restrict__ box_lf, uint32_t* refit_flag, uint32_t* __restrict__ c_out, rq_triangle* __restrict__ tris,
-    uint32_t* __restrict__ perm, uint32_t* __restrict__ keys_out, uint32_t* err) {
+    uint32_t* __restrict__ perm, uint32_t* __restrict__ keys_out, uint32_t* __restrict__ top_list,
+    uint32_t* top_cnt, uint32_t* err) {
     __shared__ uint32_t s_flag[kLocal];
     __shared__ float4 s_lf[2 * kLocal];  // leaf boxes (lo, hi) of the block's leaves
     __shared__ float4 s_in[2 * kLocal];  // boxes of the block's inner nodes
+    __shared__ uint32_t s_top[kLocal];   // the block's handed-over walks (at most one per leaf)
+    __shared__ uint32_t s_ntop, s_base;
     const uint32_t L0 = blockIdx.x * kLocal;
     const uint32_t L1 = min(L0 + kLocal, n);
     for (uint32_t i = threadIdx.x; i < kLocal; i += kT) s_flag[i] = 0u;
+    if (threadIdx.x == 0) s_ntop = 0u;
     for (uint32_t k = L0 + threadIdx.x; k < L1; k += kT) {
         rq::leaf_step(k, pos, sf, idx, max_leaf, skeys, sids, klo, khi, par_in, par_lf, box_lf, c_out, tris, perm,
                       keys_out);
@@ -114,12 +121,11 @@ __global__ void __launch_bounds__(kT) k_leaves_local(
     for (uint32_t k = L0 + threadIdx.x; k < L1; k += kT) {
         uint32_t par = par_lf[k];
         uint32_t guard = 0;
-        bool local = true;
         while (par != rq::kNoParent) {
             const uint32_t p = par >> 1;
             const int32_t a = kl[p], b = kr[p];
             float4 alo, ahi, blo, bhi;
-            if (local && __ldg(klo + p) >= L0 && __ldg(khi + p) < L1) {
+            if (__ldg(klo + p) >= L0 && __ldg(khi + p) < L1) {
                 __threadfence_block();  // release this thread's shared-memory box
                 if (atomicAdd(&s_flag[p - L0], 1u) == 0u) break;
                 __threadfence_block();  // acquire the sibling's
@@ -136,20 +142,50 @@ __global__ void __launch_bounds__(kT) k_leaves_local(
                 __stcg(box_in + 2 * size_t(p), lo);
                 __stcg(box_in + 2 * size_t(p) + 1, hi);
             } else {
-                // from here up every range crosses a block boundary
-                local = false;
-                if (rq::atom_add_acq_rel(&refit_flag[p], 1u) == 0u) break;
-                const float4* ba = a < 0 ? box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : box_in + 2 * size_t(a);
-                const float4* bb = b < 0 ? box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : box_in + 2 * size_t(b);
-                alo = rq::ld_cg4(ba);
-                ahi = rq::ld_cg4(ba + 1);
-                blo = rq::ld_cg4(bb);
-                bhi = rq::ld_cg4(bb + 1);
-                __stcg(box_in + 2 * size_t(p),
-                       make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f));
-                __stcg(box_in + 2 * size_t(p) + 1,
-                       make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f));
+                // from here up every range crosses a block boundary: k_refit_top
+                s_top[atomicAdd(&s_ntop, 1u)] = par;
+                break;
             }
+            par = par_in[p];
+            if (++guard > 128u) {
+                rq::set_err(err, RQ_DERR_REFIT);
+                break;
+            }
+        }
+    }
+    // the block's hand-offs, with one device atomic
+    __syncthreads();
+    const uint32_t nt = s_ntop;
+    if (threadIdx.x == 0 && nt) s_base = atomicAdd(top_cnt, nt);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nt; i += kT) top_list[s_base + i] = s_top[i];
+}
+
+// The walks k_leaves_local handed over: each starts at the parent link of a
+// node whose parent's range crosses a block boundary (that node's box is in
+// box_in or box_lf); at each node the second child to arrive forms the union
+// and carries on upward, as refit_walk.
+__global__ void __launch_bounds__(kT) k_refit_top(const int32_t* __restrict__ kl, const int32_t* __restrict__ kr,
+                                                  const uint32_t* __restrict__ par_in, float4* box_in,
+                                                  const float4* box_lf, uint32_t* refit_flag,
+                                                  const uint32_t* __restrict__ top_list, const uint32_t* top_cnt,
+                                                  uint32_t* err) {
+    const uint32_t m = *top_cnt;
+    for (uint32_t j = blockIdx.x * kT + threadIdx.x; j < m; j += gridDim.x * kT) {
+        uint32_t par = top_list[j];
+        uint32_t guard = 0;
+        while (par != rq::kNoParent) {
+            const uint32_t p = par >> 1;
+            if (rq::atom_add_acq_rel(&refit_flag[p], 1u) == 0u) break;
+            const int32_t a = kl[p], b = kr[p];
+            const float4* ba = a < 0 ? box_lf + 2 * size_t(uint32_t(a) & 0x7fffffffu) : box_in + 2 * size_t(a);
+            const float4* bb = b < 0 ? box_lf + 2 * size_t(uint32_t(b) & 0x7fffffffu) : box_in + 2 * size_t(b);
+            const float4 alo = rq::ld_cg4(ba), ahi = rq::ld_cg4(ba + 1);
+            const float4 blo = rq::ld_cg4(bb), bhi = rq::ld_cg4(bb + 1);
+            __stcg(box_in + 2 * size_t(p),
+                   make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f));
+            __stcg(box_in + 2 * size_t(p) + 1,
+                   make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f));
             par = par_in[p];
             if (++guard > 128u) {
                 rq::set_err(err, RQ_DERR_REFIT);
@@ -1746,10 +1782,16 @@ int rq_launch_build(rq_ctx* ctx, rq_bvh* bvh, const float* pos, uint32_t stride_
         if (collapse) return rq_launch_collapse(ctx, bvh, s, st);
         return RQ_OK;
     }
+    // the handed-over walks: listed in the centroid array (free after the
+    // Morton codes), counted in tile_ctr[12] (zeroed above, unused by the sort)
+    uint32_t* top_list = reinterpret_cast<uint32_t*>(s.cent);
+    uint32_t* top_cnt = s.tile_ctr + 12;
     k_leaves_local<<<(n + kLocal - 1) / kLocal, kT, 0, st>>>(pos, sf, idx, n, max_leaf, skeys, sids, s.kl, s.kr,
                                                              s.klo, s.khi, s.par_in, s.par_lf, s.box_in, s.box_lf,
                                                              s.refit_flag, s.c, bvh->tris, bvh->perm, bvh->skeys,
-                                                             ctx->d_err);
+                                                             top_list, top_cnt, ctx->d_err);
+    k_refit_top<<<uint32_t(sms) * 4u, kT, 0, st>>>(s.kl, s.kr, s.par_in, s.box_in, s.box_lf, s.refit_flag, top_list,
+                                                   top_cnt, ctx->d_err);
     rq_launch_scan(ctx, s.c, s.a, n, s.scan_status, s.tile_ctr + 8, st);
     k_emit2<<<grid_for(n, sms), kT, 0, st>>>(n, max_leaf, s.kr, s.klo, s.khi, s.par_in, s.par_lf, s.box_in, s.box_lf,
                                              s.c, s.a, bvh->nodes2, bvh->d_counts);
