@@ -36,11 +36,11 @@ sys.path.insert(0, os.path.join(ROOT, "rdna2-accel-raster_b200"))
 WIDTH, HEIGHT = 1920, 1080
 METRIC = "Mrays/s + BVH Mtris/s on 1 B200; p50/p99 request latency batched vs plain"
 # kernels launched by one step of the frame: the build — centroids, morton,
-# hist, hist_scan, 4 onesweep passes, karras, then leaves, scan, emit (plain
-# LBVH) or per-position boxes, SAH roots, the node queue above the block
-# size, the block subtrees, scan, emit (SAH subtrees), then collapse: 13 or
-# 16 — then G-buffer, shadow/AO and the shade finish (3)
-BUILD_KERNELS = {"lbvh": 13, "sah": 16}
+# hist, hist_scan, 4 onesweep passes, karras, then leaves, the top refit,
+# scan, emit (plain LBVH) or per-position boxes, SAH roots, the node queue
+# above the block size, the block subtrees, scan, emit (SAH subtrees), then
+# collapse: 14 or 16 — then G-buffer, shadow/AO and the shade finish (3)
+BUILD_KERNELS = {"lbvh": 14, "sah": 16}
 FRAME_KERNELS = 3
 
 
