@@ -5,7 +5,8 @@ leaf-ordered triangles and 4-wide nodes byte for byte, at sizes around the
 1,024 triangles a block rebuilds in shared memory (larger nodes are split by
 the node queue first), the 16,384-triangle subtree limit, the one-subtree case
 and the 32-triangle switch from 16 to 8 bins, for every leaf size,
-degenerate inputs (equal centroids), a grid mesh, and a refit; traversal on
+degenerate inputs (equal centroids), trees past the depth cap, a grid mesh,
+and a refit; traversal on
 the rebuilt tree bit-exact with the oracle's traversal of it."""
 import numpy as np
 import pytest
@@ -75,6 +76,22 @@ def test_sah_degenerate_centroids(ctx):
     w = soup(5000, 10)
     w[:, 2] = np.float32(0.5)
     assert_same_as_oracle(ctx, w, None)
+
+
+@pytest.mark.parametrize("n, ratio", [(200, 1.25), (3000, 1.012)])
+def test_sah_depth_cap(ctx, n, ratio):
+    # small triangles spaced geometrically along x: the cheapest split cuts off
+    # the few farthest ones, so the tree runs past the depth cap (24 levels)
+    # and continues with middle splits; at 3,000 triangles the node queue
+    # takes the first levels
+    x = (ratio ** np.arange(n, dtype=np.float64)).astype(np.float32)
+    v = np.zeros((n, 9), np.float32)
+    v[:, 0] = x
+    v[:, 3] = x + np.float32(0.1)
+    v[:, 6] = x
+    v[:, 7] = np.float32(0.1)
+    o = assert_same_as_oracle(ctx, v, None)
+    assert o["depth4"] > 12
 
 
 def test_sah_trace_bit_exact_and_refit(ctx):
